@@ -1,0 +1,359 @@
+"""Benchmark: grid-point RK4 updates/s of the BSSN + dust evolution on B200.
+
+Workload (default): one periodic BSSN + pressureless-dust box of 256^3 points
+per GPU, 8th-order stencils, harmonic lapse, FP64 (reference operand order).
+A "step" is one full RK4 step (4 fused substep launches) of that box; each
+rank evolves its own box (independent replicas, weak scaling).  Inputs are
+synthetic: a smooth random perturbation of every field (the kernels have no
+data-dependent control flow, so cost does not depend on the values).
+
+Printed JSON (rank 0, one line): value = whole-job updates/s with the state
+resident in HBM; e2e = the same through the C ABI with the full state copied
+host->device and device->host around every step; roofline = the substep
+kernel's algorithmic HBM bytes against the measured copy bandwidth;
+cpu_baseline = the reference's own sources (oracle/_ref) on the host cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+# Algorithmic HBM bytes per grid-point RK4 update of the fused FP64 scheme,
+# each value counted once (perfect stencil reuse): substep 1 reads p, writes f
+# and a^2 (3E); substeps 2-3 read a, p, f and write f, a (5E each); substep 4
+# reads a, p, f and writes p (4E): 17E values, E = 22 evolved fields, plus the
+# reference's lagged dust quantities W, sqrt(gamma), g_ij (8 values written at
+# substeps 1-3 and read at 2-4, 48 values): 422 values = 3376 bytes.
+ALGO_BYTES_PER_UPDATE = {"dust": 3376, "scalar": 3128, "vacuum": 17 * 18 * 8}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--order", type=int, default=8)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference CPU build (rank 0)")
+    ap.add_argument("--ncu", action="store_true", help="short run for profiler capture (no JSON extras)")
+    return ap.parse_args()
+
+
+def dist_setup(a):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_state(n: int, seed: int):
+    from cosmograph_b200 import ics, state as S
+
+    return ics.perturbed((n, n, n), S.DUST, seed=seed, amp=1e-2)
+
+
+def cpu_baseline(st, order: int, budget_s: float = 30.0):
+    """The reference's own sources on the host cores (oracle/_ref, fast build);
+    one RK4 step of the same box, all host threads."""
+    from oracle import build_ref
+
+    nx, ny, nz = st.shape
+    binp = build_ref.binary_path(nx, ny, nz, order, "fast")
+    threads = os.cpu_count() or 1
+    if not binp.exists():
+        return None
+    with tempfile.TemporaryDirectory(prefix="cg_bench_cpu_") as tmp:
+        tmp = Path(tmp)
+        (tmp / "config.txt").write_text("lapse = Harmonic\n")
+        st.save(tmp / "in.bin")
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        t0 = time.time()
+        proc = subprocess.run([str(binp), "evolve", str(tmp / "config.txt"), str(tmp / "in.bin"),
+                               str(tmp / "out.bin"), "1"], capture_output=True, text=True, env=env,
+                              timeout=600)
+        wall = time.time() - t0
+    if proc.returncode != 0:
+        return None
+    step_s = [float(l.split()[2]) for l in proc.stdout.splitlines() if l.startswith("CGSTEP")]
+    if not step_s:
+        return None
+    rate = nx * ny * nz * len(step_s) / sum(step_s)
+    return {"value": rate, "unit": "grid-pt RK4 updates/s", "cores": threads, "kind": "reference",
+            "sample": f"1 RK4 step of the same {nx}x{ny}x{nz} order-{order} BSSN+dust box, reference "
+                      f"sources built -O3 -ffast-math -march=x86-64-v3 -fopenmp ({binp.name}); "
+                      f"{sum(step_s):.2f} s of step loop, {wall:.1f} s wall"}
+
+
+def run_reference_arm(a, world, rank):
+    """--impl reference: the reference's CPU implementation (oracle/_ref) of the
+    same workload, all host threads, rank 0 only."""
+    if rank != 0:
+        return
+    from oracle import build_ref
+
+    n = a.n
+    binp = build_ref.binary_path(n, n, n, a.order, "fast")
+    base = {"metric": "grid-pt RK4 updates/s (BSSN+dust)", "impl": "reference"}
+    if not binp.exists():
+        print(json.dumps({"impl": "reference", "unavailable": f"{binp.name} was not built"}))
+        return
+    st = make_state(n, seed=1)
+    threads = os.cpu_count() or 1
+    # each step is a full RK4 step of the same box; cap the count so the run
+    # stays within a few minutes on the host cores
+    with tempfile.TemporaryDirectory(prefix="cg_bench_ref_") as tmp:
+        tmp = Path(tmp)
+        (tmp / "config.txt").write_text("lapse = Harmonic\n")
+        st.save(tmp / "in.bin")
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        warm = max(1, min(a.warmup, 1))
+        probe = subprocess.run([str(binp), "evolve", str(tmp / "config.txt"), str(tmp / "in.bin"),
+                                str(tmp / "out.bin"), str(warm)], capture_output=True, text=True, env=env,
+                               timeout=1800)
+        t1 = [float(l.split()[2]) for l in probe.stdout.splitlines() if l.startswith("CGSTEP")]
+        per = max(t1) if t1 else 60.0
+        k = max(1, min(a.steps, int(150.0 / per)))
+        proc = subprocess.run([str(binp), "evolve", str(tmp / "config.txt"), str(tmp / "in.bin"),
+                               str(tmp / "out.bin"), str(k)], capture_output=True, text=True, env=env,
+                              timeout=3600)
+    step_s = [float(l.split()[2]) for l in proc.stdout.splitlines() if l.startswith("CGSTEP")]
+    if proc.returncode != 0 or not step_s:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference run failed: {proc.stderr[-300:]}"}))
+        return
+    tot = sum(step_s)
+    rate = n ** 3 * len(step_s) / tot
+    line = dict(base, value=rate, unit="grid-pt RK4 updates/s", n_gpus=a.gpus, steps=len(step_s),
+                warmup=warm, ms_per_step=1e3 * tot / len(step_s), higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f64", data="synthetic",
+                config={"workload": f"bssn_dust_{n}cubed_o{a.order}", "n": n, "stencil_order": a.order,
+                        "lapse": "Harmonic", "parallelism": "host threads"},
+                cpu_baseline={"value": rate, "unit": "grid-pt RK4 updates/s", "cores": threads,
+                              "kind": "reference",
+                              "sample": f"{len(step_s)} RK4 steps (of {a.steps} requested) of the "
+                                        f"{n}^3 box; reference sources, {binp.name}"},
+                e2e={"value": rate, "unit": "grid-pt RK4 updates/s", "h2d_bytes_per_step": 0,
+                     "d2h_bytes_per_step": 0})
+    print(json.dumps(line))
+
+
+def main():
+    a = parse()
+    world, rank, local = dist_setup(a) if a.impl == "ours" else (
+        int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
+    if a.impl == "reference":
+        return run_reference_arm(a, world, rank)
+
+    import torch
+    import torch.distributed as dist
+
+    from cosmograph_b200.evolution import BoxConfig, Evolution
+
+    n = a.n
+    st = make_state(n, seed=1 + rank)
+    cfg = BoxConfig(order=a.order, lapse="Harmonic", precision=a.precision)
+    stream = torch.cuda.Stream()
+    ev = Evolution(st, cfg)
+    ev.set_stream(stream.cuda_stream)
+    pts = n ** 3
+    launches_per_step = 4
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up
+    for _ in range(max(a.warmup, 0)):
+        ev.step(1)
+    ev.synchronize()
+    torch.cuda.synchronize()
+
+    # timed: device-resident state
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(a.steps):
+            ev.step(1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ev.synchronize()
+    barrier()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    ms_per_step = ms / a.steps
+    value = world * pts * a.steps / (ms / 1e3)
+
+    if a.ncu:
+        if rank == 0:
+            print(json.dumps({"ncu_run": True, "ms_per_step": ms_per_step}))
+        ev.close()
+        return
+
+    # end to end through the C ABI: pinned host state in, one RK4 step, state out
+    state_bytes = st.fields.nbytes
+    h_in = torch.from_numpy(st.fields.reshape(-1)).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    L = ev.L
+    import ctypes
+
+    dp = ctypes.POINTER(ctypes.c_double)
+    pin = ctypes.cast(h_in.data_ptr(), dp)
+    pout = ctypes.cast(h_out.data_ptr(), dp)
+    cnt = h_in.numel()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(a.e2e_steps):
+        ev._check(L.cg_upload_state_async(ev.ctx, 0, pin, cnt))
+        ev.step(1)
+        ev._check(L.cg_download_state_async(ev.ctx, 0, pout, cnt))
+    q1.record(stream)
+    torch.cuda.synchronize()
+    ev.synchronize()
+    e2e_ms = max_over_ranks(q0.elapsed_time(q1))
+    e2e_wall = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * pts * a.e2e_steps / (e2e_ms / 1e3)
+    ev.close()
+
+    peak, peak_kind = measured_peaks()
+    algo = ALGO_BYTES_PER_UPDATE["dust"] * pts / launches_per_step
+    launch_ms = ms_per_step / launches_per_step
+    achieved = algo / (launch_ms / 1e3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / "stage_kernel_traffic.json"
+    if prof.exists():
+        try:
+            d = json.loads(prof.read_text())
+            traffic = d.get(f"{n}_{a.order}_{a.precision}")
+        except Exception:
+            traffic = None
+
+    cpu = None
+    if rank == 0 and a.cpu_baseline:
+        try:
+            cpu = cpu_baseline(st, a.order)
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "error": str(exc)[:200]}
+
+    if rank == 0:
+        line = {
+            "metric": "grid-pt RK4 updates/s (BSSN+dust)",
+            "value": value,
+            "unit": "grid-pt RK4 updates/s",
+            "n_gpus": world,
+            "steps": a.steps,
+            "warmup": a.warmup,
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"bssn_dust_{n}cubed_o{a.order}", "n": n, "stencil_order": a.order,
+                       "lapse": "Harmonic", "precision": a.precision, "boxes_per_gpu": 1,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (state %.1f GB per box)" % (state_bytes / 1e9)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": algo},
+            "e2e": {"value": e2e_value, "unit": "grid-pt RK4 updates/s",
+                    "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                    "steps": a.e2e_steps, "wall_s": e2e_wall},
+            "gpu_launches": launches_per_step * a.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

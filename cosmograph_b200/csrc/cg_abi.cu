@@ -1,0 +1,585 @@
+// cg_abi.cu -- the C ABI (include/cosmograph_b200.h): contexts, device
+// storage, the host-side FRW background and the substep sequencing.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cosmograph_b200.h"
+#include "cg_internal.h"
+
+namespace {
+
+using cg::BoxDev;
+using cg::StageBg;
+
+thread_local std::string g_create_error;
+
+// FRW reference integrator (utils/FRW.h:94-254), FP64 on the host.  The
+// substep kernels only need its getter values, which are grid-independent.
+struct FrwHost {
+  double phi = 0.0, K = 0.0;
+  int n = 0;
+  double rho[4] = {0, 0, 0, 0}, w[4] = {0, 0, 0, 0};
+  double phi_K[4] = {0, 0, 0, 0}, K_K[4] = {0, 0, 0, 0}, fl_K[4][4] = {};
+  double get_phi = 0.0, get_K = 0.0, get_rho = 0.0, get_S = 0.0;
+
+  void set_gets(double p, double k, const double* r) {
+    get_phi = p;
+    get_K = k;
+    get_rho = 0.0;
+    get_S = 0.0;
+    for (int m = 0; m < n; ++m) {
+      get_rho += r[m];
+      get_S += 3.0 * r[m] * w[m];
+    }
+  }
+  // stage n = 1,2,3 : P{n}_step ; n = 4 : RK_total_step
+  void stage(int s, double h) {
+    static const long double kPiL = 3.141592653589793238462643383279502884L;
+    double K_in = K, rho_in[4];
+    if (s == 1) {
+      for (int m = 0; m < n; ++m) rho_in[m] = rho[m];
+    } else {
+      const double c = s == 4 ? h : h / 2.0;
+      K_in = K + c * K_K[s - 2];
+      for (int m = 0; m < n; ++m) rho_in[m] = rho[m] + c * fl_K[s - 2][m];
+    }
+    phi_K[s - 1] = -1.0 * K_in / 6.0;
+    double K_source = 0.0;
+    for (int m = 0; m < n; ++m) K_source += 4.0 * kPiL * rho_in[m] * (1.0 + 3.0 * w[m]);
+    K_K[s - 1] = 1.0 / 3.0 * K_in * K_in + K_source;
+    for (int m = 0; m < n; ++m) fl_K[s - 1][m] = K_in * rho_in[m] * (1.0 + w[m]);
+    if (s < 4) {
+      const double c = s == 3 ? h : h / 2.0;
+      double r[4];
+      for (int m = 0; m < n; ++m) r[m] = rho[m] + c * fl_K[s - 1][m];
+      set_gets(phi + c * phi_K[s - 1], K + c * K_K[s - 1], r);
+    } else {
+      phi += h / 6.0 * (phi_K[0] + 2.0 * phi_K[1] + 2.0 * phi_K[2] + phi_K[3]);
+      K += h / 6.0 * (K_K[0] + 2.0 * K_K[1] + 2.0 * K_K[2] + K_K[3]);
+      for (int m = 0; m < n; ++m) rho[m] += h / 6.0 * (fl_K[0][m] + 2.0 * fl_K[1][m] + 2.0 * fl_K[2][m] + fl_K[3][m]);
+      set_gets(phi, K, rho);
+    }
+  }
+};
+
+struct Box {
+  cg_box_desc desc{};
+  BoxDev dev{};
+  FrwHost frw;
+  int variant = cg::kExact;
+  int stage_next = 0;   // 0: inputs not built; 1..4: next substep
+  double phi_prev = 0.0;
+  int64_t steps = 0;
+  bool needs_kavg = false;
+  double* kavg_partial = nullptr;  // per-block partial sums for K_avg
+  double* kavg = nullptr;          // device K_avg
+  int kavg_blocks = 0;
+};
+
+}  // namespace
+
+struct cg_ctx {
+  std::vector<Box> boxes;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  unsigned* status = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int fail(cg_ctx* ctx, int code, const std::string& msg) {
+  if (ctx)
+    ctx->err = msg;
+  else
+    g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(cg_ctx* ctx, cudaError_t e, const char* what) {
+  return fail(ctx, CG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CG_CUDA(ctx, call)                          \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+bool lapse_needs_kavg(int lapse) {
+  return lapse == CG_LAPSE_CONFORMAL_FLRW || lapse == CG_LAPSE_ANHARMONIC || lapse == CG_LAPSE_ONE_PLUS_LOG;
+}
+
+// Conformal (volume-weighted) average of DIFFK, math.h:1403-1415 as used by
+// BSSN::setExtraFieldData (bssn.cc:168): per-block partial sums in a fixed
+// order, then one block combines them in a fixed order.
+__global__ void kavg_partial_kernel(const double* __restrict__ K, const double* __restrict__ phi, int pts,
+                                    double phi_FRW, double* partial) {
+  __shared__ double sK[256], sV[256];
+  double aK = 0.0, aV = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < pts; q += gridDim.x * blockDim.x) {
+    const double e = exp(6.0 * (phi[q] + phi_FRW));
+    aK += e * K[q];
+    aV += e;
+  }
+  sK[threadIdx.x] = aK;
+  sV[threadIdx.x] = aV;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sK[threadIdx.x] += sK[threadIdx.x + o];
+      sV[threadIdx.x] += sV[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = sK[0];
+    partial[2 * blockIdx.x + 1] = sV[0];
+  }
+}
+
+__global__ void kavg_final_kernel(const double* partial, int nblk, int pts, double* out) {
+  __shared__ double sK[256], sV[256];
+  double aK = 0.0, aV = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+    aK += partial[2 * b];
+    aV += partial[2 * b + 1];
+  }
+  sK[threadIdx.x] = aK;
+  sV[threadIdx.x] = aV;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sK[threadIdx.x] += sK[threadIdx.x + o];
+      sV[threadIdx.x] += sV[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const double vol = sV[0] / pts;
+    out[0] = sK[0] / pts / vol;
+  }
+}
+
+// the register block holding the current substep input
+double* current_a(Box& b) {
+  switch (b.stage_next) {
+    case 2: case 4: return b.dev.Y;
+    default: return b.dev.X;
+  }
+}
+
+StageBg bg_for(const Box& b, int stage, double phi_next) {
+  StageBg bg{};
+  bg.phi_FRW = b.frw.get_phi;
+  bg.K_FRW = b.frw.get_K;
+  bg.rho_FRW = b.frw.get_rho;
+  bg.S_FRW = b.frw.get_S;
+  bg.K_avg = 0.0;
+  bg.phi_FRW_prev = stage == 1 ? b.frw.get_phi : b.phi_prev;
+  bg.phi_FRW_next = phi_next;
+  return bg;
+}
+
+int launch_kavg(cg_ctx* ctx, Box& b, const double* in) {
+  if (!b.needs_kavg) return CG_OK;
+  const double* K = in + (size_t)cg::F_K * b.dev.pts;
+  const double* phi = in + (size_t)cg::F_PHI * b.dev.pts;
+  kavg_partial_kernel<<<b.kavg_blocks, 256, 0, ctx->stream>>>(K, phi, b.dev.pts, b.frw.get_phi, b.kavg_partial);
+  kavg_final_kernel<<<1, 256, 0, ctx->stream>>>(b.kavg_partial, b.kavg_blocks, b.dev.pts, b.kavg);
+  CG_CUDA(ctx, cudaGetLastError());
+  return CG_OK;
+}
+
+int do_init(cg_ctx* ctx, Box& b) {
+  StageBg bg = bg_for(b, 1, b.frw.get_phi);
+  CG_CUDA(ctx, cg::launch_init(b.variant, b.dev, bg, ctx->stream));
+  b.stage_next = 1;
+  return CG_OK;
+}
+
+int do_stage(cg_ctx* ctx, Box& b, int n) {
+  // FRW getters of the next substep (for the flux primitives of the output)
+  FrwHost nxt = b.frw;
+  nxt.stage(n, b.desc.dt);
+  StageBg bg = bg_for(b, n, nxt.get_phi);
+  int rc = launch_kavg(ctx, b, current_a(b));
+  if (rc) return rc;
+  CG_CUDA(ctx, cg::launch_stage(b.variant, b.dev, bg, n, ctx->stream));
+  // BSSN::K{n}Finalize advances the FRW integrator (bssn.cc:267-305)
+  b.phi_prev = b.frw.get_phi;
+  b.frw = nxt;
+  b.stage_next = n == 4 ? 1 : n + 1;
+  if (n == 4) ++b.steps;
+  return CG_OK;
+}
+
+int check_box(cg_ctx* ctx, int box) {
+  if (!ctx) return CG_ERR_INVALID;
+  if (box < 0 || box >= (int)ctx->boxes.size()) return fail(ctx, CG_ERR_INVALID, "box index out of range");
+  return CG_OK;
+}
+
+int validate(const cg_box_desc& d, std::string& why) {
+  const int r = d.stencil_order / 2;
+  if (d.stencil_order != 2 && d.stencil_order != 4 && d.stencil_order != 6 && d.stencil_order != 8) {
+    why = "stencil_order must be 2, 4, 6 or 8";
+    return CG_ERR_INVALID;
+  }
+  if (d.nx < r + 1 || d.ny < r + 1 || d.nz < r + 1) {
+    why = "every axis needs at least stencil_order/2 + 1 points";
+    return CG_ERR_INVALID;
+  }
+  if ((long long)d.nx * d.ny * d.nz > 2000000000LL) {
+    why = "box too large for 32-bit point indices";
+    return CG_ERR_INVALID;
+  }
+  if (d.matter < 0 || d.matter > 2) { why = "unknown matter model"; return CG_ERR_INVALID; }
+  if (d.lapse < 0 || d.lapse > 8) { why = "unknown lapse gauge"; return CG_ERR_INVALID; }
+  if (d.precision != CG_PREC_FP64 && d.precision != CG_PREC_FP64_FMA) { why = "unknown precision"; return CG_ERR_INVALID; }
+  if (d.ko_coeff != 0.0) { why = "Kreiss-Oliger dissipation is not available on this path (ko_coeff must be 0)"; return CG_ERR_INVALID; }
+  if (d.nfluids < 0 || d.nfluids > 4) { why = "at most 4 FRW fluids"; return CG_ERR_INVALID; }
+  if (!(d.dx > 0.0) || !std::isfinite(d.dt)) { why = "dx must be positive and dt finite"; return CG_ERR_INVALID; }
+  return CG_OK;
+}
+
+bool is_pow2(double x) {
+  int e;
+  const double m = std::frexp(x, &e);
+  return m == 0.5;
+}
+
+void free_box(Box& b) {
+  cudaFree(b.dev.P);
+  cudaFree(b.dev.F);
+  cudaFree(b.dev.X);
+  cudaFree(b.dev.Y);
+  cudaFree(b.dev.FP0);
+  cudaFree(b.dev.FP1);
+  cudaFree(b.kavg_partial);
+  b.dev.P = b.dev.F = b.dev.X = b.dev.Y = b.dev.FP0 = b.dev.FP1 = nullptr;
+  b.kavg_partial = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cg_version(void) { return CG_ABI_VERSION; }
+
+int cg_num_fields(int matter) { return matter == CG_MATTER_DUST ? 22 : matter == CG_MATTER_SCALAR ? 23 : 18; }
+
+const char* cg_field_name(int matter, int field) {
+  static const char* bssn[18] = {"DIFFgamma11", "DIFFgamma12", "DIFFgamma13", "DIFFgamma22", "DIFFgamma23",
+                                 "DIFFgamma33", "DIFFphi", "A11", "A12", "A13", "A22", "A23", "A33",
+                                 "DIFFK", "Gamma1", "Gamma2", "Gamma3", "DIFFalpha"};
+  static const char* dust[4] = {"D", "S1", "S2", "S3"};
+  static const char* scal[5] = {"phi", "Pi", "psi1", "psi2", "psi3"};
+  if (field < 0 || field >= cg_num_fields(matter)) return nullptr;
+  if (field < 18) return bssn[field];
+  return matter == CG_MATTER_DUST ? dust[field - 18] : scal[field - 18];
+}
+
+void cg_box_desc_default(cg_box_desc* d, int n) {
+  if (!d) return;
+  std::memset(d, 0, sizeof(*d));
+  d->nx = d->ny = d->nz = n;
+  d->stencil_order = 8;
+  d->matter = CG_MATTER_DUST;
+  d->lapse = CG_LAPSE_HARMONIC;
+  d->precision = CG_PREC_FP64;
+  d->normalize_metric = 1;
+  d->potential = CG_POT_CONST;
+  d->dx = 1.0 / n;
+  d->dt = (double)(0.1L * (long double)d->dx);
+  d->gd_c = 1.0;
+  d->pot_const = 3.0e-4;
+  d->pot_mass = 1.0;
+}
+
+int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
+  if (!out) return fail(nullptr, CG_ERR_INVALID, "out is null");
+  *out = nullptr;
+  if (!boxes || nboxes <= 0) return fail(nullptr, CG_ERR_INVALID, "need at least one box");
+  for (int b = 0; b < nboxes; ++b) {
+    std::string why;
+    if (validate(boxes[b], why) != CG_OK)
+      return fail(nullptr, CG_ERR_INVALID, "box " + std::to_string(b) + ": " + why);
+  }
+  cg_ctx* ctx = new (std::nothrow) cg_ctx();
+  if (!ctx) return fail(nullptr, CG_ERR_MEMORY, "host allocation failed");
+  cudaError_t e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return fail(nullptr, CG_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  ctx->stream = ctx->own_stream;
+  e = cudaMalloc(&ctx->status, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(ctx->status, 0, sizeof(unsigned));
+  ctx->boxes.resize(nboxes);
+  for (int bi = 0; bi < nboxes && e == cudaSuccess; ++bi) {
+    Box& b = ctx->boxes[bi];
+    b.desc = boxes[bi];
+    const cg_box_desc& d = b.desc;
+    b.variant = d.precision == CG_PREC_FP64_FMA ? cg::kFast : cg::kExact;
+    b.dev.nx = d.nx;
+    b.dev.ny = d.ny;
+    b.dev.nz = d.nz;
+    b.dev.pts = d.nx * d.ny * d.nz;
+    b.dev.nfields = cg_num_fields(d.matter);
+    b.dev.order = d.stencil_order;
+    b.dev.matter = d.matter;
+    cg::Physics& ph = b.dev.ph;
+    ph.matter = d.matter;
+    ph.lapse = d.lapse;
+    ph.potential = d.potential;
+    ph.normalize = d.normalize_metric;
+    ph.dx = d.dx;
+    ph.inv_dx = 1.0 / d.dx;
+    ph.dx_pow2 = is_pow2(d.dx) ? 1 : 0;
+    ph.dt = d.dt;
+    ph.lambda = d.lambda;
+    ph.a_adj_amp = d.a_adj_amp;
+    ph.k_damping_amp = d.k_damping_amp;
+    ph.gd_c = d.gd_c;
+    ph.dw_mu_l = d.dw_mu_l;
+    ph.dw_p = d.dw_p;
+    ph.pot_const = d.pot_const;
+    ph.pot_mass = d.pot_mass;
+    b.frw.phi = d.frw_phi;
+    b.frw.K = d.frw_K;
+    b.frw.n = d.nfluids;
+    for (int m = 0; m < d.nfluids; ++m) {
+      b.frw.rho[m] = d.fluid_rho[m];
+      b.frw.w[m] = d.fluid_w[m];
+    }
+    b.frw.set_gets(b.frw.phi, b.frw.K, b.frw.rho);
+    const size_t reg = sizeof(double) * (size_t)b.dev.nfields * b.dev.pts;
+    e = cudaMalloc(&b.dev.P, reg);
+    if (e == cudaSuccess) e = cudaMalloc(&b.dev.F, reg);
+    if (e == cudaSuccess) e = cudaMalloc(&b.dev.X, reg);
+    if (e == cudaSuccess) e = cudaMalloc(&b.dev.Y, reg);
+    if (e == cudaSuccess && d.matter == CG_MATTER_DUST) {
+      const size_t fp = sizeof(double) * (size_t)cg::P_N * b.dev.pts;
+      e = cudaMalloc(&b.dev.FP0, fp);
+      if (e == cudaSuccess) e = cudaMalloc(&b.dev.FP1, fp);
+    }
+    for (double* p : {b.dev.P, b.dev.F, b.dev.X, b.dev.Y})
+      if (e == cudaSuccess) e = cudaMemset(p, 0, reg);
+    b.dev.status = ctx->status;
+    b.needs_kavg = lapse_needs_kavg(d.lapse);
+    if (e == cudaSuccess && b.needs_kavg) {
+      b.kavg_blocks = std::min(1024, (b.dev.pts + 255) / 256);
+      e = cudaMalloc(&b.kavg_partial, sizeof(double) * (2 * b.kavg_blocks + 1));
+      b.kavg = b.kavg_partial + 2 * b.kavg_blocks;
+      b.dev.kavg = b.kavg;
+    }
+  }
+  if (e != cudaSuccess) {
+    const std::string msg = std::string("device allocation: ") + cudaGetErrorString(e);
+    for (Box& b : ctx->boxes) free_box(b);
+    cudaFree(ctx->status);
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return fail(nullptr, e == cudaErrorMemoryAllocation ? CG_ERR_MEMORY : CG_ERR_CUDA, msg);
+  }
+  *out = ctx;
+  return CG_OK;
+}
+
+int cg_destroy(cg_ctx* ctx) {
+  if (!ctx) return CG_ERR_INVALID;
+  cudaStreamSynchronize(ctx->stream);
+  for (Box& b : ctx->boxes) free_box(b);
+  cudaFree(ctx->status);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return CG_OK;
+}
+
+int cg_set_stream(cg_ctx* ctx, void* stream) {
+  if (!ctx) return CG_ERR_INVALID;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return CG_OK;
+}
+
+int cg_get_stream(cg_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return CG_ERR_INVALID;
+  *stream = (void*)ctx->stream;
+  return CG_OK;
+}
+
+static int state_copy(cg_ctx* ctx, int box, double* host, size_t count, bool upload, bool async) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  Box& b = ctx->boxes[box];
+  const size_t n = (size_t)b.dev.nfields * b.dev.pts;
+  if (!host || count != n)
+    return fail(ctx, CG_ERR_INVALID, "count must be nfields*nx*ny*nz = " + std::to_string(n));
+  const size_t bytes = n * sizeof(double);
+  if (upload) {
+    CG_CUDA(ctx, cudaMemcpyAsync(b.dev.P, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    b.stage_next = 0;
+    b.steps = 0;
+  } else {
+    CG_CUDA(ctx, cudaMemcpyAsync(host, b.dev.P, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (!async) CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CG_OK;
+}
+
+int cg_upload_state(cg_ctx* ctx, int box, const double* host, size_t count) {
+  return state_copy(ctx, box, const_cast<double*>(host), count, true, false);
+}
+int cg_download_state(cg_ctx* ctx, int box, double* host, size_t count) {
+  return state_copy(ctx, box, host, count, false, false);
+}
+int cg_upload_state_async(cg_ctx* ctx, int box, const double* host, size_t count) {
+  return state_copy(ctx, box, const_cast<double*>(host), count, true, true);
+}
+int cg_download_state_async(cg_ctx* ctx, int box, double* host, size_t count) {
+  return state_copy(ctx, box, host, count, false, true);
+}
+
+static int field_copy(cg_ctx* ctx, int box, int field, char reg, double* host, size_t n, bool upload) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  Box& b = ctx->boxes[box];
+  if (field < 0 || field >= b.dev.nfields) return fail(ctx, CG_ERR_INVALID, "field index out of range");
+  if (!host || n != (size_t)b.dev.pts) return fail(ctx, CG_ERR_INVALID, "n must be nx*ny*nz");
+  double* base = nullptr;
+  if (reg == 'p')
+    base = b.dev.P;
+  else if (reg == 'f')
+    base = b.dev.F;
+  else if (reg == 'a') {
+    if (b.stage_next == 0) return fail(ctx, CG_ERR_STATE, "the 'a' register exists after cg_step_init");
+    base = current_a(b);
+  } else
+    return fail(ctx, CG_ERR_INVALID, "reg must be 'p', 'a' or 'f'");
+  double* d = base + (size_t)field * b.dev.pts;
+  const size_t bytes = n * sizeof(double);
+  if (upload) {
+    CG_CUDA(ctx, cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    if (reg == 'p') {
+      b.stage_next = 0;
+    }
+  } else {
+    CG_CUDA(ctx, cudaMemcpyAsync(host, d, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CG_OK;
+}
+
+int cg_upload_field(cg_ctx* ctx, int box, int field, char reg, const double* host, size_t n) {
+  return field_copy(ctx, box, field, reg, const_cast<double*>(host), n, true);
+}
+int cg_download_field(cg_ctx* ctx, int box, int field, char reg, double* host, size_t n) {
+  return field_copy(ctx, box, field, reg, host, n, false);
+}
+
+int cg_device_register(cg_ctx* ctx, int box, char reg, double** dptr) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  if (!dptr) return fail(ctx, CG_ERR_INVALID, "dptr is null");
+  Box& b = ctx->boxes[box];
+  if (reg == 'p')
+    *dptr = b.dev.P;
+  else if (reg == 'f')
+    *dptr = b.dev.F;
+  else
+    return fail(ctx, CG_ERR_INVALID, "reg must be 'p' or 'f'");
+  // the caller may write _p through this pointer: rebuild the inputs
+  b.stage_next = 0;
+  return CG_OK;
+}
+
+int cg_step_init(cg_ctx* ctx) {
+  if (!ctx) return CG_ERR_INVALID;
+  for (Box& b : ctx->boxes) {
+    int rc = do_init(ctx, b);
+    if (rc) return rc;
+  }
+  return CG_OK;
+}
+
+int cg_rk_stage(cg_ctx* ctx, int n) {
+  if (!ctx) return CG_ERR_INVALID;
+  if (n < 1 || n > 4) return fail(ctx, CG_ERR_INVALID, "substep must be 1..4");
+  for (Box& b : ctx->boxes)
+    if (b.stage_next != n)
+      return fail(ctx, CG_ERR_STATE, "substep " + std::to_string(n) + " called out of order (expected " +
+                                          std::to_string(b.stage_next) + ")");
+  for (Box& b : ctx->boxes) {
+    int rc = do_stage(ctx, b, n);
+    if (rc) return rc;
+  }
+  return CG_OK;
+}
+
+int cg_step(cg_ctx* ctx, int nsteps) {
+  if (!ctx) return CG_ERR_INVALID;
+  if (nsteps < 0) return fail(ctx, CG_ERR_INVALID, "nsteps must be >= 0");
+  for (Box& b : ctx->boxes)
+    if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "a step is in progress; finish it with cg_rk_stage");
+  for (int s = 0; s < nsteps; ++s) {
+    for (Box& b : ctx->boxes) {
+      if (b.stage_next == 0) {
+        int rc = do_init(ctx, b);
+        if (rc) return rc;
+      }
+      for (int n = 1; n <= 4; ++n) {
+        int rc = do_stage(ctx, b, n);
+        if (rc) return rc;
+      }
+    }
+  }
+  return CG_OK;
+}
+
+int cg_status(cg_ctx* ctx, uint32_t* flags) {
+  if (!ctx || !flags) return CG_ERR_INVALID;
+  unsigned h = 0;
+  CG_CUDA(ctx, cudaMemcpyAsync(&h, ctx->status, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+  CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *flags = h;
+  return CG_OK;
+}
+
+int cg_synchronize(cg_ctx* ctx) {
+  uint32_t f = 0;
+  int rc = cg_status(ctx, &f);
+  if (rc) return rc;
+  if (f & CG_STATUS_NAN) return fail(ctx, CG_ERR_NAN, "NaN detected in DIFFphi");
+  return CG_OK;
+}
+
+int cg_frw_state(cg_ctx* ctx, int box, double* out, int n) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  const Box& b = ctx->boxes[box];
+  if (!out || n < 2 + b.frw.n) return fail(ctx, CG_ERR_INVALID, "out needs 2 + nfluids entries");
+  out[0] = b.frw.phi;
+  out[1] = b.frw.K;
+  for (int m = 0; m < b.frw.n; ++m) out[2 + m] = b.frw.rho[m];
+  return CG_OK;
+}
+
+int cg_step_count(cg_ctx* ctx, int box, int64_t* steps) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  if (!steps) return fail(ctx, CG_ERR_INVALID, "steps is null");
+  *steps = ctx->boxes[box].steps;
+  return CG_OK;
+}
+
+const char* cg_last_error(cg_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+}  // extern "C"

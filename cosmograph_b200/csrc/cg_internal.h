@@ -1,0 +1,46 @@
+// cg_internal.h -- host-side declarations shared by the CUDA translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "cg_types.h"
+
+namespace cg {
+
+// Device storage of one periodic box.  Every register block holds
+// nfields arrays of pts doubles (field f at offset f*pts), x-major with z
+// fastest like the reference's CosmoArray (utils/Array.h:47-61).
+struct BoxDev {
+  int nx, ny, nz, pts, nfields, order, matter;
+  Physics ph;
+  double* P;    // the reference's _p register (state at the start of a step)
+  double* F;    // the reference's _f register (RK accumulator)
+  double* X;    // substep inputs a^1 (normalised), a^3 and, after a step, the next a^1
+  double* Y;    // substep inputs a^2, a^4
+  double* FP0;  // dust flux primitives (P_N arrays) of a^1, a^3
+  double* FP1;  // dust flux primitives of a^2, a^4
+  unsigned* status;
+  const double* kavg;  // device K_avg for the lapses that use it, else null
+};
+
+// Kernel variants: identical source, compiled without (exact) or with (fast)
+// FMA contraction.
+enum Variant : int { kExact = 0, kFast = 1 };
+
+namespace exact {
+cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
+cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
+}  // namespace exact
+namespace fast {
+cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
+cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
+}  // namespace fast
+
+inline cudaError_t launch_stage(int v, const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
+  return v == kFast ? fast::launch_stage(b, bg, stage, st) : exact::launch_stage(b, bg, stage, st);
+}
+inline cudaError_t launch_init(int v, const BoxDev& b, const StageBg& bg, cudaStream_t st) {
+  return v == kFast ? fast::launch_init(b, bg, st) : exact::launch_init(b, bg, st);
+}
+
+}  // namespace cg

@@ -1,0 +1,114 @@
+// cg_stage_inst.cu -- instantiates the substep and step-initialisation kernels.
+//
+// Compiled twice: with -DCG_VARIANT_NS=exact and --fmad=false (the parity
+// build: every product and sum rounds separately, as in the reference's
+// strict build), and with -DCG_VARIANT_NS=fast and --fmad=true.
+#include "cg_internal.h"
+#include "cg_stage.cuh"
+
+#ifndef CG_VARIANT_NS
+#error "CG_VARIANT_NS must be defined (exact or fast)"
+#endif
+
+namespace cg {
+namespace CG_VARIANT_NS {
+
+// BSSN::stepInit (bssn.cc:219-226) on the device: the first substep's input
+// is the normalised copy of _p (RK4Register::stepInit + set_DIFFgamma_Aij_norm);
+// for dust also the flux primitives of that input (Dust::stepInit ->
+// populateDerivedFields, dust.cc:65-72 and :121-133).
+template <int MATTER>
+__global__ void __launch_bounds__(128) init_kernel(BoxGeom geo, Physics ph, StageBg bg, const double* P,
+                                                   double* X, double* FP0) {
+  constexpr int NFLD = NF<MATTER>::value;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= geo.nz || j >= geo.ny) return;
+  const int c = (i * geo.ny + j) * geo.nz + k;
+  const int N = geo.pts;
+  double v[NFLD];
+#pragma unroll
+  for (int f = 0; f < NFLD; ++f) v[f] = P[(size_t)f * N + c];
+  if (ph.normalize) {
+    double g[6], A[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) { g[m] = v[F_G11 + m]; A[m] = v[F_A11 + m]; }
+    normalize_point(g, A);
+#pragma unroll
+    for (int m = 0; m < 6; ++m) { v[F_G11 + m] = g[m]; v[F_A11 + m] = A[m]; }
+  }
+#pragma unroll
+  for (int f = 0; f < NFLD; ++f) X[(size_t)f * N + c] = v[f];
+  if (MATTER == kDust) {
+    double g[6], gi[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) g[m] = v[F_G11 + m];
+    inv_metric(g, gi);
+    const double S[3] = {v[F_S1], v[F_S2], v[F_S3]};
+    const DustPrim dp = dust_prim(gi, v[F_PHI] + bg.phi_FRW, v[F_D], S);
+    const double al = v[F_ALPHA] + 1.0;
+    FP0[(size_t)P_AD * N + c] = al * v[F_D];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) FP0[(size_t)(P_AS1 + m) * N + c] = al * S[m];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) FP0[(size_t)(P_V1 + m) * N + c] = dp.v[m];
+  }
+}
+
+namespace {
+dim3 block_dims() { return dim3(32, 4, 1); }
+dim3 grid_dims(const BoxDev& b) {
+  return dim3((b.nz + 31) / 32, (b.ny + 3) / 4, b.nx);
+}
+
+template <int O, int M>
+cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
+  StagePtrs P{};
+  P.kavg = b.kavg;
+  P.p = b.P;
+  P.f = b.F;
+  P.status = b.status;
+  switch (stage) {
+    case 1: P.in = b.X; P.prev = nullptr; P.out = b.Y; P.fp_in = b.FP0; P.fp_out = b.FP1; break;
+    case 2: P.in = b.Y; P.prev = b.X; P.out = b.X; P.fp_in = b.FP1; P.fp_out = b.FP0; break;
+    case 3: P.in = b.X; P.prev = b.Y; P.out = b.Y; P.fp_in = b.FP0; P.fp_out = b.FP1; break;
+    default: P.in = b.Y; P.prev = b.X; P.out = b.P; P.norm = b.X; P.fp_in = b.FP1; P.fp_out = b.FP0; break;
+  }
+  BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
+  stage_kernel<O, M><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, P, stage);
+  return cudaGetLastError();
+}
+
+template <int O>
+cudaError_t go_stage_m(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
+  switch (b.matter) {
+    case kDust: return go_stage<O, kDust>(b, bg, stage, st);
+    case kScalar: return go_stage<O, kScalar>(b, bg, stage, st);
+    default: return go_stage<O, kVacuum>(b, bg, stage, st);
+  }
+}
+}  // namespace
+
+cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
+  switch (b.order) {
+    case 2: return go_stage_m<2>(b, bg, stage, st);
+    case 4: return go_stage_m<4>(b, bg, stage, st);
+    case 6: return go_stage_m<6>(b, bg, stage, st);
+    case 8: return go_stage_m<8>(b, bg, stage, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st) {
+  BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
+  switch (b.matter) {
+    case kDust: init_kernel<kDust><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
+    case kScalar: init_kernel<kScalar><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
+    default: init_kernel<kVacuum><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace CG_VARIANT_NS
+}  // namespace cg

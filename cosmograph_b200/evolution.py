@@ -1,0 +1,164 @@
+"""Python front end of the C ABI: a context of periodic boxes on one GPU.
+
+`Evolution` owns a cg_ctx; its methods follow the reference's sim-driver
+sequence (sims/dust.cc:53-169): step_init() is BSSN::stepInit + Dust::stepInit
+and the source pass, rk_stage(n) is one substep (RKEvolve + K{n}Finalize of
+every field), step(n) runs whole RK4 steps.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+
+import numpy as np
+
+from . import _lib
+from .state import BoxState, num_fields
+
+
+@dataclasses.dataclass
+class BoxConfig:
+    """Per-box options (the reference's compile-time switches and config keys)."""
+
+    order: int = 8
+    lapse: str = "Harmonic"
+    precision: str = "fp64"
+    normalize_metric: int = 1
+    potential: str = "const"
+    pot_const: float = 3.0e-4
+    pot_mass: float = 1.0
+    ko_coeff: float = 0.0
+    a_adj_amp: float = 0.0
+    k_damping_amp: float = 0.0
+    gd_c: float = 1.0
+    dw_mu_l: float = 0.0
+    dw_p: float = 0.0
+
+
+def make_desc(state: BoxState, cfg: BoxConfig) -> _lib.BoxDesc:
+    d = _lib.BoxDesc()
+    d.nx, d.ny, d.nz = state.shape
+    d.stencil_order = cfg.order
+    d.matter = state.matter
+    d.lapse = _lib.LAPSE[cfg.lapse]
+    d.precision = _lib.PRECISION[cfg.precision]
+    d.normalize_metric = cfg.normalize_metric
+    d.potential = _lib.POTENTIAL[cfg.potential]
+    d.dx, d.dt, d.lam = state.dx, state.dt, state.lam
+    d.ko_coeff, d.a_adj_amp, d.k_damping_amp = cfg.ko_coeff, cfg.a_adj_amp, cfg.k_damping_amp
+    d.gd_c, d.dw_mu_l, d.dw_p = cfg.gd_c, cfg.dw_mu_l, cfg.dw_p
+    d.pot_const, d.pot_mass = cfg.pot_const, cfg.pot_mass
+    d.frw_phi, d.frw_K = state.frw_phi, state.frw_K
+    d.nfluids = len(state.fluids)
+    for n, (rho, w) in enumerate(state.fluids):
+        d.fluid_rho[n], d.fluid_w[n] = rho, w
+    return d
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Evolution:
+    """A set of boxes evolved together on one GPU."""
+
+    def __init__(self, states, configs):
+        if isinstance(states, BoxState):
+            states, configs = [states], [configs]
+        if len(states) != len(configs):
+            raise ValueError("one BoxConfig per box")
+        self.L = _lib.load()
+        self.templates = [s.copy() for s in states]
+        descs = (_lib.BoxDesc * len(states))(*[make_desc(s, c) for s, c in zip(states, configs)])
+        h = ctypes.c_void_p()
+        rc = self.L.cg_create(descs, len(states), ctypes.byref(h))
+        if rc != _lib.CG_OK:
+            _lib.check(rc, None)
+        self.ctx = h
+        for b, s in enumerate(states):
+            self.upload(b, s)
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self) -> None:
+        if self.ctx:
+            self.L.cg_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        _lib.check(rc, self.ctx)
+
+    # -- data movement -------------------------------------------------------
+    def upload(self, box: int, state: BoxState) -> None:
+        f = np.ascontiguousarray(state.fields, dtype=np.float64)
+        self._check(self.L.cg_upload_state(self.ctx, box, _dptr(f), f.size))
+
+    def download(self, box: int = 0) -> BoxState:
+        t = self.templates[box]
+        out = np.empty((num_fields(t.matter),) + t.shape, dtype=np.float64)
+        self._check(self.L.cg_download_state(self.ctx, box, _dptr(out), out.size))
+        st = dataclasses.replace(t, fields=out)
+        frw = np.zeros(2 + 4)
+        self._check(self.L.cg_frw_state(self.ctx, box, _dptr(frw), frw.size))
+        st.frw_phi, st.frw_K = float(frw[0]), float(frw[1])
+        st.fluids = tuple((float(frw[2 + n]), w) for n, (_, w) in enumerate(t.fluids))
+        cnt = ctypes.c_int64()
+        self._check(self.L.cg_step_count(self.ctx, box, ctypes.byref(cnt)))
+        st.step = t.step + int(cnt.value)
+        return st
+
+    def download_field(self, box: int, field: int, reg: str = "p") -> np.ndarray:
+        t = self.templates[box]
+        out = np.empty(t.shape, dtype=np.float64)
+        self._check(self.L.cg_download_field(self.ctx, box, field, reg.encode(), _dptr(out), out.size))
+        return out
+
+    def upload_field(self, box: int, field: int, reg: str, data: np.ndarray) -> None:
+        a = np.ascontiguousarray(data, dtype=np.float64)
+        self._check(self.L.cg_upload_field(self.ctx, box, field, reg.encode(), _dptr(a), a.size))
+
+    # -- stepping ----------------------------------------------------------------
+    def step_init(self) -> None:
+        self._check(self.L.cg_step_init(self.ctx))
+
+    def rk_stage(self, n: int) -> None:
+        self._check(self.L.cg_rk_stage(self.ctx, n))
+
+    def step(self, nsteps: int = 1) -> None:
+        self._check(self.L.cg_step(self.ctx, nsteps))
+
+    def synchronize(self) -> None:
+        self._check(self.L.cg_synchronize(self.ctx))
+
+    def status(self) -> int:
+        f = ctypes.c_uint32()
+        self._check(self.L.cg_status(self.ctx, ctypes.byref(f)))
+        return int(f.value)
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.L.cg_get_stream(self.ctx, ctypes.byref(s)))
+        return int(s.value or 0)
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self._check(self.L.cg_set_stream(self.ctx, ctypes.c_void_p(stream_ptr)))
+
+
+def evolve(state: BoxState, steps: int, cfg: BoxConfig | None = None) -> BoxState:
+    """Evolve one box for `steps` RK4 steps on the GPU and return the new state."""
+    cfg = cfg or BoxConfig()
+    with Evolution(state, cfg) as ev:
+        ev.step(steps)
+        ev.synchronize()
+        return ev.download(0)

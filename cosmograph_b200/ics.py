@@ -233,28 +233,26 @@ def grf_scalar(n, seed: int = 9, phi0: float = 1.0e-2, rms: float = 1.0e-5, mass
 
 def perturbed(shape, matter: int, seed: int = 1, amp: float = 1.0e-2, modes: int = 3,
               box_len: float = 1.0, dt_frac: float = 0.1) -> BoxState:
-    """Every field = background + amp * (a few random smooth periodic modes).
-    Backgrounds: DIFFK = -3, D = 3/(8 pi), alpha = 1 (DIFFalpha = 0), scalar
-    phi = 0.1; everything else 0."""
+    """Every field = background + amp * (a few random smooth periodic modes,
+    each a product of one sine per axis).  Backgrounds: DIFFK = -3,
+    D = 3/(8 pi), alpha = 1 (DIFFalpha = 0), scalar phi = 0.1; everything
+    else 0.  Not a solution of the constraints: it exercises every term of the
+    right-hand side."""
     shape = tuple(shape)
     dx = box_len / shape[0]
     st = _empty(shape, matter, dx, default_dt(dx, dt_frac))
     rng = np.random.Generator(np.random.MT19937(seed))
     x = [np.arange(m, dtype=np.float64) / m for m in shape]
-    X, Y, Z = np.meshgrid(*x, indexing="ij")
     for f, name in enumerate(st.names):
         v = np.zeros(shape)
         for _ in range(modes):
-            kx, ky, kz = (int(rng.integers(-2, 3)) for _ in range(3))
-            ph = rng.uniform(0, 2 * PI)
             a = rng.uniform(-1, 1)
-            v += a * np.sin(2 * PI * (kx * X + ky * Y + kz * Z) + ph)
+            s1 = [np.sin(2 * PI * int(rng.integers(0, 3)) * xi + rng.uniform(0, 2 * PI)) for xi in x]
+            v += (a * s1[0])[:, None, None] * s1[1][None, :, None] * s1[2][None, None, :]
         v *= amp / modes
         base = {"DIFFK": -3.0, "D": RHO_FRW, "phi": 0.1}.get(name, 0.0)
-        if name in ("D",):
+        if name in ("D", "S1", "S2", "S3"):
             v = RHO_FRW * v            # keep the density positive
-        if name in ("S1", "S2", "S3"):
-            v = RHO_FRW * v
         st.fields[f] = base + v
     if matter == DUST:
         st.lam = 1.0e-6 * RHO_FRW

@@ -1,0 +1,183 @@
+/*
+ * cosmograph_b200.h -- C ABI of the B200-native BSSN (+dust / +scalar) RK4
+ * evolution path for periodic boxes.
+ *
+ * The reference (CosmoGRaPH, unigrid) exposes this path as C++ classes that
+ * its sim drivers call in a fixed order; it has no FFI layer.  Each entry
+ * point below names the reference interface it replaces.  The C++ facade in
+ * cosmograph_b200/host/ (BSSN, Dust, Scalar, Lambda, RK4Register) keeps the
+ * reference's method names on top of these calls.
+ *
+ * Conventions
+ *   - Every call returns CG_OK (0) or a negative CG_ERR_* code; the message of
+ *     the last failure is available from cg_last_error().  No C++ exception
+ *     crosses this boundary.
+ *   - Host buffers are borrowed for the duration of a call only; device memory
+ *     belongs to the context.
+ *   - Field arrays are FP64, x-major with z fastest, NP_INDEX(i,j,k) =
+ *     (nz*ny)*i + nz*j + k (reference cosmo_macros.h:118), one array per field
+ *     in the order of cg_field_name().
+ *   - A context is used by one host thread at a time; work is queued on the
+ *     context's CUDA stream.
+ */
+#ifndef COSMOGRAPH_B200_H
+#define COSMOGRAPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CG_ABI_VERSION 1
+
+/* status codes */
+#define CG_OK 0
+#define CG_ERR_INVALID (-1)   /* bad argument or unsupported option      */
+#define CG_ERR_CUDA (-2)      /* CUDA runtime error                      */
+#define CG_ERR_MEMORY (-3)    /* device allocation failed                */
+#define CG_ERR_STATE (-4)     /* call out of sequence                    */
+#define CG_ERR_NAN (-10)      /* NaN detected in DIFFphi (the reference's
+                                 `throw 10`, sims/sim.cc:179-183)          */
+
+/* matter models (reference simulation_type, cosmo.cc:51-81) */
+#define CG_MATTER_VACUUM 0
+#define CG_MATTER_DUST 1
+#define CG_MATTER_SCALAR 2
+
+/* lapse gauges (reference BSSNGaugeHandler lapse map,
+ * components/bssn/BSSNGaugeHandler.h:95-110) */
+#define CG_LAPSE_STATIC 0
+#define CG_LAPSE_HARMONIC 1
+#define CG_LAPSE_CONFORMAL_FLRW 2
+#define CG_LAPSE_CONFORMAL_SYNC 3
+#define CG_LAPSE_ANHARMONIC 4
+#define CG_LAPSE_ONE_PLUS_LOG 5
+#define CG_LAPSE_AWA_GAUGE_WAVE 6
+#define CG_LAPSE_AWA_SHIFTED_WAVE 7
+#define CG_LAPSE_DAMPED_WAVE 8
+
+/* arithmetic of the substep kernel */
+#define CG_PREC_FP64 0      /* FP64, reference operand order, no FMA contraction */
+#define CG_PREC_FP64_FMA 1  /* FP64 with FMA contraction                          */
+
+/* scalar potentials */
+#define CG_POT_CONST 0      /* V = pot_const, dV = 0 (components/scalar/scalar.cc:262-274) */
+#define CG_POT_QUADRATIC 1  /* V = m^2 phi^2 / 2                                            */
+
+/* status flags (cg_status) */
+#define CG_STATUS_NAN 1u        /* NaN in DIFFphi after a step          */
+#define CG_STATUS_NONFINITE 2u  /* NaN or Inf in any evolved field      */
+
+typedef struct cg_ctx cg_ctx;
+
+/* One periodic box: the reference's compile-time switches
+ * (cosmo_macros.h:12-84) and run-time config keys (components/bssn/bssn.cc:15-22,
+ * cosmo.cc:41-42) as plain fields. */
+typedef struct {
+  int nx, ny, nz;          /* grid points per axis (each >= stencil_order/2 + 1) */
+  int stencil_order;       /* 2, 4, 6 or 8 (STENCIL_ORDER)                       */
+  int matter;              /* CG_MATTER_*                                        */
+  int lapse;               /* CG_LAPSE_*                                         */
+  int precision;           /* CG_PREC_*                                          */
+  int normalize_metric;    /* config normalize_metric (default 1)                */
+  int potential;           /* CG_POT_* (scalar matter only)                      */
+  int reserved0;
+  double dx, dt;           /* grid spacing and time step                          */
+  double lambda;           /* rho_Lambda (Lambda::setLambda)                      */
+  double ko_coeff;         /* KO_damping_coefficient; must be 0 here              */
+  double a_adj_amp;        /* config a_adj_amp                                    */
+  double k_damping_amp;    /* config k_damping_amp                                */
+  double gd_c;             /* config gd_c (OnePlusLog), default 1                 */
+  double dw_mu_l, dw_p;    /* config dw_mu_l, dw_p (DampedWave)                   */
+  double pot_const;        /* V for CG_POT_CONST (reference COSMO_CONST = 3e-4)    */
+  double pot_mass;         /* m for CG_POT_QUADRATIC                              */
+  double frw_phi, frw_K;   /* FRW reference background (utils/FRW.h:15-16)         */
+  int nfluids;             /* FRW fluids (FRW::addFluid, utils/FRW.h:60-76), <= 4  */
+  int reserved1;
+  double fluid_rho[4], fluid_w[4];
+} cg_box_desc;
+
+/* Fill a descriptor with the reference's defaults (Harmonic lapse, order 8,
+ * dust, normalize_metric = 1, dx = 1/N, dt = 0.1 dx). */
+void cg_box_desc_default(cg_box_desc *d, int n);
+
+/* Create a context holding nboxes boxes (BSSN::BSSN + Dust::Dust / Scalar::Scalar
+ * allocation, components/bssn/bssn.cc:13-44, components/dust_fluid/dust.cc:15-44).
+ * Every field of every register starts at zero (BSSN::init, bssn.cc:126-144). */
+int cg_create(const cg_box_desc *boxes, int nboxes, cg_ctx **out);
+
+/* Release the context and its device memory. */
+int cg_destroy(cg_ctx *ctx);
+
+/* Queue all work on `stream` (a cudaStream_t; NULL = the context's own). */
+int cg_set_stream(cg_ctx *ctx, void *stream);
+int cg_get_stream(cg_ctx *ctx, void **stream);
+
+/* Number of evolved fields (18 vacuum, 22 dust, 23 scalar) and their names
+ * (BSSN_APPLY_TO_FIELDS order, bssn_macros.h:77-95, then D,S1,S2,S3 or
+ * phi,Pi,psi1,psi2,psi3). */
+int cg_num_fields(int matter);
+const char *cg_field_name(int matter, int field);
+
+/* Copy the "_p" register of every field of one box from / to host memory;
+ * count = nfields*nx*ny*nz doubles.  Replaces filling / reading
+ * RK4Register::_array_p through BSSN::fields (bssn.cc:30-39). Synchronous. */
+int cg_upload_state(cg_ctx *ctx, int box, const double *host, size_t count);
+int cg_download_state(cg_ctx *ctx, int box, double *host, size_t count);
+
+/* Same, asynchronous on the context's stream (host memory should be pinned). */
+int cg_upload_state_async(cg_ctx *ctx, int box, const double *host, size_t count);
+int cg_download_state_async(cg_ctx *ctx, int box, double *host, size_t count);
+
+/* One register of one field: reg = 'p', 'a' (current substep input), 'f'.
+ * Replaces BSSN::fields["<name>_<reg>"] access (bssn.cc:30-39). Synchronous. */
+int cg_upload_field(cg_ctx *ctx, int box, int field, char reg, const double *host, size_t n);
+int cg_download_field(cg_ctx *ctx, int box, int field, char reg, double *host, size_t n);
+
+/* Device pointer of a register block of one box (nfields arrays of pts
+ * doubles): reg = 'p' or 'f'.  For callers that keep their data on the GPU. */
+int cg_device_register(cg_ctx *ctx, int box, char reg, double **dptr);
+
+/* BSSN::stepInit (bssn.cc:219-226) + Dust::stepInit (dust.cc:65-72) +
+ * Scalar::stepInit for every box: builds the first substep's input from _p. */
+int cg_step_init(cg_ctx *ctx);
+
+/* Substep n = 1..4 for every box: sources, BSSN and matter RHS and the
+ * register update of RK4Register::K{n}Finalize in one fused kernel
+ * (replaces BSSN::RKEvolve + Dust::RKEvolve / Scalar::RKEvolvePt +
+ * BSSN::K{n}Finalize + Dust::K{n}Finalize, sims/dust.cc:114-161,
+ * sims/scalar.cc:97-151).  Substeps must be called in order after
+ * cg_step_init. */
+int cg_rk_stage(cg_ctx *ctx, int n);
+
+/* nsteps full RK4 steps for every box (stepInit + 4 substeps each; the
+ * reference's DustSim::runStep minus output, sims/dust.cc:163-169).
+ * Asynchronous: returns once the work is queued. */
+int cg_step(cg_ctx *ctx, int nsteps);
+
+/* Wait for queued work; returns CG_ERR_NAN if a NaN appeared in DIFFphi. */
+int cg_synchronize(cg_ctx *ctx);
+
+/* Sticky error flags (CG_STATUS_*), OR-reduced on the device. */
+int cg_status(cg_ctx *ctx, uint32_t *flags);
+
+/* FRW background state of a box: out[0] = phi, out[1] = K, out[2..] = fluid
+ * densities (utils/FRW.h:79-83). */
+int cg_frw_state(cg_ctx *ctx, int box, double *out, int n);
+
+/* Steps completed by a box since creation or the last upload. */
+int cg_step_count(cg_ctx *ctx, int box, int64_t *steps);
+
+/* Message of the last failure on this context (or of cg_create, when ctx is NULL). */
+const char *cg_last_error(cg_ctx *ctx);
+
+/* ABI version (CG_ABI_VERSION). */
+int cg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -206,8 +206,11 @@ int main(int argc, char **argv) {
   std::string extra;
   if (mode == "evolve") {
     for (int s = 0; s < steps; ++s) {
+      const double ts = now_s();
       sim.init_step();
       sim.run_step();
+      printf("CGSTEP %d %.6f\n", s, now_s() - ts);
+      fflush(stdout);
     }
   } else if (mode == "rhs") {
     sim.init_step();

@@ -1,0 +1,62 @@
+"""The C-ABI library: it builds, loads without a GPU, exports every symbol the
+public header declares, and rejects bad descriptors before touching CUDA."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from cosmograph_b200 import _lib
+from cosmograph_b200.build import build
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "cosmograph_b200.h"
+
+
+@pytest.fixture(scope="module")
+def L():
+    build()
+    return _lib.load()
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"\b(cg_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_what_the_binding_knows():
+    assert declared_symbols() == sorted(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol(L):
+    for name in declared_symbols():
+        assert hasattr(L, name), name
+
+
+def test_host_only_entry_points(L):
+    assert L.cg_version() == 1
+    assert [L.cg_num_fields(m) for m in (0, 1, 2)] == [18, 22, 23]
+    assert L.cg_field_name(1, 0) == b"DIFFgamma11"
+    assert L.cg_field_name(1, 21) == b"S3"
+    assert L.cg_field_name(2, 22) == b"psi3"
+    assert L.cg_field_name(0, 18) is None
+    d = _lib.BoxDesc()
+    L.cg_box_desc_default(ctypes.byref(d), 64)
+    assert (d.nx, d.stencil_order, d.lapse, d.normalize_metric) == (64, 8, 1, 1)
+    assert d.dx == 1.0 / 64 and d.dt == pytest.approx(0.1 / 64, rel=1e-15)
+
+
+@pytest.mark.parametrize("field,value,msg", [
+    ("stencil_order", 5, "stencil_order"),
+    ("nx", 2, "at least"),
+    ("ko_coeff", 0.5, "Kreiss-Oliger"),
+    ("lapse", 42, "lapse"),
+    ("nfluids", 7, "fluids"),
+])
+def test_create_rejects_bad_descriptors(L, field, value, msg):
+    d = _lib.BoxDesc()
+    L.cg_box_desc_default(ctypes.byref(d), 16)
+    setattr(d, field, value)
+    h = ctypes.c_void_p()
+    rc = L.cg_create(ctypes.byref(d), 1, ctypes.byref(h))
+    assert rc == -1 and not h.value
+    assert msg in L.cg_last_error(None).decode()

@@ -1,0 +1,139 @@
+"""Parity of the CUDA path with the reference (golden fixtures) and with the CPU
+restatement (oracle/) on seeded inputs, plus size-independent properties at
+full size.  Every call goes through the C ABI (libcosmograph_b200.so).
+
+Tolerances (norm-wise per field, max|gpu - ref| / max|ref|):
+  fp64     : 1e-12 after the full run (reference operand order, no FMA
+             contraction; CUDA's exp/log1p/expm1 differ from libm by an ulp)
+  fp64_fma : 1e-10 (FMA contraction changes every rounding)
+"""
+import numpy as np
+import pytest
+
+import oracle
+from cosmograph_b200 import ics, state as S
+from cosmograph_b200.evolution import BoxConfig, Evolution, evolve
+from helpers import field_errors, golden_index, load_golden, worst
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-12, "fp64_fma": 1e-10}
+GOLDEN_EVOLVE = [k for k, v in golden_index().items() if v["mode"] == "evolve"]
+
+
+def cfg_from(meta, precision="fp64"):
+    c = dict(meta["config"])
+    return BoxConfig(order=meta["order"], precision=precision, **c)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp64_fma"])
+@pytest.mark.parametrize("name", GOLDEN_EVOLVE)
+def test_golden_evolve(name, precision):
+    inp, out, _, meta = load_golden(name)
+    got = evolve(inp, meta["steps"], cfg_from(meta, precision))
+    errs = field_errors(got.fields, out.fields, inp.names, floor=1e-18)
+    assert worst(errs)[1] <= TOL[precision], worst(errs)
+    assert got.step == meta["steps"]
+
+
+def test_golden_first_substep_rhs():
+    """After substep 1 the _f register holds dt*RHS/6 (RK4Register.h:180)."""
+    inp, rhs_ref, _, meta = load_golden("dust_o4_rhs")
+    with Evolution(inp, cfg_from(meta)) as ev:
+        ev.step_init()
+        ev.rk_stage(1)
+        ev.synchronize()
+        got = np.stack([ev.download_field(0, f, "f") for f in range(len(inp.names))])
+    expect = inp.dt * rhs_ref.fields / 6.0
+    errs = field_errors(got, expect, inp.names, floor=1e-18)
+    assert worst(errs)[1] <= 1e-14, worst(errs)
+
+
+CASES = [
+    # matter, shape, order, lapse, steps
+    (S.DUST, (24, 24, 24), 8, "Harmonic", 4),
+    (S.DUST, (20, 18, 22), 4, "Harmonic", 10),
+    (S.DUST, (16, 16, 16), 2, "ConformalFLRW", 5),
+    (S.SCALAR, (16, 20, 24), 4, "Harmonic", 6),
+    (S.SCALAR, (18, 18, 18), 8, "DampedWave", 3),
+    (S.VACUUM, (16, 16, 32), 6, "Anharmonic", 4),
+    (S.VACUUM, (12, 12, 12), 2, "AwAGaugeWave", 6),
+]
+
+
+@pytest.mark.parametrize("matter,shape,order,lapse,steps", CASES)
+def test_against_restatement(matter, shape, order, lapse, steps):
+    st = ics.perturbed(shape, matter, seed=hash((matter, shape, order)) % 1000, amp=2e-2)
+    kw = dict(lapse=lapse)
+    if lapse == "DampedWave":
+        kw.update(dw_mu_l=0.3, dw_p=0.5)
+    ref = oracle.evolve(st, steps, order, **kw)
+    got = evolve(st, steps, BoxConfig(order=order, **kw))
+    errs = field_errors(got.fields, ref.fields, st.names, floor=1e-18)
+    assert worst(errs)[1] <= TOL["fp64"], worst(errs)
+
+
+def test_sinusoid_100_steps():
+    """Single-mode dust box, 32^3, 4th order, dt = 0.1 dx, 100 RK4 steps."""
+    st = ics.sinusoid_dust(32)
+    ref = oracle.evolve(st, 100, 4, lapse="Harmonic")
+    got = evolve(st, 100, BoxConfig(order=4, lapse="Harmonic"))
+    errs = field_errors(got.fields, ref.fields, st.names, floor=1e-12 * 1e-3)
+    assert worst(errs)[1] <= TOL["fp64"], worst(errs)
+
+
+def test_substep_api_equals_step():
+    st = ics.perturbed((16, 16, 16), S.DUST, seed=4)
+    cfg = BoxConfig(order=4)
+    with Evolution(st, cfg) as ev:
+        ev.step_init()
+        for n in (1, 2, 3, 4):
+            ev.rk_stage(n)
+        ev.synchronize()
+        a = ev.download(0).fields
+    b = evolve(st, 1, cfg).fields
+    assert np.array_equal(a, b)
+
+
+def test_translation_equivariance_full_size():
+    """Evolving a periodically shifted box gives the shifted result, bit for bit
+    (every point runs the same arithmetic on the same neighbourhood)."""
+    st = ics.grf_dust(128, seed=5, rms_delta=1e-4, order=8)
+    cfg = BoxConfig(order=8)
+    a = evolve(st, 2, cfg)
+    sh = st.copy()
+    sh.fields = np.roll(st.fields, (5, -7, 3), axis=(1, 2, 3))
+    b = evolve(sh, 2, cfg)
+    assert np.array_equal(np.roll(a.fields, (5, -7, 3), axis=(1, 2, 3)), b.fields)
+
+
+def test_uniform_box_stays_uniform_full_size():
+    st = ics.perturbed((256, 64, 64), S.DUST, amp=0.0)
+    got = evolve(st, 3, BoxConfig(order=8))
+    for f in range(got.fields.shape[0]):
+        assert np.ptp(got.fields[f]) == 0.0, st.names[f]
+    # and it matches a small box with the same uniform data
+    small = ics.perturbed((9, 9, 9), S.DUST, amp=0.0)
+    small.dt, small.dx = st.dt, st.dx
+    ref = evolve(small, 3, BoxConfig(order=8))
+    assert np.array_equal(got.fields[:, 0, 0, 0], ref.fields[:, 0, 0, 0])
+
+
+def test_nan_is_reported():
+    st = ics.perturbed((12, 12, 12), S.DUST, seed=8)
+    st.fields[S.BSSN_FIELDS.index("DIFFphi"), 3, 4, 5] = np.nan
+    with Evolution(st, BoxConfig(order=4)) as ev:
+        ev.step(1)
+        assert ev.status() & 1
+        with pytest.raises(RuntimeError, match="NaN"):
+            ev.synchronize()
+
+
+def test_out_of_order_substep_is_rejected():
+    st = ics.perturbed((12, 12, 12), S.VACUUM)
+    with Evolution(st, BoxConfig(order=4)) as ev:
+        with pytest.raises(RuntimeError, match="out of"):
+            ev.rk_stage(1)
+        ev.step_init()
+        with pytest.raises(RuntimeError, match="out of"):
+            ev.rk_stage(2)
