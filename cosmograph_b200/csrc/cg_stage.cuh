@@ -4,7 +4,7 @@
 // whole substep of its sim drivers (sims/dust.cc:119-157, sims/scalar.cc:
 // 275-317, components/bssn/bssn.cc:327-339):
 //   sources      BSSN::clearSrc + Dust::addBSSNSrc + Lambda::addBSSNSource, or
-//                Scalar::addBSSNSource (computed in registers, never stored)
+//                Scalar::addBSSNSource (computed on chip, never stored)
 //   BSSN RHS     BSSN::RKEvolve -> set_bd_values + ev_* (bssn.cc:231-831)
 //   matter RHS   Dust::RKEvolve (flux divergence, dust.cc:160-224) or
 //                Scalar::RKEvolvePt (scalar.cc:85-199)
@@ -21,6 +21,16 @@
 //   p, f  the reference's _p and _f registers
 //   out   a^{n+1} (n<4) or the new _p (n=4)
 // At n=4, norm receives the next step's first-substep input.
+//
+// Kernel shape.  A CTA owns a 4x4x8 (x,y,z) brick, one point per thread.
+// Phase 1 walks the stencil fields one at a time (a rolled loop, so the whole
+// CTA touches one field's halo region at a time and it stays in L1), computes
+// that field's derivatives at the thread's point and parks them in the
+// thread's column of a shared-memory slot array.  Phase 2 (the algebra of
+// set_bd_values and ev_*) reads the derivatives back from shared memory as it
+// needs them, so few values are live in registers at once.  Bricks whose
+// stencils never cross the periodic boundary use plain strided addressing;
+// the others wrap every tap.
 #pragma once
 
 #include "cg_point.cuh"
@@ -53,188 +63,468 @@ struct NF {
   static constexpr int value = MATTER == kDust ? 22 : (MATTER == kScalar ? 23 : 18);
 };
 
+// CTA brick
+constexpr int kBX = 4, kBY = 4, kBZ = 8, kThreads = kBX * kBY * kBZ;
+
+// Per-thread shared-memory slots (one column of kThreads doubles per slot).
+enum : int {
+  S_DG = 0,           // d_I g_q           18  (later reused for Gamma_{I q})
+  S_T1 = 18,          // g^{kl} d_k d_l g_q  6
+  S_DPHI = 24,        // d_I phi            3
+  S_DDPHI = 27,       // d_I d_J phi        6
+  S_DA = 33,          // d_I alpha          3
+  S_DDA = 36,         // d_I d_J alpha      6
+  S_DK = 42,          // d_I K              3
+  S_DGAM = 45,        // d_J Gamma^K       9  (index 3*K + J)
+  S_SRC = 54,         // sources           11
+  S_G = 65,           // Gamma^I_q         18
+  S_MAT = 83,         // dust: 4 divergences; scalar: 15 first derivatives
+};
+template <int MATTER>
+struct Slots {
+  static constexpr int value = S_MAT + (MATTER == kDust ? 4 : (MATTER == kScalar ? 15 : 0));
+};
+
 namespace CG_VARIANT_NS {
 
-// derivative along axis a of the product of two stored arrays (the dust fluxes
-// alpha*D*v^i = (alpha*D)*v^i, dust.cc:121-133, and their divergence :203-224)
-template <int O>
-__device__ __forceinline__ double der1_prod(const double* __restrict__ fa, const double* __restrict__ fb,
-                                            const Site& s, int a, const Physics& ph) {
-  auto V = [&](int n) {
-    const int q = s.ax(a, n);
-    return ld(fa, q) * ld(fb, q);
-  };
-  double t;
+// Stencil taps of one point.  WRAP=false: the brick lies at least r points
+// from every face, taps are plain offsets.  WRAP=true: periodic wrap.
+template <bool WRAP>
+struct Taps {
+  int i, j, k, nx, ny, nz, sx, sy, c;
+  __device__ __forceinline__ int at(int di, int dj, int dk) const {
+    if (!WRAP) return c + di * sx + dj * sy + dk;
+    return (wrap(i + di, nx) * ny + wrap(j + dj, ny)) * nz + wrap(k + dk, nz);
+  }
+  __device__ __forceinline__ int ax(int a, int n) const {
+    return at(a == 0 ? n : 0, a == 1 ? n : 0, a == 2 ? n : 0);
+  }
+  __device__ __forceinline__ int pl(int a, int n, int b, int m) const {
+    return at((a == 0 ? n : 0) + (b == 0 ? m : 0), (a == 1 ? n : 0) + (b == 1 ? m : 0),
+              (a == 2 ? n : 0) + (b == 2 ? m : 0));
+  }
+};
+
+// first derivative (utils/math.h:74-100, 231-263, 412-450, 554-586)
+template <int O, class T>
+__device__ __forceinline__ double d1(const double* __restrict__ f, const T& t, int a, const Physics& ph) {
+  auto V = [&](int n) { return __ldg(f + t.ax(a, n)); };
+  double s;
   if (O == 2) {
-    t = (-1.0 / 2.0 * V(-1) + 1.0 / 2.0 * V(1));
+    s = (-1.0 / 2.0 * V(-1) + 1.0 / 2.0 * V(1));
   } else if (O == 4) {
-    t = (+1.0 / 12.0 * V(-2) - 2.0 / 3.0 * V(-1) + 2.0 / 3.0 * V(1) - 1.0 / 12.0 * V(2));
+    s = (+1.0 / 12.0 * V(-2) - 2.0 / 3.0 * V(-1) + 2.0 / 3.0 * V(1) - 1.0 / 12.0 * V(2));
   } else if (O == 6) {
-    t = (-1.0 / 60.0 * V(-3) + 3.0 / 20.0 * V(-2) - 3.0 / 4.0 * V(-1) + 3.0 / 4.0 * V(1) -
+    s = (-1.0 / 60.0 * V(-3) + 3.0 / 20.0 * V(-2) - 3.0 / 4.0 * V(-1) + 3.0 / 4.0 * V(1) -
          3.0 / 20.0 * V(2) + 1.0 / 60.0 * V(3));
   } else {
-    t = ((1.0 / 280.0 * V(-4) - 1.0 / 280.0 * V(4)) - (4.0 / 105.0 * V(-3) - 4.0 / 105.0 * V(3)) +
+    s = ((1.0 / 280.0 * V(-4) - 1.0 / 280.0 * V(4)) - (4.0 / 105.0 * V(-3) - 4.0 / 105.0 * V(3)) +
          (1.0 / 5.0 * V(-2) - 1.0 / 5.0 * V(2)) - (4.0 / 5.0 * V(-1) - 4.0 / 5.0 * V(1)));
   }
-  return divdx(t, ph);
+  return divdx(s, ph);
+}
+
+// second derivative along one axis (utils/math.h:857-885, 958-993, 995-1036, 1038-1085)
+template <int O, class T>
+__device__ __forceinline__ double d2(const double* __restrict__ f, const T& t, int a, const Physics& ph) {
+  auto V = [&](int n) { return __ldg(f + t.ax(a, n)); };
+  double s;
+  if (O == 2) {
+    s = (V(-1) - 2.0 * V(0) + V(1));
+  } else if (O == 4) {
+    s = (-1.0 / 12.0 * V(-2) + 4.0 / 3.0 * V(-1) - 5.0 / 2.0 * V(0) + 4.0 / 3.0 * V(1) - 1.0 / 12.0 * V(2));
+  } else if (O == 6) {
+    s = (1.0 / 90.0 * V(-3) - 3.0 / 20.0 * V(-2) + 3.0 / 2.0 * V(-1) - 49.0 / 18.0 * V(0) + 3.0 / 2.0 * V(1) -
+         3.0 / 20.0 * V(2) + 1.0 / 90.0 * V(3));
+  } else {
+    s = (-1.0 / 560.0 * V(-4) + 8.0 / 315.0 * V(-3) - 1.0 / 5.0 * V(-2) + 8.0 / 5.0 * V(-1) -
+         205.0 / 72.0 * V(0) + 8.0 / 5.0 * V(1) - 1.0 / 5.0 * V(2) + 8.0 / 315.0 * V(3) - 1.0 / 560.0 * V(4));
+  }
+  return divdx(divdx(s, ph), ph);
+}
+
+// mixed second derivative on axes a < b (utils/math.h:676-855)
+template <int O, class T>
+__device__ __forceinline__ double dm(const double* __restrict__ f, const T& t, int a, int b, const Physics& ph) {
+  auto P = [&](int n) {
+    return -__ldg(f + t.pl(a, n, b, -n)) + __ldg(f + t.pl(a, n, b, n)) + __ldg(f + t.pl(a, -n, b, -n)) -
+           __ldg(f + t.pl(a, -n, b, n));
+  };
+  double s;
+  if (O == 2) {
+    s = P(1) / 4.0;
+  } else if (O == 4) {
+    s = (P(1) - 1.0 / 16.0 * P(2)) / 3.0;
+  } else if (O == 6) {
+    s = (135.0 * P(1) - 27.0 / 2.0 * P(2) + P(3)) / 360.0;
+  } else {
+    s = (2.0 / 5.0 * P(1) - 1.0 / 20.0 * P(2) + 2.0 / 315.0 * P(3) - 1.0 / 2240.0 * P(4));
+  }
+  return divdx(divdx(s, ph), ph);
+}
+
+// derivative of the product of two stored arrays (dust fluxes (alpha*D)*v^i,
+// dust.cc:121-133, and their divergence :203-224)
+template <int O, class T>
+__device__ __forceinline__ double d1p(const double* __restrict__ fa, const double* __restrict__ fb, const T& t,
+                                      int a, const Physics& ph) {
+  auto V = [&](int n) {
+    const int q = t.ax(a, n);
+    return __ldg(fa + q) * __ldg(fb + q);
+  };
+  double s;
+  if (O == 2) {
+    s = (-1.0 / 2.0 * V(-1) + 1.0 / 2.0 * V(1));
+  } else if (O == 4) {
+    s = (+1.0 / 12.0 * V(-2) - 2.0 / 3.0 * V(-1) + 2.0 / 3.0 * V(1) - 1.0 / 12.0 * V(2));
+  } else if (O == 6) {
+    s = (-1.0 / 60.0 * V(-3) + 3.0 / 20.0 * V(-2) - 3.0 / 4.0 * V(-1) + 3.0 / 4.0 * V(1) -
+         3.0 / 20.0 * V(2) + 1.0 / 60.0 * V(3));
+  } else {
+    s = ((1.0 / 280.0 * V(-4) - 1.0 / 280.0 * V(4)) - (4.0 / 105.0 * V(-3) - 4.0 / 105.0 * V(3)) +
+         (1.0 / 5.0 * V(-2) - 1.0 / 5.0 * V(2)) - (4.0 / 5.0 * V(-1) - 4.0 / 5.0 * V(1)));
+  }
+  return divdx(s, ph);
+}
+
+// Phase 1: every derivative the point needs, parked in shared memory.
+template <int O, int MATTER, class T>
+__device__ __forceinline__ void derivatives(const T& t, const double* __restrict__ a, const double* __restrict__ fp,
+                                            int N, const Physics& ph, const double gi[6], double* sl) {
+  // metric components, phi and alpha: first and second derivatives
+  // (calculate_dgamma / calculate_ddgamma / calculate_dalpha_dphi,
+  // bssn.cc:480-521).  For g_q the second derivatives are contracted at once
+  // with the inverse metric (BSSN_CALCULATE_RICCI_UNITARY_TERM1,
+  // bssn_macros.h:248-249, summed over (k,l) in the reference's order).
+#pragma unroll 1
+  for (int it = 0; it < 8; ++it) {
+    const int fld = it < 6 ? F_G11 + it : (it == 6 ? F_PHI : F_ALPHA);
+    const double* __restrict__ f = a + (size_t)fld * N;
+    const double g1 = d1<O>(f, t, 0, ph), g2 = d1<O>(f, t, 1, ph), g3 = d1<O>(f, t, 2, ph);
+    const double h11 = d2<O>(f, t, 0, ph), h22 = d2<O>(f, t, 1, ph), h33 = d2<O>(f, t, 2, ph);
+    const double h12 = dm<O>(f, t, 0, 1, ph), h13 = dm<O>(f, t, 0, 2, ph), h23 = dm<O>(f, t, 1, 2, ph);
+    if (it < 6) {
+      sl[(S_DG + 0 * 6 + it) * kThreads] = g1;
+      sl[(S_DG + 1 * 6 + it) * kThreads] = g2;
+      sl[(S_DG + 2 * 6 + it) * kThreads] = g3;
+      double s = gi[0] * h11;
+      s = s + gi[1] * h12;
+      s = s + gi[2] * h13;
+      s = s + gi[1] * h12;
+      s = s + gi[3] * h22;
+      s = s + gi[4] * h23;
+      s = s + gi[2] * h13;
+      s = s + gi[4] * h23;
+      s = s + gi[5] * h33;
+      sl[(S_T1 + it) * kThreads] = s;
+    } else {
+      const int b1 = it == 6 ? S_DPHI : S_DA, b2 = it == 6 ? S_DDPHI : S_DDA;
+      sl[(b1 + 0) * kThreads] = g1;
+      sl[(b1 + 1) * kThreads] = g2;
+      sl[(b1 + 2) * kThreads] = g3;
+      sl[(b2 + 0) * kThreads] = h11;
+      sl[(b2 + 1) * kThreads] = h12;
+      sl[(b2 + 2) * kThreads] = h13;
+      sl[(b2 + 3) * kThreads] = h22;
+      sl[(b2 + 4) * kThreads] = h23;
+      sl[(b2 + 5) * kThreads] = h33;
+    }
+  }
+  // K and Gamma^K: first derivatives (calculate_dK, bssn.cc:529-535; the
+  // d_J Gamma^K of BSSN_CALCULATE_RICCI_UNITARY_TERM2, bssn_macros.h:251-252)
+#pragma unroll 1
+  for (int it = 0; it < 4; ++it) {
+    const int fld = it == 0 ? F_K : F_GAM1 + it - 1;
+    const double* __restrict__ f = a + (size_t)fld * N;
+    const int b = it == 0 ? S_DK : S_DGAM + 3 * (it - 1);
+    sl[(b + 0) * kThreads] = d1<O>(f, t, 0, ph);
+    sl[(b + 1) * kThreads] = d1<O>(f, t, 1, ph);
+    sl[(b + 2) * kThreads] = d1<O>(f, t, 2, ph);
+  }
+  if (MATTER == kDust) {
+    // flux divergences d_i(alpha D v^i), d_i(alpha S_m v^i) (dust.cc:203-224)
+    const double* v1 = fp + (size_t)P_V1 * N;
+    const double* v2 = fp + (size_t)P_V2 * N;
+    const double* v3 = fp + (size_t)P_V3 * N;
+#pragma unroll 1
+    for (int m = 0; m < 4; ++m) {
+      const double* u = fp + (size_t)(P_AD + m) * N;
+      sl[(S_MAT + m) * kThreads] = d1p<O>(u, v1, t, 0, ph) + d1p<O>(u, v2, t, 1, ph) + d1p<O>(u, v3, t, 2, ph);
+    }
+  } else if (MATTER == kScalar) {
+    // Scalar::getScalarData derivatives (scalar.cc:109-127): d_d of phi, Pi, psi1..3
+#pragma unroll 1
+    for (int m = 0; m < 5; ++m) {
+      const double* __restrict__ f = a + (size_t)(F_SPHI + m) * N;
+      sl[(S_MAT + 3 * m + 0) * kThreads] = d1<O>(f, t, 0, ph);
+      sl[(S_MAT + 3 * m + 1) * kThreads] = d1<O>(f, t, 1, ph);
+      sl[(S_MAT + 3 * m + 2) * kThreads] = d1<O>(f, t, 2, ph);
+    }
+  }
 }
 
 template <int O, int MATTER>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kThreads, 2)
 stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
   constexpr int NFLD = NF<MATTER>::value;
+  constexpr int R = O / 2;
+  extern __shared__ double smem[];
+  const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
+  double* sl = smem + tid;  // this thread's slot column
+  auto S = [&](int s) -> double& { return sl[s * kThreads]; };
+
+  const int k = blockIdx.x * kBZ + threadIdx.x;
+  const int j = blockIdx.y * kBY + threadIdx.y;
+  const int i = blockIdx.z * kBX + threadIdx.z;
+  const bool live = i < geo.nx && j < geo.ny && k < geo.nz;
+  if (!live) return;  // no CTA-wide synchronisation below
   if (P.kavg) bg.K_avg = *P.kavg;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z;
-  if (k >= geo.nz || j >= geo.ny) return;
-  const Site s{i, j, k, geo.nx, geo.ny, geo.nz};
-  const int c = (i * geo.ny + j) * geo.nz + k;
   const int N = geo.pts;
+  const int c = (i * geo.ny + j) * geo.nz + k;
   const double* __restrict__ a = P.in;
-  auto F = [&](int f) { return a + (size_t)f * N; };
+  auto C = [&](int f) { return a[(size_t)f * N + c]; };
 
-  // ---- centre values (set_local_vals, bssn.cc:430-435) -------------------
-  double g[6], A[6], Gam[3];
+  // ---- centre values (set_local_vals, bssn.cc:430-435) ----------------------
+  double g[6], gi[6];
 #pragma unroll
-  for (int q = 0; q < 6; ++q) g[q] = ld(F(F_G11 + q), c);
-#pragma unroll
-  for (int q = 0; q < 6; ++q) A[q] = ld(F(F_A11 + q), c);
-#pragma unroll
-  for (int q = 0; q < 3; ++q) Gam[q] = ld(F(F_GAM1 + q), c);
-  const double phi_d = ld(F(F_PHI), c), Kd = ld(F(F_K), c), alphad = ld(F(F_ALPHA), c);
-
-  double gi[6];
+  for (int q = 0; q < 6; ++q) g[q] = C(F_G11 + q);
   inv_metric(g, gi);
-  const double phi = phi_d + bg.phi_FRW;
+
+  // ---- phase 1: derivatives into shared memory ---------------------------------
+  const int x0 = blockIdx.z * kBX, y0 = blockIdx.y * kBY, z0 = blockIdx.x * kBZ;
+  const bool interior = x0 >= R && x0 + kBX + R <= geo.nx && y0 >= R && y0 + kBY + R <= geo.ny && z0 >= R &&
+                        z0 + kBZ + R <= geo.nz;
+  if (interior) {
+    const Taps<false> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
+    derivatives<O, MATTER>(t, a, P.fp_in, N, ph, gi, sl);
+  } else {
+    const Taps<true> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
+    derivatives<O, MATTER>(t, a, P.fp_in, N, ph, gi, sl);
+  }
+
+  // ---- phase 2: the algebra of set_bd_values (bssn.cc:361-421) ----------------
+  const double phi = C(F_PHI) + bg.phi_FRW;
+  const double Kd = C(F_K);
   const double K = Kd + bg.K_FRW;
+  const double alphad = C(F_ALPHA);
+  const double alpha = alphad + 1.0;
   double gm[6];
   gm[0] = g[0] + 1.0; gm[1] = g[1]; gm[2] = g[2];
   gm[3] = g[3] + 1.0; gm[4] = g[4]; gm[5] = g[5] + 1.0;
-  const double alpha = alphad + 1.0;
+  const double em4phi = exp(-4.0 * phi);
 
-  // ---- first derivatives -------------------------------------------------
-  double dphi[3], da[3], dK[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) dphi[d] = der1<O>(F(F_PHI), s, d, ph);
-#pragma unroll
-  for (int d = 0; d < 3; ++d) da[d] = der1<O>(F(F_ALPHA), s, d, ph);
-#pragma unroll
-  for (int d = 0; d < 3; ++d) dK[d] = der1<O>(F(F_K), s, d, ph);
-  double dg[3][6];  // d_I g_JK (calculate_dgamma, bssn.cc:480-483)
-#pragma unroll
-  for (int I = 0; I < 3; ++I)
-#pragma unroll
-    for (int q = 0; q < 6; ++q) dg[I][q] = der1<O>(F(F_G11 + q), s, I, ph);
-
-  // ---- matter: sources and RHS pieces that need only the centre ----------
-  double q[Q_N];
+  // -- sources and matter centre quantities --
   double rhs_m[5] = {0, 0, 0, 0, 0};
-  double mat_c[5] = {0, 0, 0, 0, 0};  // matter centre values (dust D,S or scalar fields)
   if (MATTER == kDust) {
-    const double D = ld(F(F_D), c);
-    const double S[3] = {ld(F(F_S1), c), ld(F(F_S2), c), ld(F(F_S3), c)};
-    mat_c[0] = D; mat_c[1] = S[0]; mat_c[2] = S[1]; mat_c[3] = S[2];
-    // lagged derived fields (populateDerivedFields of the previous substep)
-    double Wl, detgl, gphys[6];
+    const double D = C(F_D);
+    const double Sv[3] = {C(F_S1), C(F_S2), C(F_S3)};
+    double Wl, detgl, gph[6];
     if (stage == 1) {
-      const DustPrim dp = dust_prim(gi, phi, D, S);
+      // the stepInit populate used this same state (sims/dust.cc:56-62)
+      const DustPrim dp = dust_prim(gi, phi, D, Sv);
       Wl = dp.W;
-      const double e4phi = exp(4.0 * phi);
+      const double e4 = exp(4.0 * phi);
       detgl = exp(6.0 * phi);
 #pragma unroll
-      for (int m = 0; m < 6; ++m) gphys[m] = e4phi * gm[m];
+      for (int m = 0; m < 6; ++m) gph[m] = e4 * gm[m];
     } else {
       const double* pv = P.prev;
-      double gp[6];
+      double gp[6], gip[6];
 #pragma unroll
       for (int m = 0; m < 6; ++m) gp[m] = pv[(size_t)(F_G11 + m) * N + c];
       const double phip = pv[(size_t)F_PHI * N + c] + bg.phi_FRW_prev;
       const double Dp = pv[(size_t)F_D * N + c];
       const double Sp[3] = {pv[(size_t)F_S1 * N + c], pv[(size_t)F_S2 * N + c], pv[(size_t)F_S3 * N + c]};
-      double gip[6];
       inv_metric(gp, gip);
       const DustPrim dp = dust_prim(gip, phip, Dp, Sp);
       Wl = dp.W;
-      const double e4phi = exp(4.0 * phip);
+      const double e4 = exp(4.0 * phip);
       detgl = exp(6.0 * phip);
-      gphys[0] = e4phi * (gp[0] + 1.0); gphys[1] = e4phi * gp[1]; gphys[2] = e4phi * gp[2];
-      gphys[3] = e4phi * (gp[3] + 1.0); gphys[4] = e4phi * gp[4]; gphys[5] = e4phi * (gp[5] + 1.0);
+      gph[0] = e4 * (gp[0] + 1.0); gph[1] = e4 * gp[1]; gph[2] = e4 * gp[2];
+      gph[3] = e4 * (gp[3] + 1.0); gph[4] = e4 * gp[4]; gph[5] = e4 * (gp[5] + 1.0);
     }
-    dust_sources(Wl, detgl, gphys, D, S, ph.lambda, q);
-    // dust RHS: flux divergence (dust.cc:203-224) + momentum source (dust.cc:135-146)
-    const DustPrim cur = dust_prim(gi, phi, D, S);
-    const double* __restrict__ fp = P.fp_in;
-    auto FP = [&](int m) { return fp + (size_t)m * N; };
-    rhs_m[0] = der1_prod<O>(FP(P_AD), FP(P_V1), s, 0, ph) + der1_prod<O>(FP(P_AD), FP(P_V2), s, 1, ph) +
-               der1_prod<O>(FP(P_AD), FP(P_V3), s, 2, ph);
-    const double e4 = exp(4.0 * phi);
+    double q[Q_N];
+    dust_sources(Wl, detgl, gph, D, Sv, ph.lambda, q);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-      const int d = m;  // momentum component S_{m+1}: derivative index of the source
-      const double* dgd = dg[d];
+    for (int m = 0; m < Q_N; ++m) S(S_SRC + m) = q[m];
+    // momentum source S_m^src (dust.cc:135-146) with the current W, v
+    const DustPrim cur = dust_prim(gi, phi, D, Sv);
+    const double e4 = exp(4.0 * phi);
+    rhs_m[0] = S(S_MAT + 0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double dp = S(S_DPHI + d);
+      auto DG = [&](int qq) { return S(S_DG + 6 * d + qq); };
       const double src =
           1.0 / 2.0 * alpha * cur.W * D * e4 *
-              (cur.v[0] * cur.v[0] * (4.0 * gm[0] * dphi[d] + dgd[0]) + cur.v[1] * cur.v[1] * (4.0 * gm[3] * dphi[d] + dgd[3]) +
-               cur.v[2] * cur.v[2] * (4.0 * gm[5] * dphi[d] + dgd[5]) +
-               2.0 * (cur.v[0] * cur.v[1] * (4.0 * gm[1] * dphi[d] + dgd[1]) +
-                      cur.v[0] * cur.v[2] * (4.0 * gm[2] * dphi[d] + dgd[2]) +
-                      cur.v[1] * cur.v[2] * (4.0 * gm[4] * dphi[d] + dgd[4]))) -
-          cur.W * D * da[d];
-      rhs_m[1 + m] = der1_prod<O>(FP(P_AS1 + m), FP(P_V1), s, 0, ph) +
-                     der1_prod<O>(FP(P_AS1 + m), FP(P_V2), s, 1, ph) +
-                     der1_prod<O>(FP(P_AS1 + m), FP(P_V3), s, 2, ph) + src;
+              (cur.v[0] * cur.v[0] * (4.0 * gm[0] * dp + DG(0)) + cur.v[1] * cur.v[1] * (4.0 * gm[3] * dp + DG(3)) +
+               cur.v[2] * cur.v[2] * (4.0 * gm[5] * dp + DG(5)) +
+               2.0 * (cur.v[0] * cur.v[1] * (4.0 * gm[1] * dp + DG(1)) + cur.v[0] * cur.v[2] * (4.0 * gm[2] * dp + DG(2)) +
+                      cur.v[1] * cur.v[2] * (4.0 * gm[4] * dp + DG(4)))) -
+          cur.W * D * S(S_DA + d);
+      rhs_m[1 + d] = S(S_MAT + 1 + d) + src;
     }
   } else if (MATTER == kScalar) {
-    // Scalar::getScalarData (scalar.cc:97-130) and addBSSNSource (:201-260)
-    const double sphi = ld(F(F_SPHI), c), sPi = ld(F(F_SPI), c);
-    const double psi[3] = {ld(F(F_SPSI1), c), ld(F(F_SPSI1 + 1), c), ld(F(F_SPSI1 + 2), c)};
-    mat_c[0] = sphi; mat_c[1] = sPi; mat_c[2] = psi[0]; mat_c[3] = psi[1]; mat_c[4] = psi[2];
-    double sdphi[3], sdPi[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) sdphi[d] = der1<O>(F(F_SPHI), s, d, ph);
-#pragma unroll
-    for (int d = 0; d < 3; ++d) sdPi[d] = der1<O>(F(F_SPI), s, d, ph);
+    // Scalar::addBSSNSource (scalar.cc:201-260) and RKEvolvePt (:85-199)
+    const double sphi = C(F_SPHI), sPi = C(F_SPI);
+    const double psi[3] = {C(F_SPSI1), C(F_SPSI1 + 1), C(F_SPSI1 + 2)};
+    auto SD = [&](int m, int d) { return S(S_MAT + 3 * m + d); };  // d_d of scalar field m
     const double nmu = ((-alpha * sPi)) / alpha;
-    const double dd = (gi[0] * sdphi[0] * sdphi[0] + gi[3] * sdphi[1] * sdphi[1] + gi[5] * sdphi[2] * sdphi[2] +
-                       2.0 * (gi[1] * sdphi[0] * sdphi[1] + gi[2] * sdphi[0] * sdphi[2] + gi[4] * sdphi[1] * sdphi[2]));
+    const double dd = (gi[0] * SD(0, 0) * SD(0, 0) + gi[3] * SD(0, 1) * SD(0, 1) + gi[5] * SD(0, 2) * SD(0, 2) +
+                       2.0 * (gi[1] * SD(0, 0) * SD(0, 1) + gi[2] * SD(0, 0) * SD(0, 2) + gi[4] * SD(0, 1) * SD(0, 2)));
     const double V = pot_V(ph, sphi);
-    const double em4 = exp(-4.0 * phi);
-    q[Q_R] = 0.5 * nmu * nmu + 0.5 * em4 * dd + V;
-    q[Q_S] = 3.0 / 2.0 * nmu * nmu - 0.5 * em4 * dd - 3.0 * V;
+    S(S_SRC + Q_R) = 0.5 * nmu * nmu + 0.5 * em4phi * dd + V;
+    S(S_SRC + Q_S) = 3.0 / 2.0 * nmu * nmu - 0.5 * em4phi * dd - 3.0 * V;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) q[Q_S1 + m] = -nmu * sdphi[m];
+    for (int m = 0; m < 3; ++m) S(S_SRC + Q_S1 + m) = -nmu * SD(0, m);
 #pragma unroll
     for (int I = 0; I < 3; ++I)
 #pragma unroll
-      for (int J = I; J < 3; ++J) q[Q_STF11 + sym(I, J)] = sdphi[I] * sdphi[J] - gm[sym(I, J)] / 3.0 * dd;
-    // scalar RHS (scalar.cc:132-199)
+      for (int J = I; J < 3; ++J) S(S_SRC + Q_STF11 + sym(I, J)) = SD(0, I) * SD(0, J) - gm[sym(I, J)] / 3.0 * dd;
     double inner = 0.0;
 #pragma unroll
     for (int X = 0; X < 3; ++X)
 #pragma unroll
       for (int Y = 0; Y < 3; ++Y) {
-        const double u = gi[sym(X, Y)] * (alpha * der1<O>(F(F_SPSI1 + Y), s, X, ph) + psi[X] * da[Y]);
+        const double u = gi[sym(X, Y)] * (alpha * SD(2 + Y, X) + psi[X] * S(S_DA + Y));
         inner = (X == 0 && Y == 0) ? u : inner + u;
       }
     double gt[3];
 #pragma unroll
     for (int I = 0; I < 3; ++I)
-      gt[I] = (Gam[I] - 2.0 * (gi[sym(I, 0)] * dphi[0] + gi[sym(I, 1)] * dphi[1] + gi[sym(I, 2)] * dphi[2]));
+      gt[I] = (C(F_GAM1 + I) - 2.0 * (gi[sym(I, 0)] * S(S_DPHI + 0) + gi[sym(I, 1)] * S(S_DPHI + 1) +
+                                      gi[sym(I, 2)] * S(S_DPHI + 2)));
     rhs_m[0] = (-alpha * sPi);
-    rhs_m[1] = (-exp(-4.0 * phi) * (inner) +
-                alpha * ((gt[0]) * psi[0] * exp(-4.0 * phi) + (gt[1]) * psi[1] * exp(-4.0 * phi) +
-                         (gt[2]) * psi[2] * exp(-4.0 * phi) + K * sPi + pot_dV(ph, sphi)));
+    rhs_m[1] = (-em4phi * (inner) +
+                alpha * ((gt[0]) * psi[0] * em4phi + (gt[1]) * psi[1] * em4phi + (gt[2]) * psi[2] * em4phi + K * sPi +
+                         pot_dV(ph, sphi)));
 #pragma unroll
-    for (int m = 0; m < 3; ++m) rhs_m[2 + m] = (-alpha * sdPi[m] - sPi * da[m]);
+    for (int m = 0; m < 3; ++m) rhs_m[2 + m] = (-alpha * SD(1, m) - sPi * S(S_DA + m));
   } else {
 #pragma unroll
-    for (int m = 0; m < Q_N; ++m) q[m] = 0.0;
+    for (int m = 0; m < Q_N; ++m) S(S_SRC + m) = 0.0;
   }
-  const double r = q[Q_R] + bg.rho_FRW;
 
-  // ---- A^ij, A_ij A^ij (calculate_Acont, bssn.cc:463-472) ------------------
-  double Ac[6];
+  // -- Christoffels (bssn.cc:577-590, bssn_macros.h:221-229) --
+  // Gamma^I_q go to their own slots; the lowered Gamma_{I q} then replace
+  // d_I g_q, which nothing reads afterwards.
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = 0; J < 3; ++J)
+#pragma unroll
+      for (int Kx = J; Kx < 3; ++Kx) {
+        auto dg = [&](int d, int qq) { return S(S_DG + 6 * d + qq); };
+        double u = gi[sym(I, 0)] * (dg(J, sym(Kx, 0)) + dg(Kx, sym(J, 0)) - dg(0, sym(J, Kx)));
+        u = u + gi[sym(I, 1)] * (dg(J, sym(Kx, 1)) + dg(Kx, sym(J, 1)) - dg(1, sym(J, Kx)));
+        u = u + gi[sym(I, 2)] * (dg(J, sym(Kx, 2)) + dg(Kx, sym(J, 2)) - dg(2, sym(J, Kx)));
+        S(S_G + 6 * I + sym(J, Kx)) = 0.5 * (u);
+      }
+  {
+    double GLv[3][6];
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int J = 0; J < 3; ++J)
+#pragma unroll
+        for (int Kx = J; Kx < 3; ++Kx) {
+          auto dg = [&](int d, int qq) { return S(S_DG + 6 * d + qq); };
+          GLv[I][sym(J, Kx)] = 0.5 * (dg(J, sym(Kx, I)) + dg(Kx, sym(J, I)) - dg(I, sym(J, Kx)));
+        }
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int qq = 0; qq < 6; ++qq) S(S_DG + 6 * I + qq) = GLv[I][qq];
+  }
+  auto G = [&](int I, int qq) { return S(S_G + 6 * I + qq); };
+  auto GL = [&](int I, int qq) { return S(S_DG + 6 * I + qq); };
+  double Gd[3];
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+    Gd[I] = G(I, 0) * gi[0] + G(I, 3) * gi[3] + G(I, 5) * gi[5] + 2.0 * (G(I, 1) * gi[1] + G(I, 2) * gi[2] + G(I, 4) * gi[4]);
+
+  // -- D_i D_j phi (bssn.cc:592-602) and (D_i D_j alpha)^TF (:604-626) --
+  double dphi[3], da[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) { dphi[d] = S(S_DPHI + d); da[d] = S(S_DA + d); }
+  double DDa[6];
+  double gld[3];
+#pragma unroll
+  for (int I = 0; I < 3; ++I) gld[I] = gi[sym(I, 0)] * dphi[0] + gi[sym(I, 1)] * dphi[1] + gi[sym(I, 2)] * dphi[2];
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = I; J < 3; ++J) {
+      const int qq = sym(I, J);
+      S(S_DDPHI + qq) = S(S_DDPHI + qq) - (G(0, qq) * dphi[0] + G(1, qq) * dphi[1] + G(2, qq) * dphi[2]);
+      double t = 0.0;
+#pragma unroll
+      for (int L = 0; L < 3; ++L) {
+        const double u = G(L, qq) + 2.0 * ((L == I ? 1.0 : 0.0) * dphi[J] + (L == J ? 1.0 : 0.0) * dphi[I] - gm[qq] * gld[L]);
+        t = L == 0 ? u * da[L] : t + u * da[L];
+      }
+      DDa[qq] = S(S_DDA + qq) - (t);
+    }
+  double DDaTR = gi[0] * DDa[0] + gi[3] * DDa[3] + gi[5] * DDa[5] + 2.0 * (gi[1] * DDa[1] + gi[2] * DDa[2] + gi[4] * DDa[4]);
+#pragma unroll
+  for (int m = 0; m < 6; ++m) S(S_DDA + m) = DDa[m] - (1.0 / 3.0) * gm[m] * DDaTR;
+  DDaTR *= em4phi;
+
+  // -- Ricci (bssn.cc:629-674, bssn_macros.h:248-277) --
+  auto DDphi = [&](int qq) { return S(S_DDPHI + qq); };
+  const double expression =
+      (gi[0] * (DDphi(0) + 2.0 * dphi[0] * dphi[0]) + gi[3] * (DDphi(3) + 2.0 * dphi[1] * dphi[1]) +
+       gi[5] * (DDphi(5) + 2.0 * dphi[2] * dphi[2]) +
+       2.0 * (gi[1] * (DDphi(1) + 2.0 * dphi[0] * dphi[1]) + gi[2] * (DDphi(2) + 2.0 * dphi[0] * dphi[2]) +
+              gi[4] * (DDphi(4) + 2.0 * dphi[1] * dphi[2])));
+  // BSSN_CALCULATE_RICCI_UNITARY_TERM4 summed over (K,L,M) in the reference's
+  // order, all six components at once so each Gamma is read once per term
+  double t4[6];
+#pragma unroll
+  for (int Kx = 0; Kx < 3; ++Kx)
+#pragma unroll
+    for (int L = 0; L < 3; ++L)
+#pragma unroll
+      for (int M = 0; M < 3; ++M) {
+        const double gLM = gi[sym(L, M)];
+        double GKL[3], GLKM[3], GKM[3], GLKL[3];
+#pragma unroll
+        for (int X = 0; X < 3; ++X) {
+          GKL[X] = G(Kx, sym(L, X));
+          GLKM[X] = GL(X, sym(Kx, M));
+          GKM[X] = G(Kx, sym(X, M));
+          GLKL[X] = GL(Kx, sym(L, X));
+        }
+#pragma unroll
+        for (int I = 0; I < 3; ++I)
+#pragma unroll
+          for (int J = I; J < 3; ++J) {
+            const double u = gLM * (GKL[I] * GLKM[J] + GKL[J] * GLKM[I] + 0.5 * (GKM[I] * GLKL[J] + GKM[J] * GLKL[I]));
+            t4[sym(I, J)] = (Kx == 0 && L == 0 && M == 0) ? u : t4[sym(I, J)] + u;
+          }
+      }
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = I; J < 3; ++J) {
+      const int ij = sym(I, J);
+      auto dGam = [&](int Jx, int Kx) { return S(S_DGAM + 3 * Kx + Jx); };
+      const double t2a = gm[sym(0, I)] * dGam(J, 0) + gm[sym(1, I)] * dGam(J, 1) + gm[sym(2, I)] * dGam(J, 2);
+      const double t2b = gm[sym(0, J)] * dGam(I, 0) + gm[sym(1, J)] * dGam(I, 1) + gm[sym(2, J)] * dGam(I, 2);
+      const double t3a = Gd[0] * GL(I, sym(J, 0)) + Gd[1] * GL(I, sym(J, 1)) + Gd[2] * GL(I, sym(J, 2));
+      const double t3b = Gd[0] * GL(J, sym(I, 0)) + Gd[1] * GL(J, sym(I, 1)) + Gd[2] * GL(J, sym(I, 2));
+      const double U = (-0.5 * (S(S_T1 + ij)) + 0.5 * (t2a + t2b) + 0.5 * (t3a + t3b) + t4[ij]);
+      S(S_T1 + ij) = U - 2.0 * (DDphi(ij) - 2.0 * dphi[I] * dphi[J] + gm[ij] * (expression));
+    }
+  auto Ric = [&](int qq) { return S(S_T1 + qq); };  // full Ricci R_ij (bssn.cc:650-655)
+  const double ricci = em4phi * (Ric(0) * gi[0] + Ric(3) * gi[3] + Ric(5) * gi[5] +
+                                 2.0 * (Ric(1) * gi[1] + Ric(2) * gi[2] + Ric(4) * gi[4]));
+  const double e4phi = exp(4.0 * phi);
+
+  // -- A^ij, A_ij A^ij (calculate_Acont, bssn.cc:463-472) --
+  double A[6], Ac[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) A[q] = C(F_A11 + q);
 #pragma unroll
   for (int I = 0; I < 3; ++I)
 #pragma unroll
@@ -251,109 +541,43 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
       Ac[sym(I, J)] = t;
     }
   const double AijAij = Ac[0] * A[0] + Ac[3] * A[3] + Ac[5] * A[5] + 2.0 * (Ac[1] * A[1] + Ac[2] * A[2] + Ac[4] * A[4]);
-
-  // ---- Christoffels (bssn.cc:577-590, bssn_macros.h:221-229) ---------------
-  double G[3][6], GL[3][6], Gd[3];
-#pragma unroll
-  for (int I = 0; I < 3; ++I)
-#pragma unroll
-    for (int J = 0; J < 3; ++J)
-#pragma unroll
-      for (int Kx = J; Kx < 3; ++Kx) {
-        double t = gi[sym(I, 0)] * (dg[J][sym(Kx, 0)] + dg[Kx][sym(J, 0)] - dg[0][sym(J, Kx)]);
-        t = t + gi[sym(I, 1)] * (dg[J][sym(Kx, 1)] + dg[Kx][sym(J, 1)] - dg[1][sym(J, Kx)]);
-        t = t + gi[sym(I, 2)] * (dg[J][sym(Kx, 2)] + dg[Kx][sym(J, 2)] - dg[2][sym(J, Kx)]);
-        G[I][sym(J, Kx)] = 0.5 * (t);
-        GL[I][sym(J, Kx)] = 0.5 * (dg[J][sym(Kx, I)] + dg[Kx][sym(J, I)] - dg[I][sym(J, Kx)]);
-      }
-#pragma unroll
-  for (int I = 0; I < 3; ++I)
-    Gd[I] = G[I][0] * gi[0] + G[I][3] * gi[3] + G[I][5] * gi[5] + 2.0 * (G[I][1] * gi[1] + G[I][2] * gi[2] + G[I][4] * gi[4]);
-
-  // ---- D_i D_j phi (bssn.cc:592-602) and (D_i D_j alpha)^TF (:604-626) -----
-  double DDphi[6], DDa[6];
-  double gld[3];
-#pragma unroll
-  for (int I = 0; I < 3; ++I) gld[I] = gi[sym(I, 0)] * dphi[0] + gi[sym(I, 1)] * dphi[1] + gi[sym(I, 2)] * dphi[2];
-#pragma unroll
-  for (int I = 0; I < 3; ++I)
-#pragma unroll
-    for (int J = I; J < 3; ++J) {
-      const int qq = sym(I, J);
-      DDphi[qq] = der2ab<O>(F(F_PHI), s, I, J, ph) - (G[0][qq] * dphi[0] + G[1][qq] * dphi[1] + G[2][qq] * dphi[2]);
-      double t = 0.0;
-#pragma unroll
-      for (int L = 0; L < 3; ++L) {
-        const double u = G[L][qq] + 2.0 * ((L == I ? 1.0 : 0.0) * dphi[J] + (L == J ? 1.0 : 0.0) * dphi[I] - gm[qq] * gld[L]);
-        t = L == 0 ? u * da[L] : t + u * da[L];
-      }
-      DDa[qq] = der2ab<O>(F(F_ALPHA), s, I, J, ph) - (t);
-    }
-  double DDaTR = gi[0] * DDa[0] + gi[3] * DDa[3] + gi[5] * DDa[5] + 2.0 * (gi[1] * DDa[1] + gi[2] * DDa[2] + gi[4] * DDa[4]);
-#pragma unroll
-  for (int m = 0; m < 6; ++m) DDa[m] -= (1.0 / 3.0) * gm[m] * DDaTR;
-  DDaTR *= exp(-4.0 * phi);
-
-  // ---- Ricci (bssn.cc:629-674, bssn_macros.h:248-277) ------------------------
-  double dGam[3][3];  // d_J Gamma^K
-#pragma unroll
-  for (int Kx = 0; Kx < 3; ++Kx)
-#pragma unroll
-    for (int J = 0; J < 3; ++J) dGam[J][Kx] = der1<O>(F(F_GAM1 + Kx), s, J, ph);
-  double Ric[6];
-  const double expression =
-      (gi[0] * (DDphi[0] + 2.0 * dphi[0] * dphi[0]) + gi[3] * (DDphi[3] + 2.0 * dphi[1] * dphi[1]) +
-       gi[5] * (DDphi[5] + 2.0 * dphi[2] * dphi[2]) +
-       2.0 * (gi[1] * (DDphi[1] + 2.0 * dphi[0] * dphi[1]) + gi[2] * (DDphi[2] + 2.0 * dphi[0] * dphi[2]) +
-              gi[4] * (DDphi[4] + 2.0 * dphi[1] * dphi[2])));
-#pragma unroll
-  for (int I = 0; I < 3; ++I)
-#pragma unroll
-    for (int J = I; J < 3; ++J) {
-      const int ij = sym(I, J);
-      const double* fg = F(F_G11 + ij);
-      double ddg[6];  // d_K d_L g_IJ (calculate_ddgamma, bssn.cc:491-494)
-#pragma unroll
-      for (int Kx = 0; Kx < 3; ++Kx)
-#pragma unroll
-        for (int L = Kx; L < 3; ++L) ddg[sym(Kx, L)] = der2ab<O>(fg, s, Kx, L, ph);
-      double t1 = 0.0;
-#pragma unroll
-      for (int Kx = 0; Kx < 3; ++Kx)
-#pragma unroll
-        for (int L = 0; L < 3; ++L) {
-          const double u = gi[sym(Kx, L)] * ddg[sym(Kx, L)];
-          t1 = (Kx == 0 && L == 0) ? u : t1 + u;
-        }
-      const double t2a = gm[sym(0, I)] * dGam[J][0] + gm[sym(1, I)] * dGam[J][1] + gm[sym(2, I)] * dGam[J][2];
-      const double t2b = gm[sym(0, J)] * dGam[I][0] + gm[sym(1, J)] * dGam[I][1] + gm[sym(2, J)] * dGam[I][2];
-      const double t3a = Gd[0] * GL[I][sym(J, 0)] + Gd[1] * GL[I][sym(J, 1)] + Gd[2] * GL[I][sym(J, 2)];
-      const double t3b = Gd[0] * GL[J][sym(I, 0)] + Gd[1] * GL[J][sym(I, 1)] + Gd[2] * GL[J][sym(I, 2)];
-      double t4 = 0.0;
-#pragma unroll
-      for (int Kx = 0; Kx < 3; ++Kx)
-#pragma unroll
-        for (int L = 0; L < 3; ++L)
-#pragma unroll
-          for (int M = 0; M < 3; ++M) {
-            const double u = gi[sym(L, M)] * (G[Kx][sym(L, I)] * GL[J][sym(Kx, M)] + G[Kx][sym(L, J)] * GL[I][sym(Kx, M)] +
-                                              0.5 * (G[Kx][sym(I, M)] * GL[Kx][sym(L, J)] + G[Kx][sym(J, M)] * GL[Kx][sym(L, I)]));
-            t4 = (Kx == 0 && L == 0 && M == 0) ? u : t4 + u;
-          }
-      const double U = (-0.5 * (t1) + 0.5 * (t2a + t2b) + 0.5 * (t3a + t3b) + t4);
-      Ric[ij] = U - 2.0 * (DDphi[ij] - 2.0 * dphi[I] * dphi[J] + gm[ij] * (expression));
-    }
-  const double ricci = exp(-4.0 * phi) * (Ric[0] * gi[0] + Ric[3] * gi[3] + Ric[5] * gi[5] +
-                                         2.0 * (Ric[1] * gi[1] + Ric[2] * gi[2] + Ric[4] * gi[4]));
-  const double e4phi = exp(4.0 * phi);
+  const double r = S(S_SRC + Q_R) + bg.rho_FRW;
   // Hamiltonian constraint, bssn.cc:1073-1084 (theta = 0)
   const double H = -exp(5.0 * phi) / 8.0 * (ricci + 2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0)) - AijAij - 16.0 * kPi * r);
 
-  // ---- evolution equations (bssn.cc:748-831, bssn_macros.h:292-385) --------
-  double rhs[NFLD];
+  // ---- evolution equations and K{n}Finalize, field by field --------------------
   const double dt = ph.dt;
+  double outv[NFLD];
+  const bool renorm = ph.normalize != 0;
+  auto finalize = [&](int fld, double cv) {
+    const double pv = P.p[(size_t)fld * N + c];
+    double o;
+    if (stage == 1) {
+      P.f[(size_t)fld * N + c] = dt * cv / 6.0;
+      o = pv + dt * cv / 2.0;
+    } else if (stage == 2) {
+      const double fv = P.f[(size_t)fld * N + c];
+      P.f[(size_t)fld * N + c] = fv + dt * cv / 3.0;
+      o = pv + dt * cv / 2.0;
+    } else if (stage == 3) {
+      const double fv = P.f[(size_t)fld * N + c];
+      P.f[(size_t)fld * N + c] = fv + dt * cv / 3.0;
+      o = pv + dt * cv;
+    } else {
+      const double fv = P.f[(size_t)fld * N + c];
+      o = fv + (dt * cv / 6.0 + pv);
+    }
+    P.out[(size_t)fld * N + c] = o;
+    outv[fld] = o;
+    // at the last substep the new state is also the next step's first input,
+    // except gamma and A, which are renormalised below
+    if (stage == 4 && !(renorm && fld < F_K && fld != F_PHI)) P.norm[(size_t)fld * N + c] = o;
+  };
+
+  // ev_DIFFgammaIJ (bssn.cc:748-753)
 #pragma unroll
-  for (int m = 0; m < 6; ++m) rhs[F_G11 + m] = (-2.0 * alpha * A[m]) + 0.5 * ph.a_adj_amp * dt * H * g[m];
+  for (int m = 0; m < 6; ++m) finalize(F_G11 + m, (-2.0 * alpha * A[m]) + 0.5 * ph.a_adj_amp * dt * H * g[m]);
+  // ev_AIJ (bssn.cc:755-760, BSSN_DT_AIJ bssn_macros.h:334-337)
 #pragma unroll
   for (int I = 0; I < 3; ++I)
 #pragma unroll
@@ -367,83 +591,71 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
           const double u = gi[sym(X, Y)] * A[sym(X, I)] * A[sym(Y, J)];
           aa = (X == 0 && Y == 0) ? u : aa + u;
         }
-      const double RTF = Ric[qq] - (1.0 / 3.0) * e4phi * gm[qq] * ricci;
-      const double dtA = (exp(-4.0 * phi) * (alpha * (RTF - 8.0 * kPi * q[Q_STF11 + qq]) - DDa[qq]) +
+      const double RTF = Ric(qq) - (1.0 / 3.0) * e4phi * gm[qq] * ricci;
+      const double dtA = (em4phi * (alpha * (RTF - 8.0 * kPi * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
                           alpha * (((K + 2.0 * 0.0) * A[qq]) - 2.0 * (aa)));
-      rhs[F_A11 + qq] = dtA - 1.0 * ph.a_adj_amp * dt * A[qq] * H;
+      finalize(F_A11 + qq, dtA - 1.0 * ph.a_adj_amp * dt * A[qq] * H);
     }
+  // ev_GammaI (bssn.cc:762-764, BSSN_DT_GAMMAI_NOSHIFT bssn_macros.h:342-361)
+  const double sq[3] = {S(S_SRC + Q_S1), S(S_SRC + Q_S2), S(S_SRC + Q_S3)};
 #pragma unroll
   for (int I = 0; I < 3; ++I) {
-    const double so = (G[I][0] * Ac[0] + G[I][3] * Ac[3] + G[I][5] * Ac[5] + 2.0 * (G[I][1] * Ac[1] + G[I][2] * Ac[2] + G[I][4] * Ac[4]) +
+    auto Gs = [&](int qq) { return S(S_G + 6 * I + qq); };
+    const double so = (Gs(0) * Ac[0] + Gs(3) * Ac[3] + Gs(5) * Ac[5] + 2.0 * (Gs(1) * Ac[1] + Gs(2) * Ac[2] + Gs(4) * Ac[4]) +
                        6.0 * (Ac[sym(I, 0)] * dphi[0] + Ac[sym(I, 1)] * dphi[1] + Ac[sym(I, 2)] * dphi[2]));
     const double ns =
         (-2.0 * (Ac[sym(I, 0)] * da[0] + Ac[sym(I, 1)] * da[1] + Ac[sym(I, 2)] * da[2]) +
          2.0 * alpha *
              (+so -
-              (1.0 / 3.0) * (2.0 * (gi[sym(I, 0)] * dK[0] + gi[sym(I, 1)] * dK[1] + gi[sym(I, 2)] * dK[2]) +
+              (1.0 / 3.0) * (2.0 * (gi[sym(I, 0)] * S(S_DK + 0) + gi[sym(I, 1)] * S(S_DK + 1) + gi[sym(I, 2)] * S(S_DK + 2)) +
                              gi[sym(I, 0)] * 0.0 + gi[sym(I, 1)] * 0.0 + gi[sym(I, 2)] * 0.0) -
-              2.0 * alpha * 0.0 * (Gam[I] - Gd[I]) -
-              8.0 * kPi * (gi[sym(I, 0)] * q[Q_S1] + gi[sym(I, 1)] * q[Q_S2] + gi[sym(I, 2)] * q[Q_S3])));
-    rhs[F_GAM1 + I] = ns + 0.0;
+              2.0 * alpha * 0.0 * (C(F_GAM1 + I) - Gd[I]) -
+              8.0 * kPi * (gi[sym(I, 0)] * sq[0] + gi[sym(I, 1)] * sq[1] + gi[sym(I, 2)] * sq[2])));
+    finalize(F_GAM1 + I, ns + 0.0);
   }
-  rhs[F_K] = (-DDaTR + alpha * (1.0 / 3.0 * (Kd + 2.0 * 0.0) * (Kd + 2.0 * 0.0 + 2.0 * bg.K_FRW) + AijAij) +
-              4.0 * kPi * alpha * (q[Q_R] + q[Q_S]) + 4.0 * kPi * alphad * (bg.rho_FRW + bg.S_FRW) -
-              1.0 * ph.k_damping_amp * H * exp(-5.0 * phi));
-  rhs[F_PHI] = (0.1 * ph.a_adj_amp * dt * H - 1.0 / 6.0 * (alpha * (Kd + 2.0 * 0.0) + alphad * bg.K_FRW - (0.0 + 0.0 + 0.0)));
-  rhs[F_ALPHA] = ev_lapse(ph, bg, alpha, K, Kd, phi);
+  // ev_DIFFK (bssn.cc:766-795)
+  {
+    double v = (-DDaTR + alpha * (1.0 / 3.0 * (Kd + 2.0 * 0.0) * (Kd + 2.0 * 0.0 + 2.0 * bg.K_FRW) + AijAij) +
+                4.0 * kPi * alpha * (S(S_SRC + Q_R) + S(S_SRC + Q_S)) + 4.0 * kPi * alphad * (bg.rho_FRW + bg.S_FRW));
+    if (ph.k_damping_amp != 0.0) v = v - 1.0 * ph.k_damping_amp * H * exp(-5.0 * phi);
+    finalize(F_K, v);
+  }
+  // ev_DIFFphi (bssn.cc:797-820)
+  finalize(F_PHI, (0.1 * ph.a_adj_amp * dt * H - 1.0 / 6.0 * (alpha * (Kd + 2.0 * 0.0) + alphad * bg.K_FRW - (0.0 + 0.0 + 0.0))));
+  // ev_DIFFalpha (bssn.cc:822-831)
+  finalize(F_ALPHA, ev_lapse(ph, bg, alpha, K, Kd, phi));
   if (MATTER == kDust) {
 #pragma unroll
-    for (int m = 0; m < 4; ++m) rhs[F_D + m] = rhs_m[m];
+    for (int m = 0; m < 4; ++m) finalize(F_D + m, rhs_m[m]);
   } else if (MATTER == kScalar) {
 #pragma unroll
-    for (int m = 0; m < 5; ++m) rhs[F_SPHI + m] = rhs_m[m];
+    for (int m = 0; m < 5; ++m) finalize(F_SPHI + m, rhs_m[m]);
   }
 
-  // ---- RK4Register::K{n}Finalize (RK4Register.h:175-222) --------------------
-  double outv[NFLD];
-#pragma unroll
-  for (int f = 0; f < NFLD; ++f) {
-    const double pv = P.p[(size_t)f * N + c];
-    const double cv = rhs[f];
-    if (stage == 1) {
-      P.f[(size_t)f * N + c] = dt * cv / 6.0;
-      outv[f] = pv + dt * cv / 2.0;
-    } else if (stage == 2) {
-      const double fv = P.f[(size_t)f * N + c];
-      P.f[(size_t)f * N + c] = fv + dt * cv / 3.0;
-      outv[f] = pv + dt * cv / 2.0;
-    } else if (stage == 3) {
-      const double fv = P.f[(size_t)f * N + c];
-      P.f[(size_t)f * N + c] = fv + dt * cv / 3.0;
-      outv[f] = pv + dt * cv;
-    } else {
-      const double fv = P.f[(size_t)f * N + c];
-      outv[f] = fv + (dt * cv / 6.0 + pv);
-    }
-    P.out[(size_t)f * N + c] = outv[f];
-  }
-  (void)mat_c;
-
-  // ---- the next substep's inputs ---------------------------------------------
+  // ---- the next substep's inputs -----------------------------------------------
   if (stage == 4) {
     // failure detection (sims/sim.cc:179-183 counts NaNs of DIFFphi)
-    bool bad_phi = isnan(outv[F_PHI]);
     bool bad_any = false;
 #pragma unroll
     for (int f = 0; f < NFLD; ++f) bad_any |= !isfinite(outv[f]);
-    if (bad_phi) atomicOr(P.status, kStatusNaN);
-    if (bad_any) atomicOr(P.status, kStatusNonFinite);
+    if (bad_any) {
+      if (isnan(outv[F_PHI])) atomicOr(P.status, kStatusNaN);
+      atomicOr(P.status, kStatusNonFinite);
+    }
     // next step's first-substep input: normalised gamma/A (bssn.cc:224-225)
-    if (ph.normalize) {
+    if (renorm) {
       double gn[6], An[6];
 #pragma unroll
       for (int m = 0; m < 6; ++m) { gn[m] = outv[F_G11 + m]; An[m] = outv[F_A11 + m]; }
       normalize_point(gn, An);
 #pragma unroll
-      for (int m = 0; m < 6; ++m) { outv[F_G11 + m] = gn[m]; outv[F_A11 + m] = An[m]; }
+      for (int m = 0; m < 6; ++m) {
+        outv[F_G11 + m] = gn[m];
+        outv[F_A11 + m] = An[m];
+        P.norm[(size_t)(F_G11 + m) * N + c] = gn[m];
+        P.norm[(size_t)(F_A11 + m) * N + c] = An[m];
+      }
     }
-#pragma unroll
-    for (int f = 0; f < NFLD; ++f) P.norm[(size_t)f * N + c] = outv[f];
   }
   if (MATTER == kDust) {
     // flux primitives of the output state for the next substep's divergence
@@ -452,8 +664,7 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
     for (int m = 0; m < 6; ++m) go[m] = outv[F_G11 + m];
     inv_metric(go, gio);
     const double So[3] = {outv[F_S1], outv[F_S2], outv[F_S3]};
-    const double phio = outv[F_PHI] + bg.phi_FRW_next;
-    const DustPrim dp = dust_prim(gio, phio, outv[F_D], So);
+    const DustPrim dp = dust_prim(gio, outv[F_PHI] + bg.phi_FRW_next, outv[F_D], So);
     const double alo = outv[F_ALPHA] + 1.0;
     double* fo = P.fp_out;
     fo[(size_t)P_AD * N + c] = alo * outv[F_D];

@@ -61,6 +61,10 @@ dim3 block_dims() { return dim3(32, 4, 1); }
 dim3 grid_dims(const BoxDev& b) {
   return dim3((b.nz + 31) / 32, (b.ny + 3) / 4, b.nx);
 }
+dim3 stage_block() { return dim3(kBZ, kBY, kBX); }
+dim3 stage_grid(const BoxDev& b) {
+  return dim3((b.nz + kBZ - 1) / kBZ, (b.ny + kBY - 1) / kBY, (b.nx + kBX - 1) / kBX);
+}
 
 template <int O, int M>
 cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
@@ -76,7 +80,14 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
     default: P.in = b.Y; P.prev = b.X; P.out = b.P; P.norm = b.X; P.fp_in = b.FP1; P.fp_out = b.FP0; break;
   }
   BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
-  stage_kernel<O, M><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, P, stage);
+  constexpr size_t smem = sizeof(double) * Slots<M>::value * kThreads;
+  static bool configured = false;  // per instantiation
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  stage_kernel<O, M><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage);
   return cudaGetLastError();
 }
 

@@ -26,12 +26,19 @@ def cfg_from(meta, precision="fp64"):
     return BoxConfig(order=meta["order"], precision=precision, **c)
 
 
+def floor_for(name: str) -> float:
+    """Components that vanish in exact arithmetic (off-diagonal metric, Gamma^2,3,
+    S_2,3 of a one-dimensional sinusoid) hold only roundoff noise; they are
+    measured against the perturbation amplitude (1e-3), not against their noise."""
+    return 1e-3 if name.startswith("sinusoid") else 1e-18
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp64_fma"])
 @pytest.mark.parametrize("name", GOLDEN_EVOLVE)
 def test_golden_evolve(name, precision):
     inp, out, _, meta = load_golden(name)
     got = evolve(inp, meta["steps"], cfg_from(meta, precision))
-    errs = field_errors(got.fields, out.fields, inp.names, floor=1e-18)
+    errs = field_errors(got.fields, out.fields, inp.names, floor=floor_for(name))
     assert worst(errs)[1] <= TOL[precision], worst(errs)
     assert got.step == meta["steps"]
 
@@ -78,7 +85,7 @@ def test_sinusoid_100_steps():
     st = ics.sinusoid_dust(32)
     ref = oracle.evolve(st, 100, 4, lapse="Harmonic")
     got = evolve(st, 100, BoxConfig(order=4, lapse="Harmonic"))
-    errs = field_errors(got.fields, ref.fields, st.names, floor=1e-12 * 1e-3)
+    errs = field_errors(got.fields, ref.fields, st.names, floor=floor_for("sinusoid"))
     assert worst(errs)[1] <= TOL["fp64"], worst(errs)
 
 
