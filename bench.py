@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference CPU build (rank 0)")
     ap.add_argument("--ncu", action="store_true", help="short run for profiler capture (no JSON extras)")
+    ap.add_argument("--variants", default="fp64_fma", help="comma list of extra precisions timed alongside")
     return ap.parse_args()
 
 
@@ -274,6 +275,27 @@ def main():
         ev.close()
         return
 
+    # the other arithmetic variants of the same kernel, same workload
+    variants = {}
+    for prec in [v for v in a.variants.split(",") if v and v != a.precision]:
+        ev_v = Evolution(st, BoxConfig(order=a.order, lapse="Harmonic", precision=prec))
+        ev_v.set_stream(stream.cuda_stream)
+        for _ in range(max(a.warmup, 0)):
+            ev_v.step(1)
+        ev_v.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        v0.record(stream)
+        for _ in range(a.steps):
+            ev_v.step(1)
+        v1.record(stream)
+        torch.cuda.synchronize()
+        ev_v.synchronize()
+        vms = max_over_ranks(v0.elapsed_time(v1))
+        variants[prec] = {"value": world * pts * a.steps / (vms / 1e3), "ms_per_step": vms / a.steps}
+        ev_v.close()
+
     # end to end through the C ABI: pinned host state in, one RK4 step, state out
     state_bytes = st.fields.nbytes
     h_in = torch.from_numpy(st.fields.reshape(-1)).pin_memory()
@@ -347,6 +369,7 @@ def main():
                     "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                     "steps": a.e2e_steps, "wall_s": e2e_wall},
             "gpu_launches": launches_per_step * a.steps,
+            "variants": variants,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
