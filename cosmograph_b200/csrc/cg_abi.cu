@@ -2,6 +2,8 @@
 // storage, the host-side FRW background and the substep sequencing.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -90,6 +92,8 @@ struct cg_ctx {
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   unsigned* status = nullptr;
+  double* red = nullptr;   // reduction scratch for cg_conformal_average
+  int red_blocks = 0;
   std::string err;
 };
 
@@ -167,6 +171,21 @@ __global__ void kavg_final_kernel(const double* partial, int nblk, int pts, doub
     out[0] = sK[0] / pts / vol;
   }
 }
+
+}  // namespace
+
+namespace cg {
+// Conformal average of `field` weighted by exp(6 (phi + phi_FRW)) into
+// out[0] on the device, using `partial` (2*nblk doubles) as scratch.
+cudaError_t launch_conformal_average(const double* field, const double* phi, int n, double phi_frw,
+                                     double* partial, int nblk, double* out, cudaStream_t st) {
+  kavg_partial_kernel<<<nblk, 256, 0, st>>>(field, phi, n, phi_frw, partial);
+  kavg_final_kernel<<<1, 256, 0, st>>>(partial, nblk, n, out);
+  return cudaGetLastError();
+}
+}  // namespace cg
+
+namespace {
 
 // the register block holding the current substep input
 double* current_a(Box& b) {
@@ -398,6 +417,7 @@ int cg_destroy(cg_ctx* ctx) {
   if (!ctx) return CG_ERR_INVALID;
   cudaStreamSynchronize(ctx->stream);
   for (Box& b : ctx->boxes) free_box(b);
+  cudaFree(ctx->red);
   cudaFree(ctx->status);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
@@ -577,6 +597,26 @@ int cg_step_count(cg_ctx* ctx, int box, int64_t* steps) {
   if (rc) return rc;
   if (!steps) return fail(ctx, CG_ERR_INVALID, "steps is null");
   *steps = ctx->boxes[box].steps;
+  return CG_OK;
+}
+
+int cg_conformal_average(cg_ctx* ctx, const double* d_field, const double* d_phi, size_t n, double phi_frw,
+                         double* out) {
+  if (!ctx) return CG_ERR_INVALID;
+  if (!d_field || !d_phi || !out) return fail(ctx, CG_ERR_INVALID, "null pointer");
+  if (n == 0 || n > (size_t)INT32_MAX) return fail(ctx, CG_ERR_INVALID, "n must be in 1..2^31-1");
+  const int nblk = (int)std::min<size_t>(1024, (n + 255) / 256);
+  if (ctx->red_blocks < nblk) {
+    cudaFree(ctx->red);
+    ctx->red = nullptr;
+    ctx->red_blocks = 0;
+    CG_CUDA(ctx, cudaMalloc(&ctx->red, sizeof(double) * (2 * 1024 + 1)));
+    ctx->red_blocks = 1024;
+  }
+  double* res = ctx->red + 2 * 1024;
+  CG_CUDA(ctx, cg::launch_conformal_average(d_field, d_phi, (int)n, phi_frw, ctx->red, nblk, res, ctx->stream));
+  CG_CUDA(ctx, cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return CG_OK;
 }
 

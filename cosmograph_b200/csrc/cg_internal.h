@@ -36,6 +36,12 @@ cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStre
 cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
 }  // namespace fast
 
+// Volume-weighted average (utils/math.h:1403-1415) of n values of `field`,
+// weights exp(6 (phi + phi_frw)); `partial` holds 2*nblk doubles of scratch,
+// the result lands in out[0] (device).  Defined in cg_abi.cu.
+cudaError_t launch_conformal_average(const double* field, const double* phi, int n, double phi_frw,
+                                     double* partial, int nblk, double* out, cudaStream_t st);
+
 inline cudaError_t launch_stage(int v, const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
   return v == kFast ? fast::launch_stage(b, bg, stage, st) : exact::launch_stage(b, bg, stage, st);
 }

@@ -170,6 +170,15 @@ int cg_frw_state(cg_ctx *ctx, int box, double *out, int n);
 /* Steps completed by a box since creation or the last upload. */
 int cg_step_count(cg_ctx *ctx, int box, int64_t *steps);
 
+/* Volume-weighted grid average of a device array, the reference's
+ * conformal_average (utils/math.h:1403-1415) used by BSSN::setExtraFieldData
+ * (components/bssn/bssn.cc:165-170):
+ *   out = [sum exp(6(phi+phi_frw)) field / n] / [sum exp(6(phi+phi_frw)) / n]
+ * over n points of d_field and d_phi (device pointers).  Uses scratch memory
+ * owned by the context; synchronous, result in *out (host). */
+int cg_conformal_average(cg_ctx *ctx, const double *d_field, const double *d_phi, size_t n,
+                         double phi_frw, double *out);
+
 /* Message of the last failure on this context (or of cg_create, when ctx is NULL). */
 const char *cg_last_error(cg_ctx *ctx);
 
