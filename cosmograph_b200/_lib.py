@@ -31,7 +31,7 @@ EXPORTS = (
     "cg_upload_state_async", "cg_download_state_async", "cg_upload_field", "cg_download_field",
     "cg_device_register", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
     "cg_status", "cg_frw_state", "cg_step_count", "cg_last_error", "cg_version",
-    "cg_conformal_average",
+    "cg_conformal_average", "cg_conformal_average_noalloc",
 )
 
 
@@ -90,6 +90,7 @@ def load() -> ctypes.CDLL:
         "cg_step_count": (i, [vp, i, ctypes.POINTER(ctypes.c_int64)]),
         "cg_last_error": (ctypes.c_char_p, [vp]),
         "cg_conformal_average": (i, [vp, vp, vp, sz, ctypes.c_double, dp]),
+        "cg_conformal_average_noalloc": (i, [vp, vp, sz, ctypes.c_double, vp, vp]),
         "cg_version": (i, []),
     }
     for name, (res, args) in sig.items():

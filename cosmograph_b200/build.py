@@ -32,6 +32,7 @@ UNITS = [
     ("stage_exact.o", "cg_stage_inst.cu", ["--fmad=false", "-DCG_VARIANT_NS=exact"]),
     ("stage_fast.o", "cg_stage_inst.cu", ["--fmad=true", "-DCG_VARIANT_NS=fast"]),
     ("abi.o", "cg_abi.cu", []),
+    ("noalloc.o", "cg_noalloc.cu", []),
 ]
 
 

@@ -175,6 +175,8 @@ __global__ void kavg_final_kernel(const double* partial, int nblk, int pts, doub
 }  // namespace
 
 namespace cg {
+void set_global_error(const char* msg) { g_create_error = msg; }
+
 // Conformal average of `field` weighted by exp(6 (phi + phi_FRW)) into
 // out[0] on the device, using `partial` (2*nblk doubles) as scratch.
 cudaError_t launch_conformal_average(const double* field, const double* phi, int n, double phi_frw,

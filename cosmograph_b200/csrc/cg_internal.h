@@ -42,6 +42,9 @@ cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
 cudaError_t launch_conformal_average(const double* field, const double* phi, int n, double phi_frw,
                                      double* partial, int nblk, double* out, cudaStream_t st);
 
+// Message returned by cg_last_error(NULL) on this host thread.
+void set_global_error(const char* msg);
+
 inline cudaError_t launch_stage(int v, const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
   return v == kFast ? fast::launch_stage(b, bg, stage, st) : exact::launch_stage(b, bg, stage, st);
 }

@@ -179,6 +179,25 @@ int cg_step_count(cg_ctx *ctx, int box, int64_t *steps);
 int cg_conformal_average(cg_ctx *ctx, const double *d_field, const double *d_phi, size_t n,
                          double phi_frw, double *out);
 
+/* cg_conformal_average without any device allocation.  No counterpart in the
+ * reference: for callers that cannot let a library call cudaMalloc (their own
+ * memory pool or a fixed memory budget, or no implicit device synchronisation
+ * allowed).  The reduction's scratch is a fixed 16 KiB array compiled into the
+ * library, held by every GPU that loads it until the process exits.
+ *   - d_field, d_phi: n device values each; n <= CG_NOALLOC_MAX_POINTS, larger
+ *     n is rejected with CG_ERR_INVALID (message via cg_last_error(NULL)).
+ *   - d_out: one device double receiving the average; queued on `stream`
+ *     (a cudaStream_t, NULL = legacy default stream), no host synchronisation.
+ *   - The first call on a device looks up the scratch array's device address
+ *     with that device current; make that first call before any stream
+ *     capture begins.
+ *   - All calls on a GPU share the scratch: calls whose kernels overlap on the
+ *     GPU (different streams, concurrent threads) race; serialise them. */
+#define CG_NOALLOC_MAX_BLOCKS 1024
+#define CG_NOALLOC_MAX_POINTS ((size_t)1 << 30)
+int cg_conformal_average_noalloc(const double *d_field, const double *d_phi, size_t n, double phi_frw,
+                                 double *d_out, void *stream);
+
 /* Message of the last failure on this context (or of cg_create, when ctx is NULL). */
 const char *cg_last_error(cg_ctx *ctx);
 
