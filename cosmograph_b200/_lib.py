@@ -9,7 +9,10 @@ from __future__ import annotations
 import ctypes
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "libcosmograph_b200.so"
+import os
+
+# CG_LIBRARY overrides the library file (an alternative build of the same ABI)
+LIB_PATH = Path(os.environ.get("CG_LIBRARY") or Path(__file__).resolve().parent / "libcosmograph_b200.so")
 
 CG_OK = 0
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "out of sequence",
@@ -31,7 +34,7 @@ EXPORTS = (
     "cg_upload_state_async", "cg_download_state_async", "cg_upload_field", "cg_download_field",
     "cg_device_register", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
     "cg_status", "cg_frw_state", "cg_step_count", "cg_last_error", "cg_version",
-    "cg_conformal_average", "cg_conformal_average_noalloc",
+    "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints",
 )
 
 
@@ -91,6 +94,7 @@ def load() -> ctypes.CDLL:
         "cg_last_error": (ctypes.c_char_p, [vp]),
         "cg_conformal_average": (i, [vp, vp, vp, sz, ctypes.c_double, dp]),
         "cg_conformal_average_noalloc": (i, [vp, vp, sz, ctypes.c_double, vp, vp]),
+        "cg_constraints": (i, [vp, i, dp, dp, dp, dp, dp]),
         "cg_version": (i, []),
     }
     for name, (res, args) in sig.items():

@@ -83,6 +83,7 @@ struct Box {
   double* kavg_partial = nullptr;  // per-block partial sums for K_avg
   double* kavg = nullptr;          // device K_avg
   int kavg_blocks = 0;
+  double* cscratch = nullptr;      // constraint statistics scratch (allocated on first use)
 };
 
 }  // namespace
@@ -170,6 +171,56 @@ __global__ void kavg_final_kernel(const double* partial, int nblk, int pts, doub
     const double vol = sV[0] / pts;
     out[0] = sK[0] / pts / vol;
   }
+}
+
+// Fixed-order reduction of per-CTA partial results: out[m] = sum (m < nsum)
+// or max (m >= nsum) of part[b*Q + m] over b < nblk.  One CTA of 256 threads.
+__global__ void part_final_kernel(const double* part, int nblk, int Q, int nsum, double* out) {
+  __shared__ double s[256];
+  for (int m = 0; m < Q; ++m) {
+    const bool sum = m < nsum;
+    double a = sum ? 0.0 : -1.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+      const double x = part[(size_t)b * Q + m];
+      a = sum ? a + x : fmax(a, x);
+    }
+    s[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) s[threadIdx.x] = sum ? s[threadIdx.x] + s[threadIdx.x + o] : fmax(s[threadIdx.x], s[threadIdx.x + o]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[m] = s[0];
+    __syncthreads();
+  }
+}
+
+// Second pass of BSSN::setConstraintCalcs (bssn.cc:1026-1054): squared
+// deviations from the means of pass 1 (r1: sums of value in [0,5), of scaled
+// value in [10,15)), per CTA, 10 partial sums.
+__global__ void constraint_stdev_kernel(const double* cvals, int n, const double* r1, double* part) {
+  __shared__ double s[10][256];
+  double acc[10];
+  double mean[10];
+  for (int m = 0; m < 5; ++m) {
+    mean[2 * m] = r1[m] / n;
+    mean[2 * m + 1] = r1[10 + m] / n;
+  }
+  for (int m = 0; m < 10; ++m) acc[m] = 0.0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    for (int m = 0; m < 10; ++m) {
+      const double d = cvals[(size_t)m * n + q] - mean[m];
+      acc[m] += d * d;
+    }
+  for (int m = 0; m < 10; ++m) s[m][threadIdx.x] = acc[m];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int m = 0; m < 10; ++m) s[m][threadIdx.x] += s[m][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int m = 0; m < 10; ++m) part[(size_t)blockIdx.x * 10 + m] = s[m][0];
 }
 
 }  // namespace
@@ -278,6 +329,8 @@ bool is_pow2(double x) {
 }
 
 void free_box(Box& b) {
+  cudaFree(b.cscratch);
+  b.cscratch = nullptr;
   cudaFree(b.dev.P);
   cudaFree(b.dev.F);
   cudaFree(b.dev.X);
@@ -599,6 +652,54 @@ int cg_step_count(cg_ctx* ctx, int box, int64_t* steps) {
   if (rc) return rc;
   if (!steps) return fail(ctx, CG_ERR_INVALID, "steps is null");
   *steps = ctx->boxes[box].steps;
+  return CG_OK;
+}
+
+int cg_constraints(cg_ctx* ctx, int box, double* H, double* M, double* G, double* A, double* S) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  if (!H || !M || !G || !A || !S) return fail(ctx, CG_ERR_INVALID, "null output array");
+  Box& b = ctx->boxes[box];
+  if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "constraints are taken between steps");
+  if (b.stage_next == 0) {
+    rc = do_init(ctx, b);
+    if (rc) return rc;
+  }
+  const int n = b.dev.pts;
+  const int nblk1 = cg::exact::constraint_blocks(b.dev);
+  const int nblk2 = std::min(1024, (n + 255) / 256);
+  // layout: cvals (10 n) | part1 (27 nblk1) | part2 (10 nblk2) | r1 (27) | r2 (10)
+  const size_t need = (size_t)10 * n + 27 * (size_t)nblk1 + 10 * (size_t)nblk2 + 37;
+  if (!b.cscratch) CG_CUDA(ctx, cudaMalloc(&b.cscratch, sizeof(double) * need));
+  double* cvals = b.cscratch;
+  double* part1 = cvals + (size_t)10 * n;
+  double* part2 = part1 + (size_t)27 * nblk1;
+  double* r1 = part2 + (size_t)10 * nblk2;
+  double* r2 = r1 + 27;
+  StageBg bg = bg_for(b, 1, b.frw.get_phi);
+  CG_CUDA(ctx, cg::exact::launch_constraints(b.dev, bg, cvals, part1, ctx->stream));
+  part_final_kernel<<<1, 256, 0, ctx->stream>>>(part1, nblk1, 27, 17, r1);
+  constraint_stdev_kernel<<<nblk2, 256, 0, ctx->stream>>>(cvals, n, r1, part2);
+  part_final_kernel<<<1, 256, 0, ctx->stream>>>(part2, nblk2, 10, 10, r2);
+  CG_CUDA(ctx, cudaGetLastError());
+  double h1[27], h2[10];
+  CG_CUDA(ctx, cudaMemcpyAsync(h1, r1, sizeof(h1), cudaMemcpyDeviceToHost, ctx->stream));
+  CG_CUDA(ctx, cudaMemcpyAsync(h2, r2, sizeof(h2), cudaMemcpyDeviceToHost, ctx->stream));
+  CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // BSSN_NORMALIZE_MEAN / _STDEV and BSSN_STORE_CONSTRAINT_STAT_VARS (bssn_macros.h:539-560)
+  double* outs[5] = {H, M, G, A, S};
+  for (int c = 0; c < 5; ++c) {
+    double* o = outs[c];
+    o[0] = h1[c] / n;
+    o[1] = std::sqrt(h2[2 * c] / (n - 1.0));
+    o[2] = h1[17 + c];
+    o[3] = h1[5 + c];
+    o[4] = h1[10 + c] / n;
+    o[5] = std::sqrt(h2[2 * c + 1] / (n - 1.0));
+    o[6] = h1[22 + c];
+  }
+  H[7] = std::sqrt(h1[15]);
+  M[7] = std::sqrt(h1[16]);
   return CG_OK;
 }
 

@@ -30,6 +30,10 @@ enum Variant : int { kExact = 0, kFast = 1 };
 namespace exact {
 cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
 cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
+// constraint statistics pass 1 on the first-substep input X: per-point values
+// (10 arrays of pts) into cvals, 27 partial results per CTA into cpart
+cudaError_t launch_constraints(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st);
+int constraint_blocks(const BoxDev& b);
 }  // namespace exact
 namespace fast {
 cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);

@@ -48,6 +48,8 @@ struct StagePtrs {
   double* fp_out;        // flux primitives of the output state
   unsigned* status;      // error flags (bit 0: NaN in DIFFphi, bit 1: non-finite field)
   const double* kavg;    // device-side K_avg of a^n, or null (bssn.cc:168)
+  double* cvals;         // constraint mode: per-point value and scaled value of H, M, G, A, S (10 arrays)
+  double* cpart;         // constraint mode: kCPart partial results per CTA
 };
 
 struct BoxGeom {
@@ -84,6 +86,17 @@ template <int MATTER>
 struct Slots {
   static constexpr int value = S_MAT + (MATTER == kDust ? 4 : (MATTER == kScalar ? 15 : 0));
 };
+
+// What a launch of the point kernel does with the geometry it computes.
+enum Mode : int { kEvolve = 0, kConstraints = 1 };
+// constraint mode: d_d A_q after the matter slots (18)
+template <int MATTER>
+struct SlotsC {
+  static constexpr int dA = Slots<MATTER>::value;
+  static constexpr int value = dA + 18;
+};
+// per-block partial results of the constraint pass (see constraint_reduce)
+constexpr int kCPart = 27;
 
 namespace CG_VARIANT_NS {
 
@@ -188,9 +201,19 @@ __device__ __forceinline__ double d1p(const double* __restrict__ fa, const doubl
 }
 
 // Phase 1: every derivative the point needs, parked in shared memory.
-template <int O, int MATTER, class T>
+template <int O, int MATTER, int MODE, class T>
 __device__ __forceinline__ void derivatives(const T& t, const double* __restrict__ a, const double* __restrict__ fp,
                                             int N, const Physics& ph, const double gi[6], double* sl) {
+  if (MODE == kConstraints) {
+    // d_d A_q for the momentum constraint (BSSN_MI, bssn_macros.h:498-500)
+#pragma unroll 1
+    for (int q = 0; q < 6; ++q) {
+      const double* __restrict__ f = a + (size_t)(F_A11 + q) * N;
+      sl[(SlotsC<MATTER>::dA + 3 * q + 0) * kThreads] = d1<O>(f, t, 0, ph);
+      sl[(SlotsC<MATTER>::dA + 3 * q + 1) * kThreads] = d1<O>(f, t, 1, ph);
+      sl[(SlotsC<MATTER>::dA + 3 * q + 2) * kThreads] = d1<O>(f, t, 2, ph);
+    }
+  }
   // metric components, phi and alpha: first and second derivatives
   // (calculate_dgamma / calculate_ddgamma / calculate_dalpha_dphi,
   // bssn.cc:480-521).  For g_q the second derivatives are contracted at once
@@ -263,21 +286,56 @@ __device__ __forceinline__ void derivatives(const T& t, const double* __restrict
   }
 }
 
-template <int O, int MATTER>
+// Deterministic CTA reduction of Q values per thread: the first NSUM are
+// summed, the rest maximised; warp shuffles, then the warps in order.  Thread
+// 0 writes the Q results of this CTA to part[cta * Q].
+template <int Q, int NSUM>
+__device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part) {
+  __shared__ double red[kThreads / 32][Q];
+  const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
+  const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int m = 0; m < Q; ++m) {
+    double x = q[m];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_down_sync(0xffffffffu, x, o);
+      x = m < NSUM ? x + y : fmax(x, y);
+    }
+    if (lane == 0) red[warp][m] = x;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int cta = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+#pragma unroll 1
+    for (int m = 0; m < Q; ++m) {
+      double x = red[0][m];
+      for (int w = 1; w < kThreads / 32; ++w) x = m < NSUM ? x + red[w][m] : fmax(x, red[w][m]);
+      part[(size_t)cta * Q + m] = x;
+    }
+  }
+}
+
+template <int O, int MATTER, int MODE>
 __global__ void __launch_bounds__(kThreads, 2)
 stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
   constexpr int NFLD = NF<MATTER>::value;
+  constexpr int NSLOT = MODE == kConstraints ? SlotsC<MATTER>::value : Slots<MATTER>::value;
+  (void)NSLOT;
   constexpr int R = O / 2;
   extern __shared__ double smem[];
   const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
   double* sl = smem + tid;  // this thread's slot column
   auto S = [&](int s) -> double& { return sl[s * kThreads]; };
 
-  const int k = blockIdx.x * kBZ + threadIdx.x;
-  const int j = blockIdx.y * kBY + threadIdx.y;
-  const int i = blockIdx.z * kBX + threadIdx.z;
-  const bool live = i < geo.nx && j < geo.ny && k < geo.nz;
-  if (!live) return;  // no CTA-wide synchronisation below
+  const int k0 = blockIdx.x * kBZ + threadIdx.x;
+  const int j0 = blockIdx.y * kBY + threadIdx.y;
+  const int i0 = blockIdx.z * kBX + threadIdx.z;
+  const bool live = i0 < geo.nx && j0 < geo.ny && k0 < geo.nz;
+  if (MODE == kEvolve && !live) return;  // no CTA-wide synchronisation in this mode
+  // constraint mode: every thread reaches the CTA reduction; threads past the
+  // box edge compute a valid point and contribute nothing
+  const int k = min(k0, geo.nz - 1), j = min(j0, geo.ny - 1), i = min(i0, geo.nx - 1);
   if (P.kavg) bg.K_avg = *P.kavg;
   const int N = geo.pts;
   const int c = (i * geo.ny + j) * geo.nz + k;
@@ -296,10 +354,10 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
                         z0 + kBZ + R <= geo.nz;
   if (interior) {
     const Taps<false> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
-    derivatives<O, MATTER>(t, a, P.fp_in, N, ph, gi, sl);
+    derivatives<O, MATTER, MODE>(t, a, P.fp_in, N, ph, gi, sl);
   } else {
     const Taps<true> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
-    derivatives<O, MATTER>(t, a, P.fp_in, N, ph, gi, sl);
+    derivatives<O, MATTER, MODE>(t, a, P.fp_in, N, ph, gi, sl);
   }
 
   // ---- phase 2: the algebra of set_bd_values (bssn.cc:361-421) ----------------
@@ -544,6 +602,93 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
   const double r = S(S_SRC + Q_R) + bg.rho_FRW;
   // Hamiltonian constraint, bssn.cc:1073-1084 (theta = 0)
   const double H = -exp(5.0 * phi) / 8.0 * (ricci + 2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0)) - AijAij - 16.0 * kPi * r);
+
+  if constexpr (MODE == kConstraints) {
+    // BSSN::setConstraintCalcs per point (bssn.cc:983-1006)
+    double v[5], sc[5];
+    v[0] = H;  // hamiltonianConstraintCalc / Scale, bssn.cc:1073-1100
+    sc[0] = (exp(5.0 * phi) / 8.0) * sqrt(ricci * ricci + AijAij * AijAij +
+                                          (2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0))) *
+                                              (2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0))) +
+                                          (16.0 * kPi * r) * (16.0 * kPi * r));
+    {  // momentum, BSSN_MI / BSSN_MI_SCALE (bssn_macros.h:487-527)
+      const double e6 = exp(6.0 * phi);
+      double mv[3], ms[3];
+#pragma unroll
+      for (int I = 0; I < 3; ++I) {
+        double t6 = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+          for (int X = 0; X < 3; ++X) {
+            const double u = gi[sym(X, d)] * A[sym(X, I)] * dphi[d];
+            t6 = (d == 0 && X == 0) ? u : t6 + u;
+          }
+        double tD = 0.0;
+#pragma unroll
+        for (int X = 0; X < 3; ++X)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const double u = gi[sym(X, d)] * S(SlotsC<MATTER>::dA + 3 * sym(X, I) + d);
+            tD = (X == 0 && d == 0) ? u : tD + u;
+          }
+        tD = tD - Gd[0] * A[sym(0, I)] - Gd[1] * A[sym(1, I)] - Gd[2] * A[sym(2, I)];
+#pragma unroll
+        for (int X = 0; X < 3; ++X)
+#pragma unroll
+          for (int Y = 0; Y < 3; ++Y) tD = tD - GL(Y, sym(X, I)) * Ac[sym(Y, X)];
+        const double sI = S(S_SRC + Q_S1 + I);
+        mv[I] = e6 * (-2.0 / 3.0 * S(S_DK + I) - 8 * kPi * (sI) - 2.0 / 3.0 * 2.0 * 0.0 + 6.0 * (t6) + (tD));
+        ms[I] = e6 * (fabs(2.0 / 3.0 * S(S_DK + I)) + fabs(8 * kPi * (sI)) + fabs(2.0 / 3.0 * 2.0 * 0.0) +
+                      6.0 * fabs(t6) + fabs(tD));
+      }
+      v[1] = sqrt(mv[0] * mv[0] + mv[1] * mv[1] + mv[2] * mv[2]);
+      sc[1] = sqrt(ms[0] * ms[0] + ms[1] * ms[1] + ms[2] * ms[2]);
+    }
+    {  // christoffel constraint, BSSN_GI_CALC / BSSN_GI_SCALE (bssn_macros.h:530-536)
+      double gv[3], gs[3];
+#pragma unroll
+      for (int I = 0; I < 3; ++I) {
+        const double Gam = C(F_GAM1 + I);
+        gv[I] = Gam - gi[0] * G(I, 0) - gi[3] * G(I, 3) - gi[5] * G(I, 5) -
+                2.0 * (gi[1] * G(I, 1) + gi[2] * G(I, 2) + gi[4] * G(I, 4));
+        gs[I] = fabs(Gam) + fabs(gi[0] * G(I, 0) - gi[3] * G(I, 3) - gi[5] * G(I, 5) -
+                                 2.0 * (gi[1] * G(I, 1) + gi[2] * G(I, 2) + gi[4] * G(I, 4)));
+      }
+      v[2] = sqrt(gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2]);
+      sc[2] = sqrt(gs[0] * gs[0] + gs[1] * gs[1] + gs[2] * gs[2]);
+    }
+    // AijTFConstraintCalc / Scale (bssn.cc:1182-1192)
+    v[3] = gi[0] * A[0] + gi[3] * A[3] + gi[5] * A[5] + 2.0 * (gi[1] * A[1] + gi[2] * A[2] + gi[4] * A[4]);
+    sc[3] = fabs(gi[0] * A[0]) + fabs(gi[3] * A[3]) + fabs(gi[5] * A[5]) +
+            2.0 * (fabs(gi[1] * A[1]) + fabs(gi[2] * A[2]) + fabs(gi[4] * A[4]));
+    // unitDetConstraintCalc / Scale (bssn.cc:1199-1219)
+    v[4] = fabs(g[0] + g[3] + g[5] - g[1] * g[1] - g[2] * g[2] - g[4] * g[4] + g[0] * g[3] + g[0] * g[5] +
+                g[3] * g[5] - g[4] * g[4] * g[0] - g[2] * g[2] * g[3] - g[1] * g[1] * g[5] +
+                2.0 * g[1] * g[2] * g[4] + g[0] * g[3] * g[5]);
+    sc[4] = (fabs(g[0]) + fabs(g[3]) + fabs(g[5]) + g[1] * g[1] + g[2] * g[2] + g[4] * g[4] + fabs(g[0] * g[3]) +
+             fabs(g[0] * g[5]) + fabs(g[3] * g[5]) + g[4] * g[4] * g[0] + g[2] * g[2] * g[3] +
+             g[1] * g[1] * g[5] + 2.0 * fabs(g[1] * g[2] * g[4]) + fabs(g[0] * g[3] * g[5]));
+    double q[kCPart];
+    const double dx = ph.dx;
+#pragma unroll
+    for (int m = 0; m < 5; ++m) {
+      const double sd = v[m] / sc[m];
+      q[m] = live ? v[m] : 0.0;
+      q[5 + m] = live ? sc[m] : 0.0;
+      q[10 + m] = live ? sd : 0.0;
+      q[17 + m] = live ? fabs(v[m]) : 0.0;
+      q[22 + m] = live ? fabs(sd) : 0.0;
+      if (live) {
+        P.cvals[(size_t)(2 * m) * N + c] = v[m];
+        P.cvals[(size_t)(2 * m + 1) * N + c] = sd;
+      }
+    }
+    q[15] = live ? v[0] * v[0] * dx * dx * dx : 0.0;
+    q[16] = live ? v[1] * v[1] * dx * dx * dx : 0.0;
+    cta_reduce<kCPart, 17>(q, P.cpart);
+    return;
+  }
 
   // ---- evolution equations and K{n}Finalize, field by field --------------------
   const double dt = ph.dt;

@@ -83,12 +83,44 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
   constexpr size_t smem = sizeof(double) * Slots<M>::value * kThreads;
   static bool configured = false;  // per instantiation
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M, kEvolve>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  stage_kernel<O, M><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage);
+  stage_kernel<O, M, kEvolve><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage);
   return cudaGetLastError();
+}
+
+template <int O, int M>
+cudaError_t go_constraints(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st) {
+  StagePtrs P{};
+  P.in = b.X;
+  P.p = b.P;
+  P.fp_in = b.FP0;
+  P.status = b.status;
+  P.kavg = b.kavg;
+  P.cvals = cvals;
+  P.cpart = cpart;
+  BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
+  constexpr size_t smem = sizeof(double) * SlotsC<M>::value * kThreads;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e =
+        cudaFuncSetAttribute(stage_kernel<O, M, kConstraints>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  stage_kernel<O, M, kConstraints><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, 1);
+  return cudaGetLastError();
+}
+
+template <int O>
+cudaError_t go_constraints_m(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st) {
+  switch (b.matter) {
+    case kDust: return go_constraints<O, kDust>(b, bg, cvals, cpart, st);
+    case kScalar: return go_constraints<O, kScalar>(b, bg, cvals, cpart, st);
+    default: return go_constraints<O, kVacuum>(b, bg, cvals, cpart, st);
+  }
 }
 
 template <int O>
@@ -109,6 +141,21 @@ cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStre
     case 8: return go_stage_m<8>(b, bg, stage, st);
     default: return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t launch_constraints(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st) {
+  switch (b.order) {
+    case 2: return go_constraints_m<2>(b, bg, cvals, cpart, st);
+    case 4: return go_constraints_m<4>(b, bg, cvals, cpart, st);
+    case 6: return go_constraints_m<6>(b, bg, cvals, cpart, st);
+    case 8: return go_constraints_m<8>(b, bg, cvals, cpart, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int constraint_blocks(const BoxDev& b) {
+  const dim3 g = stage_grid(b);
+  return (int)(g.x * g.y * g.z);
 }
 
 cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st) {

@@ -138,6 +138,12 @@ class Evolution:
     def step(self, nsteps: int = 1) -> None:
         self._check(self.L.cg_step(self.ctx, nsteps))
 
+    def constraints(self, box: int = 0) -> dict:
+        """BSSN::setConstraintCalcs statistics of the current state (between steps)."""
+        arrs = {k: np.zeros(8 if k in "HM" else 7) for k in "HMGAS"}
+        self._check(self.L.cg_constraints(self.ctx, box, *(_dptr(arrs[k]) for k in "HMGAS")))
+        return arrs
+
     def synchronize(self) -> None:
         self._check(self.L.cg_synchronize(self.ctx))
 

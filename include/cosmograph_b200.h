@@ -170,6 +170,17 @@ int cg_frw_state(cg_ctx *ctx, int box, double *out, int n);
 /* Steps completed by a box since creation or the last upload. */
 int cg_step_count(cg_ctx *ctx, int box, int64_t *steps);
 
+/* Constraint statistics of one box between steps (after cg_step_init or a
+ * whole step), BSSN::setConstraintCalcs (components/bssn/bssn.cc:965-1071)
+ * on the first-substep input with its sources: Hamiltonian (H), momentum
+ * magnitude (M), Christoffel (G), trace of A (A) and unit-determinant (S)
+ * constraints; each array holds mean, stdev, max|.|, sum of scales, mean of
+ * scaled, stdev of scaled, max|scaled| (BSSN_STORE_CONSTRAINT_STAT_VARS,
+ * bssn_macros.h:553-560); H[7], M[7] are the L2 norms sqrt(sum C^2 dx^3).
+ * FP64, fixed-order (deterministic) reductions; scratch owned by the context.
+ * Synchronous. */
+int cg_constraints(cg_ctx *ctx, int box, double *H, double *M, double *G, double *A, double *S);
+
 /* Volume-weighted grid average of a device array, the reference's
  * conformal_average (utils/math.h:1403-1415) used by BSSN::setExtraFieldData
  * (components/bssn/bssn.cc:165-170):

@@ -1,0 +1,52 @@
+"""cg_constraints (BSSN::setConstraintCalcs on the GPU) against the reference's
+own output (golden fixture) and against the CPU restatement."""
+import numpy as np
+import pytest
+
+import oracle
+from cosmograph_b200 import ics, state as S
+from cosmograph_b200.evolution import BoxConfig, Evolution
+from helpers import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def assert_close(got, ref, tol):
+    for c in "HMGAS":
+        rel = np.abs(got[c] - ref[c]) / np.maximum(np.abs(ref[c]), 1e-300)
+        assert rel.max() <= tol, (c, got[c], ref[c])
+
+
+def test_constraints_match_reference_fixture():
+    inp, _, ref, meta = load_golden("dust_o8_constraints")
+    with Evolution(inp, BoxConfig(order=meta["order"], **meta["config"])) as ev:
+        got = ev.constraints(0)
+    # fixed-order GPU reductions vs OpenMP reductions: last-bits differences
+    assert_close(got, ref, 1e-11)
+
+
+@pytest.mark.parametrize("matter,shape,order", [
+    (S.DUST, (24, 20, 16), 4), (S.SCALAR, (16, 16, 16), 6), (S.VACUUM, (12, 14, 16), 2),
+])
+def test_constraints_match_restatement(matter, shape, order):
+    st = ics.perturbed(shape, matter, seed=21, amp=2e-2)
+    ref = oracle.constraints(st, order, lapse="Harmonic")
+    with Evolution(st, BoxConfig(order=order)) as ev:
+        got = ev.constraints(0)
+    assert_close(got, ref, 1e-11)
+
+
+def test_constraints_after_steps_and_between_substeps():
+    st = ics.grf_dust(32, seed=3, rms_delta=1e-3, order=4)
+    with Evolution(st, BoxConfig(order=4)) as ev:
+        h0 = ev.constraints(0)["H"]
+        ev.step(5)
+        got = ev.constraints(0)
+        ev.step_init()
+        ev.rk_stage(1)
+        with pytest.raises(RuntimeError, match="between steps"):
+            ev.constraints(0)
+        st5 = None
+    ref = oracle.constraints(oracle.evolve(st, 5, 4), 4)
+    assert_close(got, ref, 1e-10)
+    assert np.all(np.isfinite(h0))
