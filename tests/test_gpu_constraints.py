@@ -11,9 +11,16 @@ from helpers import load_golden
 pytestmark = pytest.mark.gpu
 
 
+# The trace-of-A and unit-determinant constraints vanish after the step's
+# normalisation up to roundoff (~1e-16 and ~1e-18); CUDA's log1p/expm1 round
+# differently from libm in the last bit, so those statistics are compared
+# against an absolute floor instead of their own noise.
+FLOOR = {"H": 1e-300, "M": 1e-300, "G": 1e-300, "A": 1e-13, "S": 1e-15}
+
+
 def assert_close(got, ref, tol):
     for c in "HMGAS":
-        rel = np.abs(got[c] - ref[c]) / np.maximum(np.abs(ref[c]), 1e-300)
+        rel = np.abs(got[c] - ref[c]) / np.maximum(np.abs(ref[c]), FLOOR[c])
         assert rel.max() <= tol, (c, got[c], ref[c])
 
 
