@@ -12,10 +12,12 @@ pytestmark = pytest.mark.gpu
 
 
 # The trace-of-A and unit-determinant constraints vanish after the step's
-# normalisation up to roundoff (~1e-16 and ~1e-18); CUDA's log1p/expm1 round
-# differently from libm in the last bit, so those statistics are compared
-# against an absolute floor instead of their own noise.
-FLOOR = {"H": 1e-300, "M": 1e-300, "G": 1e-300, "A": 1e-13, "S": 1e-15}
+# normalisation up to roundoff (values ~1e-16 and ~1e-18); CUDA's log1p/expm1
+# round differently from libm in the last bit, so those statistics are
+# measured against a floor of 1e-3 (the amplitude of the metric perturbation)
+# instead of against their own noise.  Their sums of scales are O(1) and stay
+# relative.
+FLOOR = {"H": 1e-300, "M": 1e-300, "G": 1e-300, "A": 1e-3, "S": 1e-3}
 
 
 def assert_close(got, ref, tol):
