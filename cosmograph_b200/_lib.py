@@ -23,7 +23,7 @@ LAPSE = {
     "Static": 0, "Harmonic": 1, "ConformalFLRW": 2, "ConformalSync": 3, "Anharmonic": 4,
     "OnePlusLog": 5, "AwAGaugeWave": 6, "AwAShiftedWave": 7, "DampedWave": 8,
 }
-PRECISION = {"fp64": 0, "fp64_fma": 1}
+PRECISION = {"fp64": 0, "fp64_fma": 1, "mixed": 2}
 POTENTIAL = {"const": 0, "quadratic": 1}
 STATUS_NAN, STATUS_NONFINITE = 1, 2
 

@@ -33,6 +33,7 @@ UNITS = [
     ("stage_fast.o", "cg_stage_inst.cu", ["--fmad=true", "-DCG_VARIANT_NS=fast"]),
     ("abi.o", "cg_abi.cu", []),
     ("noalloc.o", "cg_noalloc.cu", []),
+    ("mixed.o", "cg_mixed_inst.cu", []),
 ]
 
 

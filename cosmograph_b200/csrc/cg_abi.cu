@@ -14,6 +14,7 @@
 
 #include "../../include/cosmograph_b200.h"
 #include "cg_internal.h"
+#include "cg_mixed.cuh"
 
 namespace {
 
@@ -84,6 +85,10 @@ struct Box {
   double* kavg = nullptr;          // device K_avg
   int kavg_blocks = 0;
   double* cscratch = nullptr;      // constraint statistics scratch (allocated on first use)
+  // FP32-mixed boxes
+  bool mixed = false;
+  cg::MixedBox mdev{};
+  double bp[23] = {}, bf[23] = {}, ba[23] = {}, bprev[23] = {};  // uniform background registers
 };
 
 }  // namespace
@@ -195,6 +200,28 @@ __global__ void part_final_kernel(const double* part, int nblk, int Q, int nsum,
   }
 }
 
+// Sums of four fields (for the mixed form's uniform background): per CTA.
+__global__ void field_sums_kernel(const double* f0, const double* f1, const double* f2, const double* f3, int n,
+                                  double* part) {
+  __shared__ double s[4][256];
+  double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    a0 += f0[q];
+    a1 += f1[q];
+    a2 += f2[q];
+    a3 += f3 ? f3[q] : 0.0;
+  }
+  s[0][threadIdx.x] = a0; s[1][threadIdx.x] = a1; s[2][threadIdx.x] = a2; s[3][threadIdx.x] = a3;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int m = 0; m < 4; ++m) s[m][threadIdx.x] += s[m][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int m = 0; m < 4; ++m) part[(size_t)blockIdx.x * 4 + m] = s[m][0];
+}
+
 // Second pass of BSSN::setConstraintCalcs (bssn.cc:1026-1054): squared
 // deviations from the means of pass 1 (r1: sums of value in [0,5), of scaled
 // value in [10,15)), per CTA, 10 partial sums.
@@ -270,7 +297,93 @@ int launch_kavg(cg_ctx* ctx, Box& b, const double* in) {
   return CG_OK;
 }
 
+// Right-hand side of the uniform background (the reference's equations for a
+// spatially constant state, trivial FRW): dK/dt, dphi/dt, dalpha/dt.
+void mixed_bg_rhs(const Box& b, const double* a, double phi_lag, double* rhs) {
+  for (int f = 0; f < 23; ++f) rhs[f] = 0.0;
+  const double Kd = a[cg::F_K], ad = a[cg::F_ALPHA], al = ad + 1.0;
+  double rS = 0.0;  // DIFFr + DIFFS of the uniform state (W = 1)
+  if (b.desc.matter == CG_MATTER_DUST)
+    rS = (a[cg::F_D] * std::exp(-6.0 * phi_lag) + b.desc.lambda) + (-3.0 * b.desc.lambda);
+  rhs[cg::F_K] = al * (1.0 / 3.0 * Kd * Kd) + 4.0 * cg::kPi * al * rS;
+  rhs[cg::F_PHI] = -1.0 / 6.0 * (al * Kd);
+  rhs[cg::F_ALPHA] = b.desc.lapse == CG_LAPSE_HARMONIC ? -1.0 * al * Kd : 0.0;
+}
+
+int mixed_init(cg_ctx* ctx, Box& b) {
+  // background registers from the means of _p (K, phi, alpha, D)
+  const int n = b.dev.pts;
+  const int nblk = std::min(1024, (n + 255) / 256);
+  if (!b.cscratch) {
+    const size_t need = (size_t)10 * n + 27 * (size_t)cg::exact::constraint_blocks(b.dev) + 10 * (size_t)nblk + 37;
+    CG_CUDA(ctx, cudaMalloc(&b.cscratch, sizeof(double) * need));
+  }
+  double* part = b.cscratch;
+  double* res = part + 4 * (size_t)nblk;
+  const double* P = b.mdev.P;
+  field_sums_kernel<<<nblk, 256, 0, ctx->stream>>>(P + (size_t)cg::F_K * n, P + (size_t)cg::F_PHI * n,
+                                                   P + (size_t)cg::F_ALPHA * n,
+                                                   b.desc.matter == CG_MATTER_DUST ? P + (size_t)cg::F_D * n : nullptr,
+                                                   n, part);
+  part_final_kernel<<<1, 256, 0, ctx->stream>>>(part, nblk, 4, 4, res);
+  CG_CUDA(ctx, cudaGetLastError());
+  double h[4];
+  CG_CUDA(ctx, cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int f = 0; f < 23; ++f) b.bp[f] = b.ba[f] = b.bprev[f] = b.bf[f] = 0.0;
+  b.bp[cg::F_K] = h[0] / n;
+  b.bp[cg::F_PHI] = h[1] / n;
+  b.bp[cg::F_ALPHA] = h[2] / n;
+  if (b.desc.matter == CG_MATTER_DUST) b.bp[cg::F_D] = h[3] / n;
+  for (int f = 0; f < 23; ++f) b.ba[f] = b.bprev[f] = b.bp[f];
+  cg::mixed::Bg bg{};
+  for (int f = 0; f < 23; ++f) bg.in[f] = b.ba[f];
+  CG_CUDA(ctx, cg::mixed::launch_init(b.mdev, bg, ctx->stream));
+  b.stage_next = 1;
+  return CG_OK;
+}
+
+int mixed_stage(cg_ctx* ctx, Box& b, int n) {
+  cg::mixed::Bg bg{};
+  const double phi_lag = n == 1 ? b.ba[cg::F_PHI] : b.bprev[cg::F_PHI];
+  mixed_bg_rhs(b, b.ba, phi_lag, bg.rhs);
+  const double dt = b.desc.dt;
+  double o[23];
+  for (int f = 0; f < 23; ++f) {
+    const double cv = bg.rhs[f], pv = b.bp[f];
+    if (n == 1) {
+      b.bf[f] = dt * cv / 6.0;
+      o[f] = pv + dt * cv / 2.0;
+    } else if (n == 2) {
+      b.bf[f] = b.bf[f] + dt * cv / 3.0;
+      o[f] = pv + dt * cv / 2.0;
+    } else if (n == 3) {
+      b.bf[f] = b.bf[f] + dt * cv / 3.0;
+      o[f] = pv + dt * cv;
+    } else {
+      o[f] = b.bf[f] + (dt * cv / 6.0 + pv);
+    }
+  }
+  for (int f = 0; f < 23; ++f) {
+    bg.in[f] = b.ba[f];
+    bg.prev[f] = b.bprev[f];
+    bg.out[f] = o[f];
+  }
+  bg.e6l = std::exp(-6.0 * phi_lag);
+  bg.lambda = b.desc.lambda;
+  CG_CUDA(ctx, cg::mixed::launch_stage(b.mdev, bg, n, ctx->stream));
+  for (int f = 0; f < 23; ++f) {
+    b.bprev[f] = b.ba[f];
+    b.ba[f] = o[f];
+    if (n == 4) b.bp[f] = o[f];
+  }
+  b.stage_next = n == 4 ? 1 : n + 1;
+  if (n == 4) ++b.steps;
+  return CG_OK;
+}
+
 int do_init(cg_ctx* ctx, Box& b) {
+  if (b.mixed) return mixed_init(ctx, b);
   StageBg bg = bg_for(b, 1, b.frw.get_phi);
   CG_CUDA(ctx, cg::launch_init(b.variant, b.dev, bg, ctx->stream));
   b.stage_next = 1;
@@ -278,6 +391,7 @@ int do_init(cg_ctx* ctx, Box& b) {
 }
 
 int do_stage(cg_ctx* ctx, Box& b, int n) {
+  if (b.mixed) return mixed_stage(ctx, b, n);
   // FRW getters of the next substep (for the flux primitives of the output)
   FrwHost nxt = b.frw;
   nxt.stage(n, b.desc.dt);
@@ -315,7 +429,25 @@ int validate(const cg_box_desc& d, std::string& why) {
   }
   if (d.matter < 0 || d.matter > 2) { why = "unknown matter model"; return CG_ERR_INVALID; }
   if (d.lapse < 0 || d.lapse > 8) { why = "unknown lapse gauge"; return CG_ERR_INVALID; }
-  if (d.precision != CG_PREC_FP64 && d.precision != CG_PREC_FP64_FMA) { why = "unknown precision"; return CG_ERR_INVALID; }
+  if (d.precision != CG_PREC_FP64 && d.precision != CG_PREC_FP64_FMA && d.precision != CG_PREC_MIXED) {
+    why = "unknown precision";
+    return CG_ERR_INVALID;
+  }
+  if (d.precision == CG_PREC_MIXED) {
+    if (d.matter == CG_MATTER_SCALAR) { why = "the FP32-mixed form covers vacuum and dust"; return CG_ERR_INVALID; }
+    if (d.lapse != CG_LAPSE_HARMONIC && d.lapse != CG_LAPSE_STATIC) {
+      why = "the FP32-mixed form supports the Harmonic and Static lapses";
+      return CG_ERR_INVALID;
+    }
+    if (d.frw_phi != 0.0 || d.frw_K != 0.0 || d.nfluids != 0) {
+      why = "the FP32-mixed form evolves about its own uniform background (trivial FRW reference)";
+      return CG_ERR_INVALID;
+    }
+    if (d.a_adj_amp != 0.0 || d.k_damping_amp != 0.0) {
+      why = "the FP32-mixed form needs a_adj_amp = k_damping_amp = 0";
+      return CG_ERR_INVALID;
+    }
+  }
   if (d.ko_coeff != 0.0) { why = "Kreiss-Oliger dissipation is not available on this path (ko_coeff must be 0)"; return CG_ERR_INVALID; }
   if (d.nfluids < 0 || d.nfluids > 4) { why = "at most 4 FRW fluids"; return CG_ERR_INVALID; }
   if (!(d.dx > 0.0) || !std::isfinite(d.dt)) { why = "dx must be positive and dt finite"; return CG_ERR_INVALID; }
@@ -331,6 +463,14 @@ bool is_pow2(double x) {
 void free_box(Box& b) {
   cudaFree(b.cscratch);
   b.cscratch = nullptr;
+  if (b.mixed) {
+    cudaFree(b.mdev.X);
+    cudaFree(b.mdev.Y);
+    cudaFree(b.mdev.FP0);
+    cudaFree(b.mdev.FP1);
+    b.mdev.X = b.mdev.Y = nullptr;
+    b.mdev.FP0 = b.mdev.FP1 = nullptr;
+  }
   cudaFree(b.dev.P);
   cudaFree(b.dev.F);
   cudaFree(b.dev.X);
@@ -436,17 +576,38 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
     }
     b.frw.set_gets(b.frw.phi, b.frw.K, b.frw.rho);
     const size_t reg = sizeof(double) * (size_t)b.dev.nfields * b.dev.pts;
+    b.mixed = d.precision == CG_PREC_MIXED;
     e = cudaMalloc(&b.dev.P, reg);
     if (e == cudaSuccess) e = cudaMalloc(&b.dev.F, reg);
-    if (e == cudaSuccess) e = cudaMalloc(&b.dev.X, reg);
-    if (e == cudaSuccess) e = cudaMalloc(&b.dev.Y, reg);
-    if (e == cudaSuccess && d.matter == CG_MATTER_DUST) {
-      const size_t fp = sizeof(double) * (size_t)cg::P_N * b.dev.pts;
-      e = cudaMalloc(&b.dev.FP0, fp);
-      if (e == cudaSuccess) e = cudaMalloc(&b.dev.FP1, fp);
+    if (!b.mixed) {
+      if (e == cudaSuccess) e = cudaMalloc(&b.dev.X, reg);
+      if (e == cudaSuccess) e = cudaMalloc(&b.dev.Y, reg);
+      if (e == cudaSuccess && d.matter == CG_MATTER_DUST) {
+        const size_t fp = sizeof(double) * (size_t)cg::P_N * b.dev.pts;
+        e = cudaMalloc(&b.dev.FP0, fp);
+        if (e == cudaSuccess) e = cudaMalloc(&b.dev.FP1, fp);
+      }
+      for (double* p : {b.dev.P, b.dev.F, b.dev.X, b.dev.Y})
+        if (e == cudaSuccess) e = cudaMemset(p, 0, reg);
+    } else {
+      cg::MixedBox& m = b.mdev;
+      m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.pts = b.dev.pts; m.nfields = b.dev.nfields;
+      m.order = d.stencil_order; m.matter = d.matter; m.lapse = d.lapse; m.normalize = d.normalize_metric;
+      m.dx = d.dx; m.dt = d.dt;
+      m.P = b.dev.P;
+      m.F = b.dev.F;
+      m.status = ctx->status;
+      const size_t reg32 = sizeof(float) * (size_t)b.dev.nfields * b.dev.pts;
+      if (e == cudaSuccess) e = cudaMalloc(&m.X, reg32);
+      if (e == cudaSuccess) e = cudaMalloc(&m.Y, reg32);
+      if (e == cudaSuccess && d.matter == CG_MATTER_DUST) {
+        const size_t fp = sizeof(float) * (size_t)cg::P_N * b.dev.pts;
+        e = cudaMalloc(&m.FP0, fp);
+        if (e == cudaSuccess) e = cudaMalloc(&m.FP1, fp);
+      }
+      for (double* p : {b.dev.P, b.dev.F})
+        if (e == cudaSuccess) e = cudaMemset(p, 0, reg);
     }
-    for (double* p : {b.dev.P, b.dev.F, b.dev.X, b.dev.Y})
-      if (e == cudaSuccess) e = cudaMemset(p, 0, reg);
     b.dev.status = ctx->status;
     b.needs_kavg = lapse_needs_kavg(d.lapse);
     if (e == cudaSuccess && b.needs_kavg) {
@@ -671,13 +832,32 @@ int cg_constraints(cg_ctx* ctx, int box, double* H, double* M, double* G, double
   // layout: cvals (10 n) | part1 (27 nblk1) | part2 (10 nblk2) | r1 (27) | r2 (10)
   const size_t need = (size_t)10 * n + 27 * (size_t)nblk1 + 10 * (size_t)nblk2 + 37;
   if (!b.cscratch) CG_CUDA(ctx, cudaMalloc(&b.cscratch, sizeof(double) * need));
+  cg::BoxDev dev = b.dev;
+  double* xtmp = nullptr;
+  if (b.mixed) {
+    // FP64 first-substep input of the current _p for the FP64 constraint pass
+    const size_t nx64 = (size_t)b.dev.nfields * n + (size_t)cg::P_N * n;
+    CG_CUDA(ctx, cudaMalloc(&xtmp, sizeof(double) * nx64));
+    dev.X = xtmp;
+    dev.FP0 = xtmp + (size_t)b.dev.nfields * n;
+    StageBg bg0 = bg_for(b, 1, b.frw.get_phi);
+    cudaError_t ei = cg::launch_init(cg::kExact, dev, bg0, ctx->stream);
+    if (ei != cudaSuccess) {
+      cudaFree(xtmp);
+      return cuda_fail(ctx, ei, "init");
+    }
+  }
   double* cvals = b.cscratch;
   double* part1 = cvals + (size_t)10 * n;
   double* part2 = part1 + (size_t)27 * nblk1;
   double* r1 = part2 + (size_t)10 * nblk2;
   double* r2 = r1 + 27;
   StageBg bg = bg_for(b, 1, b.frw.get_phi);
-  CG_CUDA(ctx, cg::exact::launch_constraints(b.dev, bg, cvals, part1, ctx->stream));
+  cudaError_t ec = cg::exact::launch_constraints(dev, bg, cvals, part1, ctx->stream);
+  if (ec != cudaSuccess) {
+    cudaFree(xtmp);
+    return cuda_fail(ctx, ec, "constraints");
+  }
   part_final_kernel<<<1, 256, 0, ctx->stream>>>(part1, nblk1, 27, 17, r1);
   constraint_stdev_kernel<<<nblk2, 256, 0, ctx->stream>>>(cvals, n, r1, part2);
   part_final_kernel<<<1, 256, 0, ctx->stream>>>(part2, nblk2, 10, 10, r2);
@@ -686,6 +866,7 @@ int cg_constraints(cg_ctx* ctx, int box, double* H, double* M, double* G, double
   CG_CUDA(ctx, cudaMemcpyAsync(h1, r1, sizeof(h1), cudaMemcpyDeviceToHost, ctx->stream));
   CG_CUDA(ctx, cudaMemcpyAsync(h2, r2, sizeof(h2), cudaMemcpyDeviceToHost, ctx->stream));
   CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  cudaFree(xtmp);
   // BSSN_NORMALIZE_MEAN / _STDEV and BSSN_STORE_CONSTRAINT_STAT_VARS (bssn_macros.h:539-560)
   double* outs[5] = {H, M, G, A, S};
   for (int c = 0; c < 5; ++c) {

@@ -23,6 +23,25 @@ struct BoxDev {
   const double* kavg;  // device K_avg for the lapses that use it, else null
 };
 
+// Device storage of one box evolved in the FP32-mixed form: FP64 _p and _f,
+// FP32 perturbation substep inputs and dust flux primitives.
+struct MixedBox {
+  int nx, ny, nz, pts, nfields, order, matter, lapse, normalize;
+  double dx, dt;
+  double* P;
+  double* F;
+  float* X;
+  float* Y;
+  float* FP0;
+  float* FP1;
+  unsigned* status;
+};
+namespace mixed {
+struct Bg;
+cudaError_t launch_stage(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st);
+cudaError_t launch_init(const MixedBox& b, const Bg& bg, cudaStream_t st);
+}  // namespace mixed
+
 // Kernel variants: identical source, compiled without (exact) or with (fast)
 // FMA contraction.
 enum Variant : int { kExact = 0, kFast = 1 };

@@ -1,0 +1,613 @@
+// cg_mixed.cuh -- the FP32-mixed RK4 substep kernel (BSSN + dust or vacuum).
+//
+// Same fused substep as cg_stage.cuh (sources, BSSN and dust right-hand
+// sides, RK4Register::K{n}Finalize, next-substep inputs) with a different
+// split of precision:
+//   * the substep inputs a^n are stored as FP32 perturbations
+//       delta_f = a_f - abar_f
+//     about a spatially uniform background abar (one value per field and
+//     substep) that the host integrates in FP64 with the same RK4 stages;
+//   * stencils and the right-hand side are evaluated in FP32 in perturbation
+//     form: the kernel computes RHS(abar + delta) - RHS(abar), and the host
+//     adds RHS(abar) in FP64.  Every term of the BSSN and dust equations is
+//     already first order in the perturbation except the zeroth-order parts
+//     of dK/dt, dphi/dt, dalpha/dt and the dust density source; those are
+//     expanded explicitly (e.g. alpha K^2 - abar Kbar^2 =
+//     abar (2 Kbar + dK) dK + dalpha K^2) so no FP32 cancellation occurs;
+//   * the RK registers _p and _f and the register update stay FP64.
+// The equations are the reference's (components/bssn/bssn.cc:361-831,
+// bssn_macros.h:221-385, components/dust_fluid/dust.cc:109-264) with a
+// trivial FRW reference (the dust driver's FRW(0,0), bssn.cc:25), harmonic or
+// static lapse, a_adj_amp = k_damping_amp = 0.
+#pragma once
+
+#include "cg_types.h"
+
+namespace cg {
+namespace mixed {
+
+constexpr int kBX = 4, kBY = 4, kBZ = 8, kThreads = kBX * kBY * kBZ;
+
+struct Ptrs {
+  const float* in;     // delta of a^n
+  const float* prev;   // delta of a^{n-1} (substeps 2-4)
+  const double* p;     // _p (FP64, full values)
+  double* f;           // _f (FP64)
+  double* newp;        // substep 4: the new _p (same block as p)
+  float* out;          // delta of a^{n+1}, or of the next step's a^1 at substep 4
+  const float* fp_in;  // dust flux primitives of a^n (FP32)
+  float* fp_out;       // flux primitives of the output state
+  unsigned* status;
+};
+
+// Uniform background of one substep (FP64, one value per field).
+struct Bg {
+  double in[23];     // abar of a^n
+  double prev[23];   // abar of a^{n-1}
+  double out[23];    // abar of the substep output
+  double rhs[23];    // RHS(abar of a^n), added to the kernel's perturbation RHS
+  double e6l;        // exp(-6 phibar) of the state whose W, sqrt(gamma) the sources lag on
+  double lambda;     // rho_Lambda
+};
+
+// per-thread FP32 slots (same meaning as the FP64 kernel's)
+enum : int {
+  S_DG = 0, S_T1 = 18, S_DPHI = 24, S_DDPHI = 27, S_DA = 33, S_DDA = 36, S_DK = 42,
+  S_DGAM = 45, S_SRC = 54, S_G = 65, S_MAT = 83, S_NSLOT = 87
+};
+
+__device__ __forceinline__ int wrapf(int v, int n) {
+  v = v < 0 ? v + n : v;
+  return v >= n ? v - n : v;
+}
+
+template <bool WRAP>
+struct Taps {
+  int i, j, k, nx, ny, nz, sx, sy, c;
+  __device__ __forceinline__ int at(int di, int dj, int dk) const {
+    if (!WRAP) return c + di * sx + dj * sy + dk;
+    return (wrapf(i + di, nx) * ny + wrapf(j + dj, ny)) * nz + wrapf(k + dk, nz);
+  }
+  __device__ __forceinline__ int ax(int a, int n) const {
+    return at(a == 0 ? n : 0, a == 1 ? n : 0, a == 2 ? n : 0);
+  }
+  __device__ __forceinline__ int pl(int a, int n, int b, int m) const {
+    return at((a == 0 ? n : 0) + (b == 0 ? m : 0), (a == 1 ? n : 0) + (b == 1 ? m : 0),
+              (a == 2 ? n : 0) + (b == 2 ? m : 0));
+  }
+};
+
+// FP32 centred stencils (utils/math.h:74-1085 coefficients)
+template <int O, class T>
+__device__ __forceinline__ float d1(const float* __restrict__ f, const T& t, int a, float idx) {
+  auto V = [&](int n) { return __ldg(f + t.ax(a, n)); };
+  float s;
+  if (O == 2) s = 0.5f * (V(1) - V(-1));
+  else if (O == 4) s = (2.0f / 3.0f) * (V(1) - V(-1)) - (1.0f / 12.0f) * (V(2) - V(-2));
+  else if (O == 6) s = 0.75f * (V(1) - V(-1)) - 0.15f * (V(2) - V(-2)) + (1.0f / 60.0f) * (V(3) - V(-3));
+  else s = 0.8f * (V(1) - V(-1)) - 0.2f * (V(2) - V(-2)) + (4.0f / 105.0f) * (V(3) - V(-3)) - (1.0f / 280.0f) * (V(4) - V(-4));
+  return s * idx;
+}
+template <int O, class T>
+__device__ __forceinline__ float d2(const float* __restrict__ f, const T& t, int a, float idx2) {
+  auto V = [&](int n) { return __ldg(f + t.ax(a, n)); };
+  float s;
+  if (O == 2) s = (V(1) + V(-1)) - 2.0f * V(0);
+  else if (O == 4) s = (4.0f / 3.0f) * (V(1) + V(-1)) - (1.0f / 12.0f) * (V(2) + V(-2)) - 2.5f * V(0);
+  else if (O == 6) s = 1.5f * (V(1) + V(-1)) - 0.15f * (V(2) + V(-2)) + (1.0f / 90.0f) * (V(3) + V(-3)) - (49.0f / 18.0f) * V(0);
+  else s = 1.6f * (V(1) + V(-1)) - 0.2f * (V(2) + V(-2)) + (8.0f / 315.0f) * (V(3) + V(-3)) - (1.0f / 560.0f) * (V(4) + V(-4)) - (205.0f / 72.0f) * V(0);
+  return s * idx2;
+}
+template <int O, class T>
+__device__ __forceinline__ float dm(const float* __restrict__ f, const T& t, int a, int b, float idx2) {
+  auto P = [&](int n) {
+    return (__ldg(f + t.pl(a, n, b, n)) + __ldg(f + t.pl(a, -n, b, -n))) -
+           (__ldg(f + t.pl(a, n, b, -n)) + __ldg(f + t.pl(a, -n, b, n)));
+  };
+  float s;
+  if (O == 2) s = 0.25f * P(1);
+  else if (O == 4) s = (1.0f / 3.0f) * P(1) - (1.0f / 48.0f) * P(2);
+  else if (O == 6) s = 0.375f * P(1) - 0.0375f * P(2) + (1.0f / 360.0f) * P(3);
+  else s = 0.4f * P(1) - 0.05f * P(2) + (2.0f / 315.0f) * P(3) - (1.0f / 2240.0f) * P(4);
+  return s * idx2;
+}
+template <int O, class T>
+__device__ __forceinline__ float d1p(const float* __restrict__ fa, const float* __restrict__ fb, const T& t, int a,
+                                     float idx) {
+  auto V = [&](int n) {
+    const int q = t.ax(a, n);
+    return __ldg(fa + q) * __ldg(fb + q);
+  };
+  float s;
+  if (O == 2) s = 0.5f * (V(1) - V(-1));
+  else if (O == 4) s = (2.0f / 3.0f) * (V(1) - V(-1)) - (1.0f / 12.0f) * (V(2) - V(-2));
+  else if (O == 6) s = 0.75f * (V(1) - V(-1)) - 0.15f * (V(2) - V(-2)) + (1.0f / 60.0f) * (V(3) - V(-3));
+  else s = 0.8f * (V(1) - V(-1)) - 0.2f * (V(2) - V(-2)) + (4.0f / 105.0f) * (V(3) - V(-3)) - (1.0f / 280.0f) * (V(4) - V(-4));
+  return s * idx;
+}
+
+__device__ __forceinline__ void inv_metricf(const float g[6], float gi[6]) {
+  gi[0] = 1.0f + g[3] + g[5] - g[4] * g[4] + g[3] * g[5];
+  gi[3] = 1.0f + g[0] + g[5] - g[2] * g[2] + g[0] * g[5];
+  gi[5] = 1.0f + g[0] + g[3] - g[1] * g[1] + g[0] * g[3];
+  gi[1] = g[2] * g[4] - g[1] * (1.0f + g[5]);
+  gi[2] = g[1] * g[4] - g[2] * (1.0f + g[3]);
+  gi[4] = g[1] * g[2] - g[4] * (1.0f + g[0]);
+}
+
+// W - 1 (as w2/(W+1), no cancellation) and v^i of Dust::getDustData (dust.cc:177-200)
+struct DustF {
+  float W, Wm1, w2, v[3];
+};
+__device__ __forceinline__ DustF dust_primf(const float gi[6], float em4, float e6, float D, const float S[3]) {
+  DustF d;
+  d.w2 = em4 * (gi[0] * S[0] * S[0] + gi[3] * S[1] * S[1] + gi[5] * S[2] * S[2] +
+                2.0f * (gi[1] * S[0] * S[1] + gi[2] * S[0] * S[2] + gi[4] * S[1] * S[2])) / (D * D);
+  d.W = sqrtf(1.0f + d.w2);
+  d.Wm1 = d.w2 / (d.W + 1.0f);
+  const float c = em4 / e6;
+  d.v[0] = c * (gi[0] * S[0] + gi[1] * S[1] + gi[2] * S[2]);
+  d.v[1] = c * (gi[1] * S[0] + gi[3] * S[1] + gi[4] * S[2]);
+  d.v[2] = c * (gi[2] * S[0] + gi[4] * S[1] + gi[5] * S[2]);
+  return d;
+}
+
+template <int O, int MATTER, class T>
+__device__ __forceinline__ void derivatives(const T& t, const float* __restrict__ a, const float* __restrict__ fp,
+                                            int N, float idx, float idx2, const float gi[6], float* sl) {
+#pragma unroll 1
+  for (int it = 0; it < 8; ++it) {
+    const int fld = it < 6 ? F_G11 + it : (it == 6 ? F_PHI : F_ALPHA);
+    const float* __restrict__ f = a + (size_t)fld * N;
+    const float g1 = d1<O>(f, t, 0, idx), g2 = d1<O>(f, t, 1, idx), g3 = d1<O>(f, t, 2, idx);
+    const float h11 = d2<O>(f, t, 0, idx2), h22 = d2<O>(f, t, 1, idx2), h33 = d2<O>(f, t, 2, idx2);
+    const float h12 = dm<O>(f, t, 0, 1, idx2), h13 = dm<O>(f, t, 0, 2, idx2), h23 = dm<O>(f, t, 1, 2, idx2);
+    if (it < 6) {
+      sl[(S_DG + 0 * 6 + it) * kThreads] = g1;
+      sl[(S_DG + 1 * 6 + it) * kThreads] = g2;
+      sl[(S_DG + 2 * 6 + it) * kThreads] = g3;
+      sl[(S_T1 + it) * kThreads] =
+          gi[0] * h11 + gi[3] * h22 + gi[5] * h33 + 2.0f * (gi[1] * h12 + gi[2] * h13 + gi[4] * h23);
+    } else {
+      const int b1 = it == 6 ? S_DPHI : S_DA, b2 = it == 6 ? S_DDPHI : S_DDA;
+      sl[(b1 + 0) * kThreads] = g1;
+      sl[(b1 + 1) * kThreads] = g2;
+      sl[(b1 + 2) * kThreads] = g3;
+      sl[(b2 + 0) * kThreads] = h11;
+      sl[(b2 + 1) * kThreads] = h12;
+      sl[(b2 + 2) * kThreads] = h13;
+      sl[(b2 + 3) * kThreads] = h22;
+      sl[(b2 + 4) * kThreads] = h23;
+      sl[(b2 + 5) * kThreads] = h33;
+    }
+  }
+#pragma unroll 1
+  for (int it = 0; it < 4; ++it) {
+    const int fld = it == 0 ? F_K : F_GAM1 + it - 1;
+    const float* __restrict__ f = a + (size_t)fld * N;
+    const int b = it == 0 ? S_DK : S_DGAM + 3 * (it - 1);
+    sl[(b + 0) * kThreads] = d1<O>(f, t, 0, idx);
+    sl[(b + 1) * kThreads] = d1<O>(f, t, 1, idx);
+    sl[(b + 2) * kThreads] = d1<O>(f, t, 2, idx);
+  }
+  if (MATTER == kDust) {
+    const float* v1 = fp + (size_t)P_V1 * N;
+    const float* v2 = fp + (size_t)P_V2 * N;
+    const float* v3 = fp + (size_t)P_V3 * N;
+#pragma unroll 1
+    for (int m = 0; m < 4; ++m) {
+      const float* u = fp + (size_t)(P_AD + m) * N;
+      sl[(S_MAT + m) * kThreads] = d1p<O>(u, v1, t, 0, idx) + d1p<O>(u, v2, t, 1, idx) + d1p<O>(u, v3, t, 2, idx);
+    }
+  }
+}
+
+template <int O, int MATTER>
+__global__ void __launch_bounds__(kThreads, 4)
+mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt, Bg bg, Ptrs P, int stage) {
+  constexpr int NFLD = MATTER == kDust ? 22 : 18;
+  constexpr int R = O / 2;
+  constexpr float kPif = 3.14159265358979f;
+  extern __shared__ float smf[];
+  const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
+  float* sl = smf + tid;
+  auto S = [&](int s) -> float& { return sl[s * kThreads]; };
+  const int k = blockIdx.x * kBZ + threadIdx.x;
+  const int j = blockIdx.y * kBY + threadIdx.y;
+  const int i = blockIdx.z * kBX + threadIdx.z;
+  if (i >= nx || j >= ny || k >= nz) return;
+  const int N = nx * ny * nz;
+  const int c = (i * ny + j) * nz + k;
+  const float* __restrict__ a = P.in;
+  auto D_ = [&](int f) { return a[(size_t)f * N + c]; };  // delta at the centre
+
+  float g[6], gi[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) g[q] = D_(F_G11 + q);
+  inv_metricf(g, gi);
+
+  const int x0 = blockIdx.z * kBX, y0 = blockIdx.y * kBY, z0 = blockIdx.x * kBZ;
+  const bool interior = x0 >= R && x0 + kBX + R <= nx && y0 >= R && y0 + kBY + R <= ny && z0 >= R && z0 + kBZ + R <= nz;
+  const float idx2 = idx * idx;
+  if (interior) {
+    const Taps<false> t{i, j, k, nx, ny, nz, ny * nz, nz, c};
+    derivatives<O, MATTER>(t, a, P.fp_in, N, idx, idx2, gi, sl);
+  } else {
+    const Taps<true> t{i, j, k, nx, ny, nz, ny * nz, nz, c};
+    derivatives<O, MATTER>(t, a, P.fp_in, N, idx, idx2, gi, sl);
+  }
+
+  // ---- centre values: perturbations and full values -------------------------
+  const float dphi0 = D_(F_PHI), dK = D_(F_K), dal = D_(F_ALPHA);
+  const float phib = (float)bg.in[F_PHI], Kb = (float)bg.in[F_K], alb = (float)(1.0 + bg.in[F_ALPHA]);
+  const float phi = phib + dphi0, K = Kb + dK, alpha = alb + dal;
+  float gm[6];
+  gm[0] = g[0] + 1.0f; gm[1] = g[1]; gm[2] = g[2];
+  gm[3] = g[3] + 1.0f; gm[4] = g[4]; gm[5] = g[5] + 1.0f;
+  const float em4phi = __expf(-4.0f * phi);
+
+  // ---- dust sources in perturbation form ---------------------------------------
+  float rhs_m[4] = {0.f, 0.f, 0.f, 0.f};
+  float dr = 0.f, Sdust = 0.f, rS_full = 0.f;  // delta rho, S (second order), full rho + S
+  if (MATTER == kDust) {
+    const float Db = (float)bg.in[F_D];
+    const float D = Db + D_(F_D);
+    const float Sv[3] = {D_(F_S1), D_(F_S2), D_(F_S3)};
+    // lagged W, sqrt(gamma), g_ij (Dust::addBSSNSrc, dust.cc:226-264)
+    float gl[6], gil[6], dphil, phil, Dl, Sl[3];
+    if (stage == 1) {
+#pragma unroll
+      for (int m = 0; m < 6; ++m) { gl[m] = g[m]; gil[m] = gi[m]; }
+      dphil = dphi0; phil = phi; Dl = D;
+      Sl[0] = Sv[0]; Sl[1] = Sv[1]; Sl[2] = Sv[2];
+    } else {
+      const float* pv = P.prev;
+#pragma unroll
+      for (int m = 0; m < 6; ++m) gl[m] = pv[(size_t)(F_G11 + m) * N + c];
+      inv_metricf(gl, gil);
+      dphil = pv[(size_t)F_PHI * N + c];
+      phil = (float)bg.prev[F_PHI] + dphil;
+      Dl = (float)bg.prev[F_D] + pv[(size_t)F_D * N + c];
+      Sl[0] = pv[(size_t)F_S1 * N + c]; Sl[1] = pv[(size_t)F_S2 * N + c]; Sl[2] = pv[(size_t)F_S3 * N + c];
+    }
+    const float em4l = __expf(-4.0f * phil), e6l = __expf(6.0f * phil), e4l = __expf(4.0f * phil);
+    const DustF dl = dust_primf(gil, em4l, e6l, Dl, Sl);
+    const float e6bl = (float)bg.e6l;  // exp(-6 phibar_lag)
+    // rho = W D / sqrt(gamma); rhobar = Dbar exp(-6 phibar_lag)
+    dr = e6bl * (dl.W * D * expm1f(-6.0f * dphil) + dl.Wm1 * D + D_(F_D));
+    const float inv_detg = 1.0f / e6l;
+    Sdust = D * inv_detg * dl.w2 / dl.W;
+    rS_full = (float)(bg.in[F_D] * bg.e6l) + dr + Sdust - 2.0f * (float)bg.lambda;
+    S(S_SRC + Q_R) = dr;
+    S(S_SRC + Q_S) = Sdust;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) S(S_SRC + Q_S1 + m) = Sv[m] * inv_detg;
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int J = I; J < 3; ++J)
+        S(S_SRC + Q_STF11 + sym(I, J)) = Sv[I] * Sv[J] / (dl.W * D) * inv_detg - (1.0f / 3.0f) * (e4l * (gl[sym(I, J)] + (I == J ? 1.0f : 0.0f))) * Sdust;
+    // dust RHS: divergence + momentum source with the current W, v (dust.cc:135-146)
+    const DustF cur = dust_primf(gi, em4phi, __expf(6.0f * phi), D, Sv);
+    const float e4 = __expf(4.0f * phi);
+    rhs_m[0] = S(S_MAT + 0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float dp = S(S_DPHI + d);
+      auto DG = [&](int qq) { return S(S_DG + 6 * d + qq); };
+      const float src =
+          0.5f * alpha * cur.W * D * e4 *
+              (cur.v[0] * cur.v[0] * (4.0f * gm[0] * dp + DG(0)) + cur.v[1] * cur.v[1] * (4.0f * gm[3] * dp + DG(3)) +
+               cur.v[2] * cur.v[2] * (4.0f * gm[5] * dp + DG(5)) +
+               2.0f * (cur.v[0] * cur.v[1] * (4.0f * gm[1] * dp + DG(1)) + cur.v[0] * cur.v[2] * (4.0f * gm[2] * dp + DG(2)) +
+                       cur.v[1] * cur.v[2] * (4.0f * gm[4] * dp + DG(4)))) -
+          cur.W * D * S(S_DA + d);
+      rhs_m[1 + d] = S(S_MAT + 1 + d) + src;
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < Q_N; ++m) S(S_SRC + m) = 0.f;
+  }
+
+  // ---- Christoffels, D_iD_j phi, (D_iD_j alpha)^TF, Ricci (first order) ---------
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = 0; J < 3; ++J)
+#pragma unroll
+      for (int Kx = J; Kx < 3; ++Kx) {
+        auto dg = [&](int d, int qq) { return S(S_DG + 6 * d + qq); };
+        S(S_G + 6 * I + sym(J, Kx)) =
+            0.5f * (gi[sym(I, 0)] * (dg(J, sym(Kx, 0)) + dg(Kx, sym(J, 0)) - dg(0, sym(J, Kx))) +
+                    gi[sym(I, 1)] * (dg(J, sym(Kx, 1)) + dg(Kx, sym(J, 1)) - dg(1, sym(J, Kx))) +
+                    gi[sym(I, 2)] * (dg(J, sym(Kx, 2)) + dg(Kx, sym(J, 2)) - dg(2, sym(J, Kx))));
+      }
+  {
+    float GLv[3][6];
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int J = 0; J < 3; ++J)
+#pragma unroll
+        for (int Kx = J; Kx < 3; ++Kx) {
+          auto dg = [&](int d, int qq) { return S(S_DG + 6 * d + qq); };
+          GLv[I][sym(J, Kx)] = 0.5f * (dg(J, sym(Kx, I)) + dg(Kx, sym(J, I)) - dg(I, sym(J, Kx)));
+        }
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int qq = 0; qq < 6; ++qq) S(S_DG + 6 * I + qq) = GLv[I][qq];
+  }
+  auto G = [&](int I, int qq) { return S(S_G + 6 * I + qq); };
+  auto GL = [&](int I, int qq) { return S(S_DG + 6 * I + qq); };
+  float Gd[3];
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+    Gd[I] = G(I, 0) * gi[0] + G(I, 3) * gi[3] + G(I, 5) * gi[5] + 2.0f * (G(I, 1) * gi[1] + G(I, 2) * gi[2] + G(I, 4) * gi[4]);
+  float dphi[3], da[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) { dphi[d] = S(S_DPHI + d); da[d] = S(S_DA + d); }
+  float DDa[6], gld[3];
+#pragma unroll
+  for (int I = 0; I < 3; ++I) gld[I] = gi[sym(I, 0)] * dphi[0] + gi[sym(I, 1)] * dphi[1] + gi[sym(I, 2)] * dphi[2];
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = I; J < 3; ++J) {
+      const int qq = sym(I, J);
+      S(S_DDPHI + qq) = S(S_DDPHI + qq) - (G(0, qq) * dphi[0] + G(1, qq) * dphi[1] + G(2, qq) * dphi[2]);
+      float t = 0.f;
+#pragma unroll
+      for (int L = 0; L < 3; ++L)
+        t += (G(L, qq) + 2.0f * ((L == I ? dphi[J] : 0.f) + (L == J ? dphi[I] : 0.f) - gm[qq] * gld[L])) * da[L];
+      DDa[qq] = S(S_DDA + qq) - t;
+    }
+  float DDaTR = gi[0] * DDa[0] + gi[3] * DDa[3] + gi[5] * DDa[5] + 2.0f * (gi[1] * DDa[1] + gi[2] * DDa[2] + gi[4] * DDa[4]);
+#pragma unroll
+  for (int m = 0; m < 6; ++m) S(S_DDA + m) = DDa[m] - (1.0f / 3.0f) * gm[m] * DDaTR;
+  DDaTR *= em4phi;
+  auto DDphi = [&](int qq) { return S(S_DDPHI + qq); };
+  const float expression =
+      gi[0] * (DDphi(0) + 2.0f * dphi[0] * dphi[0]) + gi[3] * (DDphi(3) + 2.0f * dphi[1] * dphi[1]) +
+      gi[5] * (DDphi(5) + 2.0f * dphi[2] * dphi[2]) +
+      2.0f * (gi[1] * (DDphi(1) + 2.0f * dphi[0] * dphi[1]) + gi[2] * (DDphi(2) + 2.0f * dphi[0] * dphi[2]) +
+              gi[4] * (DDphi(4) + 2.0f * dphi[1] * dphi[2]));
+  float t4[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int Kx = 0; Kx < 3; ++Kx)
+#pragma unroll
+    for (int L = 0; L < 3; ++L)
+#pragma unroll
+      for (int M = 0; M < 3; ++M) {
+        const float gLM = gi[sym(L, M)];
+        float GKL[3], GLKM[3], GKM[3], GLKL[3];
+#pragma unroll
+        for (int X = 0; X < 3; ++X) {
+          GKL[X] = G(Kx, sym(L, X));
+          GLKM[X] = GL(X, sym(Kx, M));
+          GKM[X] = G(Kx, sym(X, M));
+          GLKL[X] = GL(Kx, sym(L, X));
+        }
+#pragma unroll
+        for (int I = 0; I < 3; ++I)
+#pragma unroll
+          for (int J = I; J < 3; ++J)
+            t4[sym(I, J)] += gLM * (GKL[I] * GLKM[J] + GKL[J] * GLKM[I] + 0.5f * (GKM[I] * GLKL[J] + GKM[J] * GLKL[I]));
+      }
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = I; J < 3; ++J) {
+      const int ij = sym(I, J);
+      auto dGam = [&](int Jx, int Kx) { return S(S_DGAM + 3 * Kx + Jx); };
+      const float t2 = gm[sym(0, I)] * dGam(J, 0) + gm[sym(1, I)] * dGam(J, 1) + gm[sym(2, I)] * dGam(J, 2) +
+                       gm[sym(0, J)] * dGam(I, 0) + gm[sym(1, J)] * dGam(I, 1) + gm[sym(2, J)] * dGam(I, 2);
+      const float t3 = Gd[0] * (GL(I, sym(J, 0)) + GL(J, sym(I, 0))) + Gd[1] * (GL(I, sym(J, 1)) + GL(J, sym(I, 1))) +
+                       Gd[2] * (GL(I, sym(J, 2)) + GL(J, sym(I, 2)));
+      const float U = -0.5f * S(S_T1 + ij) + 0.5f * t2 + 0.5f * t3 + t4[ij];
+      S(S_T1 + ij) = U - 2.0f * (DDphi(ij) - 2.0f * dphi[I] * dphi[J] + gm[ij] * expression);
+    }
+  auto Ric = [&](int qq) { return S(S_T1 + qq); };
+  const float ricci = em4phi * (Ric(0) * gi[0] + Ric(3) * gi[3] + Ric(5) * gi[5] + 2.0f * (Ric(1) * gi[1] + Ric(2) * gi[2] + Ric(4) * gi[4]));
+  const float e4phi = __expf(4.0f * phi);
+  float A[6], Ac[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) A[q] = D_(F_A11 + q);
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = I; J < 3; ++J) {
+      float t = 0.f;
+#pragma unroll
+      for (int X = 0; X < 3; ++X)
+#pragma unroll
+        for (int Y = 0; Y < 3; ++Y) t += gi[sym(I, X)] * gi[sym(J, Y)] * A[sym(X, Y)];
+      Ac[sym(I, J)] = t;
+    }
+  const float AijAij = Ac[0] * A[0] + Ac[3] * A[3] + Ac[5] * A[5] + 2.0f * (Ac[1] * A[1] + Ac[2] * A[2] + Ac[4] * A[4]);
+
+  // ---- perturbation right-hand sides + FP64 register update ----------------------
+  double outv[NFLD];
+  auto finalize = [&](int fld, float drhs) {
+    const double cv = bg.rhs[fld] + (double)drhs;
+    const double pv = P.p[(size_t)fld * N + c];
+    double o;
+    if (stage == 1) {
+      P.f[(size_t)fld * N + c] = dt * cv / 6.0;
+      o = pv + dt * cv / 2.0;
+    } else if (stage == 2) {
+      const double fv = P.f[(size_t)fld * N + c];
+      P.f[(size_t)fld * N + c] = fv + dt * cv / 3.0;
+      o = pv + dt * cv / 2.0;
+    } else if (stage == 3) {
+      const double fv = P.f[(size_t)fld * N + c];
+      P.f[(size_t)fld * N + c] = fv + dt * cv / 3.0;
+      o = pv + dt * cv;
+    } else {
+      const double fv = P.f[(size_t)fld * N + c];
+      o = fv + (dt * cv / 6.0 + pv);
+      P.newp[(size_t)fld * N + c] = o;
+    }
+    outv[fld] = o;
+  };
+#pragma unroll
+  for (int m = 0; m < 6; ++m) finalize(F_G11 + m, -2.0f * alpha * A[m]);
+#pragma unroll
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = I; J < 3; ++J) {
+      const int qq = sym(I, J);
+      float aa = 0.f;
+#pragma unroll
+      for (int X = 0; X < 3; ++X)
+#pragma unroll
+        for (int Y = 0; Y < 3; ++Y) aa += gi[sym(X, Y)] * A[sym(X, I)] * A[sym(Y, J)];
+      const float RTF = Ric(qq) - (1.0f / 3.0f) * e4phi * gm[qq] * ricci;
+      finalize(F_A11 + qq, em4phi * (alpha * (RTF - 8.0f * kPif * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
+                               alpha * (K * A[qq] - 2.0f * aa));
+    }
+#pragma unroll
+  for (int I = 0; I < 3; ++I) {
+    const float so = G(I, 0) * Ac[0] + G(I, 3) * Ac[3] + G(I, 5) * Ac[5] + 2.0f * (G(I, 1) * Ac[1] + G(I, 2) * Ac[2] + G(I, 4) * Ac[4]) +
+                     6.0f * (Ac[sym(I, 0)] * dphi[0] + Ac[sym(I, 1)] * dphi[1] + Ac[sym(I, 2)] * dphi[2]);
+    const float gdK = gi[sym(I, 0)] * S(S_DK + 0) + gi[sym(I, 1)] * S(S_DK + 1) + gi[sym(I, 2)] * S(S_DK + 2);
+    const float gS = gi[sym(I, 0)] * S(S_SRC + Q_S1) + gi[sym(I, 1)] * S(S_SRC + Q_S2) + gi[sym(I, 2)] * S(S_SRC + Q_S3);
+    finalize(F_GAM1 + I, -2.0f * (Ac[sym(I, 0)] * da[0] + Ac[sym(I, 1)] * da[1] + Ac[sym(I, 2)] * da[2]) +
+                             2.0f * alpha * (so - (2.0f / 3.0f) * gdK - 8.0f * kPif * gS));
+  }
+  // zeroth-order equations in explicit perturbation form
+  const float dRK = -DDaTR + (alb * (2.0f * Kb + dK) * dK + dal * K * K) * (1.0f / 3.0f) + alpha * AijAij +
+                    4.0f * kPif * (alb * (dr + Sdust) + dal * rS_full);
+  finalize(F_K, dRK);
+  finalize(F_PHI, -(1.0f / 6.0f) * (alb * dK + dal * K));
+  finalize(F_ALPHA, lapse == kHarmonic ? -(alb * dK + dal * K) : 0.0f);
+  if (MATTER == kDust) {
+#pragma unroll
+    for (int m = 0; m < 4; ++m) finalize(F_D + m, rhs_m[m]);
+  }
+
+  if (stage == 4) {
+    bool bad_any = false;
+#pragma unroll
+    for (int f = 0; f < NFLD; ++f) bad_any |= !isfinite(outv[f]);
+    if (bad_any) {
+      if (isnan(outv[F_PHI])) atomicOr(P.status, 1u);
+      atomicOr(P.status, 2u);
+    }
+    // the next step's first-substep input is the normalised new state (bssn.cc:224-225)
+    if (normalize) {
+    double gn[6], An[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) { gn[m] = outv[F_G11 + m]; An[m] = outv[F_A11 + m]; }
+    {
+      double omd = -1.0 * (gn[0] + gn[3] + gn[5] - gn[1] * gn[1] - gn[2] * gn[2] - gn[4] * gn[4] + gn[0] * gn[3] +
+                           gn[0] * gn[5] + gn[3] * gn[5] - gn[4] * gn[4] * gn[0] - gn[2] * gn[2] * gn[3] -
+                           gn[1] * gn[1] * gn[5] + 2.0 * gn[1] * gn[2] * gn[4] + gn[0] * gn[3] * gn[5]);
+      const double tt = -1.0 * expm1(log1p(-1.0 * omd) / 3.0);
+      const double inv = 1.0 / (1.0 - tt);
+      gn[0] = (gn[0] + tt) * inv; gn[3] = (gn[3] + tt) * inv; gn[5] = (gn[5] + tt) * inv;
+      gn[1] *= inv; gn[2] *= inv; gn[4] *= inv;
+      double gin[6];
+      gin[0] = 1.0 + gn[3] + gn[5] - gn[4] * gn[4] + gn[3] * gn[5];
+      gin[3] = 1.0 + gn[0] + gn[5] - gn[2] * gn[2] + gn[0] * gn[5];
+      gin[5] = 1.0 + gn[0] + gn[3] - gn[1] * gn[1] + gn[0] * gn[3];
+      gin[1] = gn[2] * gn[4] - gn[1] * (1.0 + gn[5]);
+      gin[2] = gn[1] * gn[4] - gn[2] * (1.0 + gn[3]);
+      gin[4] = gn[1] * gn[2] - gn[4] * (1.0 + gn[0]);
+      const double trA = gin[0] * An[0] + gin[3] * An[3] + gin[5] * An[5] + 2.0 * (gin[1] * An[1] + gin[2] * An[2] + gin[4] * An[4]);
+      An[0] = (An[0] - 1.0 / 3.0 * (1.0 + gn[0]) * trA) * inv;
+      An[3] = (An[3] - 1.0 / 3.0 * (1.0 + gn[3]) * trA) * inv;
+      An[5] = (An[5] - 1.0 / 3.0 * (1.0 + gn[5]) * trA) * inv;
+      An[1] = (An[1] - 1.0 / 3.0 * gn[1] * trA) * inv;
+      An[2] = (An[2] - 1.0 / 3.0 * gn[2] * trA) * inv;
+      An[4] = (An[4] - 1.0 / 3.0 * gn[4] * trA) * inv;
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) { outv[F_G11 + m] = gn[m]; outv[F_A11 + m] = An[m]; }
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < NFLD; ++f) P.out[(size_t)f * N + c] = (float)(outv[f] - bg.out[f]);
+  if (MATTER == kDust) {
+    float go[6], gio[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) go[m] = (float)outv[F_G11 + m];
+    inv_metricf(go, gio);
+    const float So[3] = {(float)outv[F_S1], (float)outv[F_S2], (float)outv[F_S3]};
+    const float phio = (float)outv[F_PHI];
+    const float Do = (float)outv[F_D];
+    const DustF dp = dust_primf(gio, __expf(-4.0f * phio), __expf(6.0f * phio), Do, So);
+    const float alo = (float)(outv[F_ALPHA] + 1.0);
+    float* fo = P.fp_out;
+    fo[(size_t)P_AD * N + c] = alo * Do;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) fo[(size_t)(P_AS1 + m) * N + c] = alo * So[m];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) fo[(size_t)(P_V1 + m) * N + c] = dp.v[m];
+  }
+}
+
+// first-substep input of a step: normalised _p minus the background, FP32;
+// dust flux primitives of that state
+template <int MATTER>
+__global__ void __launch_bounds__(kThreads) mixed_init_kernel(int nx, int ny, int nz, int normalize, Bg bg,
+                                                              const double* Pp, float* X, float* FP0) {
+  constexpr int NFLD = MATTER == kDust ? 22 : 18;
+  const int k = blockIdx.x * kBZ + threadIdx.x;
+  const int j = blockIdx.y * kBY + threadIdx.y;
+  const int i = blockIdx.z * kBX + threadIdx.z;
+  if (i >= nx || j >= ny || k >= nz) return;
+  const int N = nx * ny * nz;
+  const int c = (i * ny + j) * nz + k;
+  double v[NFLD];
+#pragma unroll
+  for (int f = 0; f < NFLD; ++f) v[f] = Pp[(size_t)f * N + c];
+  double gn[6], An[6];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) { gn[m] = v[F_G11 + m]; An[m] = v[F_A11 + m]; }
+  if (normalize) {
+    double omd = -1.0 * (gn[0] + gn[3] + gn[5] - gn[1] * gn[1] - gn[2] * gn[2] - gn[4] * gn[4] + gn[0] * gn[3] +
+                         gn[0] * gn[5] + gn[3] * gn[5] - gn[4] * gn[4] * gn[0] - gn[2] * gn[2] * gn[3] -
+                         gn[1] * gn[1] * gn[5] + 2.0 * gn[1] * gn[2] * gn[4] + gn[0] * gn[3] * gn[5]);
+    const double tt = -1.0 * expm1(log1p(-1.0 * omd) / 3.0);
+    const double inv = 1.0 / (1.0 - tt);
+    gn[0] = (gn[0] + tt) * inv; gn[3] = (gn[3] + tt) * inv; gn[5] = (gn[5] + tt) * inv;
+    gn[1] *= inv; gn[2] *= inv; gn[4] *= inv;
+    double gin[6];
+    gin[0] = 1.0 + gn[3] + gn[5] - gn[4] * gn[4] + gn[3] * gn[5];
+    gin[3] = 1.0 + gn[0] + gn[5] - gn[2] * gn[2] + gn[0] * gn[5];
+    gin[5] = 1.0 + gn[0] + gn[3] - gn[1] * gn[1] + gn[0] * gn[3];
+    gin[1] = gn[2] * gn[4] - gn[1] * (1.0 + gn[5]);
+    gin[2] = gn[1] * gn[4] - gn[2] * (1.0 + gn[3]);
+    gin[4] = gn[1] * gn[2] - gn[4] * (1.0 + gn[0]);
+    const double trA = gin[0] * An[0] + gin[3] * An[3] + gin[5] * An[5] + 2.0 * (gin[1] * An[1] + gin[2] * An[2] + gin[4] * An[4]);
+    An[0] = (An[0] - 1.0 / 3.0 * (1.0 + gn[0]) * trA) * inv;
+    An[3] = (An[3] - 1.0 / 3.0 * (1.0 + gn[3]) * trA) * inv;
+    An[5] = (An[5] - 1.0 / 3.0 * (1.0 + gn[5]) * trA) * inv;
+    An[1] = (An[1] - 1.0 / 3.0 * gn[1] * trA) * inv;
+    An[2] = (An[2] - 1.0 / 3.0 * gn[2] * trA) * inv;
+    An[4] = (An[4] - 1.0 / 3.0 * gn[4] * trA) * inv;
+  }
+#pragma unroll
+  for (int m = 0; m < 6; ++m) { v[F_G11 + m] = gn[m]; v[F_A11 + m] = An[m]; }
+#pragma unroll
+  for (int f = 0; f < NFLD; ++f) X[(size_t)f * N + c] = (float)(v[f] - bg.in[f]);
+  if (MATTER == kDust) {
+    float go[6], gio[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) go[m] = (float)v[F_G11 + m];
+    inv_metricf(go, gio);
+    const float So[3] = {(float)v[F_S1], (float)v[F_S2], (float)v[F_S3]};
+    const float phio = (float)v[F_PHI];
+    const DustF dp = dust_primf(gio, __expf(-4.0f * phio), __expf(6.0f * phio), (float)v[F_D], So);
+    const float alo = (float)(v[F_ALPHA] + 1.0);
+    FP0[(size_t)P_AD * N + c] = alo * (float)v[F_D];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) FP0[(size_t)(P_AS1 + m) * N + c] = alo * So[m];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) FP0[(size_t)(P_V1 + m) * N + c] = dp.v[m];
+  }
+}
+
+}  // namespace mixed
+}  // namespace cg

@@ -1,0 +1,66 @@
+"""The FP32-mixed substep kernel against the FP64 GPU path.
+
+Accuracy is stated relative to the perturbation: for each field,
+max|mixed - fp64| / max|fp64 - mean(fp64)| (the spread of the field about its
+mean).  Fields whose perturbation vanishes identically are skipped.
+"""
+import numpy as np
+import pytest
+
+from cosmograph_b200 import ics, state as S
+from cosmograph_b200.evolution import BoxConfig, Evolution, evolve
+
+pytestmark = pytest.mark.gpu
+
+
+def perturbation_errors(got, ref, names):
+    out = {}
+    for f, n in enumerate(names):
+        spread = float(np.abs(ref[f] - ref[f].mean()).max())
+        if spread == 0.0:
+            continue
+        out[n] = float(np.abs(got[f] - ref[f]).max()) / spread
+    return out
+
+
+def test_uniform_box_follows_the_background():
+    st = ics.perturbed((16, 16, 16), S.DUST, amp=0.0)
+    a = evolve(st, 20, BoxConfig(order=8, precision="mixed"))
+    b = evolve(st, 20, BoxConfig(order=8, precision="fp64"))
+    for f in range(a.fields.shape[0]):
+        assert np.ptp(a.fields[f]) == 0.0
+    rel = np.abs(a.fields - b.fields).max(axis=(1, 2, 3)) / np.maximum(np.abs(b.fields).max(axis=(1, 2, 3)), 1e-300)
+    assert rel.max() < 1e-13
+
+
+@pytest.mark.parametrize("order,steps", [(4, 60), (8, 40)])
+def test_grf_dust_against_fp64(order, steps):
+    st = ics.grf_dust(32, seed=11, rms_delta=1e-4, order=order)
+    a = evolve(st, steps, BoxConfig(order=order, precision="mixed"))
+    b = evolve(st, steps, BoxConfig(order=order, precision="fp64"))
+    errs = perturbation_errors(a.fields, b.fields, st.names)
+    worst = max(errs, key=errs.get)
+    print("mixed vs fp64, worst field", worst, errs[worst])
+    assert errs[worst] < 1e-4, errs
+
+
+def test_hamiltonian_constraint_no_worse_than_twice_fp64():
+    st = ics.grf_dust(32, seed=12, rms_delta=1e-4, order=4)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        with Evolution(st, BoxConfig(order=4, precision=prec)) as ev:
+            ev.step(40)
+            res[prec] = ev.constraints(0)
+    h64, hmx = res["fp64"]["H"][7], res["mixed"]["H"][7]
+    print("H L2: fp64", h64, "mixed", hmx)
+    assert hmx <= 2.0 * h64
+
+
+def test_vacuum_mixed_runs_and_rejects_unsupported():
+    st = ics.perturbed((16, 16, 16), S.VACUUM, amp=1e-3)
+    a = evolve(st, 5, BoxConfig(order=4, precision="mixed"))
+    b = evolve(st, 5, BoxConfig(order=4, precision="fp64"))
+    errs = perturbation_errors(a.fields, b.fields, st.names)
+    assert max(errs.values()) < 1e-4
+    with pytest.raises(RuntimeError, match="mixed"):
+        evolve(ics.perturbed((16, 16, 16), S.SCALAR), 1, BoxConfig(order=4, precision="mixed"))
