@@ -4,8 +4,11 @@ Workload (default): one periodic BSSN + pressureless-dust box of 256^3 points
 per GPU, 8th-order stencils, harmonic lapse, FP64 (reference operand order).
 A "step" is one full RK4 step (4 fused substep launches) of that box; each
 rank evolves its own box (independent replicas, weak scaling).  Inputs are
-synthetic: a smooth random perturbation of every field (the kernels have no
-data-dependent control flow, so cost does not depend on the values).
+synthetic: the seeded Gaussian-random-field dust initial data (rms density
+contrast 1e-4, P(k) ~ k^0.96 with a Gaussian cutoff at N/4, synchronous gauge,
+constraint-satisfying), generated on the host.  The other precisions of the
+same kernel (fp64_fma, mixed) are timed on the same box and state their field
+and Hamiltonian-constraint error against the FP64 run after the same steps.
 
 Printed JSON (rank 0, one line): value = whole-job updates/s with the state
 resident in HBM; e2e = the same through the C ABI with the full state copied
@@ -38,6 +41,16 @@ sys.path.insert(0, str(ROOT))
 # reference's lagged dust quantities W, sqrt(gamma), g_ij (8 values written at
 # substeps 1-3 and read at 2-4, 48 values): 422 values = 3376 bytes.
 ALGO_BYTES_PER_UPDATE = {"dust": 3376, "scalar": 3128, "vacuum": 17 * 18 * 8}
+# FP32-mixed layout, same counting rule: per field the stage inputs a are FP32
+# (substep 1: p 8 + f 8 + a 4; substeps 2-3: a 4 + p 8 + f 8 + f 8 + a 4;
+# substep 4: a 4 + p 8 + f 8 + p 8 = 112 B) and the lagged dust quantities
+# are recomputed from the previous substep's FP32 input (11 values read at
+# substeps 2-4): 22 * 112 + 3 * 11 * 4 = 2596 bytes.
+ALGO_BYTES_MIXED_DUST = 22 * 112 + 3 * 11 * 4
+
+
+def algo_bytes(precision: str) -> int:
+    return ALGO_BYTES_MIXED_DUST if precision == "mixed" else ALGO_BYTES_PER_UPDATE["dust"]
 
 
 def parse():
@@ -125,10 +138,30 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def make_state(n: int, seed: int):
-    from cosmograph_b200 import ics, state as S
+def make_state(n: int, seed: int, order: int):
+    from cosmograph_b200 import ics
 
-    return ics.perturbed((n, n, n), S.DUST, seed=seed, amp=1e-2)
+    return ics.grf_dust(n, seed=seed, rms_delta=1.0e-4, order=order)
+
+
+def accuracy(ref, got, h_ref, h_got) -> dict:
+    """Per-field max|got - ref| / max|ref - mean(ref)| (fields with a nonzero
+    spread) and the Hamiltonian-constraint L2 norms of both runs."""
+    import numpy as np
+
+    worst, wname = 0.0, None
+    for f, name in enumerate(ref.names):
+        r = ref.fields[f]
+        spread = float(np.abs(r - r.mean()).max())
+        if spread == 0.0:
+            continue
+        e = float(np.abs(got.fields[f] - r).max()) / spread
+        if e > worst:
+            worst, wname = e, name
+    return {"field_err_rel_perturbation": worst, "worst_field": wname,
+            "H_L2": float(h_got["H"][7]), "H_L2_fp64": float(h_ref["H"][7]),
+            "H_ratio": float(h_got["H"][7] / h_ref["H"][7]),
+            "M_L2": float(h_got["M"][7]), "M_L2_fp64": float(h_ref["M"][7])}
 
 
 def cpu_baseline(st, order: int, budget_s: float = 30.0):
@@ -176,7 +209,7 @@ def run_reference_arm(a, world, rank):
     if not binp.exists():
         print(json.dumps({"impl": "reference", "unavailable": f"{binp.name} was not built"}))
         return
-    st = make_state(n, seed=1)
+    st = make_state(n, seed=1, order=a.order)
     threads = os.cpu_count() or 1
     # each step is a full RK4 step of the same box; cap the count so the run
     # stays within a few minutes on the host cores
@@ -228,7 +261,7 @@ def main():
     from cosmograph_b200.evolution import BoxConfig, Evolution
 
     n = a.n
-    st = make_state(n, seed=1 + rank)
+    st = make_state(n, seed=1 + rank, order=a.order)
     cfg = BoxConfig(order=a.order, lapse="Harmonic", precision=a.precision)
     stream = torch.cuda.Stream()
     ev = Evolution(st, cfg)
@@ -275,6 +308,11 @@ def main():
         ev.close()
         return
 
+    # FP64 state and constraints after warm-up + timed steps (accuracy reference)
+    ref_state = ev.download(0) if a.precision == "fp64" else None
+    ref_h = ev.constraints(0) if a.precision == "fp64" else None
+    peak, peak_kind = measured_peaks()
+
     # the other arithmetic variants of the same kernel, same workload
     variants = {}
     for prec in [v for v in a.variants.split(",") if v and v != a.precision]:
@@ -293,8 +331,16 @@ def main():
         torch.cuda.synchronize()
         ev_v.synchronize()
         vms = max_over_ranks(v0.elapsed_time(v1))
-        variants[prec] = {"value": world * pts * a.steps / (vms / 1e3), "ms_per_step": vms / a.steps}
+        vms_step = vms / a.steps
+        v_ach = algo_bytes(prec) * pts / launches_per_step / (vms_step / launches_per_step / 1e3) / 1e9
+        variants[prec] = {"value": world * pts * a.steps / (vms / 1e3), "ms_per_step": vms_step,
+                          "speedup_vs_fp64": ms_per_step / vms_step if a.precision == "fp64" else None,
+                          "roofline": {"achieved": v_ach, "peak": peak, "unit": "GB/s", "frac": v_ach / peak,
+                                       "algorithmic_bytes_per_update": algo_bytes(prec)}}
+        if ref_state is not None:
+            variants[prec]["accuracy_vs_fp64"] = accuracy(ref_state, ev_v.download(0), ref_h, ev_v.constraints(0))
         ev_v.close()
+    del ref_state
 
     # end to end through the C ABI: pinned host state in, one RK4 step, state out
     state_bytes = st.fields.nbytes
@@ -324,8 +370,7 @@ def main():
     e2e_value = world * pts * a.e2e_steps / (e2e_ms / 1e3)
     ev.close()
 
-    peak, peak_kind = measured_peaks()
-    algo = ALGO_BYTES_PER_UPDATE["dust"] * pts / launches_per_step
+    algo = algo_bytes(a.precision) * pts / launches_per_step
     launch_ms = ms_per_step / launches_per_step
     achieved = algo / (launch_ms / 1e3) / 1e9
     traffic = None

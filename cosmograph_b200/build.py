@@ -1,4 +1,5 @@
-"""Build the CUDA library in-tree: cosmograph_b200/libcosmograph_b200.so.
+"""Build the CUDA library in-tree: cosmograph_b200/libcosmograph_b200.so, and
+the config-file driver cosmograph_b200/cosmo_b200 (C++ facade, g++).
 
 Every kernel is compiled for sm_100a only.  The substep kernels are compiled
 twice from the same source: without FMA contraction (the FP64 parity build)
@@ -22,6 +23,8 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libcosmograph_b200.so"
 INCLUDE = ROOT / "include"
+HOST = PKG / "host"
+DRIVER = PKG / "cosmo_b200"   # config-file driver (C++ facade over the C ABI)
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -70,7 +73,25 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         tmp = LIB.with_suffix(".so.tmp")
         run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(tmp)])
         os.replace(tmp, LIB)
+    build_driver(force)
     return LIB
+
+
+def build_driver(force: bool = False) -> Path:
+    """g++ build of the C++ facade (BSSN, Dust, Scalar, Lambda, sims) and the
+    config-file driver `cosmo_b200`, linked against the CUDA library."""
+    srcs = sorted(HOST.glob("*.cc"))
+    deps = srcs + sorted(HOST.glob("*.hpp")) + [INCLUDE / "cosmograph_b200.h", LIB, Path(__file__)]
+    if not force and DRIVER.exists() and DRIVER.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
+        return DRIVER
+    tmp = DRIVER.with_suffix(".tmp")
+    cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-Wall", "-Wextra", f"-I{INCLUDE}", f"-I{HOST}",
+           *map(str, srcs), f"-L{PKG}", "-lcosmograph_b200", "-lz", "-Wl,-rpath,$ORIGIN", "-o", str(tmp)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"g++ failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, DRIVER)
+    return DRIVER
 
 
 def main(argv=None) -> int:

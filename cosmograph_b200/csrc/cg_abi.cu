@@ -697,6 +697,17 @@ static int field_copy(cg_ctx* ctx, int box, int field, char reg, double* host, s
     base = b.dev.F;
   else if (reg == 'a') {
     if (b.stage_next == 0) return fail(ctx, CG_ERR_STATE, "the 'a' register exists after cg_step_init");
+    if (b.mixed) {
+      // FP32 perturbation about the uniform background: a = abar + delta
+      if (upload) return fail(ctx, CG_ERR_INVALID, "the 'a' register of a mixed box is read-only");
+      const float* src = (b.stage_next == 2 || b.stage_next == 4 ? b.mdev.Y : b.mdev.X) + (size_t)field * b.dev.pts;
+      std::vector<float> tmp(n);
+      CG_CUDA(ctx, cudaMemcpyAsync(tmp.data(), src, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+      CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      const double abar = b.ba[field];
+      for (size_t q = 0; q < n; ++q) host[q] = abar + (double)tmp[q];
+      return CG_OK;
+    }
     base = current_a(b);
   } else
     return fail(ctx, CG_ERR_INVALID, "reg must be 'p', 'a' or 'f'");

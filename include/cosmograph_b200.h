@@ -135,7 +135,10 @@ int cg_upload_state_async(cg_ctx *ctx, int box, const double *host, size_t count
 int cg_download_state_async(cg_ctx *ctx, int box, double *host, size_t count);
 
 /* One register of one field: reg = 'p', 'a' (current substep input), 'f'.
- * Replaces BSSN::fields["<name>_<reg>"] access (bssn.cc:30-39). Synchronous. */
+ * Replaces BSSN::fields["<name>_<reg>"] access (bssn.cc:30-39). Synchronous.
+ * On a CG_PREC_MIXED box 'a' is held as an FP32 perturbation about a uniform
+ * FP64 background: a download returns background + perturbation in FP64, an
+ * upload is rejected (CG_ERR_INVALID). */
 int cg_upload_field(cg_ctx *ctx, int box, int field, char reg, const double *host, size_t n);
 int cg_download_field(cg_ctx *ctx, int box, int field, char reg, double *host, size_t n);
 

@@ -66,3 +66,21 @@ def test_vacuum_mixed_runs_and_rejects_unsupported():
     assert max(errs.values()) < 1e-4
     with pytest.raises(RuntimeError, match="mixed"):
         evolve(ics.perturbed((16, 16, 16), S.SCALAR), 1, BoxConfig(order=4, precision="mixed"))
+
+
+def test_a_register_of_a_mixed_box():
+    st = ics.grf_dust(32, seed=13, rms_delta=1e-4, order=4)
+    with Evolution(st, BoxConfig(order=4, precision="mixed")) as em, \
+            Evolution(st, BoxConfig(order=4, precision="fp64")) as ef:
+        for ev in (em, ef):
+            ev.step(2)
+            ev.step_init()
+            ev.rk_stage(1)
+        for f, name in enumerate(st.names):
+            a = em.download_field(0, f, "a")
+            b = ef.download_field(0, f, "a")
+            spread = np.abs(b - b.mean()).max()
+            if spread > 0:
+                assert np.abs(a - b).max() <= 1e-5 * spread, name
+        with pytest.raises(RuntimeError, match="read-only"):
+            em.upload_field(0, 0, "a", np.zeros(st.shape))
