@@ -12,7 +12,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/cosmograph_b200.h"
+#include "cosmograph_b200.h"
 #include "cg_internal.h"
 #include "cg_mixed.cuh"
 

@@ -21,12 +21,17 @@
 // static lapse, a_adj_amp = k_damping_amp = 0.
 #pragma once
 
+#include "cg_tile.cuh"
 #include "cg_types.h"
 
 namespace cg {
 namespace mixed {
 
-constexpr int kBX = 4, kBY = 4, kBZ = 8, kThreads = kBX * kBY * kBZ;
+using Brick = tile::Brick32;
+constexpr int kBX = Brick::BX, kBY = Brick::BY, kBZ = Brick::BZ, kThreads = Brick::THREADS;
+// FP32 tiles with a 24-float row pitch: conflict-free taps (cg_tile.cuh)
+template <int O>
+using TileG = tile::Geom<O, Brick, 24>;
 
 struct Ptrs {
   const float* in;     // delta of a^n
@@ -55,6 +60,8 @@ enum : int {
   S_DG = 0, S_T1 = 18, S_DPHI = 24, S_DDPHI = 27, S_DA = 33, S_DDA = 36, S_DK = 42,
   S_DGAM = 45, S_SRC = 54, S_G = 65, S_MAT = 83, S_NSLOT = 87
 };
+// phase 1 writes no slot in [S_SRC, S_MAT): the field tile lives there
+constexpr int kTileSlot = S_SRC, kTileSlots = S_MAT - S_SRC;
 
 __device__ __forceinline__ int wrapf(int v, int n) {
   v = v < 0 ? v + n : v;
@@ -79,8 +86,8 @@ struct Taps {
 
 // FP32 centred stencils (utils/math.h:74-1085 coefficients)
 template <int O, class T>
-__device__ __forceinline__ float d1(const float* __restrict__ f, const T& t, int a, float idx) {
-  auto V = [&](int n) { return __ldg(f + t.ax(a, n)); };
+__device__ __forceinline__ float d1(const T& t, int a, float idx) {
+  auto V = [&](int n) { return t.ax(a, n); };
   float s;
   if (O == 2) s = 0.5f * (V(1) - V(-1));
   else if (O == 4) s = (2.0f / 3.0f) * (V(1) - V(-1)) - (1.0f / 12.0f) * (V(2) - V(-2));
@@ -89,8 +96,8 @@ __device__ __forceinline__ float d1(const float* __restrict__ f, const T& t, int
   return s * idx;
 }
 template <int O, class T>
-__device__ __forceinline__ float d2(const float* __restrict__ f, const T& t, int a, float idx2) {
-  auto V = [&](int n) { return __ldg(f + t.ax(a, n)); };
+__device__ __forceinline__ float d2(const T& t, int a, float idx2) {
+  auto V = [&](int n) { return t.ax(a, n); };
   float s;
   if (O == 2) s = (V(1) + V(-1)) - 2.0f * V(0);
   else if (O == 4) s = (4.0f / 3.0f) * (V(1) + V(-1)) - (1.0f / 12.0f) * (V(2) + V(-2)) - 2.5f * V(0);
@@ -99,11 +106,8 @@ __device__ __forceinline__ float d2(const float* __restrict__ f, const T& t, int
   return s * idx2;
 }
 template <int O, class T>
-__device__ __forceinline__ float dm(const float* __restrict__ f, const T& t, int a, int b, float idx2) {
-  auto P = [&](int n) {
-    return (__ldg(f + t.pl(a, n, b, n)) + __ldg(f + t.pl(a, -n, b, -n))) -
-           (__ldg(f + t.pl(a, n, b, -n)) + __ldg(f + t.pl(a, -n, b, n)));
-  };
+__device__ __forceinline__ float dm(const T& t, int a, int b, float idx2) {
+  auto P = [&](int n) { return (t.pl(a, n, b, n) + t.pl(a, -n, b, -n)) - (t.pl(a, n, b, -n) + t.pl(a, -n, b, n)); };
   float s;
   if (O == 2) s = 0.25f * P(1);
   else if (O == 4) s = (1.0f / 3.0f) * P(1) - (1.0f / 48.0f) * P(2);
@@ -152,53 +156,69 @@ __device__ __forceinline__ DustF dust_primf(const float gi[6], float em4, float 
   return d;
 }
 
-template <int O, int MATTER, class T>
-__device__ __forceinline__ void derivatives(const T& t, const float* __restrict__ a, const float* __restrict__ fp,
-                                            int N, float idx, float idx2, const float gi[6], float* sl) {
+// Phase 1 (as in the FP64 kernel): the metric components, phi and alpha with
+// first and second derivatives, K and Gamma^i with first derivatives, one
+// field tile at a time, the next field fetched into registers meanwhile.
+__device__ __forceinline__ int phase1_field(int it) {
+  return it < 6 ? F_G11 + it : (it == 6 ? F_PHI : (it == 7 ? F_ALPHA : (it == 8 ? F_K : F_GAM1 + it - 9)));
+}
+
+template <int O>
+__device__ __forceinline__ void derivatives(const float* __restrict__ a, int N, float idx, float idx2,
+                                            const float gi[6], float* sl, float* tl, const int* rowoff, int tid,
+                                            int z0, int nz, int cc) {
+  tile::Loader<TileG<O>, Brick, float> ld;
+  ld.init(tid, z0, nz);
+  ld.fetch(a + (size_t)phase1_field(0) * N, rowoff);
+  const tile::Taps<TileG<O>, float> t{tl, cc};
 #pragma unroll 1
-  for (int it = 0; it < 8; ++it) {
-    const int fld = it < 6 ? F_G11 + it : (it == 6 ? F_PHI : F_ALPHA);
-    const float* __restrict__ f = a + (size_t)fld * N;
-    const float g1 = d1<O>(f, t, 0, idx), g2 = d1<O>(f, t, 1, idx), g3 = d1<O>(f, t, 2, idx);
-    const float h11 = d2<O>(f, t, 0, idx2), h22 = d2<O>(f, t, 1, idx2), h33 = d2<O>(f, t, 2, idx2);
-    const float h12 = dm<O>(f, t, 0, 1, idx2), h13 = dm<O>(f, t, 0, 2, idx2), h23 = dm<O>(f, t, 1, 2, idx2);
-    if (it < 6) {
-      sl[(S_DG + 0 * 6 + it) * kThreads] = g1;
-      sl[(S_DG + 1 * 6 + it) * kThreads] = g2;
-      sl[(S_DG + 2 * 6 + it) * kThreads] = g3;
-      sl[(S_T1 + it) * kThreads] =
-          gi[0] * h11 + gi[3] * h22 + gi[5] * h33 + 2.0f * (gi[1] * h12 + gi[2] * h13 + gi[4] * h23);
+  for (int it = 0; it < 12; ++it) {
+    __syncthreads();
+    ld.store(tl);
+    __syncthreads();
+    if (it + 1 < 12) ld.fetch(a + (size_t)phase1_field(it + 1) * N, rowoff);
+    if (it < 8) {
+      const float g1 = d1<O>(t, 0, idx), g2 = d1<O>(t, 1, idx), g3 = d1<O>(t, 2, idx);
+      const float h11 = d2<O>(t, 0, idx2), h22 = d2<O>(t, 1, idx2), h33 = d2<O>(t, 2, idx2);
+      const float h12 = dm<O>(t, 0, 1, idx2), h13 = dm<O>(t, 0, 2, idx2), h23 = dm<O>(t, 1, 2, idx2);
+      if (it < 6) {
+        sl[(S_DG + 0 * 6 + it) * kThreads] = g1;
+        sl[(S_DG + 1 * 6 + it) * kThreads] = g2;
+        sl[(S_DG + 2 * 6 + it) * kThreads] = g3;
+        sl[(S_T1 + it) * kThreads] =
+            gi[0] * h11 + gi[3] * h22 + gi[5] * h33 + 2.0f * (gi[1] * h12 + gi[2] * h13 + gi[4] * h23);
+      } else {
+        const int b1 = it == 6 ? S_DPHI : S_DA, b2 = it == 6 ? S_DDPHI : S_DDA;
+        sl[(b1 + 0) * kThreads] = g1;
+        sl[(b1 + 1) * kThreads] = g2;
+        sl[(b1 + 2) * kThreads] = g3;
+        sl[(b2 + 0) * kThreads] = h11;
+        sl[(b2 + 1) * kThreads] = h12;
+        sl[(b2 + 2) * kThreads] = h13;
+        sl[(b2 + 3) * kThreads] = h22;
+        sl[(b2 + 4) * kThreads] = h23;
+        sl[(b2 + 5) * kThreads] = h33;
+      }
     } else {
-      const int b1 = it == 6 ? S_DPHI : S_DA, b2 = it == 6 ? S_DDPHI : S_DDA;
-      sl[(b1 + 0) * kThreads] = g1;
-      sl[(b1 + 1) * kThreads] = g2;
-      sl[(b1 + 2) * kThreads] = g3;
-      sl[(b2 + 0) * kThreads] = h11;
-      sl[(b2 + 1) * kThreads] = h12;
-      sl[(b2 + 2) * kThreads] = h13;
-      sl[(b2 + 3) * kThreads] = h22;
-      sl[(b2 + 4) * kThreads] = h23;
-      sl[(b2 + 5) * kThreads] = h33;
+      const int b = it == 8 ? S_DK : S_DGAM + 3 * (it - 9);
+      sl[(b + 0) * kThreads] = d1<O>(t, 0, idx);
+      sl[(b + 1) * kThreads] = d1<O>(t, 1, idx);
+      sl[(b + 2) * kThreads] = d1<O>(t, 2, idx);
     }
   }
+}
+
+// dust flux divergences from the stored FP32 flux primitives (global taps)
+template <int O, class T>
+__device__ __forceinline__ void flux_divergences(const T& t, const float* __restrict__ fp, int N, float idx,
+                                                 float* sl) {
+  const float* v1 = fp + (size_t)P_V1 * N;
+  const float* v2 = fp + (size_t)P_V2 * N;
+  const float* v3 = fp + (size_t)P_V3 * N;
 #pragma unroll 1
-  for (int it = 0; it < 4; ++it) {
-    const int fld = it == 0 ? F_K : F_GAM1 + it - 1;
-    const float* __restrict__ f = a + (size_t)fld * N;
-    const int b = it == 0 ? S_DK : S_DGAM + 3 * (it - 1);
-    sl[(b + 0) * kThreads] = d1<O>(f, t, 0, idx);
-    sl[(b + 1) * kThreads] = d1<O>(f, t, 1, idx);
-    sl[(b + 2) * kThreads] = d1<O>(f, t, 2, idx);
-  }
-  if (MATTER == kDust) {
-    const float* v1 = fp + (size_t)P_V1 * N;
-    const float* v2 = fp + (size_t)P_V2 * N;
-    const float* v3 = fp + (size_t)P_V3 * N;
-#pragma unroll 1
-    for (int m = 0; m < 4; ++m) {
-      const float* u = fp + (size_t)(P_AD + m) * N;
-      sl[(S_MAT + m) * kThreads] = d1p<O>(u, v1, t, 0, idx) + d1p<O>(u, v2, t, 1, idx) + d1p<O>(u, v3, t, 2, idx);
-    }
+  for (int m = 0; m < 4; ++m) {
+    const float* u = fp + (size_t)(P_AD + m) * N;
+    sl[(S_MAT + m) * kThreads] = d1p<O>(u, v1, t, 0, idx) + d1p<O>(u, v2, t, 1, idx) + d1p<O>(u, v3, t, 2, idx);
   }
 }
 
@@ -212,10 +232,13 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
   const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
   float* sl = smf + tid;
   auto S = [&](int s) -> float& { return sl[s * kThreads]; };
-  const int k = blockIdx.x * kBZ + threadIdx.x;
-  const int j = blockIdx.y * kBY + threadIdx.y;
-  const int i = blockIdx.z * kBX + threadIdx.z;
-  if (i >= nx || j >= ny || k >= nz) return;
+  const int k0 = blockIdx.x * kBZ + threadIdx.x;
+  const int j0 = blockIdx.y * kBY + threadIdx.y;
+  const int i0 = blockIdx.z * kBX + threadIdx.z;
+  // every thread takes part in the tile copies; threads past the box edge
+  // compute a valid point and leave after phase 1
+  const bool live = i0 < nx && j0 < ny && k0 < nz;
+  const int k = min(k0, nz - 1), j = min(j0, ny - 1), i = min(i0, nx - 1);
   const int N = nx * ny * nz;
   const int c = (i * ny + j) * nz + k;
   const float* __restrict__ a = P.in;
@@ -227,14 +250,30 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
   inv_metricf(g, gi);
 
   const int x0 = blockIdx.z * kBX, y0 = blockIdx.y * kBY, z0 = blockIdx.x * kBZ;
-  const bool interior = x0 >= R && x0 + kBX + R <= nx && y0 >= R && y0 + kBY + R <= ny && z0 >= R && z0 + kBZ + R <= nz;
   const float idx2 = idx * idx;
-  if (interior) {
-    const Taps<false> t{i, j, k, nx, ny, nz, ny * nz, nz, c};
-    derivatives<O, MATTER>(t, a, P.fp_in, N, idx, idx2, gi, sl);
-  } else {
-    const Taps<true> t{i, j, k, nx, ny, nz, ny * nz, nz, c};
-    derivatives<O, MATTER>(t, a, P.fp_in, N, idx, idx2, gi, sl);
+  {
+    static_assert(TileG<O>::SIZE * sizeof(float) + TileG<O>::ROWS * sizeof(int) <=
+                      (size_t)kTileSlots * kThreads * sizeof(float),
+                  "tile and row offsets fit the phase-2-only slots");
+    float* tl = smf + kTileSlot * kThreads;
+    int* rowoff = reinterpret_cast<int*>(tl + TileG<O>::SIZE);
+    tile::row_offsets<TileG<O>, Brick>(x0, y0, nx, ny, nz, tid, rowoff);
+    __syncthreads();  // every warp reads every row offset
+    derivatives<O>(a, N, idx, idx2, gi, sl, tl, rowoff, tid, z0, nz,
+                   tile::centre<TileG<O>>(threadIdx.z, threadIdx.y, threadIdx.x));
+    __syncthreads();
+  }
+  if (!live) return;
+  if (MATTER == kDust) {
+    const bool interior =
+        x0 >= R && x0 + kBX + R <= nx && y0 >= R && y0 + kBY + R <= ny && z0 >= R && z0 + kBZ + R <= nz;
+    if (interior) {
+      const Taps<false> t{i, j, k, nx, ny, nz, ny * nz, nz, c};
+      flux_divergences<O>(t, P.fp_in, N, idx, sl);
+    } else {
+      const Taps<true> t{i, j, k, nx, ny, nz, ny * nz, nz, c};
+      flux_divergences<O>(t, P.fp_in, N, idx, sl);
+    }
   }
 
   // ---- centre values: perturbations and full values -------------------------

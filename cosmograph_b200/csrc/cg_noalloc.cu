@@ -15,7 +15,7 @@
 #include <mutex>
 #include <string>
 
-#include "../../include/cosmograph_b200.h"
+#include "cosmograph_b200.h"
 #include "cg_internal.h"
 
 namespace {

@@ -34,6 +34,7 @@
 #pragma once
 
 #include "cg_point.cuh"
+#include "cg_tile.cuh"
 
 namespace cg {
 
@@ -65,8 +66,11 @@ struct NF {
   static constexpr int value = MATTER == kDust ? 22 : (MATTER == kScalar ? 23 : 18);
 };
 
-// CTA brick
-constexpr int kBX = 4, kBY = 4, kBZ = 8, kThreads = kBX * kBY * kBZ;
+// CTA brick and field tiles (cg_tile.cuh)
+using Brick = tile::Brick64;
+constexpr int kBX = Brick::BX, kBY = Brick::BY, kBZ = Brick::BZ, kThreads = Brick::THREADS;
+template <int O>
+using TileG = tile::Geom<O, Brick>;
 
 // Per-thread shared-memory slots (one column of kThreads doubles per slot).
 enum : int {
@@ -82,6 +86,9 @@ enum : int {
   S_G = 65,           // Gamma^I_q         18
   S_MAT = 83,         // dust: 4 divergences; scalar: 15 first derivatives
 };
+// Phase 1 writes no slot in [S_SRC, S_MAT): that region holds the field tile
+// and its row offsets until phase 2 starts.
+constexpr int kTileSlot = S_SRC, kTileSlots = S_MAT - S_SRC;
 template <int MATTER>
 struct Slots {
   static constexpr int value = S_MAT + (MATTER == kDust ? 4 : (MATTER == kScalar ? 15 : 0));
@@ -120,8 +127,8 @@ struct Taps {
 
 // first derivative (utils/math.h:74-100, 231-263, 412-450, 554-586)
 template <int O, class T>
-__device__ __forceinline__ double d1(const double* __restrict__ f, const T& t, int a, const Physics& ph) {
-  auto V = [&](int n) { return __ldg(f + t.ax(a, n)); };
+__device__ __forceinline__ double d1(const T& t, int a, const Physics& ph) {
+  auto V = [&](int n) { return t.ax(a, n); };
   double s;
   if (O == 2) {
     s = (-1.0 / 2.0 * V(-1) + 1.0 / 2.0 * V(1));
@@ -139,8 +146,8 @@ __device__ __forceinline__ double d1(const double* __restrict__ f, const T& t, i
 
 // second derivative along one axis (utils/math.h:857-885, 958-993, 995-1036, 1038-1085)
 template <int O, class T>
-__device__ __forceinline__ double d2(const double* __restrict__ f, const T& t, int a, const Physics& ph) {
-  auto V = [&](int n) { return __ldg(f + t.ax(a, n)); };
+__device__ __forceinline__ double d2(const T& t, int a, const Physics& ph) {
+  auto V = [&](int n) { return t.ax(a, n); };
   double s;
   if (O == 2) {
     s = (V(-1) - 2.0 * V(0) + V(1));
@@ -158,11 +165,8 @@ __device__ __forceinline__ double d2(const double* __restrict__ f, const T& t, i
 
 // mixed second derivative on axes a < b (utils/math.h:676-855)
 template <int O, class T>
-__device__ __forceinline__ double dm(const double* __restrict__ f, const T& t, int a, int b, const Physics& ph) {
-  auto P = [&](int n) {
-    return -__ldg(f + t.pl(a, n, b, -n)) + __ldg(f + t.pl(a, n, b, n)) + __ldg(f + t.pl(a, -n, b, -n)) -
-           __ldg(f + t.pl(a, -n, b, n));
-  };
+__device__ __forceinline__ double dm(const T& t, int a, int b, const Physics& ph) {
+  auto P = [&](int n) { return -t.pl(a, n, b, -n) + t.pl(a, n, b, n) + t.pl(a, -n, b, -n) - t.pl(a, -n, b, n); };
   double s;
   if (O == 2) {
     s = P(1) / 4.0;
@@ -200,89 +204,114 @@ __device__ __forceinline__ double d1p(const double* __restrict__ fa, const doubl
   return divdx(s, ph);
 }
 
-// Phase 1: every derivative the point needs, parked in shared memory.
-template <int O, int MATTER, int MODE, class T>
-__device__ __forceinline__ void derivatives(const T& t, const double* __restrict__ a, const double* __restrict__ fp,
-                                            int N, const Physics& ph, const double gi[6], double* sl) {
-  if (MODE == kConstraints) {
-    // d_d A_q for the momentum constraint (BSSN_MI, bssn_macros.h:498-500)
-#pragma unroll 1
-    for (int q = 0; q < 6; ++q) {
-      const double* __restrict__ f = a + (size_t)(F_A11 + q) * N;
-      sl[(SlotsC<MATTER>::dA + 3 * q + 0) * kThreads] = d1<O>(f, t, 0, ph);
-      sl[(SlotsC<MATTER>::dA + 3 * q + 1) * kThreads] = d1<O>(f, t, 1, ph);
-      sl[(SlotsC<MATTER>::dA + 3 * q + 2) * kThreads] = d1<O>(f, t, 2, ph);
-    }
+// Fields of phase 1, in order: (constraint mode) A_q with first derivatives;
+// the metric components, phi and alpha with first and second derivatives;
+// K and Gamma^i with first derivatives; (scalar) phi, Pi, psi_i with first
+// derivatives.
+template <int MATTER, int MODE>
+struct Phase1 {
+  static constexpr int NA = MODE == kConstraints ? 6 : 0;
+  static constexpr int NS = MATTER == kScalar ? 5 : 0;
+  static constexpr int N = NA + 8 + 4 + NS;
+  __device__ __forceinline__ static int field(int it) {
+    if (it < NA) return F_A11 + it;
+    it -= NA;
+    if (it < 8) return it < 6 ? F_G11 + it : (it == 6 ? F_PHI : F_ALPHA);
+    it -= 8;
+    if (it < 4) return it == 0 ? F_K : F_GAM1 + it - 1;
+    return F_SPHI + it - 4;
   }
-  // metric components, phi and alpha: first and second derivatives
-  // (calculate_dgamma / calculate_ddgamma / calculate_dalpha_dphi,
-  // bssn.cc:480-521).  For g_q the second derivatives are contracted at once
-  // with the inverse metric (BSSN_CALCULATE_RICCI_UNITARY_TERM1,
-  // bssn_macros.h:248-249, summed over (k,l) in the reference's order).
+};
+
+// Phase 1: every derivative the point needs, parked in shared memory.  One
+// field at a time is copied into the tile (the next one is fetched into
+// registers meanwhile); all threads of the CTA take part.
+template <int O, int MATTER, int MODE>
+__device__ __forceinline__ void derivatives(const double* __restrict__ a, int N, const Physics& ph, const double gi[6],
+                                            double* sl, double* tl, const int* rowoff, int tid, int z0, int nz,
+                                            int cc) {
+  using PF = Phase1<MATTER, MODE>;
+  tile::Loader<TileG<O>, Brick, double> ld;
+  ld.init(tid, z0, nz);
+  ld.fetch(a + (size_t)PF::field(0) * N, rowoff);
+  const tile::Taps<TileG<O>, double> t{tl, cc};
 #pragma unroll 1
-  for (int it = 0; it < 8; ++it) {
-    const int fld = it < 6 ? F_G11 + it : (it == 6 ? F_PHI : F_ALPHA);
-    const double* __restrict__ f = a + (size_t)fld * N;
-    const double g1 = d1<O>(f, t, 0, ph), g2 = d1<O>(f, t, 1, ph), g3 = d1<O>(f, t, 2, ph);
-    const double h11 = d2<O>(f, t, 0, ph), h22 = d2<O>(f, t, 1, ph), h33 = d2<O>(f, t, 2, ph);
-    const double h12 = dm<O>(f, t, 0, 1, ph), h13 = dm<O>(f, t, 0, 2, ph), h23 = dm<O>(f, t, 1, 2, ph);
-    if (it < 6) {
-      sl[(S_DG + 0 * 6 + it) * kThreads] = g1;
-      sl[(S_DG + 1 * 6 + it) * kThreads] = g2;
-      sl[(S_DG + 2 * 6 + it) * kThreads] = g3;
-      double s = gi[0] * h11;
-      s = s + gi[1] * h12;
-      s = s + gi[2] * h13;
-      s = s + gi[1] * h12;
-      s = s + gi[3] * h22;
-      s = s + gi[4] * h23;
-      s = s + gi[2] * h13;
-      s = s + gi[4] * h23;
-      s = s + gi[5] * h33;
-      sl[(S_T1 + it) * kThreads] = s;
+  for (int it = 0; it < PF::N; ++it) {
+    __syncthreads();  // the previous tile has been read
+    ld.store(tl);
+    __syncthreads();
+    if (it + 1 < PF::N) ld.fetch(a + (size_t)PF::field(it + 1) * N, rowoff);
+    if (it < PF::NA) {
+      // d_d A_q for the momentum constraint (BSSN_MI, bssn_macros.h:498-500)
+      const int q = it;
+      sl[(SlotsC<MATTER>::dA + 3 * q + 0) * kThreads] = d1<O>(t, 0, ph);
+      sl[(SlotsC<MATTER>::dA + 3 * q + 1) * kThreads] = d1<O>(t, 1, ph);
+      sl[(SlotsC<MATTER>::dA + 3 * q + 2) * kThreads] = d1<O>(t, 2, ph);
+    } else if (it < PF::NA + 8) {
+      // calculate_dgamma / calculate_ddgamma / calculate_dalpha_dphi
+      // (bssn.cc:480-521).  For g_q the second derivatives are contracted at
+      // once with the inverse metric (BSSN_CALCULATE_RICCI_UNITARY_TERM1,
+      // bssn_macros.h:248-249, summed over (k,l) in the reference's order).
+      const int q = it - PF::NA;
+      const double g1 = d1<O>(t, 0, ph), g2 = d1<O>(t, 1, ph), g3 = d1<O>(t, 2, ph);
+      const double h11 = d2<O>(t, 0, ph), h22 = d2<O>(t, 1, ph), h33 = d2<O>(t, 2, ph);
+      const double h12 = dm<O>(t, 0, 1, ph), h13 = dm<O>(t, 0, 2, ph), h23 = dm<O>(t, 1, 2, ph);
+      if (q < 6) {
+        sl[(S_DG + 0 * 6 + q) * kThreads] = g1;
+        sl[(S_DG + 1 * 6 + q) * kThreads] = g2;
+        sl[(S_DG + 2 * 6 + q) * kThreads] = g3;
+        double s = gi[0] * h11;
+        s = s + gi[1] * h12;
+        s = s + gi[2] * h13;
+        s = s + gi[1] * h12;
+        s = s + gi[3] * h22;
+        s = s + gi[4] * h23;
+        s = s + gi[2] * h13;
+        s = s + gi[4] * h23;
+        s = s + gi[5] * h33;
+        sl[(S_T1 + q) * kThreads] = s;
+      } else {
+        const int b1 = q == 6 ? S_DPHI : S_DA, b2 = q == 6 ? S_DDPHI : S_DDA;
+        sl[(b1 + 0) * kThreads] = g1;
+        sl[(b1 + 1) * kThreads] = g2;
+        sl[(b1 + 2) * kThreads] = g3;
+        sl[(b2 + 0) * kThreads] = h11;
+        sl[(b2 + 1) * kThreads] = h12;
+        sl[(b2 + 2) * kThreads] = h13;
+        sl[(b2 + 3) * kThreads] = h22;
+        sl[(b2 + 4) * kThreads] = h23;
+        sl[(b2 + 5) * kThreads] = h33;
+      }
+    } else if (it < PF::NA + 12) {
+      // K and Gamma^K: first derivatives (calculate_dK, bssn.cc:529-535; the
+      // d_J Gamma^K of BSSN_CALCULATE_RICCI_UNITARY_TERM2, bssn_macros.h:251-252)
+      const int q = it - PF::NA - 8;
+      const int b = q == 0 ? S_DK : S_DGAM + 3 * (q - 1);
+      sl[(b + 0) * kThreads] = d1<O>(t, 0, ph);
+      sl[(b + 1) * kThreads] = d1<O>(t, 1, ph);
+      sl[(b + 2) * kThreads] = d1<O>(t, 2, ph);
     } else {
-      const int b1 = it == 6 ? S_DPHI : S_DA, b2 = it == 6 ? S_DDPHI : S_DDA;
-      sl[(b1 + 0) * kThreads] = g1;
-      sl[(b1 + 1) * kThreads] = g2;
-      sl[(b1 + 2) * kThreads] = g3;
-      sl[(b2 + 0) * kThreads] = h11;
-      sl[(b2 + 1) * kThreads] = h12;
-      sl[(b2 + 2) * kThreads] = h13;
-      sl[(b2 + 3) * kThreads] = h22;
-      sl[(b2 + 4) * kThreads] = h23;
-      sl[(b2 + 5) * kThreads] = h33;
+      // Scalar::getScalarData derivatives (scalar.cc:109-127): d_d of phi, Pi, psi1..3
+      const int m = it - PF::NA - 12;
+      sl[(S_MAT + 3 * m + 0) * kThreads] = d1<O>(t, 0, ph);
+      sl[(S_MAT + 3 * m + 1) * kThreads] = d1<O>(t, 1, ph);
+      sl[(S_MAT + 3 * m + 2) * kThreads] = d1<O>(t, 2, ph);
     }
   }
-  // K and Gamma^K: first derivatives (calculate_dK, bssn.cc:529-535; the
-  // d_J Gamma^K of BSSN_CALCULATE_RICCI_UNITARY_TERM2, bssn_macros.h:251-252)
+}
+
+// Dust flux divergences d_i(alpha D v^i), d_i(alpha S_m v^i) (dust.cc:203-224)
+// from the stored flux primitives, taps read from global memory.
+template <int O, class T>
+__device__ __forceinline__ void flux_divergences(const T& t, const double* __restrict__ fp, int N, const Physics& ph,
+                                                 double* sl) {
+  const double* v1 = fp + (size_t)P_V1 * N;
+  const double* v2 = fp + (size_t)P_V2 * N;
+  const double* v3 = fp + (size_t)P_V3 * N;
 #pragma unroll 1
-  for (int it = 0; it < 4; ++it) {
-    const int fld = it == 0 ? F_K : F_GAM1 + it - 1;
-    const double* __restrict__ f = a + (size_t)fld * N;
-    const int b = it == 0 ? S_DK : S_DGAM + 3 * (it - 1);
-    sl[(b + 0) * kThreads] = d1<O>(f, t, 0, ph);
-    sl[(b + 1) * kThreads] = d1<O>(f, t, 1, ph);
-    sl[(b + 2) * kThreads] = d1<O>(f, t, 2, ph);
-  }
-  if (MATTER == kDust) {
-    // flux divergences d_i(alpha D v^i), d_i(alpha S_m v^i) (dust.cc:203-224)
-    const double* v1 = fp + (size_t)P_V1 * N;
-    const double* v2 = fp + (size_t)P_V2 * N;
-    const double* v3 = fp + (size_t)P_V3 * N;
-#pragma unroll 1
-    for (int m = 0; m < 4; ++m) {
-      const double* u = fp + (size_t)(P_AD + m) * N;
-      sl[(S_MAT + m) * kThreads] = d1p<O>(u, v1, t, 0, ph) + d1p<O>(u, v2, t, 1, ph) + d1p<O>(u, v3, t, 2, ph);
-    }
-  } else if (MATTER == kScalar) {
-    // Scalar::getScalarData derivatives (scalar.cc:109-127): d_d of phi, Pi, psi1..3
-#pragma unroll 1
-    for (int m = 0; m < 5; ++m) {
-      const double* __restrict__ f = a + (size_t)(F_SPHI + m) * N;
-      sl[(S_MAT + 3 * m + 0) * kThreads] = d1<O>(f, t, 0, ph);
-      sl[(S_MAT + 3 * m + 1) * kThreads] = d1<O>(f, t, 1, ph);
-      sl[(S_MAT + 3 * m + 2) * kThreads] = d1<O>(f, t, 2, ph);
-    }
+  for (int m = 0; m < 4; ++m) {
+    const double* u = fp + (size_t)(P_AD + m) * N;
+    sl[(S_MAT + m) * kThreads] = d1p<O>(u, v1, t, 0, ph) + d1p<O>(u, v2, t, 1, ph) + d1p<O>(u, v3, t, 2, ph);
   }
 }
 
@@ -321,7 +350,10 @@ __global__ void __launch_bounds__(kThreads, 2)
 stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
   constexpr int NFLD = NF<MATTER>::value;
   constexpr int NSLOT = MODE == kConstraints ? SlotsC<MATTER>::value : Slots<MATTER>::value;
-  (void)NSLOT;
+  static_assert(NSLOT >= S_MAT, "the tile region lies inside the slot array");
+  static_assert(TileG<O>::SIZE * sizeof(double) + TileG<O>::ROWS * sizeof(int) <=
+                    (size_t)kTileSlots * kThreads * sizeof(double),
+                "tile and row offsets fit the phase-2-only slots");
   constexpr int R = O / 2;
   extern __shared__ double smem[];
   const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
@@ -332,9 +364,9 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
   const int j0 = blockIdx.y * kBY + threadIdx.y;
   const int i0 = blockIdx.z * kBX + threadIdx.z;
   const bool live = i0 < geo.nx && j0 < geo.ny && k0 < geo.nz;
-  if (MODE == kEvolve && !live) return;  // no CTA-wide synchronisation in this mode
-  // constraint mode: every thread reaches the CTA reduction; threads past the
-  // box edge compute a valid point and contribute nothing
+  // every thread takes part in the tile copies of phase 1 (and, in constraint
+  // mode, in the CTA reduction); threads past the box edge compute a valid
+  // point and write nothing
   const int k = min(k0, geo.nz - 1), j = min(j0, geo.ny - 1), i = min(i0, geo.nx - 1);
   if (P.kavg) bg.K_avg = *P.kavg;
   const int N = geo.pts;
@@ -350,14 +382,26 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
 
   // ---- phase 1: derivatives into shared memory ---------------------------------
   const int x0 = blockIdx.z * kBX, y0 = blockIdx.y * kBY, z0 = blockIdx.x * kBZ;
-  const bool interior = x0 >= R && x0 + kBX + R <= geo.nx && y0 >= R && y0 + kBY + R <= geo.ny && z0 >= R &&
-                        z0 + kBZ + R <= geo.nz;
-  if (interior) {
-    const Taps<false> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
-    derivatives<O, MATTER, MODE>(t, a, P.fp_in, N, ph, gi, sl);
-  } else {
-    const Taps<true> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
-    derivatives<O, MATTER, MODE>(t, a, P.fp_in, N, ph, gi, sl);
+  {
+    double* tl = smem + kTileSlot * kThreads;
+    int* rowoff = reinterpret_cast<int*>(tl + TileG<O>::SIZE);
+    tile::row_offsets<TileG<O>, Brick>(x0, y0, geo.nx, geo.ny, geo.nz, tid, rowoff);
+    __syncthreads();  // every warp reads every row offset
+    derivatives<O, MATTER, MODE>(a, N, ph, gi, sl, tl, rowoff, tid, z0, geo.nz,
+                                 tile::centre<TileG<O>>(threadIdx.z, threadIdx.y, threadIdx.x));
+    __syncthreads();  // the tile region becomes slots again
+  }
+  if (MODE == kEvolve && !live) return;  // no CTA-wide synchronisation after this point
+  if (MATTER == kDust) {
+    const bool interior = x0 >= R && x0 + kBX + R <= geo.nx && y0 >= R && y0 + kBY + R <= geo.ny && z0 >= R &&
+                          z0 + kBZ + R <= geo.nz;
+    if (interior) {
+      const Taps<false> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
+      flux_divergences<O>(t, P.fp_in, N, ph, sl);
+    } else {
+      const Taps<true> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
+      flux_divergences<O>(t, P.fp_in, N, ph, sl);
+    }
   }
 
   // ---- phase 2: the algebra of set_bd_values (bssn.cc:361-421) ----------------
