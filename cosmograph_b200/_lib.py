@@ -35,7 +35,9 @@ EXPORTS = (
     "cg_device_register", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
     "cg_status", "cg_frw_state", "cg_step_count", "cg_last_error", "cg_version",
     "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints",
+    "cg_set_option", "cg_num_groups", "cg_group_info",
 )
+OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID = 1, 2, 3, 4
 
 
 class BoxDesc(ctypes.Structure):
@@ -95,6 +97,9 @@ def load() -> ctypes.CDLL:
         "cg_conformal_average": (i, [vp, vp, vp, sz, ctypes.c_double, dp]),
         "cg_conformal_average_noalloc": (i, [vp, vp, sz, ctypes.c_double, vp, vp]),
         "cg_constraints": (i, [vp, i, dp, dp, dp, dp, dp]),
+        "cg_set_option": (i, [vp, i, i]),
+        "cg_num_groups": (i, [vp, ctypes.POINTER(i)]),
+        "cg_group_info": (i, [vp, i, ctypes.POINTER(i), i]),
         "cg_version": (i, []),
     }
     for name, (res, args) in sig.items():

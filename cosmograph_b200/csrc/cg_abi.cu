@@ -93,8 +93,29 @@ struct Box {
 
 }  // namespace
 
+namespace {
+// Boxes of the same arithmetic, order and matter model advanced by one launch
+// per substep (see stage_group_kernel / mixed_group_kernel).
+struct Group {
+  std::vector<int> members;  // box indices in launch order
+  bool mixed = false;
+  int variant = 0, order = 0, matter = 0;
+  void* table = nullptr;     // device GroupBox table in launch order
+  int total = 0;             // bricks of all members
+  int grid = 0;              // CTAs of a launch (0: one per brick)
+  int lpt = 0;               // launch order: 0 box index, 1 largest box first
+  bool tuned = false;
+};
+}  // namespace
+
 struct cg_ctx {
   std::vector<Box> boxes;
+  std::vector<Group> groups;
+  std::vector<int> singles;  // boxes launched on their own
+  bool grouped = false;      // groups and singles are current
+  int opt_batch = 1, opt_graph = 0, opt_autotune = 1, opt_group_grid = 0;
+  cudaGraphExec_t gexec = nullptr;
+  int gexec_steps = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
   unsigned* status = nullptr;
@@ -310,6 +331,10 @@ void mixed_bg_rhs(const Box& b, const double* a, double phi_lag, double* rhs) {
   rhs[cg::F_ALPHA] = b.desc.lapse == CG_LAPSE_HARMONIC ? -1.0 * al * Kd : 0.0;
 }
 
+void pack_bg(const double* full, double* compact) {
+  for (int f : {cg::F_K, cg::F_PHI, cg::F_ALPHA, cg::F_D}) compact[cg::mixed::bgi(f)] = full[f];
+}
+
 int mixed_init(cg_ctx* ctx, Box& b) {
   // background registers from the means of _p (K, phi, alpha, D)
   const int n = b.dev.pts;
@@ -337,20 +362,23 @@ int mixed_init(cg_ctx* ctx, Box& b) {
   if (b.desc.matter == CG_MATTER_DUST) b.bp[cg::F_D] = h[3] / n;
   for (int f = 0; f < 23; ++f) b.ba[f] = b.bprev[f] = b.bp[f];
   cg::mixed::Bg bg{};
-  for (int f = 0; f < 23; ++f) bg.in[f] = b.ba[f];
+  pack_bg(b.ba, bg.in);
   CG_CUDA(ctx, cg::mixed::launch_init(b.mdev, bg, ctx->stream));
   b.stage_next = 1;
   return CG_OK;
 }
 
-int mixed_stage(cg_ctx* ctx, Box& b, int n) {
+// Background of substep n of a mixed box: RK4 stage of the uniform state on
+// the host (FP64), then the bookkeeping of K{n}Finalize.
+cg::mixed::Bg mixed_prepare(Box& b, int n) {
   cg::mixed::Bg bg{};
   const double phi_lag = n == 1 ? b.ba[cg::F_PHI] : b.bprev[cg::F_PHI];
-  mixed_bg_rhs(b, b.ba, phi_lag, bg.rhs);
+  double rhs[23];
+  mixed_bg_rhs(b, b.ba, phi_lag, rhs);
   const double dt = b.desc.dt;
   double o[23];
   for (int f = 0; f < 23; ++f) {
-    const double cv = bg.rhs[f], pv = b.bp[f];
+    const double cv = rhs[f], pv = b.bp[f];
     if (n == 1) {
       b.bf[f] = dt * cv / 6.0;
       o[f] = pv + dt * cv / 2.0;
@@ -364,14 +392,12 @@ int mixed_stage(cg_ctx* ctx, Box& b, int n) {
       o[f] = b.bf[f] + (dt * cv / 6.0 + pv);
     }
   }
-  for (int f = 0; f < 23; ++f) {
-    bg.in[f] = b.ba[f];
-    bg.prev[f] = b.bprev[f];
-    bg.out[f] = o[f];
-  }
+  pack_bg(b.ba, bg.in);
+  pack_bg(b.bprev, bg.prev);
+  pack_bg(o, bg.out);
+  pack_bg(rhs, bg.rhs);
   bg.e6l = std::exp(-6.0 * phi_lag);
   bg.lambda = b.desc.lambda;
-  CG_CUDA(ctx, cg::mixed::launch_stage(b.mdev, bg, n, ctx->stream));
   for (int f = 0; f < 23; ++f) {
     b.bprev[f] = b.ba[f];
     b.ba[f] = o[f];
@@ -379,6 +405,12 @@ int mixed_stage(cg_ctx* ctx, Box& b, int n) {
   }
   b.stage_next = n == 4 ? 1 : n + 1;
   if (n == 4) ++b.steps;
+  return bg;
+}
+
+int mixed_stage(cg_ctx* ctx, Box& b, int n) {
+  const cg::mixed::Bg bg = mixed_prepare(b, n);
+  CG_CUDA(ctx, cg::mixed::launch_stage(b.mdev, bg, n, ctx->stream));
   return CG_OK;
 }
 
@@ -390,20 +422,28 @@ int do_init(cg_ctx* ctx, Box& b) {
   return CG_OK;
 }
 
-int do_stage(cg_ctx* ctx, Box& b, int n) {
-  if (b.mixed) return mixed_stage(ctx, b, n);
-  // FRW getters of the next substep (for the flux primitives of the output)
-  FrwHost nxt = b.frw;
+// Substep n of an FP64 box: the K_avg reduction its lapse may need (queued),
+// the FRW values of the launch, then the bookkeeping of K{n}Finalize, which
+// advances the FRW integrator (bssn.cc:267-305).
+int fp64_prepare(cg_ctx* ctx, Box& b, int n, StageBg* bg) {
+  FrwHost nxt = b.frw;  // FRW getters of the next substep (flux primitives of the output)
   nxt.stage(n, b.desc.dt);
-  StageBg bg = bg_for(b, n, nxt.get_phi);
+  *bg = bg_for(b, n, nxt.get_phi);
   int rc = launch_kavg(ctx, b, current_a(b));
   if (rc) return rc;
-  CG_CUDA(ctx, cg::launch_stage(b.variant, b.dev, bg, n, ctx->stream));
-  // BSSN::K{n}Finalize advances the FRW integrator (bssn.cc:267-305)
   b.phi_prev = b.frw.get_phi;
   b.frw = nxt;
   b.stage_next = n == 4 ? 1 : n + 1;
   if (n == 4) ++b.steps;
+  return CG_OK;
+}
+
+int do_stage(cg_ctx* ctx, Box& b, int n) {
+  if (b.mixed) return mixed_stage(ctx, b, n);
+  StageBg bg;
+  int rc = fp64_prepare(ctx, b, n, &bg);
+  if (rc) return rc;
+  CG_CUDA(ctx, cg::launch_stage(b.variant, b.dev, bg, n, ctx->stream));
   return CG_OK;
 }
 
@@ -632,6 +672,8 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
 int cg_destroy(cg_ctx* ctx) {
   if (!ctx) return CG_ERR_INVALID;
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  for (Group& g : ctx->groups) cudaFree(g.table);
   for (Box& b : ctx->boxes) free_box(b);
   cudaFree(ctx->red);
   cudaFree(ctx->status);
@@ -748,6 +790,272 @@ int cg_device_register(cg_ctx* ctx, int box, char reg, double** dptr) {
   return CG_OK;
 }
 
+}  // extern "C" (reopened below)
+namespace {
+// ---- launch groups --------------------------------------------------------------
+// Boxes with the same arithmetic, stencil order and matter model (up to
+// kMaxGroupBoxes per group) are advanced by one launch per substep when
+// CG_OPT_BATCH is on; a box without a partner keeps its own launch.
+
+template <class B>
+int bricks_along(int n, int b) { return (n + b - 1) / b; }
+
+// Device table of a group in its launch order (lpt: largest box first).
+int write_table(cg_ctx* ctx, Group& g) {
+  std::vector<int> order = g.members;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return g.lpt ? ctx->boxes[a].dev.pts > ctx->boxes[b].dev.pts : a < b;
+  });
+  g.members = order;
+  const size_t m = order.size();
+  int first = 0;
+  if (g.mixed) {
+    using Br = cg::tile::Brick32;
+    std::vector<cg::mixed::GroupBox> t(m);
+    for (size_t q = 0; q < m; ++q) {
+      const Box& b = ctx->boxes[order[q]];
+      cg::mixed::GroupBox& e = t[q];
+      e.nx = b.mdev.nx; e.ny = b.mdev.ny; e.nz = b.mdev.nz; e.pts = b.mdev.pts;
+      e.lapse = b.mdev.lapse; e.normalize = b.mdev.normalize;
+      e.idx = (float)(1.0 / b.mdev.dx);
+      e.dt = b.mdev.dt;
+      e.P = b.mdev.P; e.F = b.mdev.F; e.X = b.mdev.X; e.Y = b.mdev.Y; e.FP0 = b.mdev.FP0; e.FP1 = b.mdev.FP1;
+      e.status = b.mdev.status;
+      e.nbx = bricks_along<Br>(e.nx, Br::BX); e.nby = bricks_along<Br>(e.ny, Br::BY); e.nbz = bricks_along<Br>(e.nz, Br::BZ);
+      e.first = first;
+      first += e.nbx * e.nby * e.nbz;
+    }
+    if (!g.table) CG_CUDA(ctx, cudaMalloc(&g.table, sizeof(cg::mixed::GroupBox) * m));
+    CG_CUDA(ctx, cudaMemcpyAsync(g.table, t.data(), sizeof(cg::mixed::GroupBox) * m, cudaMemcpyHostToDevice, ctx->stream));
+    CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  } else {
+    using Br = cg::tile::Brick64;
+    std::vector<cg::GroupBox> t(m);
+    for (size_t q = 0; q < m; ++q) {
+      const Box& b = ctx->boxes[order[q]];
+      cg::GroupBox& e = t[q];
+      e.nx = b.dev.nx; e.ny = b.dev.ny; e.nz = b.dev.nz; e.pts = b.dev.pts;
+      e.ph = b.dev.ph;
+      e.kavg = b.dev.kavg;
+      e.P = b.dev.P; e.F = b.dev.F; e.X = b.dev.X; e.Y = b.dev.Y; e.FP0 = b.dev.FP0; e.FP1 = b.dev.FP1;
+      e.status = b.dev.status;
+      e.nbx = bricks_along<Br>(e.nx, Br::BX); e.nby = bricks_along<Br>(e.ny, Br::BY); e.nbz = bricks_along<Br>(e.nz, Br::BZ);
+      e.first = first;
+      first += e.nbx * e.nby * e.nbz;
+    }
+    if (!g.table) CG_CUDA(ctx, cudaMalloc(&g.table, sizeof(cg::GroupBox) * m));
+    CG_CUDA(ctx, cudaMemcpyAsync(g.table, t.data(), sizeof(cg::GroupBox) * m, cudaMemcpyHostToDevice, ctx->stream));
+    CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  g.total = first;
+  return CG_OK;
+}
+
+int ensure_groups(cg_ctx* ctx) {
+  if (ctx->grouped) return CG_OK;
+  for (Group& g : ctx->groups) cudaFree(g.table);
+  ctx->groups.clear();
+  ctx->singles.clear();
+  if (ctx->gexec) {
+    cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+  }
+  std::vector<bool> used(ctx->boxes.size(), false);
+  for (size_t a = 0; a < ctx->boxes.size(); ++a) {
+    if (used[a]) continue;
+    const Box& ba = ctx->boxes[a];
+    Group g;
+    g.mixed = ba.mixed;
+    g.variant = ba.variant;
+    g.order = ba.desc.stencil_order;
+    g.matter = ba.desc.matter;
+    for (size_t b = a; b < ctx->boxes.size() && g.members.size() < (size_t)cg::kMaxGroupBoxes; ++b) {
+      const Box& bb = ctx->boxes[b];
+      if (used[b] || bb.mixed != g.mixed || bb.variant != g.variant || bb.desc.stencil_order != g.order ||
+          bb.desc.matter != g.matter)
+        continue;
+      g.members.push_back((int)b);
+      used[b] = true;
+    }
+    if (!ctx->opt_batch || g.members.size() < 2) {
+      for (int q : g.members) ctx->singles.push_back(q);
+      continue;
+    }
+    g.grid = ctx->opt_group_grid;
+    int rc = write_table(ctx, g);
+    if (rc) {
+      cudaFree(g.table);
+      return rc;
+    }
+    ctx->groups.push_back(g);
+  }
+  std::sort(ctx->singles.begin(), ctx->singles.end());
+  ctx->grouped = true;
+  return CG_OK;
+}
+
+// Substep n of every member: backgrounds prepared (and the host state
+// advanced) box by box, one launch for the group.  `boxes` may be a scratch
+// copy of the context's boxes (the autotuner's trial launches).
+int group_launch(cg_ctx* ctx, Group& g, std::vector<Box>& boxes, int n) {
+  if (g.grid < 0) {
+    // the autotuner found the members' own launches faster
+    for (int q : g.members) {
+      int rc = do_stage(ctx, boxes[q], n);
+      if (rc) return rc;
+    }
+    return CG_OK;
+  }
+  if (g.mixed) {
+    cg::mixed::GroupBg gb{};
+    gb.nboxes = (int)g.members.size();
+    gb.total = g.total;
+    for (size_t q = 0; q < g.members.size(); ++q) gb.bg[q] = mixed_prepare(boxes[g.members[q]], n);
+    CG_CUDA(ctx, cg::mixed::launch_group(static_cast<const cg::mixed::GroupBox*>(g.table), gb, g.order, g.matter, n,
+                                         g.grid, ctx->stream));
+  } else {
+    cg::GroupBg gb{};
+    gb.nboxes = (int)g.members.size();
+    gb.total = g.total;
+    for (size_t q = 0; q < g.members.size(); ++q) {
+      int rc = fp64_prepare(ctx, boxes[g.members[q]], n, &gb.bg[q]);
+      if (rc) return rc;
+    }
+    CG_CUDA(ctx, cg::launch_group(g.variant, static_cast<const cg::GroupBox*>(g.table), gb, g.order, g.matter, n,
+                                  g.grid, ctx->stream));
+  }
+  return CG_OK;
+}
+
+int all_stage(cg_ctx* ctx, int n) {
+  for (Group& g : ctx->groups) {
+    int rc = group_launch(ctx, g, ctx->boxes, n);
+    if (rc) return rc;
+  }
+  for (int q : ctx->singles) {
+    int rc = do_stage(ctx, ctx->boxes[q], n);
+    if (rc) return rc;
+  }
+  return CG_OK;
+}
+
+// Autotuner: for each untuned group, time the substep-1 launch (it rewrites
+// only _f, the substep-2 input and its flux primitives, so repeating it
+// changes nothing) for both launch orders and for one CTA per brick or a
+// persistent grid of 1, 2 or 4 waves of resident CTAs, and the members' own
+// launches one after another; keep the fastest.
+int tune_groups(cg_ctx* ctx) {
+  if (!ctx->opt_autotune) return CG_OK;
+  int dev = 0, sms = 0;
+  CG_CUDA(ctx, cudaGetDevice(&dev));
+  CG_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  cudaEvent_t e0, e1;
+  CG_CUDA(ctx, cudaEventCreate(&e0));
+  cudaError_t ce = cudaEventCreate(&e1);
+  if (ce != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return cuda_fail(ctx, ce, "cudaEventCreate");
+  }
+  int rc = CG_OK;
+  for (Group& g : ctx->groups) {
+    if (g.tuned) continue;
+    bool ready = true;
+    for (int q : g.members) ready = ready && ctx->boxes[q].stage_next == 1;
+    if (!ready) continue;
+    const int per_sm = g.mixed ? cg::mixed::group_ctas_per_sm(g.order, g.matter)
+                               : cg::group_ctas_per_sm(g.variant, g.order, g.matter);
+    float best = 1e30f;
+    int best_lpt = 0, best_grid = 0;
+    for (int lpt = 0; lpt < 2 && rc == CG_OK; ++lpt) {
+      g.lpt = lpt;
+      rc = write_table(ctx, g);
+      for (int waves : {-1, 0, 1, 2, 4}) {
+        if (rc) break;
+        if (waves < 0 && lpt) continue;  // own launches: the order does not matter
+        const int grid = waves < 0 ? -1 : waves * sms * per_sm;
+        if (waves > 0 && grid >= g.total) continue;
+        g.grid = grid;
+        float ms = 0.0f;
+        for (int rep = 0; rep < 4 && rc == CG_OK; ++rep) {
+          std::vector<Box> trial = ctx->boxes;  // the trial's host bookkeeping is discarded
+          if (rep == 1) cudaEventRecord(e0, ctx->stream);
+          rc = group_launch(ctx, g, trial, 1);
+        }
+        if (rc) break;
+        cudaEventRecord(e1, ctx->stream);
+        ce = cudaEventSynchronize(e1);
+        if (ce != cudaSuccess) {
+          rc = cuda_fail(ctx, ce, "autotune");
+          break;
+        }
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+          best = ms;
+          best_lpt = lpt;
+          best_grid = grid;
+        }
+      }
+    }
+    if (rc) break;
+    g.lpt = best_lpt;
+    g.grid = best_grid;
+    rc = write_table(ctx, g);
+    if (rc) break;
+    g.tuned = true;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+// nsteps whole steps recorded as one CUDA graph and replayed; the executable
+// graph is kept and updated in place while the launch sequence keeps its shape.
+int graph_steps(cg_ctx* ctx, int nsteps) {
+  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    // e.g. the legacy default stream: run the launches directly
+    cudaGetLastError();
+    for (int s = 0; s < nsteps; ++s)
+      for (int n = 1; n <= 4; ++n) {
+        int rc = all_stage(ctx, n);
+        if (rc) return rc;
+      }
+    return CG_OK;
+  }
+  int rc = CG_OK;
+  for (int s = 0; s < nsteps && rc == CG_OK; ++s)
+    for (int n = 1; n <= 4 && rc == CG_OK; ++n) rc = all_stage(ctx, n);
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(ctx->stream, &graph);
+  if (rc) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+  bool updated = false;
+  if (ctx->gexec && ctx->gexec_steps == nsteps) {
+    cudaGraphExecUpdateResultInfo info{};
+    updated = cudaGraphExecUpdate(ctx->gexec, graph, &info) == cudaSuccess;
+    if (!updated) cudaGetLastError();
+  }
+  if (!updated) {
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    ctx->gexec = nullptr;
+    e = cudaGraphInstantiate(&ctx->gexec, graph, 0);
+    if (e != cudaSuccess) {
+      ctx->gexec = nullptr;
+      cudaGraphDestroy(graph);
+      return cuda_fail(ctx, e, "cudaGraphInstantiate");
+    }
+    ctx->gexec_steps = nsteps;
+  }
+  cudaGraphDestroy(graph);
+  CG_CUDA(ctx, cudaGraphLaunch(ctx->gexec, ctx->stream));
+  return CG_OK;
+}
+
+}  // namespace
+extern "C" {
 int cg_step_init(cg_ctx* ctx) {
   if (!ctx) return CG_ERR_INVALID;
   for (Box& b : ctx->boxes) {
@@ -764,11 +1072,13 @@ int cg_rk_stage(cg_ctx* ctx, int n) {
     if (b.stage_next != n)
       return fail(ctx, CG_ERR_STATE, "substep " + std::to_string(n) + " called out of order (expected " +
                                           std::to_string(b.stage_next) + ")");
-  for (Box& b : ctx->boxes) {
-    int rc = do_stage(ctx, b, n);
+  int rc = ensure_groups(ctx);
+  if (rc) return rc;
+  if (n == 1) {
+    rc = tune_groups(ctx);
     if (rc) return rc;
   }
-  return CG_OK;
+  return all_stage(ctx, n);
 }
 
 int cg_step(cg_ctx* ctx, int nsteps) {
@@ -776,18 +1086,69 @@ int cg_step(cg_ctx* ctx, int nsteps) {
   if (nsteps < 0) return fail(ctx, CG_ERR_INVALID, "nsteps must be >= 0");
   for (Box& b : ctx->boxes)
     if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "a step is in progress; finish it with cg_rk_stage");
-  for (int s = 0; s < nsteps; ++s) {
-    for (Box& b : ctx->boxes) {
-      if (b.stage_next == 0) {
-        int rc = do_init(ctx, b);
-        if (rc) return rc;
-      }
-      for (int n = 1; n <= 4; ++n) {
-        int rc = do_stage(ctx, b, n);
-        if (rc) return rc;
-      }
+  if (nsteps == 0) return CG_OK;
+  for (Box& b : ctx->boxes)
+    if (b.stage_next == 0) {
+      int rc = do_init(ctx, b);
+      if (rc) return rc;
     }
+  int rc = ensure_groups(ctx);
+  if (rc) return rc;
+  rc = tune_groups(ctx);
+  if (rc) return rc;
+  if (ctx->opt_graph) return graph_steps(ctx, nsteps);
+  for (int s = 0; s < nsteps; ++s)
+    for (int n = 1; n <= 4; ++n) {
+      rc = all_stage(ctx, n);
+      if (rc) return rc;
+    }
+  return CG_OK;
+}
+
+int cg_set_option(cg_ctx* ctx, int option, int value) {
+  if (!ctx) return CG_ERR_INVALID;
+  switch (option) {
+    case CG_OPT_BATCH:
+      if (ctx->opt_batch != (value != 0)) {
+        for (Box& b : ctx->boxes)
+          if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "change CG_OPT_BATCH between steps");
+        ctx->opt_batch = value != 0;
+        ctx->grouped = false;
+      }
+      return CG_OK;
+    case CG_OPT_GRAPH: ctx->opt_graph = value != 0; return CG_OK;
+    case CG_OPT_AUTOTUNE: ctx->opt_autotune = value != 0; return CG_OK;
+    case CG_OPT_GROUP_GRID:
+      if (value < -1) return fail(ctx, CG_ERR_INVALID, "CG_OPT_GROUP_GRID must be >= -1");
+      ctx->opt_group_grid = value;
+      for (Group& g : ctx->groups)
+        if (!g.tuned) g.grid = value;
+      return CG_OK;
+    default: return fail(ctx, CG_ERR_INVALID, "unknown option");
   }
+}
+
+int cg_num_groups(cg_ctx* ctx, int* n) {
+  if (!ctx || !n) return CG_ERR_INVALID;
+  int rc = ensure_groups(ctx);
+  if (rc) return rc;
+  *n = (int)ctx->groups.size();
+  return CG_OK;
+}
+
+int cg_group_info(cg_ctx* ctx, int group, int* info, int n) {
+  if (!ctx) return CG_ERR_INVALID;
+  if (!info || n < 6) return fail(ctx, CG_ERR_INVALID, "info needs 6 entries");
+  int rc = ensure_groups(ctx);
+  if (rc) return rc;
+  if (group < 0 || group >= (int)ctx->groups.size()) return fail(ctx, CG_ERR_INVALID, "group index out of range");
+  const Group& g = ctx->groups[group];
+  info[0] = (int)g.members.size();
+  info[1] = g.total;
+  info[2] = g.grid;
+  info[3] = g.lpt;
+  info[4] = g.tuned ? 1 : 0;
+  info[5] = g.members.empty() ? -1 : g.members[0];
   return CG_OK;
 }
 

@@ -1,0 +1,28 @@
+// cg_group.h -- launch groups: boxes of the same order, matter model and
+// arithmetic advanced by one launch per substep (host and device types).
+#pragma once
+
+#include "cg_types.h"
+
+namespace cg {
+
+// One FP64 box of a launch group: geometry, numerics and register blocks, its
+// brick counts along x, y, z and the index of its first brick in the launch's
+// work list.  Device table, written once when the group is formed.
+struct GroupBox {
+  int nx, ny, nz, pts;
+  Physics ph;
+  const double* kavg;
+  double *P, *F, *X, *Y, *FP0, *FP1;
+  unsigned* status;
+  int nbx, nby, nbz;
+  int first;
+};
+constexpr int kMaxGroupBoxes = 64;
+// Per-substep values of every box of an FP64 group (kernel parameter, by value).
+struct GroupBg {
+  int nboxes, total;
+  StageBg bg[kMaxGroupBoxes];
+};
+
+}  // namespace cg

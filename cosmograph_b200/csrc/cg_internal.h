@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include "cg_group.h"
 #include "cg_types.h"
 
 namespace cg {
@@ -38,8 +39,14 @@ struct MixedBox {
 };
 namespace mixed {
 struct Bg;
+struct GroupBox;
+struct GroupBg;
 cudaError_t launch_stage(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st);
 cudaError_t launch_init(const MixedBox& b, const Bg& bg, cudaStream_t st);
+// one launch for substep `stage` of every box of a mixed group (as launch_group)
+cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
+                         cudaStream_t st);
+int group_ctas_per_sm(int order, int matter);
 }  // namespace mixed
 
 // Kernel variants: identical source, compiled without (exact) or with (fast)
@@ -58,6 +65,28 @@ namespace fast {
 cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
 cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
 }  // namespace fast
+
+// One launch for substep `stage` of every box of an FP64 group (table: device
+// copy of the group's GroupBox entries in launch order).  grid <= 0: one CTA
+// per brick; otherwise a persistent grid of that many CTAs.
+namespace exact {
+cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
+                         cudaStream_t st);
+int group_ctas_per_sm(int order, int matter);
+}  // namespace exact
+namespace fast {
+cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
+                         cudaStream_t st);
+int group_ctas_per_sm(int order, int matter);
+}  // namespace fast
+inline cudaError_t launch_group(int v, const GroupBox* table, const GroupBg& gb, int order, int matter, int stage,
+                                int grid, cudaStream_t st) {
+  return v == kFast ? fast::launch_group(table, gb, order, matter, stage, grid, st)
+                    : exact::launch_group(table, gb, order, matter, stage, grid, st);
+}
+inline int group_ctas_per_sm(int v, int order, int matter) {
+  return v == kFast ? fast::group_ctas_per_sm(order, matter) : exact::group_ctas_per_sm(order, matter);
+}
 
 // Volume-weighted average (utils/math.h:1403-1415) of n values of `field`,
 // weights exp(6 (phi + phi_frw)); `partial` holds 2*nblk doubles of scratch,

@@ -21,6 +21,7 @@
 // static lapse, a_adj_amp = k_damping_amp = 0.
 #pragma once
 
+#include "cg_group.h"
 #include "cg_tile.cuh"
 #include "cg_types.h"
 
@@ -45,14 +46,37 @@ struct Ptrs {
   unsigned* status;
 };
 
-// Uniform background of one substep (FP64, one value per field).
+// Uniform background of one substep (FP64).  A uniform state keeps every
+// field but K, phi, alpha and D at zero, so only those four are stored, at
+// index bgi(field).
 struct Bg {
-  double in[23];     // abar of a^n
-  double prev[23];   // abar of a^{n-1}
-  double out[23];    // abar of the substep output
-  double rhs[23];    // RHS(abar of a^n), added to the kernel's perturbation RHS
+  double in[4];      // abar of a^n
+  double prev[4];    // abar of a^{n-1}
+  double out[4];     // abar of the substep output
+  double rhs[4];     // RHS(abar of a^n), added to the kernel's perturbation RHS
   double e6l;        // exp(-6 phibar) of the state whose W, sqrt(gamma) the sources lag on
   double lambda;     // rho_Lambda
+};
+__host__ __device__ constexpr int bgi(int f) {
+  return f == F_K ? 0 : (f == F_PHI ? 1 : (f == F_ALPHA ? 2 : (f == F_D ? 3 : -1)));
+}
+__host__ __device__ inline double bgv(const double* a, int f) { return bgi(f) < 0 ? 0.0 : a[bgi(f)]; }
+
+// One box of a mixed launch group (device table) and the per-substep
+// backgrounds of a group (kernel parameter); as the FP64 GroupBox / GroupBg.
+struct GroupBox {
+  int nx, ny, nz, pts, lapse, normalize;
+  float idx;
+  double dt;
+  double *P, *F;
+  float *X, *Y, *FP0, *FP1;
+  unsigned* status;
+  int nbx, nby, nbz;
+  int first;
+};
+struct GroupBg {
+  int nboxes, total;
+  Bg bg[kMaxGroupBoxes];
 };
 
 // per-thread FP32 slots (same meaning as the FP64 kernel's)
@@ -222,9 +246,10 @@ __device__ __forceinline__ void flux_divergences(const T& t, const float* __rest
   }
 }
 
+// The FP32-mixed substep for the brick at brick coordinates (cx, cy, cz).
 template <int O, int MATTER>
-__global__ void __launch_bounds__(kThreads, 4)
-mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt, Bg bg, Ptrs P, int stage) {
+__device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt,
+                                           const Bg& bg, const Ptrs& P, int stage, int cx, int cy, int cz) {
   constexpr int NFLD = MATTER == kDust ? 22 : 18;
   constexpr int R = O / 2;
   constexpr float kPif = 3.14159265358979f;
@@ -232,9 +257,9 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
   const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
   float* sl = smf + tid;
   auto S = [&](int s) -> float& { return sl[s * kThreads]; };
-  const int k0 = blockIdx.x * kBZ + threadIdx.x;
-  const int j0 = blockIdx.y * kBY + threadIdx.y;
-  const int i0 = blockIdx.z * kBX + threadIdx.z;
+  const int k0 = cz * kBZ + threadIdx.x;
+  const int j0 = cy * kBY + threadIdx.y;
+  const int i0 = cx * kBX + threadIdx.z;
   // every thread takes part in the tile copies; threads past the box edge
   // compute a valid point and leave after phase 1
   const bool live = i0 < nx && j0 < ny && k0 < nz;
@@ -249,7 +274,7 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
   for (int q = 0; q < 6; ++q) g[q] = D_(F_G11 + q);
   inv_metricf(g, gi);
 
-  const int x0 = blockIdx.z * kBX, y0 = blockIdx.y * kBY, z0 = blockIdx.x * kBZ;
+  const int x0 = cx * kBX, y0 = cy * kBY, z0 = cz * kBZ;
   const float idx2 = idx * idx;
   {
     static_assert(TileG<O>::SIZE * sizeof(float) + TileG<O>::ROWS * sizeof(int) <=
@@ -278,7 +303,7 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
 
   // ---- centre values: perturbations and full values -------------------------
   const float dphi0 = D_(F_PHI), dK = D_(F_K), dal = D_(F_ALPHA);
-  const float phib = (float)bg.in[F_PHI], Kb = (float)bg.in[F_K], alb = (float)(1.0 + bg.in[F_ALPHA]);
+  const float phib = (float)bgv(bg.in, F_PHI), Kb = (float)bgv(bg.in, F_K), alb = (float)(1.0 + bgv(bg.in, F_ALPHA));
   const float phi = phib + dphi0, K = Kb + dK, alpha = alb + dal;
   float gm[6];
   gm[0] = g[0] + 1.0f; gm[1] = g[1]; gm[2] = g[2];
@@ -289,7 +314,7 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
   float rhs_m[4] = {0.f, 0.f, 0.f, 0.f};
   float dr = 0.f, Sdust = 0.f, rS_full = 0.f;  // delta rho, S (second order), full rho + S
   if (MATTER == kDust) {
-    const float Db = (float)bg.in[F_D];
+    const float Db = (float)bgv(bg.in, F_D);
     const float D = Db + D_(F_D);
     const float Sv[3] = {D_(F_S1), D_(F_S2), D_(F_S3)};
     // lagged W, sqrt(gamma), g_ij (Dust::addBSSNSrc, dust.cc:226-264)
@@ -305,8 +330,8 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
       for (int m = 0; m < 6; ++m) gl[m] = pv[(size_t)(F_G11 + m) * N + c];
       inv_metricf(gl, gil);
       dphil = pv[(size_t)F_PHI * N + c];
-      phil = (float)bg.prev[F_PHI] + dphil;
-      Dl = (float)bg.prev[F_D] + pv[(size_t)F_D * N + c];
+      phil = (float)bgv(bg.prev, F_PHI) + dphil;
+      Dl = (float)bgv(bg.prev, F_D) + pv[(size_t)F_D * N + c];
       Sl[0] = pv[(size_t)F_S1 * N + c]; Sl[1] = pv[(size_t)F_S2 * N + c]; Sl[2] = pv[(size_t)F_S3 * N + c];
     }
     const float em4l = __expf(-4.0f * phil), e6l = __expf(6.0f * phil), e4l = __expf(4.0f * phil);
@@ -316,7 +341,7 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
     dr = e6bl * (dl.W * D * expm1f(-6.0f * dphil) + dl.Wm1 * D + D_(F_D));
     const float inv_detg = 1.0f / e6l;
     Sdust = D * inv_detg * dl.w2 / dl.W;
-    rS_full = (float)(bg.in[F_D] * bg.e6l) + dr + Sdust - 2.0f * (float)bg.lambda;
+    rS_full = (float)(bgv(bg.in, F_D) * bg.e6l) + dr + Sdust - 2.0f * (float)bg.lambda;
     S(S_SRC + Q_R) = dr;
     S(S_SRC + Q_S) = Sdust;
 #pragma unroll
@@ -468,7 +493,7 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
   // ---- perturbation right-hand sides + FP64 register update ----------------------
   double outv[NFLD];
   auto finalize = [&](int fld, float drhs) {
-    const double cv = bg.rhs[fld] + (double)drhs;
+    const double cv = bgv(bg.rhs, fld) + (double)drhs;
     const double pv = P.p[(size_t)fld * N + c];
     double o;
     if (stage == 1) {
@@ -566,7 +591,7 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
     }
   }
 #pragma unroll
-  for (int f = 0; f < NFLD; ++f) P.out[(size_t)f * N + c] = (float)(outv[f] - bg.out[f]);
+  for (int f = 0; f < NFLD; ++f) P.out[(size_t)f * N + c] = (float)(outv[f] - bgv(bg.out, f));
   if (MATTER == kDust) {
     float go[6], gio[6];
 #pragma unroll
@@ -583,6 +608,57 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
     for (int m = 0; m < 3; ++m) fo[(size_t)(P_AS1 + m) * N + c] = alo * So[m];
 #pragma unroll
     for (int m = 0; m < 3; ++m) fo[(size_t)(P_V1 + m) * N + c] = dp.v[m];
+  }
+}
+
+// One box: one CTA per brick.
+template <int O, int MATTER>
+__global__ void __launch_bounds__(kThreads, 4)
+mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt, Bg bg, Ptrs P, int stage) {
+  mixed_body<O, MATTER>(nx, ny, nz, lapse, normalize, idx, dt, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x);
+}
+
+// Register roles of substep n (X/Y ping-pong, as in the single-box launcher).
+__device__ __forceinline__ Ptrs group_ptrs(const GroupBox& b, int stage) {
+  Ptrs p{};
+  p.p = b.P;
+  p.f = b.F;
+  p.newp = b.P;
+  p.status = b.status;
+  switch (stage) {
+    case 1: p.in = b.X; p.prev = nullptr; p.out = b.Y; p.fp_in = b.FP0; p.fp_out = b.FP1; break;
+    case 2: p.in = b.Y; p.prev = b.X; p.out = b.X; p.fp_in = b.FP1; p.fp_out = b.FP0; break;
+    case 3: p.in = b.X; p.prev = b.Y; p.out = b.Y; p.fp_in = b.FP0; p.fp_out = b.FP1; break;
+    default: p.in = b.Y; p.prev = b.X; p.out = b.X; p.fp_in = b.FP1; p.fp_out = b.FP0; break;
+  }
+  return p;
+}
+
+// A group of mixed boxes, one launch per substep over the work list of all
+// their bricks (see the FP64 stage_group_kernel).
+template <int O, int MATTER>
+__global__ void __launch_bounds__(kThreads, 4)
+mixed_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
+  __shared__ GroupBox sb;
+  __shared__ Ptrs sp;
+  __shared__ Bg sbg;
+  const bool lead = threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0;
+  for (int w = blockIdx.x; w < gb.total; w += gridDim.x) {
+    __syncthreads();  // the previous brick is finished with the slots, the tile and sb
+    if (lead) {
+      int lo = 0, hi = gb.nboxes - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (boxes[mid].first <= w) lo = mid; else hi = mid - 1;
+      }
+      sb = boxes[lo];
+      sp = group_ptrs(sb, stage);
+      sbg = gb.bg[lo];
+    }
+    __syncthreads();
+    const int l = w - sb.first;
+    const int cz = l % sb.nbz, cy = (l / sb.nbz) % sb.nby, cx = l / (sb.nbz * sb.nby);
+    mixed_body<O, MATTER>(sb.nx, sb.ny, sb.nz, sb.lapse, sb.normalize, sb.idx, sb.dt, sbg, sp, stage, cx, cy, cz);
   }
 }
 
@@ -630,7 +706,7 @@ __global__ void __launch_bounds__(kThreads) mixed_init_kernel(int nx, int ny, in
 #pragma unroll
   for (int m = 0; m < 6; ++m) { v[F_G11 + m] = gn[m]; v[F_A11 + m] = An[m]; }
 #pragma unroll
-  for (int f = 0; f < NFLD; ++f) X[(size_t)f * N + c] = (float)(v[f] - bg.in[f]);
+  for (int f = 0; f < NFLD; ++f) X[(size_t)f * N + c] = (float)(v[f] - bgv(bg.in, f));
   if (MATTER == kDust) {
     float go[6], gio[6];
 #pragma unroll

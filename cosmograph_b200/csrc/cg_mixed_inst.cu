@@ -30,7 +30,50 @@ template <int O>
 cudaError_t go_m(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
   return b.matter == kDust ? go<O, kDust>(b, bg, stage, st) : go<O, kVacuum>(b, bg, stage, st);
 }
+template <int O, int M>
+cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, cudaStream_t st) {
+  constexpr size_t smem = sizeof(float) * S_NSLOT * kThreads;
+  const int g = grid > 0 ? grid : gb.total;
+  mixed_group_kernel<O, M><<<g, dim3(kBZ, kBY, kBX), smem, st>>>(table, gb, stage);
+  return cudaGetLastError();
+}
+template <int O>
+cudaError_t go_group_m(const GroupBox* table, const GroupBg& gb, int matter, int stage, int grid, cudaStream_t st) {
+  return matter == kDust ? go_group<O, kDust>(table, gb, stage, grid, st) : go_group<O, kVacuum>(table, gb, stage, grid, st);
+}
+template <int O, int M>
+int ctas() {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mixed_group_kernel<O, M>, kThreads,
+                                                    sizeof(float) * S_NSLOT * kThreads) != cudaSuccess)
+    return 1;
+  return n > 0 ? n : 1;
+}
+template <int O>
+int ctas_m(int matter) {
+  return matter == kDust ? ctas<O, kDust>() : ctas<O, kVacuum>();
+}
 }  // namespace
+
+cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
+                         cudaStream_t st) {
+  switch (order) {
+    case 2: return go_group_m<2>(table, gb, matter, stage, grid, st);
+    case 4: return go_group_m<4>(table, gb, matter, stage, grid, st);
+    case 6: return go_group_m<6>(table, gb, matter, stage, grid, st);
+    case 8: return go_group_m<8>(table, gb, matter, stage, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int group_ctas_per_sm(int order, int matter) {
+  switch (order) {
+    case 2: return ctas_m<2>(matter);
+    case 4: return ctas_m<4>(matter);
+    case 6: return ctas_m<6>(matter);
+    default: return ctas_m<8>(matter);
+  }
+}
 
 cudaError_t launch_stage(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
   switch (b.order) {

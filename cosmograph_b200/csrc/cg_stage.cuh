@@ -33,6 +33,7 @@
 // the others wrap every tap.
 #pragma once
 
+#include "cg_group.h"
 #include "cg_point.cuh"
 #include "cg_tile.cuh"
 
@@ -104,6 +105,22 @@ struct SlotsC {
 };
 // per-block partial results of the constraint pass (see constraint_reduce)
 constexpr int kCPart = 27;
+
+// Register roles of substep n, the same for every box (X/Y ping-pong).
+__device__ __forceinline__ StagePtrs group_ptrs(const GroupBox& b, int stage) {
+  StagePtrs p{};
+  p.p = b.P;
+  p.f = b.F;
+  p.status = b.status;
+  p.kavg = b.kavg;
+  switch (stage) {
+    case 1: p.in = b.X; p.prev = nullptr; p.out = b.Y; p.fp_in = b.FP0; p.fp_out = b.FP1; break;
+    case 2: p.in = b.Y; p.prev = b.X; p.out = b.X; p.fp_in = b.FP1; p.fp_out = b.FP0; break;
+    case 3: p.in = b.X; p.prev = b.Y; p.out = b.Y; p.fp_in = b.FP0; p.fp_out = b.FP1; break;
+    default: p.in = b.Y; p.prev = b.X; p.out = b.P; p.norm = b.X; p.fp_in = b.FP1; p.fp_out = b.FP0; break;
+  }
+  return p;
+}
 
 namespace CG_VARIANT_NS {
 
@@ -319,7 +336,7 @@ __device__ __forceinline__ void flux_divergences(const T& t, const double* __res
 // summed, the rest maximised; warp shuffles, then the warps in order.  Thread
 // 0 writes the Q results of this CTA to part[cta * Q].
 template <int Q, int NSUM>
-__device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part) {
+__device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part, int cta) {
   __shared__ double red[kThreads / 32][Q];
   const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
   const int lane = tid & 31, warp = tid >> 5;
@@ -335,7 +352,6 @@ __device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part) {
   }
   __syncthreads();
   if (tid == 0) {
-    const int cta = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
 #pragma unroll 1
     for (int m = 0; m < Q; ++m) {
       double x = red[0][m];
@@ -345,9 +361,11 @@ __device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part) {
   }
 }
 
+// The fused substep for the brick at brick coordinates (cx, cy, cz) of one
+// box; cta numbers the CTA's partial results in constraint mode.
 template <int O, int MATTER, int MODE>
-__global__ void __launch_bounds__(kThreads, 2)
-stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
+__device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph, StageBg bg, const StagePtrs& P,
+                                           int stage, int cx, int cy, int cz, int cta) {
   constexpr int NFLD = NF<MATTER>::value;
   constexpr int NSLOT = MODE == kConstraints ? SlotsC<MATTER>::value : Slots<MATTER>::value;
   static_assert(NSLOT >= S_MAT, "the tile region lies inside the slot array");
@@ -360,9 +378,9 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
   double* sl = smem + tid;  // this thread's slot column
   auto S = [&](int s) -> double& { return sl[s * kThreads]; };
 
-  const int k0 = blockIdx.x * kBZ + threadIdx.x;
-  const int j0 = blockIdx.y * kBY + threadIdx.y;
-  const int i0 = blockIdx.z * kBX + threadIdx.z;
+  const int k0 = cz * kBZ + threadIdx.x;
+  const int j0 = cy * kBY + threadIdx.y;
+  const int i0 = cx * kBX + threadIdx.z;
   const bool live = i0 < geo.nx && j0 < geo.ny && k0 < geo.nz;
   // every thread takes part in the tile copies of phase 1 (and, in constraint
   // mode, in the CTA reduction); threads past the box edge compute a valid
@@ -381,7 +399,7 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
   inv_metric(g, gi);
 
   // ---- phase 1: derivatives into shared memory ---------------------------------
-  const int x0 = blockIdx.z * kBX, y0 = blockIdx.y * kBY, z0 = blockIdx.x * kBZ;
+  const int x0 = cx * kBX, y0 = cy * kBY, z0 = cz * kBZ;
   {
     double* tl = smem + kTileSlot * kThreads;
     int* rowoff = reinterpret_cast<int*>(tl + TileG<O>::SIZE);
@@ -730,7 +748,7 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
     }
     q[15] = live ? v[0] * v[0] * dx * dx * dx : 0.0;
     q[16] = live ? v[1] * v[1] * dx * dx * dx : 0.0;
-    cta_reduce<kCPart, 17>(q, P.cpart);
+    cta_reduce<kCPart, 17>(q, P.cpart, cta);
     return;
   }
 
@@ -861,6 +879,46 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
     for (int m = 0; m < 3; ++m) fo[(size_t)(P_AS1 + m) * N + c] = alo * So[m];
 #pragma unroll
     for (int m = 0; m < 3; ++m) fo[(size_t)(P_V1 + m) * N + c] = dp.v[m];
+  }
+}
+
+// One box: one CTA per brick.
+template <int O, int MATTER, int MODE>
+__global__ void __launch_bounds__(kThreads, 2)
+stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
+  stage_body<O, MATTER, MODE>(geo, ph, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x,
+                              blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
+}
+
+// A group of boxes of the same order and matter model, one launch per
+// substep: the bricks of all boxes form one work list (boxes[] in launch
+// order, box b's bricks at [first, first + bricks)); each CTA takes work
+// items blockIdx.x, blockIdx.x + gridDim.x, ... (a persistent launch when the
+// grid is smaller than the list).
+template <int O, int MATTER>
+__global__ void __launch_bounds__(kThreads, 2)
+stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
+  __shared__ GroupBox sb;
+  __shared__ StagePtrs sp;
+  __shared__ StageBg sbg;
+  const bool lead = threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0;
+  for (int w = blockIdx.x; w < gb.total; w += gridDim.x) {
+    __syncthreads();  // the previous brick is finished with the slots, the tile and sb
+    if (lead) {
+      int lo = 0, hi = gb.nboxes - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (boxes[mid].first <= w) lo = mid; else hi = mid - 1;
+      }
+      sb = boxes[lo];
+      sp = group_ptrs(sb, stage);
+      sbg = gb.bg[lo];
+    }
+    __syncthreads();
+    const int l = w - sb.first;
+    const int cz = l % sb.nbz, cy = (l / sb.nbz) % sb.nby, cx = l / (sb.nbz * sb.nby);
+    const BoxGeom geo{sb.nx, sb.ny, sb.nz, sb.pts};
+    stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0);
   }
 }
 

@@ -123,6 +123,49 @@ cudaError_t go_constraints_m(const BoxDev& b, const StageBg& bg, double* cvals, 
   }
 }
 
+template <int O, int M>
+cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, cudaStream_t st) {
+  constexpr size_t smem = sizeof(double) * Slots<M>::value * kThreads;
+  static bool configured = false;
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(stage_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  const int g = grid > 0 ? grid : gb.total;
+  stage_group_kernel<O, M><<<g, stage_block(), smem, st>>>(table, gb, stage);
+  return cudaGetLastError();
+}
+
+template <int O, int M>
+int ctas_per_sm() {
+  constexpr size_t smem = sizeof(double) * Slots<M>::value * kThreads;
+  if (cudaFuncSetAttribute(stage_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_group_kernel<O, M>, kThreads, smem) != cudaSuccess)
+    return 1;
+  return n > 0 ? n : 1;
+}
+
+template <int O>
+cudaError_t go_group_m(const GroupBox* table, const GroupBg& gb, int matter, int stage, int grid, cudaStream_t st) {
+  switch (matter) {
+    case kDust: return go_group<O, kDust>(table, gb, stage, grid, st);
+    case kScalar: return go_group<O, kScalar>(table, gb, stage, grid, st);
+    default: return go_group<O, kVacuum>(table, gb, stage, grid, st);
+  }
+}
+template <int O>
+int ctas_m(int matter) {
+  switch (matter) {
+    case kDust: return ctas_per_sm<O, kDust>();
+    case kScalar: return ctas_per_sm<O, kScalar>();
+    default: return ctas_per_sm<O, kVacuum>();
+  }
+}
+
 template <int O>
 cudaError_t go_stage_m(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
   switch (b.matter) {
@@ -150,6 +193,26 @@ cudaError_t launch_constraints(const BoxDev& b, const StageBg& bg, double* cvals
     case 6: return go_constraints_m<6>(b, bg, cvals, cpart, st);
     case 8: return go_constraints_m<8>(b, bg, cvals, cpart, st);
     default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
+                         cudaStream_t st) {
+  switch (order) {
+    case 2: return go_group_m<2>(table, gb, matter, stage, grid, st);
+    case 4: return go_group_m<4>(table, gb, matter, stage, grid, st);
+    case 6: return go_group_m<6>(table, gb, matter, stage, grid, st);
+    case 8: return go_group_m<8>(table, gb, matter, stage, grid, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+int group_ctas_per_sm(int order, int matter) {
+  switch (order) {
+    case 2: return ctas_m<2>(matter);
+    case 4: return ctas_m<4>(matter);
+    case 6: return ctas_m<6>(matter);
+    default: return ctas_m<8>(matter);
   }
 }
 

@@ -152,6 +152,24 @@ class Evolution:
         self._check(self.L.cg_status(self.ctx, ctypes.byref(f)))
         return int(f.value)
 
+    def set_option(self, option: str, value: int) -> None:
+        """Launch options: "batch", "graph", "autotune", "group_grid" (cg_set_option)."""
+        code = {"batch": _lib.OPT_BATCH, "graph": _lib.OPT_GRAPH, "autotune": _lib.OPT_AUTOTUNE,
+                "group_grid": _lib.OPT_GROUP_GRID}[option]
+        self._check(self.L.cg_set_option(self.ctx, code, int(value)))
+
+    def groups(self) -> list[dict]:
+        """Launch groups: boxes, bricks, CTAs per launch, launch order, tuned."""
+        n = ctypes.c_int()
+        self._check(self.L.cg_num_groups(self.ctx, ctypes.byref(n)))
+        out = []
+        for g in range(n.value):
+            info = (ctypes.c_int * 6)()
+            self._check(self.L.cg_group_info(self.ctx, g, info, 6))
+            out.append({"boxes": info[0], "bricks": info[1], "grid": info[2], "largest_first": info[3],
+                        "tuned": bool(info[4]), "first_box": info[5]})
+        return out
+
     def stream(self) -> int:
         s = ctypes.c_void_p()
         self._check(self.L.cg_get_stream(self.ctx, ctypes.byref(s)))

@@ -163,6 +163,37 @@ int cg_rk_stage(cg_ctx *ctx, int n);
  * Asynchronous: returns once the work is queued. */
 int cg_step(cg_ctx *ctx, int nsteps);
 
+/* Launch options (cg_set_option).  No reference counterpart: the reference
+ * evolves one box per process.
+ *   CG_OPT_BATCH     1 (default): boxes of a context with the same precision,
+ *                    stencil order and matter model (up to 64 per group) share
+ *                    one launch per substep; 0: one launch per box.  Change it
+ *                    between steps only.
+ *   CG_OPT_GRAPH     1: cg_step records its launches as one CUDA graph and
+ *                    replays it (the graph is kept and updated in place while
+ *                    nsteps stays the same); 0 (default): direct launches.
+ *   CG_OPT_AUTOTUNE  1 (default): before the first substep of a batched group,
+ *                    time its launch shapes (launch order of the boxes, one CTA
+ *                    per brick, a persistent grid of 1, 2 or 4 waves, or the
+ *                    boxes' own launches) and keep the fastest.  Results do
+ *                    not depend on the choice.
+ *   CG_OPT_GROUP_GRID the launch shape of groups the autotuner has not set:
+ *                    0 (default) one CTA per brick, n > 0 a persistent grid of
+ *                    n CTAs, -1 one launch per box. */
+#define CG_OPT_BATCH 1
+#define CG_OPT_GRAPH 2
+#define CG_OPT_AUTOTUNE 3
+#define CG_OPT_GROUP_GRID 4
+int cg_set_option(cg_ctx *ctx, int option, int value);
+
+/* Launch groups of the context (formed on first use), and for group g:
+ * info[0] boxes, [1] bricks, [2] CTAs per launch (0: one per brick, -1: one
+ * launch per box),
+ * [3] launch order (0: box index, 1: largest box first), [4] tuned (0/1),
+ * [5] the first box of the launch order.  n >= 6. */
+int cg_num_groups(cg_ctx *ctx, int *n);
+int cg_group_info(cg_ctx *ctx, int group, int *info, int n);
+
 /* Wait for queued work; returns CG_ERR_NAN if a NaN appeared in DIFFphi. */
 int cg_synchronize(cg_ctx *ctx);
 
