@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference CPU build (rank 0)")
     ap.add_argument("--ncu", action="store_true", help="short run for profiler capture (no JSON extras)")
     ap.add_argument("--variants", default="fp64_fma,mixed", help="comma list of extra precisions timed alongside")
+    ap.add_argument("--workload", choices=["box", "ensemble"], default="box",
+                    help="box: one 256^3 box per GPU; ensemble: 48 boxes of 32^3/64^3/96^3 split over the GPUs")
     return ap.parse_args()
 
 
@@ -196,6 +198,144 @@ def cpu_baseline(st, order: int, budget_s: float = 30.0):
                       f"{sum(step_s):.2f} s of step loop, {wall:.1f} s wall"}
 
 
+def run_ensemble(a, world, rank, local):
+    """--workload ensemble: 48 independent BSSN + dust boxes (16 each of 32^3,
+    64^3, 96^3), order 4, FP32-mixed, seeded GRF initial data with rms delta
+    log-uniform in [1e-5, 1e-3]; the boxes are split across ranks (no data-path
+    communication).  value: updates/s of the batched launch (one launch per
+    substep, autotuned); variants: the boxes' own launches, CUDA-graph replay;
+    accuracy: every box against an FP64 run of the same steps."""
+    import ctypes
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from cosmograph_b200 import ensemble
+    from cosmograph_b200.evolution import BoxConfig, Evolution
+
+    specs = ensemble.standard_ensemble()
+    mine = ensemble.local_share(specs, rank, world)
+    states = ensemble.initial_states(mine, order=4)
+    pts = sum(s.fields[0].size for s in states)
+    all_pts = sum(s.points for s in specs)
+    cfg = BoxConfig(order=4, lapse="Harmonic", precision="mixed")
+    stream = torch.cuda.Stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(opts, steps, clk=None):
+        ev = Evolution(states, [cfg] * len(states))
+        for k, v in opts.items():
+            ev.set_option(k, v)
+        ev.set_stream(stream.cuda_stream)
+        ev.step(max(a.warmup, 0))
+        ev.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if clk:
+            clk.__enter__()
+        e0.record(stream)
+        ev.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if clk:
+            clk.__exit__(None, None, None)
+        ev.synchronize()
+        barrier()
+        return ev, max_over_ranks(e0.elapsed_time(e1))
+
+    clk = ClockSampler(local)
+    ev, ms = timed({}, a.steps, clk)
+    groups = ev.groups()
+    value = all_pts * a.steps / (ms / 1e3)
+    # accuracy: each box against an FP64 run of the same warm-up + timed steps
+    fp64 = Evolution(states, [BoxConfig(order=4, lapse="Harmonic")] * len(states))
+    fp64.set_stream(stream.cuda_stream)
+    fp64.step(max(a.warmup, 0) + a.steps)
+    fp64.synchronize()
+    acc = {}
+    for q, s in enumerate(mine):
+        ref, got = fp64.download(q), ev.download(q)
+        hr, hg = fp64.constraints(q), ev.constraints(q)
+        acc[s.box_id] = {**accuracy(ref, got, hr, hg), "n": s.n, "rms_delta": s.rms_delta}
+    fp64.close()
+    # end to end: every box's state host -> device, one step, device -> host
+    h_in = [torch.from_numpy(st.fields.reshape(-1)).pin_memory() for st in states]
+    h_out = [torch.empty_like(h).pin_memory() for h in h_in]
+    dp = ctypes.POINTER(ctypes.c_double)
+    L = ev.L
+    barrier()
+    torch.cuda.synchronize()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(a.e2e_steps):
+        for b, h in enumerate(h_in):
+            ev._check(L.cg_upload_state_async(ev.ctx, b, ctypes.cast(h.data_ptr(), dp), h.numel()))
+        ev.step(1)
+        for b, h in enumerate(h_out):
+            ev._check(L.cg_download_state_async(ev.ctx, b, ctypes.cast(h.data_ptr(), dp), h.numel()))
+    q1.record(stream)
+    torch.cuda.synchronize()
+    ev.synchronize()
+    e2e_ms = max_over_ranks(q0.elapsed_time(q1))
+    state_bytes = sum(h.numel() * 8 for h in h_in)
+    ev.close()
+    variants = {}
+    for name, opts in (("per_box_launches", {"batch": 0}), ("graph", {"graph": 1})):
+        evv, vms = timed(opts, a.steps)
+        evv.close()
+        variants[name] = {"value": all_pts * a.steps / (vms / 1e3), "ms_per_step": vms / a.steps}
+    acc_all = ensemble.gather(acc, world)
+    cpu = None
+    if rank == 0 and a.cpu_baseline:
+        try:
+            cpu = cpu_baseline(ensemble.initial_states([specs[16]], order=4)[0], 4)
+        except Exception as exc:  # reported, not fatal
+            cpu = {"value": None, "error": str(exc)[:200]}
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peaks()
+    ms_step = ms / a.steps
+    achieved = ALGO_BYTES_MIXED_DUST * all_pts / world / (ms_step / 1e3) / 1e9
+    line = {
+        "metric": "grid-pt RK4 updates/s (BSSN+dust)", "value": value, "unit": "grid-pt RK4 updates/s",
+        "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic",
+        "config": {"workload": "ensemble_48_boxes_16x32c_16x64c_16x96c_o4_mixed", "boxes": len(specs),
+                   "points": all_pts, "stencil_order": 4, "lapse": "Harmonic", "precision": "mixed",
+                   "seeds": f"{specs[0].seed}..{specs[-1].seed}", "parallelism": f"boxes split over {world} ranks",
+                   "l2": "inputs larger than L2 (ensemble state %.1f GB)" % (state_bytes * world / 1e9),
+                   "groups": groups},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_update": ALGO_BYTES_MIXED_DUST},
+        "e2e": {"value": all_pts * a.e2e_steps / (e2e_ms / 1e3), "unit": "grid-pt RK4 updates/s",
+                "h2d_bytes_per_step": state_bytes * world, "d2h_bytes_per_step": state_bytes * world,
+                "steps": a.e2e_steps},
+        "gpu_launches": 4 * a.steps * max(1, len(groups)),
+        "variants": variants,
+        "accuracy_vs_fp64": {
+            "max_field_err_rel_perturbation": max(v["field_err_rel_perturbation"] for v in acc_all.values()),
+            "max_H_ratio": max(v["H_ratio"] for v in acc_all.values()),
+            "min_H_ratio": min(v["H_ratio"] for v in acc_all.values()),
+            "boxes": len(acc_all)},
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
 def run_reference_arm(a, world, rank):
     """--impl reference: the reference's CPU implementation (oracle/_ref) of the
     same workload, all host threads, rank 0 only."""
@@ -203,13 +343,22 @@ def run_reference_arm(a, world, rank):
         return
     from oracle import build_ref
 
-    n = a.n
-    binp = build_ref.binary_path(n, n, n, a.order, "fast")
+    n, order = a.n, a.order
+    if a.workload == "ensemble":
+        # the reference runs one box per process: one 64^3 box of the ensemble
+        from cosmograph_b200 import ensemble
+
+        spec = ensemble.standard_ensemble()[16]
+        n, order = spec.n, 4
+    binp = build_ref.binary_path(n, n, n, order, "fast")
     base = {"metric": "grid-pt RK4 updates/s (BSSN+dust)", "impl": "reference"}
     if not binp.exists():
         print(json.dumps({"impl": "reference", "unavailable": f"{binp.name} was not built"}))
         return
-    st = make_state(n, seed=1, order=a.order)
+    if a.workload == "ensemble":
+        st = ensemble.initial_states([spec], order=4)[0]
+    else:
+        st = make_state(n, seed=1, order=order)
     threads = os.cpu_count() or 1
     # each step is a full RK4 step of the same box; cap the count so the run
     # stays within a few minutes on the host cores
@@ -237,11 +386,12 @@ def run_reference_arm(a, world, rank):
     line = dict(base, value=rate, unit="grid-pt RK4 updates/s", n_gpus=a.gpus, steps=len(step_s),
                 warmup=warm, ms_per_step=1e3 * tot / len(step_s), higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="f64", data="synthetic",
-                config={"workload": f"bssn_dust_{n}cubed_o{a.order}", "n": n, "stencil_order": a.order,
-                        "lapse": "Harmonic", "parallelism": "host threads"},
+                config={"workload": (f"bssn_dust_{n}cubed_o{order}" if a.workload == "box" else
+                                     "ensemble_48_boxes_16x32c_16x64c_16x96c_o4_mixed"),
+                        "n": n, "stencil_order": order, "lapse": "Harmonic", "parallelism": "host threads"},
                 cpu_baseline={"value": rate, "unit": "grid-pt RK4 updates/s", "cores": threads,
                               "kind": "reference",
-                              "sample": f"{len(step_s)} RK4 steps (of {a.steps} requested) of the "
+                              "sample": f"{len(step_s)} RK4 steps (of {a.steps} requested) of one "
                                         f"{n}^3 box; reference sources, {binp.name}"},
                 e2e={"value": rate, "unit": "grid-pt RK4 updates/s", "h2d_bytes_per_step": 0,
                      "d2h_bytes_per_step": 0})
@@ -254,6 +404,13 @@ def main():
         int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
     if a.impl == "reference":
         return run_reference_arm(a, world, rank)
+    if a.workload == "ensemble":
+        run_ensemble(a, world, rank, local)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
 
     import torch
     import torch.distributed as dist
