@@ -221,26 +221,28 @@ __global__ void part_final_kernel(const double* part, int nblk, int Q, int nsum,
   }
 }
 
-// Sums of four fields (for the mixed form's uniform background): per CTA.
-__global__ void field_sums_kernel(const double* f0, const double* f1, const double* f2, const double* f3, int n,
-                                  double* part) {
-  __shared__ double s[4][256];
-  double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+// Sums of five fields (for the mixed form's uniform background): per CTA,
+// fixed order.  f3, f4 may be null (sum 0).
+__global__ void field_sums_kernel(const double* f0, const double* f1, const double* f2, const double* f3,
+                                  const double* f4, int n, double* part) {
+  __shared__ double s[5][256];
+  double a[5] = {0, 0, 0, 0, 0};
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-    a0 += f0[q];
-    a1 += f1[q];
-    a2 += f2[q];
-    a3 += f3 ? f3[q] : 0.0;
+    a[0] += f0[q];
+    a[1] += f1[q];
+    a[2] += f2[q];
+    a[3] += f3 ? f3[q] : 0.0;
+    a[4] += f4 ? f4[q] : 0.0;
   }
-  s[0][threadIdx.x] = a0; s[1][threadIdx.x] = a1; s[2][threadIdx.x] = a2; s[3][threadIdx.x] = a3;
+  for (int m = 0; m < 5; ++m) s[m][threadIdx.x] = a[m];
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
     if (threadIdx.x < o)
-      for (int m = 0; m < 4; ++m) s[m][threadIdx.x] += s[m][threadIdx.x + o];
+      for (int m = 0; m < 5; ++m) s[m][threadIdx.x] += s[m][threadIdx.x + o];
     __syncthreads();
   }
   if (threadIdx.x == 0)
-    for (int m = 0; m < 4; ++m) part[(size_t)blockIdx.x * 4 + m] = s[m][0];
+    for (int m = 0; m < 5; ++m) part[(size_t)blockIdx.x * 5 + m] = s[m][0];
 }
 
 // Second pass of BSSN::setConstraintCalcs (bssn.cc:1026-1054): squared
@@ -319,20 +321,32 @@ int launch_kavg(cg_ctx* ctx, Box& b, const double* in) {
 }
 
 // Right-hand side of the uniform background (the reference's equations for a
-// spatially constant state, trivial FRW): dK/dt, dphi/dt, dalpha/dt.
+// spatially constant state, trivial FRW): dK/dt, dphi/dt, dalpha/dt and, for
+// a scalar field, dphi_s/dt = -alpha Pi, dPi/dt = alpha (K Pi + V'(phi_s))
+// (scalar.cc:142-163 with every gradient zero).
 void mixed_bg_rhs(const Box& b, const double* a, double phi_lag, double* rhs) {
   for (int f = 0; f < 23; ++f) rhs[f] = 0.0;
   const double Kd = a[cg::F_K], ad = a[cg::F_ALPHA], al = ad + 1.0;
-  double rS = 0.0;  // DIFFr + DIFFS of the uniform state (W = 1)
-  if (b.desc.matter == CG_MATTER_DUST)
-    rS = (a[cg::F_D] * std::exp(-6.0 * phi_lag) + b.desc.lambda) + (-3.0 * b.desc.lambda);
+  double rS = 0.0;  // DIFFr + DIFFS of the uniform state
+  if (b.desc.matter == CG_MATTER_DUST) {
+    rS = (a[cg::F_D] * std::exp(-6.0 * phi_lag) + b.desc.lambda) + (-3.0 * b.desc.lambda);  // W = 1
+  } else if (b.desc.matter == CG_MATTER_SCALAR) {
+    const double sphi = a[cg::F_SPHI], Pi = a[cg::F_SPI];
+    const bool quad = b.desc.potential == CG_POT_QUADRATIC;
+    const double m2 = b.desc.pot_mass * b.desc.pot_mass;
+    const double V = quad ? 0.5 * m2 * sphi * sphi : b.desc.pot_const;
+    const double dV = quad ? m2 * sphi : 0.0;
+    rS = 2.0 * Pi * Pi - 2.0 * V;  // rho + S with n^mu d_mu phi_s = -Pi
+    rhs[cg::F_SPHI] = -al * Pi;
+    rhs[cg::F_SPI] = al * (Kd * Pi + dV);
+  }
   rhs[cg::F_K] = al * (1.0 / 3.0 * Kd * Kd) + 4.0 * cg::kPi * al * rS;
   rhs[cg::F_PHI] = -1.0 / 6.0 * (al * Kd);
   rhs[cg::F_ALPHA] = b.desc.lapse == CG_LAPSE_HARMONIC ? -1.0 * al * Kd : 0.0;
 }
 
 void pack_bg(const double* full, double* compact) {
-  for (int f : {cg::F_K, cg::F_PHI, cg::F_ALPHA, cg::F_D}) compact[cg::mixed::bgi(f)] = full[f];
+  for (int f : {(int)cg::F_K, (int)cg::F_PHI, (int)cg::F_ALPHA, 18, 19}) compact[cg::mixed::bgi(f)] = full[f];
 }
 
 int mixed_init(cg_ctx* ctx, Box& b) {
@@ -344,22 +358,25 @@ int mixed_init(cg_ctx* ctx, Box& b) {
     CG_CUDA(ctx, cudaMalloc(&b.cscratch, sizeof(double) * need));
   }
   double* part = b.cscratch;
-  double* res = part + 4 * (size_t)nblk;
+  double* res = part + 5 * (size_t)nblk;
   const double* P = b.mdev.P;
+  const bool dust = b.desc.matter == CG_MATTER_DUST, scalar = b.desc.matter == CG_MATTER_SCALAR;
+  // D (dust) or the scalar phi and Pi (fields 18, 19) have a background
   field_sums_kernel<<<nblk, 256, 0, ctx->stream>>>(P + (size_t)cg::F_K * n, P + (size_t)cg::F_PHI * n,
                                                    P + (size_t)cg::F_ALPHA * n,
-                                                   b.desc.matter == CG_MATTER_DUST ? P + (size_t)cg::F_D * n : nullptr,
-                                                   n, part);
-  part_final_kernel<<<1, 256, 0, ctx->stream>>>(part, nblk, 4, 4, res);
+                                                   dust || scalar ? P + (size_t)18 * n : nullptr,
+                                                   scalar ? P + (size_t)19 * n : nullptr, n, part);
+  part_final_kernel<<<1, 256, 0, ctx->stream>>>(part, nblk, 5, 5, res);
   CG_CUDA(ctx, cudaGetLastError());
-  double h[4];
+  double h[5];
   CG_CUDA(ctx, cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
   CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   for (int f = 0; f < 23; ++f) b.bp[f] = b.ba[f] = b.bprev[f] = b.bf[f] = 0.0;
   b.bp[cg::F_K] = h[0] / n;
   b.bp[cg::F_PHI] = h[1] / n;
   b.bp[cg::F_ALPHA] = h[2] / n;
-  if (b.desc.matter == CG_MATTER_DUST) b.bp[cg::F_D] = h[3] / n;
+  if (dust || scalar) b.bp[18] = h[3] / n;
+  if (scalar) b.bp[19] = h[4] / n;
   for (int f = 0; f < 23; ++f) b.ba[f] = b.bprev[f] = b.bp[f];
   cg::mixed::Bg bg{};
   pack_bg(b.ba, bg.in);
@@ -398,6 +415,9 @@ cg::mixed::Bg mixed_prepare(Box& b, int n) {
   pack_bg(rhs, bg.rhs);
   bg.e6l = std::exp(-6.0 * phi_lag);
   bg.lambda = b.desc.lambda;
+  bg.potential = b.desc.potential;
+  bg.pot_const = b.desc.pot_const;
+  bg.pot_mass = b.desc.pot_mass;
   for (int f = 0; f < 23; ++f) {
     b.bprev[f] = b.ba[f];
     b.ba[f] = o[f];
@@ -474,7 +494,6 @@ int validate(const cg_box_desc& d, std::string& why) {
     return CG_ERR_INVALID;
   }
   if (d.precision == CG_PREC_MIXED) {
-    if (d.matter == CG_MATTER_SCALAR) { why = "the FP32-mixed form covers vacuum and dust"; return CG_ERR_INVALID; }
     if (d.lapse != CG_LAPSE_HARMONIC && d.lapse != CG_LAPSE_STATIC) {
       why = "the FP32-mixed form supports the Harmonic and Static lapses";
       return CG_ERR_INVALID;

@@ -47,18 +47,22 @@ struct Ptrs {
 };
 
 // Uniform background of one substep (FP64).  A uniform state keeps every
-// field but K, phi, alpha and D at zero, so only those four are stored, at
-// index bgi(field).
+// field but K, phi, alpha and, for matter, D or the scalar phi and Pi at
+// zero, so only those five are stored, at index bgi(field) (field 18 is D or
+// the scalar phi, field 19 is S1 or Pi).
+constexpr int kBgN = 5;
 struct Bg {
-  double in[4];      // abar of a^n
-  double prev[4];    // abar of a^{n-1}
-  double out[4];     // abar of the substep output
-  double rhs[4];     // RHS(abar of a^n), added to the kernel's perturbation RHS
-  double e6l;        // exp(-6 phibar) of the state whose W, sqrt(gamma) the sources lag on
-  double lambda;     // rho_Lambda
+  double in[kBgN];    // abar of a^n
+  double prev[kBgN];  // abar of a^{n-1}
+  double out[kBgN];   // abar of the substep output
+  double rhs[kBgN];   // RHS(abar of a^n), added to the kernel's perturbation RHS
+  double e6l;         // exp(-6 phibar) of the state whose W, sqrt(gamma) the sources lag on
+  double lambda;      // rho_Lambda
+  double pot_const, pot_mass;  // scalar potential V = pot_const or m^2 phi^2 / 2
+  int potential;
 };
 __host__ __device__ constexpr int bgi(int f) {
-  return f == F_K ? 0 : (f == F_PHI ? 1 : (f == F_ALPHA ? 2 : (f == F_D ? 3 : -1)));
+  return f == F_K ? 0 : (f == F_PHI ? 1 : (f == F_ALPHA ? 2 : (f == 18 ? 3 : (f == 19 ? 4 : -1))));
 }
 __host__ __device__ inline double bgv(const double* a, int f) { return bgi(f) < 0 ? 0.0 : a[bgi(f)]; }
 
@@ -83,6 +87,11 @@ struct GroupBg {
 enum : int {
   S_DG = 0, S_T1 = 18, S_DPHI = 24, S_DDPHI = 27, S_DA = 33, S_DDA = 36, S_DK = 42,
   S_DGAM = 45, S_SRC = 54, S_G = 65, S_MAT = 83, S_NSLOT = 87
+};
+// slots per thread: dust 4 flux divergences, scalar 15 first derivatives
+template <int MATTER>
+struct NSlot {
+  static constexpr int value = S_MAT + (MATTER == kDust ? 4 : (MATTER == kScalar ? 15 : 0));
 };
 // phase 1 writes no slot in [S_SRC, S_MAT): the field tile lives there
 constexpr int kTileSlot = S_SRC, kTileSlots = S_MAT - S_SRC;
@@ -184,10 +193,11 @@ __device__ __forceinline__ DustF dust_primf(const float gi[6], float em4, float 
 // first and second derivatives, K and Gamma^i with first derivatives, one
 // field tile at a time, the next field fetched into registers meanwhile.
 __device__ __forceinline__ int phase1_field(int it) {
-  return it < 6 ? F_G11 + it : (it == 6 ? F_PHI : (it == 7 ? F_ALPHA : (it == 8 ? F_K : F_GAM1 + it - 9)));
+  return it < 6 ? F_G11 + it
+                : (it == 6 ? F_PHI : (it == 7 ? F_ALPHA : (it == 8 ? F_K : (it < 12 ? F_GAM1 + it - 9 : F_SPHI + it - 12))));
 }
 
-template <int O>
+template <int O, int MATTER>
 __device__ __forceinline__ void derivatives(const float* __restrict__ a, int N, float idx, float idx2,
                                             const float gi[6], float* sl, float* tl, const int* rowoff, int tid,
                                             int z0, int nz, int cc) {
@@ -195,12 +205,13 @@ __device__ __forceinline__ void derivatives(const float* __restrict__ a, int N, 
   ld.init(tid, z0, nz);
   ld.fetch(a + (size_t)phase1_field(0) * N, rowoff);
   const tile::Taps<TileG<O>, float> t{tl, cc};
+  constexpr int NIT = MATTER == kScalar ? 17 : 12;  // scalar: phi, Pi, psi_i first derivatives
 #pragma unroll 1
-  for (int it = 0; it < 12; ++it) {
+  for (int it = 0; it < NIT; ++it) {
     __syncthreads();
     ld.store(tl);
     __syncthreads();
-    if (it + 1 < 12) ld.fetch(a + (size_t)phase1_field(it + 1) * N, rowoff);
+    if (it + 1 < NIT) ld.fetch(a + (size_t)phase1_field(it + 1) * N, rowoff);
     if (it < 8) {
       const float g1 = d1<O>(t, 0, idx), g2 = d1<O>(t, 1, idx), g3 = d1<O>(t, 2, idx);
       const float h11 = d2<O>(t, 0, idx2), h22 = d2<O>(t, 1, idx2), h33 = d2<O>(t, 2, idx2);
@@ -224,7 +235,7 @@ __device__ __forceinline__ void derivatives(const float* __restrict__ a, int N, 
         sl[(b2 + 5) * kThreads] = h33;
       }
     } else {
-      const int b = it == 8 ? S_DK : S_DGAM + 3 * (it - 9);
+      const int b = it == 8 ? S_DK : (it < 12 ? S_DGAM + 3 * (it - 9) : S_MAT + 3 * (it - 12));
       sl[(b + 0) * kThreads] = d1<O>(t, 0, idx);
       sl[(b + 1) * kThreads] = d1<O>(t, 1, idx);
       sl[(b + 2) * kThreads] = d1<O>(t, 2, idx);
@@ -250,7 +261,7 @@ __device__ __forceinline__ void flux_divergences(const T& t, const float* __rest
 template <int O, int MATTER>
 __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt,
                                            const Bg& bg, const Ptrs& P, int stage, int cx, int cy, int cz) {
-  constexpr int NFLD = MATTER == kDust ? 22 : 18;
+  constexpr int NFLD = MATTER == kDust ? 22 : (MATTER == kScalar ? 23 : 18);
   constexpr int R = O / 2;
   constexpr float kPif = 3.14159265358979f;
   extern __shared__ float smf[];
@@ -284,7 +295,7 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
     int* rowoff = reinterpret_cast<int*>(tl + TileG<O>::SIZE);
     tile::row_offsets<TileG<O>, Brick>(x0, y0, nx, ny, nz, tid, rowoff);
     __syncthreads();  // every warp reads every row offset
-    derivatives<O>(a, N, idx, idx2, gi, sl, tl, rowoff, tid, z0, nz,
+    derivatives<O, MATTER>(a, N, idx, idx2, gi, sl, tl, rowoff, tid, z0, nz,
                    tile::centre<TileG<O>>(threadIdx.z, threadIdx.y, threadIdx.x));
     __syncthreads();
   }
@@ -311,7 +322,7 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
   const float em4phi = __expf(-4.0f * phi);
 
   // ---- dust sources in perturbation form ---------------------------------------
-  float rhs_m[4] = {0.f, 0.f, 0.f, 0.f};
+  float rhs_m[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   float dr = 0.f, Sdust = 0.f, rS_full = 0.f;  // delta rho, S (second order), full rho + S
   if (MATTER == kDust) {
     const float Db = (float)bgv(bg.in, F_D);
@@ -368,6 +379,52 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
           cur.W * D * S(S_DA + d);
       rhs_m[1 + d] = S(S_MAT + 1 + d) + src;
     }
+  } else if (MATTER == kScalar) {
+    // Scalar::addBSSNSource and RKEvolvePt (scalar.cc:85-260) in perturbation
+    // form about the uniform phi_s, Pi (psi_i has no background); with
+    // n^mu d_mu phi = -Pi the sources are rho = Pi^2/2 + e^{-4phi} dd/2 + V,
+    // S = 3 Pi^2/2 - e^{-4phi} dd/2 - 3V, S_i = Pi d_i phi_s,
+    // S_ij^TF = d_i phi_s d_j phi_s - gamma_ij dd/3, dd = g^ij d_i phi_s d_j phi_s.
+    const float sphib = (float)bgv(bg.in, F_SPHI), Pib = (float)bgv(bg.in, F_SPI);
+    const float dsphi = D_(F_SPHI), dPi = D_(F_SPI);
+    const float sphi = sphib + dsphi, Pi = Pib + dPi;
+    const float psi[3] = {D_(F_SPSI1), D_(F_SPSI1 + 1), D_(F_SPSI1 + 2)};
+    auto SD = [&](int m, int d) { return S(S_MAT + 3 * m + d); };  // d_d of scalar field m
+    const float dd = gi[0] * SD(0, 0) * SD(0, 0) + gi[3] * SD(0, 1) * SD(0, 1) + gi[5] * SD(0, 2) * SD(0, 2) +
+                     2.0f * (gi[1] * SD(0, 0) * SD(0, 1) + gi[2] * SD(0, 0) * SD(0, 2) + gi[4] * SD(0, 1) * SD(0, 2));
+    const bool quad = bg.potential == kPotQuadratic;
+    const float m2 = (float)(bg.pot_mass * bg.pot_mass);
+    const float V = quad ? 0.5f * m2 * sphi * sphi : (float)bg.pot_const;
+    const float dV = quad ? 0.5f * m2 * (2.0f * sphib + dsphi) * dsphi : 0.0f;  // V - Vbar
+    const float dPi2 = (2.0f * Pib + dPi) * dPi;                              // Pi^2 - Pibar^2
+    dr = 2.0f * dPi2 - 2.0f * dV;  // delta(rho + S); the dd terms cancel
+    Sdust = 0.0f;
+    rS_full = 2.0f * Pi * Pi - 2.0f * V;
+    S(S_SRC + Q_R) = 0.5f * dPi2 + 0.5f * em4phi * dd + dV;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) S(S_SRC + Q_S1 + m) = Pi * SD(0, m);
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int J = I; J < 3; ++J) S(S_SRC + Q_STF11 + sym(I, J)) = SD(0, I) * SD(0, J) - gm[sym(I, J)] * (1.0f / 3.0f) * dd;
+    float inner = 0.0f;
+#pragma unroll
+    for (int X = 0; X < 3; ++X)
+#pragma unroll
+      for (int Y = 0; Y < 3; ++Y) inner += gi[sym(X, Y)] * (alpha * SD(2 + Y, X) + psi[X] * S(S_DA + Y));
+    float gtpsi = 0.0f;
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+      gtpsi += (D_(F_GAM1 + I) - 2.0f * (gi[sym(I, 0)] * S(S_DPHI + 0) + gi[sym(I, 1)] * S(S_DPHI + 1) +
+                                         gi[sym(I, 2)] * S(S_DPHI + 2))) * psi[I];
+    // alpha (K Pi + V') - alphabar (Kbar Pibar + V'bar), expanded
+    const float ddV = quad ? m2 * dsphi : 0.0f;
+    const float X = K * Pi + (quad ? m2 * sphi : 0.0f);
+    const float dX = Kb * dPi + dK * Pi + ddV;
+    rhs_m[0] = -(alb * dPi + dal * Pi);
+    rhs_m[1] = -em4phi * inner + alpha * gtpsi * em4phi + (alb * dX + dal * X);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) rhs_m[2 + m] = -alpha * SD(1, m) - Pi * S(S_DA + m);
   } else {
 #pragma unroll
     for (int m = 0; m < Q_N; ++m) S(S_SRC + m) = 0.f;
@@ -548,6 +605,9 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
   if (MATTER == kDust) {
 #pragma unroll
     for (int m = 0; m < 4; ++m) finalize(F_D + m, rhs_m[m]);
+  } else if (MATTER == kScalar) {
+#pragma unroll
+    for (int m = 0; m < 5; ++m) finalize(F_SPHI + m, rhs_m[m]);
   }
 
   if (stage == 4) {
@@ -667,7 +727,7 @@ mixed_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
 template <int MATTER>
 __global__ void __launch_bounds__(kThreads) mixed_init_kernel(int nx, int ny, int nz, int normalize, Bg bg,
                                                               const double* Pp, float* X, float* FP0) {
-  constexpr int NFLD = MATTER == kDust ? 22 : 18;
+  constexpr int NFLD = MATTER == kDust ? 22 : (MATTER == kScalar ? 23 : 18);
   const int k = blockIdx.x * kBZ + threadIdx.x;
   const int j = blockIdx.y * kBY + threadIdx.y;
   const int i = blockIdx.z * kBX + threadIdx.z;

@@ -8,6 +8,21 @@ namespace mixed {
 namespace {
 dim3 grid3(int nx, int ny, int nz) { return dim3((nz + kBZ - 1) / kBZ, (ny + kBY - 1) / kBY, (nx + kBX - 1) / kBX); }
 
+template <int M>
+constexpr size_t smem_bytes() {
+  return sizeof(float) * NSlot<M>::value * kThreads;
+}
+
+// dynamic shared memory above the 48 KB default (the scalar slots) needs
+// the kernel's attribute raised once
+template <class K>
+cudaError_t allow_smem(K kernel, size_t smem, bool& done) {
+  if (done || smem <= 48 * 1024) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) done = true;
+  return e;
+}
+
 template <int O, int M>
 cudaError_t go(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
   Ptrs P{};
@@ -21,37 +36,58 @@ cudaError_t go(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
     case 3: P.in = b.X; P.prev = b.Y; P.out = b.Y; P.fp_in = b.FP0; P.fp_out = b.FP1; break;
     default: P.in = b.Y; P.prev = b.X; P.out = b.X; P.fp_in = b.FP1; P.fp_out = b.FP0; break;
   }
-  constexpr size_t smem = sizeof(float) * S_NSLOT * kThreads;
+  constexpr size_t smem = smem_bytes<M>();
+  static bool done = false;
+  cudaError_t e = allow_smem(mixed_kernel<O, M>, smem, done);
+  if (e != cudaSuccess) return e;
   mixed_kernel<O, M><<<grid3(b.nx, b.ny, b.nz), dim3(kBZ, kBY, kBX), smem, st>>>(
       b.nx, b.ny, b.nz, b.lapse, b.normalize, (float)(1.0 / b.dx), b.dt, bg, P, stage);
   return cudaGetLastError();
 }
 template <int O>
 cudaError_t go_m(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
-  return b.matter == kDust ? go<O, kDust>(b, bg, stage, st) : go<O, kVacuum>(b, bg, stage, st);
+  switch (b.matter) {
+    case kDust: return go<O, kDust>(b, bg, stage, st);
+    case kScalar: return go<O, kScalar>(b, bg, stage, st);
+    default: return go<O, kVacuum>(b, bg, stage, st);
+  }
 }
+
 template <int O, int M>
 cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, cudaStream_t st) {
-  constexpr size_t smem = sizeof(float) * S_NSLOT * kThreads;
+  constexpr size_t smem = smem_bytes<M>();
+  static bool done = false;
+  cudaError_t e = allow_smem(mixed_group_kernel<O, M>, smem, done);
+  if (e != cudaSuccess) return e;
   const int g = grid > 0 ? grid : gb.total;
   mixed_group_kernel<O, M><<<g, dim3(kBZ, kBY, kBX), smem, st>>>(table, gb, stage);
   return cudaGetLastError();
 }
 template <int O>
 cudaError_t go_group_m(const GroupBox* table, const GroupBg& gb, int matter, int stage, int grid, cudaStream_t st) {
-  return matter == kDust ? go_group<O, kDust>(table, gb, stage, grid, st) : go_group<O, kVacuum>(table, gb, stage, grid, st);
+  switch (matter) {
+    case kDust: return go_group<O, kDust>(table, gb, stage, grid, st);
+    case kScalar: return go_group<O, kScalar>(table, gb, stage, grid, st);
+    default: return go_group<O, kVacuum>(table, gb, stage, grid, st);
+  }
 }
 template <int O, int M>
 int ctas() {
+  constexpr size_t smem = smem_bytes<M>();
+  static bool done = false;
+  if (allow_smem(mixed_group_kernel<O, M>, smem, done) != cudaSuccess) return 1;
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mixed_group_kernel<O, M>, kThreads,
-                                                    sizeof(float) * S_NSLOT * kThreads) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, mixed_group_kernel<O, M>, kThreads, smem) != cudaSuccess)
     return 1;
   return n > 0 ? n : 1;
 }
 template <int O>
 int ctas_m(int matter) {
-  return matter == kDust ? ctas<O, kDust>() : ctas<O, kVacuum>();
+  switch (matter) {
+    case kDust: return ctas<O, kDust>();
+    case kScalar: return ctas<O, kScalar>();
+    default: return ctas<O, kVacuum>();
+  }
 }
 }  // namespace
 
@@ -87,10 +123,11 @@ cudaError_t launch_stage(const MixedBox& b, const Bg& bg, int stage, cudaStream_
 
 cudaError_t launch_init(const MixedBox& b, const Bg& bg, cudaStream_t st) {
   const dim3 g = grid3(b.nx, b.ny, b.nz), blk(kBZ, kBY, kBX);
-  if (b.matter == kDust)
-    mixed_init_kernel<kDust><<<g, blk, 0, st>>>(b.nx, b.ny, b.nz, b.normalize, bg, b.P, b.X, b.FP0);
-  else
-    mixed_init_kernel<kVacuum><<<g, blk, 0, st>>>(b.nx, b.ny, b.nz, b.normalize, bg, b.P, b.X, b.FP0);
+  switch (b.matter) {
+    case kDust: mixed_init_kernel<kDust><<<g, blk, 0, st>>>(b.nx, b.ny, b.nz, b.normalize, bg, b.P, b.X, b.FP0); break;
+    case kScalar: mixed_init_kernel<kScalar><<<g, blk, 0, st>>>(b.nx, b.ny, b.nz, b.normalize, bg, b.P, b.X, b.FP0); break;
+    default: mixed_init_kernel<kVacuum><<<g, blk, 0, st>>>(b.nx, b.ny, b.nz, b.normalize, bg, b.P, b.X, b.FP0); break;
+  }
   return cudaGetLastError();
 }
 

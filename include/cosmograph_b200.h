@@ -63,7 +63,8 @@ extern "C" {
 #define CG_PREC_FP64_FMA 1  /* FP64 with FMA contraction                          */
 #define CG_PREC_MIXED 2     /* FP32 perturbations about an FP64 uniform background,
                                FP32 stencils and right-hand side, FP64 RK registers
-                               (vacuum or dust; Harmonic or Static lapse)          */
+                               (vacuum, dust or scalar; Harmonic or Static lapse;
+                               trivial FRW reference)                               */
 
 /* scalar potentials */
 #define CG_POT_CONST 0      /* V = pot_const, dV = 0 (components/scalar/scalar.cc:262-274) */

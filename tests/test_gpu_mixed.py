@@ -65,7 +65,26 @@ def test_vacuum_mixed_runs_and_rejects_unsupported():
     errs = perturbation_errors(a.fields, b.fields, st.names)
     assert max(errs.values()) < 1e-4
     with pytest.raises(RuntimeError, match="mixed"):
-        evolve(ics.perturbed((16, 16, 16), S.SCALAR), 1, BoxConfig(order=4, precision="mixed"))
+        evolve(ics.perturbed((16, 16, 16), S.DUST), 1, BoxConfig(order=4, precision="mixed", lapse="OnePlusLog"))
+
+
+@pytest.mark.parametrize("order,potential", [(4, "const"), (8, "quadratic")])
+def test_grf_scalar_against_fp64(order, potential):
+    """BSSN + scalar field, phi_0 = 1e-2 with a k^-3 Gaussian random
+    fluctuation of rms 1e-5: mixed vs FP64 fields and Hamiltonian constraint."""
+    st = ics.grf_scalar(32, seed=14, phi0=1e-2, rms=1e-5, order=order)
+    cfgs = {p: BoxConfig(order=order, precision=p, potential=potential, pot_mass=1.0) for p in ("fp64", "mixed")}
+    res = {}
+    for prec, cfg in cfgs.items():
+        with Evolution(st, cfg) as ev:
+            ev.step(30)
+            res[prec] = (ev.download(0), ev.constraints(0))
+    errs = perturbation_errors(res["mixed"][0].fields, res["fp64"][0].fields, st.names)
+    worst = max(errs, key=errs.get)
+    print("scalar mixed vs fp64", order, potential, worst, errs[worst],
+          "H", res["mixed"][1]["H"][7], res["fp64"][1]["H"][7])
+    assert errs[worst] < 1e-4, errs
+    assert res["mixed"][1]["H"][7] <= 2.0 * res["fp64"][1]["H"][7]
 
 
 def test_a_register_of_a_mixed_box():
