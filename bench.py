@@ -140,6 +140,15 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def profiled_traffic(n: int, order: int, precision: str):
+    """DRAM bytes per substep launch from the committed ncu summary, or None."""
+    prof = ROOT / "profiles" / "stage_kernel_traffic.json"
+    try:
+        return json.loads(prof.read_text()).get(f"{n}_{order}_{precision}")
+    except Exception:
+        return None
+
+
 def make_state(n: int, seed: int, order: int):
     from cosmograph_b200 import ics
 
@@ -493,7 +502,8 @@ def main():
         variants[prec] = {"value": world * pts * a.steps / (vms / 1e3), "ms_per_step": vms_step,
                           "speedup_vs_fp64": ms_per_step / vms_step if a.precision == "fp64" else None,
                           "roofline": {"achieved": v_ach, "peak": peak, "unit": "GB/s", "frac": v_ach / peak,
-                                       "algorithmic_bytes_per_update": algo_bytes(prec)}}
+                                       "algorithmic_bytes_per_update": algo_bytes(prec),
+                                       "traffic": profiled_traffic(n, a.order, prec)}}
         if ref_state is not None:
             variants[prec]["accuracy_vs_fp64"] = accuracy(ref_state, ev_v.download(0), ref_h, ev_v.constraints(0))
         ev_v.close()
@@ -530,14 +540,7 @@ def main():
     algo = algo_bytes(a.precision) * pts / launches_per_step
     launch_ms = ms_per_step / launches_per_step
     achieved = algo / (launch_ms / 1e3) / 1e9
-    traffic = None
-    prof = ROOT / "profiles" / "stage_kernel_traffic.json"
-    if prof.exists():
-        try:
-            d = json.loads(prof.read_text())
-            traffic = d.get(f"{n}_{a.order}_{a.precision}")
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic(n, a.order, a.precision)
 
     cpu = None
     if rank == 0 and a.cpu_baseline:

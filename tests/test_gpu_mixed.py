@@ -103,3 +103,29 @@ def test_a_register_of_a_mixed_box():
                 assert np.abs(a - b).max() <= 1e-5 * spread, name
         with pytest.raises(RuntimeError, match="read-only"):
             em.upload_field(0, 0, "a", np.zeros(st.shape))
+
+
+def test_grf_dust_128_order8_500_steps():
+    """128^3, 8th order, GRF dust at rms delta 1e-4, 500 RK4 steps: the mixed
+    form against the FP64 GPU run.  Field errors relative to each field's
+    spread (printed with the density-contrast amplitude) and the Hamiltonian
+    and momentum constraint norms."""
+    st = ics.grf_dust(128, seed=17, rms_delta=1e-4, order=8)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        with Evolution(st, BoxConfig(order=8, precision=prec)) as ev:
+            ev.step(500)
+            ev.synchronize()
+            res[prec] = (ev.download(0), ev.constraints(0))
+    ref, got = res["fp64"][0], res["mixed"][0]
+    errs = perturbation_errors(got.fields, ref.fields, st.names)
+    worst = max(errs, key=errs.get)
+    D = ref.field("D")
+    delta_err = float(np.abs(got.field("D") - D).max() / D.mean())
+    h64, hmx = res["fp64"][1]["H"][7], res["mixed"][1]["H"][7]
+    m64, mmx = res["fp64"][1]["M"][7], res["mixed"][1]["M"][7]
+    print("128^3 o8 500 steps: worst field", worst, errs[worst], "density-contrast error", delta_err,
+          "H L2", hmx, h64, "M L2", mmx, m64)
+    assert errs[worst] < 1e-4
+    assert delta_err < 1e-4 * 1e-4  # below 1e-4 of the density-contrast amplitude
+    assert hmx <= 2.0 * h64 and mmx <= 2.0 * m64
