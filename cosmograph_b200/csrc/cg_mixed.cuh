@@ -279,6 +279,13 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
   const int c = (i * ny + j) * nz + k;
   const float* __restrict__ a = P.in;
   auto D_ = [&](int f) { return a[(size_t)f * N + c]; };  // delta at the centre
+  // warm L2 with the epilogue's FP64 register reads; those reads and the
+  // epilogue writes are single-use streams (ld/st .cs), as in the FP64 kernel
+#pragma unroll 1
+  for (int f = 0; f < NFLD; ++f) {
+    asm volatile("prefetch.global.L2 [%0];" :: "l"(P.p + (size_t)f * N + c));
+    if (stage > 1) asm volatile("prefetch.global.L2 [%0];" :: "l"(P.f + (size_t)f * N + c));
+  }
 
   float g[6], gi[6];
 #pragma unroll
@@ -338,12 +345,12 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
     } else {
       const float* pv = P.prev;
 #pragma unroll
-      for (int m = 0; m < 6; ++m) gl[m] = pv[(size_t)(F_G11 + m) * N + c];
+      for (int m = 0; m < 6; ++m) gl[m] = __ldcs(&pv[(size_t)(F_G11 + m) * N + c]);
       inv_metricf(gl, gil);
-      dphil = pv[(size_t)F_PHI * N + c];
+      dphil = __ldcs(&pv[(size_t)F_PHI * N + c]);
       phil = (float)bgv(bg.prev, F_PHI) + dphil;
-      Dl = (float)bgv(bg.prev, F_D) + pv[(size_t)F_D * N + c];
-      Sl[0] = pv[(size_t)F_S1 * N + c]; Sl[1] = pv[(size_t)F_S2 * N + c]; Sl[2] = pv[(size_t)F_S3 * N + c];
+      Dl = (float)bgv(bg.prev, F_D) + __ldcs(&pv[(size_t)F_D * N + c]);
+      Sl[0] = __ldcs(&pv[(size_t)F_S1 * N + c]); Sl[1] = __ldcs(&pv[(size_t)F_S2 * N + c]); Sl[2] = __ldcs(&pv[(size_t)F_S3 * N + c]);
     }
     const float em4l = __expf(-4.0f * phil), e6l = __expf(6.0f * phil), e4l = __expf(4.0f * phil);
     const DustF dl = dust_primf(gil, em4l, e6l, Dl, Sl);
@@ -551,23 +558,23 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
   double outv[NFLD];
   auto finalize = [&](int fld, float drhs) {
     const double cv = bgv(bg.rhs, fld) + (double)drhs;
-    const double pv = P.p[(size_t)fld * N + c];
+    const double pv = __ldcs(&P.p[(size_t)fld * N + c]);
     double o;
     if (stage == 1) {
-      P.f[(size_t)fld * N + c] = dt * cv / 6.0;
+      __stcs(&P.f[(size_t)fld * N + c], dt * cv / 6.0);
       o = pv + dt * cv / 2.0;
     } else if (stage == 2) {
-      const double fv = P.f[(size_t)fld * N + c];
-      P.f[(size_t)fld * N + c] = fv + dt * cv / 3.0;
+      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
+      __stcs(&P.f[(size_t)fld * N + c], fv + dt * cv / 3.0);
       o = pv + dt * cv / 2.0;
     } else if (stage == 3) {
-      const double fv = P.f[(size_t)fld * N + c];
-      P.f[(size_t)fld * N + c] = fv + dt * cv / 3.0;
+      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
+      __stcs(&P.f[(size_t)fld * N + c], fv + dt * cv / 3.0);
       o = pv + dt * cv;
     } else {
-      const double fv = P.f[(size_t)fld * N + c];
+      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
       o = fv + (dt * cv / 6.0 + pv);
-      P.newp[(size_t)fld * N + c] = o;
+      __stcs(&P.newp[(size_t)fld * N + c], o);
     }
     outv[fld] = o;
   };
@@ -651,7 +658,7 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
     }
   }
 #pragma unroll
-  for (int f = 0; f < NFLD; ++f) P.out[(size_t)f * N + c] = (float)(outv[f] - bgv(bg.out, f));
+  for (int f = 0; f < NFLD; ++f) __stcs(&P.out[(size_t)f * N + c], (float)(outv[f] - bgv(bg.out, f)));
   if (MATTER == kDust) {
     float go[6], gio[6];
 #pragma unroll
@@ -663,11 +670,11 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
     const DustF dp = dust_primf(gio, __expf(-4.0f * phio), __expf(6.0f * phio), Do, So);
     const float alo = (float)(outv[F_ALPHA] + 1.0);
     float* fo = P.fp_out;
-    fo[(size_t)P_AD * N + c] = alo * Do;
+    __stcs(&fo[(size_t)P_AD * N + c], alo * Do);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) fo[(size_t)(P_AS1 + m) * N + c] = alo * So[m];
+    for (int m = 0; m < 3; ++m) __stcs(&fo[(size_t)(P_AS1 + m) * N + c], alo * So[m]);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) fo[(size_t)(P_V1 + m) * N + c] = dp.v[m];
+    for (int m = 0; m < 3; ++m) __stcs(&fo[(size_t)(P_V1 + m) * N + c], dp.v[m]);
   }
 }
 

@@ -142,6 +142,14 @@ struct Taps {
   }
 };
 
+// taps of one field read from global memory through index taps T
+template <class T>
+struct GTaps {
+  const double* f;
+  T t;
+  __device__ __forceinline__ double ax(int a, int n) const { return __ldg(f + t.ax(a, n)); }
+};
+
 // first derivative (utils/math.h:74-100, 231-263, 412-450, 554-586)
 template <int O, class T>
 __device__ __forceinline__ double d1(const T& t, int a, const Physics& ph) {
@@ -221,22 +229,27 @@ __device__ __forceinline__ double d1p(const double* __restrict__ fa, const doubl
   return divdx(s, ph);
 }
 
-// Fields of phase 1, in order: (constraint mode) A_q with first derivatives;
-// the metric components, phi and alpha with first and second derivatives;
-// K and Gamma^i with first derivatives; (scalar) phi, Pi, psi_i with first
-// derivatives.
+// Fields copied into tiles in phase 1, in order: (constraint mode) A_q with
+// first derivatives; the metric components, phi and alpha with first and
+// second derivatives; (constraint mode) K and Gamma^i with first derivatives;
+// (scalar) phi, Pi, psi_i with first derivatives.  In evolve mode K and
+// Gamma^i take their 24 first-derivative taps straight from global memory
+// (cheaper than a tile copy for first derivatives only).
 template <int MATTER, int MODE>
 struct Phase1 {
   static constexpr int NA = MODE == kConstraints ? 6 : 0;
   static constexpr int NS = MATTER == kScalar ? 5 : 0;
-  static constexpr int N = NA + 8 + 4 + NS;
+  static constexpr int N = NA + 8 + (MODE == kEvolve ? 0 : 4) + NS;
   __device__ __forceinline__ static int field(int it) {
     if (it < NA) return F_A11 + it;
     it -= NA;
     if (it < 8) return it < 6 ? F_G11 + it : (it == 6 ? F_PHI : F_ALPHA);
     it -= 8;
-    if (it < 4) return it == 0 ? F_K : F_GAM1 + it - 1;
-    return F_SPHI + it - 4;
+    if (MODE != kEvolve) {
+      if (it < 4) return it == 0 ? F_K : F_GAM1 + it - 1;
+      it -= 4;
+    }
+    return F_SPHI + it;
   }
 };
 
@@ -299,7 +312,7 @@ __device__ __forceinline__ void derivatives(const double* __restrict__ a, int N,
         sl[(b2 + 4) * kThreads] = h23;
         sl[(b2 + 5) * kThreads] = h33;
       }
-    } else if (it < PF::NA + 12) {
+    } else if (MODE != kEvolve && it < PF::NA + 12) {
       // K and Gamma^K: first derivatives (calculate_dK, bssn.cc:529-535; the
       // d_J Gamma^K of BSSN_CALCULATE_RICCI_UNITARY_TERM2, bssn_macros.h:251-252)
       const int q = it - PF::NA - 8;
@@ -309,7 +322,7 @@ __device__ __forceinline__ void derivatives(const double* __restrict__ a, int N,
       sl[(b + 2) * kThreads] = d1<O>(t, 2, ph);
     } else {
       // Scalar::getScalarData derivatives (scalar.cc:109-127): d_d of phi, Pi, psi1..3
-      const int m = it - PF::NA - 12;
+      const int m = it - PF::NA - (MODE == kEvolve ? 8 : 12);
       sl[(S_MAT + 3 * m + 0) * kThreads] = d1<O>(t, 0, ph);
       sl[(S_MAT + 3 * m + 1) * kThreads] = d1<O>(t, 1, ph);
       sl[(S_MAT + 3 * m + 2) * kThreads] = d1<O>(t, 2, ph);
@@ -391,6 +404,17 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   const int c = (i * geo.ny + j) * geo.nz + k;
   const double* __restrict__ a = P.in;
   auto C = [&](int f) { return a[(size_t)f * N + c]; };
+  // The epilogue's register reads (_p, _f) are issued long after this point;
+  // warm L2 with them now.  Those reads and every epilogue write are
+  // single-use streams (ld/st .cs, evict first), which leaves L2 to the
+  // neighbouring bricks' tile rows.
+  if (MODE == kEvolve) {
+#pragma unroll 1
+    for (int f = 0; f < NFLD; ++f) {
+      asm volatile("prefetch.global.L2 [%0];" :: "l"(P.p + (size_t)f * N + c));
+      if (stage > 1) asm volatile("prefetch.global.L2 [%0];" :: "l"(P.f + (size_t)f * N + c));
+    }
+  }
 
   // ---- centre values (set_local_vals, bssn.cc:430-435) ----------------------
   double g[6], gi[6];
@@ -410,16 +434,28 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     __syncthreads();  // the tile region becomes slots again
   }
   if (MODE == kEvolve && !live) return;  // no CTA-wide synchronisation after this point
-  if (MATTER == kDust) {
+  {
     const bool interior = x0 >= R && x0 + kBX + R <= geo.nx && y0 >= R && y0 + kBY + R <= geo.ny && z0 >= R &&
                           z0 + kBZ + R <= geo.nz;
-    if (interior) {
-      const Taps<false> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
-      flux_divergences<O>(t, P.fp_in, N, ph, sl);
-    } else {
-      const Taps<true> t{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
-      flux_divergences<O>(t, P.fp_in, N, ph, sl);
-    }
+    // K and Gamma^K first derivatives (calculate_dK, bssn.cc:529-535; the
+    // d_J Gamma^K of BSSN_CALCULATE_RICCI_UNITARY_TERM2, bssn_macros.h:251-252)
+    // and the dust flux divergences, taps from global memory
+    auto gpass = [&](auto t) {
+      if (MODE == kEvolve) {
+#pragma unroll 1
+        for (int q = 0; q < 4; ++q) {
+          const int fld = q == 0 ? F_K : F_GAM1 + q - 1;
+          const int b = q == 0 ? S_DK : S_DGAM + 3 * (q - 1);
+          const GTaps<decltype(t)> gt{a + (size_t)fld * N, t};
+          S(b + 0) = d1<O>(gt, 0, ph);
+          S(b + 1) = d1<O>(gt, 1, ph);
+          S(b + 2) = d1<O>(gt, 2, ph);
+        }
+      }
+      if (MATTER == kDust) flux_divergences<O>(t, P.fp_in, N, ph, sl);
+    };
+    if (interior) gpass(Taps<false>{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c});
+    else gpass(Taps<true>{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c});
   }
 
   // ---- phase 2: the algebra of set_bd_values (bssn.cc:361-421) ----------------
@@ -451,10 +487,10 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       const double* pv = P.prev;
       double gp[6], gip[6];
 #pragma unroll
-      for (int m = 0; m < 6; ++m) gp[m] = pv[(size_t)(F_G11 + m) * N + c];
-      const double phip = pv[(size_t)F_PHI * N + c] + bg.phi_FRW_prev;
-      const double Dp = pv[(size_t)F_D * N + c];
-      const double Sp[3] = {pv[(size_t)F_S1 * N + c], pv[(size_t)F_S2 * N + c], pv[(size_t)F_S3 * N + c]};
+      for (int m = 0; m < 6; ++m) gp[m] = __ldcs(&pv[(size_t)(F_G11 + m) * N + c]);
+      const double phip = __ldcs(&pv[(size_t)F_PHI * N + c]) + bg.phi_FRW_prev;
+      const double Dp = __ldcs(&pv[(size_t)F_D * N + c]);
+      const double Sp[3] = {__ldcs(&pv[(size_t)F_S1 * N + c]), __ldcs(&pv[(size_t)F_S2 * N + c]), __ldcs(&pv[(size_t)F_S3 * N + c])};
       inv_metric(gp, gip);
       const DustPrim dp = dust_prim(gip, phip, Dp, Sp);
       Wl = dp.W;
@@ -757,28 +793,28 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   double outv[NFLD];
   const bool renorm = ph.normalize != 0;
   auto finalize = [&](int fld, double cv) {
-    const double pv = P.p[(size_t)fld * N + c];
+    const double pv = __ldcs(&P.p[(size_t)fld * N + c]);
     double o;
     if (stage == 1) {
-      P.f[(size_t)fld * N + c] = dt * cv / 6.0;
+      __stcs(&P.f[(size_t)fld * N + c], dt * cv / 6.0);
       o = pv + dt * cv / 2.0;
     } else if (stage == 2) {
-      const double fv = P.f[(size_t)fld * N + c];
-      P.f[(size_t)fld * N + c] = fv + dt * cv / 3.0;
+      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
+      __stcs(&P.f[(size_t)fld * N + c], fv + dt * cv / 3.0);
       o = pv + dt * cv / 2.0;
     } else if (stage == 3) {
-      const double fv = P.f[(size_t)fld * N + c];
-      P.f[(size_t)fld * N + c] = fv + dt * cv / 3.0;
+      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
+      __stcs(&P.f[(size_t)fld * N + c], fv + dt * cv / 3.0);
       o = pv + dt * cv;
     } else {
-      const double fv = P.f[(size_t)fld * N + c];
+      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
       o = fv + (dt * cv / 6.0 + pv);
     }
-    P.out[(size_t)fld * N + c] = o;
+    __stcs(&P.out[(size_t)fld * N + c], o);
     outv[fld] = o;
     // at the last substep the new state is also the next step's first input,
     // except gamma and A, which are renormalised below
-    if (stage == 4 && !(renorm && fld < F_K && fld != F_PHI)) P.norm[(size_t)fld * N + c] = o;
+    if (stage == 4 && !(renorm && fld < F_K && fld != F_PHI)) __stcs(&P.norm[(size_t)fld * N + c], o);
   };
 
   // ev_DIFFgammaIJ (bssn.cc:748-753)
@@ -859,8 +895,8 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       for (int m = 0; m < 6; ++m) {
         outv[F_G11 + m] = gn[m];
         outv[F_A11 + m] = An[m];
-        P.norm[(size_t)(F_G11 + m) * N + c] = gn[m];
-        P.norm[(size_t)(F_A11 + m) * N + c] = An[m];
+        __stcs(&P.norm[(size_t)(F_G11 + m) * N + c], gn[m]);
+        __stcs(&P.norm[(size_t)(F_A11 + m) * N + c], An[m]);
       }
     }
   }
@@ -874,11 +910,11 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     const DustPrim dp = dust_prim(gio, outv[F_PHI] + bg.phi_FRW_next, outv[F_D], So);
     const double alo = outv[F_ALPHA] + 1.0;
     double* fo = P.fp_out;
-    fo[(size_t)P_AD * N + c] = alo * outv[F_D];
+    __stcs(&fo[(size_t)P_AD * N + c], alo * outv[F_D]);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) fo[(size_t)(P_AS1 + m) * N + c] = alo * So[m];
+    for (int m = 0; m < 3; ++m) __stcs(&fo[(size_t)(P_AS1 + m) * N + c], alo * So[m]);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) fo[(size_t)(P_V1 + m) * N + c] = dp.v[m];
+    for (int m = 0; m < 3; ++m) __stcs(&fo[(size_t)(P_V1 + m) * N + c], dp.v[m]);
   }
 }
 
