@@ -117,6 +117,14 @@ struct Taps {
   }
 };
 
+// taps of one field read from global memory through index taps T
+template <class T>
+struct GTaps {
+  const float* f;
+  T t;
+  __device__ __forceinline__ float ax(int a, int n) const { return __ldg(f + t.ax(a, n)); }
+};
+
 // FP32 centred stencils (utils/math.h:74-1085 coefficients)
 template <int O, class T>
 __device__ __forceinline__ float d1(const T& t, int a, float idx) {
@@ -190,8 +198,10 @@ __device__ __forceinline__ DustF dust_primf(const float gi[6], float em4, float 
 }
 
 // Phase 1 (as in the FP64 kernel): the metric components, phi and alpha with
-// first and second derivatives, K and Gamma^i with first derivatives, one
-// field tile at a time, the next field fetched into registers meanwhile.
+// first and second derivatives, one field tile at a time, the next field
+// fetched into registers meanwhile.  The fields with first derivatives only
+// (K, Gamma^i, the scalar field) read their taps from global memory after
+// the tiles (mixed_body).
 __device__ __forceinline__ int phase1_field(int it) {
   return it < 6 ? F_G11 + it
                 : (it == 6 ? F_PHI : (it == 7 ? F_ALPHA : (it == 8 ? F_K : (it < 12 ? F_GAM1 + it - 9 : F_SPHI + it - 12))));
@@ -205,7 +215,7 @@ __device__ __forceinline__ void derivatives(const float* __restrict__ a, int N, 
   ld.init(tid, z0, nz);
   ld.fetch(a + (size_t)phase1_field(0) * N, rowoff);
   const tile::Taps<TileG<O>, float> t{tl, cc};
-  constexpr int NIT = MATTER == kScalar ? 17 : 12;  // scalar: phi, Pi, psi_i first derivatives
+  constexpr int NIT = 8;  // fields with second derivatives; first-derivative-only fields use global taps
 #pragma unroll 1
   for (int it = 0; it < NIT; ++it) {
     __syncthreads();
@@ -307,16 +317,24 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
     __syncthreads();
   }
   if (!live) return;
-  if (MATTER == kDust) {
+  {
     const bool interior =
         x0 >= R && x0 + kBX + R <= nx && y0 >= R && y0 + kBY + R <= ny && z0 >= R && z0 + kBZ + R <= nz;
-    if (interior) {
-      const Taps<false> t{i, j, k, nx, ny, nz, ny * nz, nz, c};
-      flux_divergences<O>(t, P.fp_in, N, idx, sl);
-    } else {
-      const Taps<true> t{i, j, k, nx, ny, nz, ny * nz, nz, c};
-      flux_divergences<O>(t, P.fp_in, N, idx, sl);
-    }
+    auto gpass = [&](auto t) {
+      constexpr int NG = MATTER == kScalar ? 9 : 4;  // K, Gamma^i (and phi_s, Pi, psi_i)
+#pragma unroll 1
+      for (int q = 0; q < NG; ++q) {
+        const int fld = q == 0 ? F_K : (q < 4 ? F_GAM1 + q - 1 : F_SPHI + q - 4);
+        const int b = q == 0 ? S_DK : (q < 4 ? S_DGAM + 3 * (q - 1) : S_MAT + 3 * (q - 4));
+        const GTaps<decltype(t)> gt{a + (size_t)fld * N, t};
+        S(b + 0) = d1<O>(gt, 0, idx);
+        S(b + 1) = d1<O>(gt, 1, idx);
+        S(b + 2) = d1<O>(gt, 2, idx);
+      }
+      if (MATTER == kDust) flux_divergences<O>(t, P.fp_in, N, idx, sl);
+    };
+    if (interior) gpass(Taps<false>{i, j, k, nx, ny, nz, ny * nz, nz, c});
+    else gpass(Taps<true>{i, j, k, nx, ny, nz, ny * nz, nz, c});
   }
 
   // ---- centre values: perturbations and full values -------------------------

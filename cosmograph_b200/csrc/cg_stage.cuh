@@ -232,13 +232,14 @@ __device__ __forceinline__ double d1p(const double* __restrict__ fa, const doubl
 // Fields copied into tiles in phase 1, in order: (constraint mode) A_q with
 // first derivatives; the metric components, phi and alpha with first and
 // second derivatives; (constraint mode) K and Gamma^i with first derivatives;
-// (scalar) phi, Pi, psi_i with first derivatives.  In evolve mode K and
-// Gamma^i take their 24 first-derivative taps straight from global memory
-// (cheaper than a tile copy for first derivatives only).
+// (constraint mode, scalar) phi, Pi, psi_i with first derivatives.  In evolve
+// mode K, Gamma^i and the scalar fields take their first-derivative taps
+// straight from global memory (cheaper than a tile copy for first
+// derivatives only).
 template <int MATTER, int MODE>
 struct Phase1 {
   static constexpr int NA = MODE == kConstraints ? 6 : 0;
-  static constexpr int NS = MATTER == kScalar ? 5 : 0;
+  static constexpr int NS = (MATTER == kScalar && MODE != kEvolve) ? 5 : 0;
   static constexpr int N = NA + 8 + (MODE == kEvolve ? 0 : 4) + NS;
   __device__ __forceinline__ static int field(int it) {
     if (it < NA) return F_A11 + it;
@@ -442,10 +443,11 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     // and the dust flux divergences, taps from global memory
     auto gpass = [&](auto t) {
       if (MODE == kEvolve) {
+        constexpr int NG = MATTER == kScalar ? 9 : 4;  // K, Gamma^i (and phi_s, Pi, psi_i)
 #pragma unroll 1
-        for (int q = 0; q < 4; ++q) {
-          const int fld = q == 0 ? F_K : F_GAM1 + q - 1;
-          const int b = q == 0 ? S_DK : S_DGAM + 3 * (q - 1);
+        for (int q = 0; q < NG; ++q) {
+          const int fld = q == 0 ? F_K : (q < 4 ? F_GAM1 + q - 1 : F_SPHI + q - 4);
+          const int b = q == 0 ? S_DK : (q < 4 ? S_DGAM + 3 * (q - 1) : S_MAT + 3 * (q - 4));
           const GTaps<decltype(t)> gt{a + (size_t)fld * N, t};
           S(b + 0) = d1<O>(gt, 0, ph);
           S(b + 1) = d1<O>(gt, 1, ph);
