@@ -149,9 +149,14 @@ def profiled_traffic(n: int, order: int, precision: str):
         return None
 
 
-def make_state(n: int, seed: int, order: int):
+def make_state(n: int, seed: int, order: int, gpu: bool = True):
+    """GRF dust initial data: the random field drawn on the host, the
+    construction on the GPU (the host construction when gpu=False); both give
+    the same data to rounding."""
     from cosmograph_b200 import ics
 
+    if gpu:
+        return ics.grf_dust_gpu(n, seed=seed, rms_delta=1.0e-4, order=order, host_delta=True)
     return ics.grf_dust(n, seed=seed, rms_delta=1.0e-4, order=order)
 
 
@@ -225,7 +230,7 @@ def run_ensemble(a, world, rank, local):
 
     specs = ensemble.standard_ensemble()
     mine = ensemble.local_share(specs, rank, world)
-    states = ensemble.initial_states(mine, order=4)
+    states = ensemble.initial_states(mine, order=4, gpu=True)
     pts = sum(s.fields[0].size for s in states)
     all_pts = sum(s.points for s in specs)
     cfg = BoxConfig(order=4, lapse="Harmonic", precision="mixed")
@@ -309,7 +314,7 @@ def run_ensemble(a, world, rank, local):
     cpu = None
     if rank == 0 and a.cpu_baseline:
         try:
-            cpu = cpu_baseline(ensemble.initial_states([specs[16]], order=4)[0], 4)
+            cpu = cpu_baseline(ensemble.initial_states([specs[16]], order=4, gpu=True)[0], 4)
         except Exception as exc:  # reported, not fatal
             cpu = {"value": None, "error": str(exc)[:200]}
     if rank != 0:
@@ -365,9 +370,9 @@ def run_reference_arm(a, world, rank):
         print(json.dumps({"impl": "reference", "unavailable": f"{binp.name} was not built"}))
         return
     if a.workload == "ensemble":
-        st = ensemble.initial_states([spec], order=4)[0]
+        st = ensemble.initial_states([spec], order=4, gpu=False)[0]
     else:
-        st = make_state(n, seed=1, order=order)
+        st = make_state(n, seed=1, order=order, gpu=False)
     threads = os.cpu_count() or 1
     # each step is a full RK4 step of the same box; cap the count so the run
     # stays within a few minutes on the host cores

@@ -37,6 +37,7 @@ UNITS = [
     ("abi.o", "cg_abi.cu", []),
     ("noalloc.o", "cg_noalloc.cu", []),
     ("mixed.o", "cg_mixed_inst.cu", []),
+    ("ics.o", "cg_ics.cu", []),
 ]
 
 
@@ -71,7 +72,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             list(ex.map(run, jobs))
     if force or jobs or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         tmp = LIB.with_suffix(".so.tmp")
-        run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), "-o", str(tmp)])
+        run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *map(str, objs), "-lcufft", "-o", str(tmp)])
         os.replace(tmp, LIB)
     build_driver(force)
     return LIB

@@ -1124,6 +1124,29 @@ int cg_step(cg_ctx* ctx, int nsteps) {
   return CG_OK;
 }
 
+int cg_ic_grf_dust(cg_ctx* ctx, int box, const double* delta, uint64_t seed, double rms_delta, double ns,
+                   double cutoff) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  Box& b = ctx->boxes[box];
+  if (b.desc.matter != CG_MATTER_DUST) return fail(ctx, CG_ERR_INVALID, "GRF dust initial data need a dust box");
+  if (!(rms_delta >= 0.0) || !std::isfinite(ns)) return fail(ctx, CG_ERR_INVALID, "rms_delta >= 0 and finite ns");
+  for (Box& o : ctx->boxes)
+    if (o.stage_next > 1) return fail(ctx, CG_ERR_STATE, "initial data are set between steps");
+  const cg::GridSpec gs{b.desc.nx, b.desc.ny, b.desc.nz, b.desc.stencil_order, b.desc.dx};
+  const double kc = cutoff > 0.0 ? cutoff : std::min({gs.nx, gs.ny, gs.nz}) / 4.0;
+  double* scratch = nullptr;
+  CG_CUDA(ctx, cudaMalloc(&scratch, sizeof(double) * cg::ics::grf_scratch_doubles(gs)));
+  std::string err;
+  rc = cg::ics::grf_dust(gs, b.dev.P, scratch, delta, seed, rms_delta, ns, kc, b.desc.lambda, ctx->stream, err);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(scratch);
+  if (rc) return fail(ctx, rc, "GRF initial data: " + err);
+  b.stage_next = 0;
+  b.steps = 0;
+  return CG_OK;
+}
+
 int cg_set_option(cg_ctx* ctx, int option, int value) {
   if (!ctx) return CG_ERR_INVALID;
   switch (option) {

@@ -3,6 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <string>
+
 #include "cg_group.h"
 #include "cg_types.h"
 
@@ -93,6 +96,17 @@ inline int group_ctas_per_sm(int v, int order, int matter) {
 // the result lands in out[0] (device).  Defined in cg_abi.cu.
 cudaError_t launch_conformal_average(const double* field, const double* phi, int n, double phi_frw,
                                      double* partial, int nblk, double* out, cudaStream_t st);
+
+// GPU initial data (cg_ics.cu)
+struct GridSpec {
+  int nx, ny, nz, order;
+  double dx;
+};
+namespace ics {
+size_t grf_scratch_doubles(const GridSpec& s);
+int grf_dust(const GridSpec& s, double* P, double* scratch, const double* delta_host, uint64_t seed, double rms,
+             double ns, double kc, double rho_L, cudaStream_t st, std::string& err);
+}  // namespace ics
 
 // Message returned by cg_last_error(NULL) on this host thread.
 void set_global_error(const char* msg);

@@ -44,8 +44,13 @@ def standard_ensemble(base_seed: int = 1000, per_size: int = 16, sizes=(32, 64, 
     return specs
 
 
-def initial_states(specs, order: int = 4):
-    """Seeded Gaussian-random-field dust initial data for each box."""
+def initial_states(specs, order: int = 4, gpu: bool = False):
+    """Seeded Gaussian-random-field dust initial data for each box (random
+    field on the host; the construction on the GPU when gpu=True, the same
+    data to rounding)."""
+    if gpu:
+        return [ics.grf_dust_gpu(s.n, seed=s.seed, rms_delta=s.rms_delta, order=order, host_delta=True)
+                for s in specs]
     return [ics.grf_dust(s.n, seed=s.seed, rms_delta=s.rms_delta, order=order) for s in specs]
 
 

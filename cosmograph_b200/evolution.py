@@ -152,6 +152,18 @@ class Evolution:
         self._check(self.L.cg_status(self.ctx, ctypes.byref(f)))
         return int(f.value)
 
+    def ic_grf_dust(self, box: int, seed: int = 9, rms_delta: float = 1.0e-4, ns: float = 0.96,
+                    cutoff: float = 0.0, delta: np.ndarray | None = None) -> None:
+        """GRF dust initial data built on the GPU (cg_ic_grf_dust); `delta`
+        (host density contrast) replaces the GPU's own random field."""
+        dptr = None
+        if delta is not None:
+            delta = np.ascontiguousarray(delta, dtype=np.float64)
+            if delta.shape != self.templates[box].shape:
+                raise ValueError("delta must have the box's shape")
+            dptr = _dptr(delta)
+        self._check(self.L.cg_ic_grf_dust(self.ctx, box, dptr, ctypes.c_uint64(seed), rms_delta, ns, cutoff))
+
     def set_option(self, option: str, value: int) -> None:
         """Launch options: "batch", "graph", "autotune", "group_grid" (cg_set_option)."""
         code = {"batch": _lib.OPT_BATCH, "graph": _lib.OPT_GRAPH, "autotune": _lib.OPT_AUTOTUNE,

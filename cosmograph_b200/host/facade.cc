@@ -620,7 +620,21 @@ void DustSim::init() {
 
 void DustSim::setICs() {
   iodata->log("Setting dust initial conditions.");
-  loadICs();
+  if (cfg->has("ic_file")) {
+    loadICs();
+  } else {
+    // dust_ic_set_random (sims/dust.cc:40-51) built on the GPU from a seeded
+    // Gaussian random density contrast: rms_delta, spectral index ns, cutoff
+    // ic_spec_cut (modes; default N/4), rho_Lambda = Omega_L * 3 / (8 pi)
+    const double omega_l = std::stod((*cfg)("Omega_L", "0.0"));
+    bssnSim->desc().lambda = omega_l * 3.0 / (8.0 * 3.14159265358979323846);
+    const uint64_t seed = std::stoull((*cfg)("seed", "9"));
+    const double rms = std::stod((*cfg)("rms_delta", "1.0e-4"));
+    const double ns = std::stod((*cfg)("ns", "0.96"));
+    const double cut = std::stod((*cfg)("ic_spec_cut", "0"));
+    iodata->log("Setting cosmological ICs (GPU): seed " + std::to_string(seed) + ", rms delta " + fmt15(rms));
+    bssnSim->check(cg_ic_grf_dust(bssnSim->ctx(), 0, nullptr, seed, rms, ns, cut), "GRF initial data");
+  }
   lambda->setLambda(bssnSim->desc().lambda);
   iodata->log("Finished setting ICs.");
 }

@@ -103,11 +103,11 @@ def inverse_laplacian(f: np.ndarray, box_len: float) -> np.ndarray:
     (utils/Fourier.h:251-298)."""
     px, py, pz = _kgrid(f.shape)
     p2 = (px ** 2 + py ** 2 + pz ** 2) * (2.0 * PI / box_len) ** 2
-    fk = np.fft.rfftn(f)
+    fk = np.fft.rfftn(f, axes=(0, 1, 2))
     with np.errstate(divide="ignore", invalid="ignore"):
         fk = fk / (-p2)
     fk[0, 0, 0] = 0.0
-    return np.fft.irfftn(fk, s=f.shape)
+    return np.fft.irfftn(fk, s=f.shape, axes=(0, 1, 2))
 
 
 def gaussian_random_field(shape, seed: int, spectrum, rms: float) -> np.ndarray:
@@ -119,7 +119,7 @@ def gaussian_random_field(shape, seed: int, spectrum, rms: float) -> np.ndarray:
     with np.errstate(divide="ignore", invalid="ignore"):
         amp = np.sqrt(np.where(k > 0, spectrum(np.maximum(k, 1e-30)), 0.0))
     noise = rng.standard_normal(k.shape) + 1j * rng.standard_normal(k.shape)
-    field = np.fft.irfftn(amp * noise, s=shape)
+    field = np.fft.irfftn(amp * noise, s=shape, axes=(0, 1, 2))
     field -= field.mean()
     s = field.std()
     return field * (rms / s) if s > 0 else field
@@ -206,6 +206,29 @@ def grf_dust(n, seed: int = 9, rms_delta: float = 1.0e-4, order: int = 4, box_le
         st.field(f"A{i + 1}{j + 1}")[...] = v
     st.field("D")[...] = e6p * rho_0
     return st
+
+
+def grf_dust_gpu(n, seed: int = 9, rms_delta: float = 1.0e-4, order: int = 4, box_len: float = 1.0,
+                 omega_l: float = 1.0e-6, ns: float = 0.96, dt_frac: float = 0.1, delta=None,
+                 host_delta: bool = False) -> BoxState:
+    """grf_dust built on the GPU (cg_ic_grf_dust): the same construction with
+    cuFFT inverse Laplacians.  The random field comes from the GPU's own
+    generator unless `delta` is given; host_delta=True draws it on the host
+    exactly as grf_dust does, so the result equals grf_dust's to rounding."""
+    from .evolution import BoxConfig, Evolution
+
+    shape = (n, n, n) if np.isscalar(n) else tuple(n)
+    if host_delta and delta is None:
+        kc = min(shape) / 4.0
+        delta = gaussian_random_field(shape, seed, lambda k: k ** ns * np.exp(-(k / kc) ** 2), rms_delta)
+    dx = box_len / shape[0]
+    st = _empty(shape, DUST, dx, default_dt(dx, dt_frac))
+    st.lam = omega_l * RHO_FRW
+    with Evolution(st, BoxConfig(order=order)) as ev:
+        ev.ic_grf_dust(0, seed=seed, rms_delta=rms_delta, ns=ns, cutoff=min(shape) / 4.0, delta=delta)
+        out = ev.download(0)
+    out.step = 0
+    return out
 
 
 def grf_scalar(n, seed: int = 9, phi0: float = 1.0e-2, rms: float = 1.0e-5, mass: float = 1.0,

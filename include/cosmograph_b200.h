@@ -164,6 +164,21 @@ int cg_rk_stage(cg_ctx *ctx, int n);
  * Asynchronous: returns once the work is queued. */
 int cg_step(cg_ctx *ctx, int nsteps);
 
+/* Initial data on the GPU for a dust box: the reference's dust_ic_set_random
+ * (components/dust_fluid/dust_ic.cc:23-140) in synchronous gauge from a
+ * Gaussian random density contrast delta with P(k) ~ k^ns exp(-(k/cutoff)^2)
+ * (k in units of the fundamental mode; cutoff <= 0: min(nx,ny,nz)/4), zero
+ * mean and rms rms_delta, drawn from a counter-based generator seeded with
+ * `seed`, or taken from `delta` (host, nx*ny*nz doubles) when it is not NULL.
+ * Spectral inverse Laplacians on cuFFT (utils/Fourier.h:251-298), the box's
+ * stencil order for derivatives, rho_Lambda = the box's lambda.  Writes the
+ * _p register (every other field zero, FRW reference untouched) and resets
+ * the box like cg_upload_state.  CG_ERR_INVALID if the density turns
+ * negative somewhere.  Synchronous; allocates its scratch (about 11 doubles
+ * per point) for the duration of the call. */
+int cg_ic_grf_dust(cg_ctx *ctx, int box, const double *delta, uint64_t seed, double rms_delta, double ns,
+                   double cutoff);
+
 /* Launch options (cg_set_option).  No reference counterpart: the reference
  * evolves one box per process.
  *   CG_OPT_BATCH     1 (default): boxes of a context with the same precision,

@@ -102,3 +102,18 @@ def test_nan_stops_the_run_with_code_10(tmp_path):
                        timeout=600)
     assert r.returncode == 10, r.stdout[-1000:] + r.stderr[-1000:]
     assert "NAN detected" in (tmp_path / "out" / "log.txt").read_text()
+
+
+def test_dust_run_with_gpu_initial_data(tmp_path):
+    """Without ic_file the dust driver builds GRF initial data on the GPU
+    (the reference's DustSim::setICs path) and evolves them."""
+    run_driver(tmp_path, "\n".join([
+        "simulation_type = dust", "steps = 4", "N = 32", "stencil_order = 4", "lapse = Harmonic",
+        "seed = 11", "rms_delta = 1e-4", "Omega_L = 1e-6", "output_file = final.bin", "output_dir = out",
+        "IO_constraint_interval = 1", ""]))
+    got = S.load(tmp_path / "final.bin")
+    ic = ics.grf_dust_gpu(32, seed=11, rms_delta=1e-4, order=4)
+    ic.dx, ic.dt = got.dx, got.dt  # H_LEN_FRAC default 0.5: dx = 0.5/32
+    assert got.step == 5 and np.isfinite(got.fields).all()
+    h = rows(tmp_path / "out" / "H_violations.dat.gz")
+    assert len(h) == 5 and all(np.isfinite(r).all() for r in h)

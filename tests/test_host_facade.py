@@ -67,7 +67,7 @@ def test_driver_required_steps(driver, tmp_path):
 
 def test_driver_output_dir_not_overwritten(driver, tmp_path):
     out = tmp_path / "out"
-    (tmp_path / "c.txt").write_text(f"simulation_type = dust\nsteps = 2\noutput_dir = {out}\n")
+    (tmp_path / "c.txt").write_text(f"simulation_type = vacuum\nsteps = 2\noutput_dir = {out}\n")
     for _ in range(2):
         r = run(driver, ["c.txt"], tmp_path)
         assert r.returncode == 1
