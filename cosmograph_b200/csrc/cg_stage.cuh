@@ -637,30 +637,37 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
               gi[4] * (DDphi(4) + 2.0 * dphi[1] * dphi[2])));
   // BSSN_CALCULATE_RICCI_UNITARY_TERM4 summed over (K,L,M) in the reference's
   // order, all six components at once so each Gamma is read once per term
-  double t4[6];
+  // Ricci term 4 (BSSN_CALCULATE_RICCI_UNITARY_TERM4, bssn_macros.h:248-277):
+  // sum_{K,L,M} g^{LM} (G^K_{LI} G_{J,KM} + G^K_{LJ} G_{I,KM}
+  // + (G^K_{IM} G_{K,LJ} + G^K_{JM} G_{K,LI}) / 2), contracted through the
+  // raised symbols H^K_{MX} = sum_L g^{LM} G^K_{LX}:
+  // t4_IJ = sum_{K,M} (H^K_{MI} G_{J,KM} + H^K_{MJ} G_{I,KM})
+  //       + sum_{K,L} (H^K_{LI} G_{K,LJ} + H^K_{LJ} G_{K,LI}) / 2.
+  // A third of the reference's multiplications, in a different summation
+  // order (the one departure from the reference's operand order in this
+  // kernel; the parity tests hold it to the same bound).
+  double t4[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-  for (int Kx = 0; Kx < 3; ++Kx)
+  for (int Kx = 0; Kx < 3; ++Kx) {
+    double Hm[3][3];  // H^K_{MX} = sum_L g^{LM} G^K_{LX}
 #pragma unroll
-    for (int L = 0; L < 3; ++L)
+    for (int M = 0; M < 3; ++M)
 #pragma unroll
-      for (int M = 0; M < 3; ++M) {
-        const double gLM = gi[sym(L, M)];
-        double GKL[3], GLKM[3], GKM[3], GLKL[3];
+      for (int X = 0; X < 3; ++X)
+        Hm[M][X] = gi[sym(0, M)] * G(Kx, sym(0, X)) + gi[sym(1, M)] * G(Kx, sym(1, X)) + gi[sym(2, M)] * G(Kx, sym(2, X));
 #pragma unroll
-        for (int X = 0; X < 3; ++X) {
-          GKL[X] = G(Kx, sym(L, X));
-          GLKM[X] = GL(X, sym(Kx, M));
-          GKM[X] = G(Kx, sym(X, M));
-          GLKL[X] = GL(Kx, sym(L, X));
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int J = I; J < 3; ++J) {
+        double u = 0.0, w = 0.0;
+#pragma unroll
+        for (int M = 0; M < 3; ++M) {
+          u = u + (Hm[M][I] * GL(J, sym(Kx, M)) + Hm[M][J] * GL(I, sym(Kx, M)));
+          w = w + (Hm[M][I] * GL(Kx, sym(M, J)) + Hm[M][J] * GL(Kx, sym(M, I)));
         }
-#pragma unroll
-        for (int I = 0; I < 3; ++I)
-#pragma unroll
-          for (int J = I; J < 3; ++J) {
-            const double u = gLM * (GKL[I] * GLKM[J] + GKL[J] * GLKM[I] + 0.5 * (GKM[I] * GLKL[J] + GKM[J] * GLKL[I]));
-            t4[sym(I, J)] = (Kx == 0 && L == 0 && M == 0) ? u : t4[sym(I, J)] + u;
-          }
+        t4[sym(I, J)] = t4[sym(I, J)] + (u + 0.5 * w);
       }
+  }
 #pragma unroll
   for (int I = 0; I < 3; ++I)
 #pragma unroll
