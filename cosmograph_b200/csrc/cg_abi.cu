@@ -507,7 +507,17 @@ int validate(const cg_box_desc& d, std::string& why) {
       return CG_ERR_INVALID;
     }
   }
-  if (d.ko_coeff != 0.0) { why = "Kreiss-Oliger dissipation is not available on this path (ko_coeff must be 0)"; return CG_ERR_INVALID; }
+  if (d.ko_coeff != 0.0) {
+    if (d.precision == CG_PREC_MIXED) {
+      why = "Kreiss-Oliger dissipation is not available in the FP32-mixed form";
+      return CG_ERR_INVALID;
+    }
+    const int rko = d.stencil_order == 8 ? 5 : 2;  // orders 4 and 6: no dissipation (utils/math.h:36-72)
+    if ((d.stencil_order == 2 || d.stencil_order == 8) && (d.nx < rko + 1 || d.ny < rko + 1 || d.nz < rko + 1)) {
+      why = "Kreiss-Oliger dissipation needs stencil_order/2 + 2 points per axis (order 2) or 6 (order 8)";
+      return CG_ERR_INVALID;
+    }
+  }
   if (d.nfluids < 0 || d.nfluids > 4) { why = "at most 4 FRW fluids"; return CG_ERR_INVALID; }
   if (!(d.dx > 0.0) || !std::isfinite(d.dt)) { why = "dx must be positive and dt finite"; return CG_ERR_INVALID; }
   return CG_OK;
@@ -620,6 +630,7 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
     ph.dt = d.dt;
     ph.lambda = d.lambda;
     ph.a_adj_amp = d.a_adj_amp;
+    ph.ko_coeff = d.ko_coeff;
     ph.k_damping_amp = d.k_damping_amp;
     ph.gd_c = d.gd_c;
     ph.dw_mu_l = d.dw_mu_l;
@@ -888,10 +899,15 @@ int ensure_groups(cg_ctx* ctx) {
     g.variant = ba.variant;
     g.order = ba.desc.stencil_order;
     g.matter = ba.desc.matter;
-    for (size_t b = a; b < ctx->boxes.size() && g.members.size() < (size_t)cg::kMaxGroupBoxes; ++b) {
+    g.members.push_back((int)a);
+    used[a] = true;
+    // boxes with Kreiss-Oliger dissipation keep their own launches
+    for (size_t b = a + 1; ba.desc.ko_coeff == 0.0 && b < ctx->boxes.size() &&
+                           g.members.size() < (size_t)cg::kMaxGroupBoxes;
+         ++b) {
       const Box& bb = ctx->boxes[b];
       if (used[b] || bb.mixed != g.mixed || bb.variant != g.variant || bb.desc.stencil_order != g.order ||
-          bb.desc.matter != g.matter)
+          bb.desc.matter != g.matter || bb.desc.ko_coeff != 0.0)
         continue;
       g.members.push_back((int)b);
       used[b] = true;
@@ -909,6 +925,10 @@ int ensure_groups(cg_ctx* ctx) {
     ctx->groups.push_back(g);
   }
   std::sort(ctx->singles.begin(), ctx->singles.end());
+  // every box is launched exactly once per substep
+  size_t scheduled = ctx->singles.size();
+  for (const Group& g : ctx->groups) scheduled += g.members.size();
+  if (scheduled != ctx->boxes.size()) return fail(ctx, CG_ERR_STATE, "launch groups do not cover every box");
   ctx->grouped = true;
   return CG_OK;
 }

@@ -346,6 +346,42 @@ __device__ __forceinline__ void flux_divergences(const T& t, const double* __res
   }
 }
 
+// Kreiss-Oliger dissipation of one field at (i, j, k) (utils/math.h:36-72;
+// the reference defines it for stencil orders 2 and 8 only): the sixth
+// (order 2: fourth) undivided difference along each axis, taps from global
+// memory, plain offsets when the taps stay inside the box.
+template <int O>
+__device__ __forceinline__ double ko_dissipation(const double* __restrict__ f, int i, int j, int k, int nx, int ny, int nz,
+                                              bool inside, double c, double dx) {
+  auto at = [&](int a, int n) {
+    int ii = i + (a == 0 ? n : 0), jj = j + (a == 1 ? n : 0), kk = k + (a == 2 ? n : 0);
+    if (!inside) {
+      ii = wrap(ii, nx);
+      jj = wrap(jj, ny);
+      kk = wrap(kk, nz);
+    }
+    return __ldg(f + ((size_t)ii * ny + jj) * nz + kk);
+  };
+  auto X = [&](int n) { return at(0, n); };
+  auto Y = [&](int n) { return at(1, n); };
+  auto Z = [&](int n) { return at(2, n); };
+  if (O == 2) {
+    const double st = (1.0 * X(-2) + 1.0 * Y(-2) + 1.0 * Z(-2) - 4.0 * X(-1) - 4.0 * Y(-1) - 4.0 * Z(-1) +
+                       6.0 * X(0) + 6.0 * Y(0) + 6.0 * Z(0) - 4.0 * X(1) - 4.0 * Y(1) - 4.0 * Z(1) + 1.0 * X(2) +
+                       1.0 * Y(2) + 1.0 * Z(2)) /
+                      pow(dx, 4.0);
+    return c * pow(dx, 3.0) / 64.0 * st;
+  }
+  const double st = (1.0 * X(-5) + 1.0 * Y(-5) + 1.0 * Z(-5) - 10.0 * X(-4) - 10.0 * Y(-4) - 10.0 * Z(-4) +
+                     45.0 * X(-3) + 45.0 * Y(-3) + 45.0 * Z(-3) - 120.0 * X(-2) - 120.0 * Y(-2) - 120.0 * Z(-2) +
+                     210.0 * X(-1) + 210.0 * Y(-1) + 210.0 * Z(-1) - 252.0 * X(0) - 252.0 * Y(0) - 252.0 * Z(0) +
+                     210.0 * X(1) + 210.0 * Y(1) + 210.0 * Z(1) - 120.0 * X(2) - 120.0 * Y(2) - 120.0 * Z(2) +
+                     45.0 * X(3) + 45.0 * Y(3) + 45.0 * Z(3) - 10.0 * X(4) - 10.0 * Y(4) - 10.0 * Z(4) +
+                     1.0 * X(5) + 1.0 * Y(5) + 1.0 * Z(5)) /
+                    pow(dx, 10.0);
+  return -c * pow(dx, 9.0) / 1024.0 * st;
+}
+
 // Deterministic CTA reduction of Q values per thread: the first NSUM are
 // summed, the rest maximised; warp shuffles, then the warps in order.  Thread
 // 0 writes the Q results of this CTA to part[cta * Q].
@@ -376,8 +412,10 @@ __device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part, int cta
 }
 
 // The fused substep for the brick at brick coordinates (cx, cy, cz) of one
-// box; cta numbers the CTA's partial results in constraint mode.
-template <int O, int MATTER, int MODE>
+// box; cta numbers the CTA's partial results in constraint mode.  KO: the
+// Kreiss-Oliger terms are compiled in (a separate instantiation, so that the
+// common case carries none of their code).
+template <int O, int MATTER, int MODE, bool KO = false>
 __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph, StageBg bg, const StagePtrs& P,
                                            int stage, int cx, int cy, int cz, int cta) {
   constexpr int NFLD = NF<MATTER>::value;
@@ -801,6 +839,21 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   const double dt = ph.dt;
   double outv[NFLD];
   const bool renorm = ph.normalize != 0;
+  // Kreiss-Oliger terms of the 18 BSSN fields (subtracted from their RHS,
+  // bssn.cc:748-831), parked in the slots of the lowered Christoffels, which
+  // nothing reads after the Ricci tensor
+  constexpr int RKO = O == 8 ? 5 : 2;
+  const bool ko_on = KO && (O == 2 || O == 8) && ph.ko_coeff != 0.0;
+  if constexpr (KO) {
+    if (ko_on) {
+      const bool inside = x0 >= RKO && x0 + kBX + RKO <= geo.nx && y0 >= RKO && y0 + kBY + RKO <= geo.ny &&
+                          z0 >= RKO && z0 + kBZ + RKO <= geo.nz;
+#pragma unroll 1
+      for (int f = 0; f < F_NBSSN; ++f)
+        S(S_DG + f) = ko_dissipation<O>(a + (size_t)f * N, i, j, k, geo.nx, geo.ny, geo.nz, inside, ph.ko_coeff, ph.dx);
+    }
+  }
+  auto ko = [&](int fld) -> double { return ko_on ? S(S_DG + fld) : 0.0; };
   auto finalize = [&](int fld, double cv) {
     const double pv = __ldcs(&P.p[(size_t)fld * N + c]);
     double o;
@@ -828,7 +881,8 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
 
   // ev_DIFFgammaIJ (bssn.cc:748-753)
 #pragma unroll
-  for (int m = 0; m < 6; ++m) finalize(F_G11 + m, (-2.0 * alpha * A[m]) + 0.5 * ph.a_adj_amp * dt * H * g[m]);
+  for (int m = 0; m < 6; ++m)
+    finalize(F_G11 + m, (-2.0 * alpha * A[m]) + 0.5 * ph.a_adj_amp * dt * H * g[m] - ko(F_G11 + m));
   // ev_AIJ (bssn.cc:755-760, BSSN_DT_AIJ bssn_macros.h:334-337)
 #pragma unroll
   for (int I = 0; I < 3; ++I)
@@ -846,7 +900,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       const double RTF = Ric(qq) - (1.0 / 3.0) * e4phi * gm[qq] * ricci;
       const double dtA = (em4phi * (alpha * (RTF - 8.0 * kPi * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
                           alpha * (((K + 2.0 * 0.0) * A[qq]) - 2.0 * (aa)));
-      finalize(F_A11 + qq, dtA - 1.0 * ph.a_adj_amp * dt * A[qq] * H);
+      finalize(F_A11 + qq, dtA - 1.0 * ph.a_adj_amp * dt * A[qq] * H - ko(F_A11 + qq));
     }
   // ev_GammaI (bssn.cc:762-764, BSSN_DT_GAMMAI_NOSHIFT bssn_macros.h:342-361)
   const double sq[3] = {S(S_SRC + Q_S1), S(S_SRC + Q_S2), S(S_SRC + Q_S3)};
@@ -863,19 +917,20 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
                              gi[sym(I, 0)] * 0.0 + gi[sym(I, 1)] * 0.0 + gi[sym(I, 2)] * 0.0) -
               2.0 * alpha * 0.0 * (C(F_GAM1 + I) - Gd[I]) -
               8.0 * kPi * (gi[sym(I, 0)] * sq[0] + gi[sym(I, 1)] * sq[1] + gi[sym(I, 2)] * sq[2])));
-    finalize(F_GAM1 + I, ns + 0.0);
+    finalize(F_GAM1 + I, ns + 0.0 - ko(F_GAM1 + I));
   }
   // ev_DIFFK (bssn.cc:766-795)
   {
     double v = (-DDaTR + alpha * (1.0 / 3.0 * (Kd + 2.0 * 0.0) * (Kd + 2.0 * 0.0 + 2.0 * bg.K_FRW) + AijAij) +
                 4.0 * kPi * alpha * (S(S_SRC + Q_R) + S(S_SRC + Q_S)) + 4.0 * kPi * alphad * (bg.rho_FRW + bg.S_FRW));
     if (ph.k_damping_amp != 0.0) v = v - 1.0 * ph.k_damping_amp * H * exp(-5.0 * phi);
-    finalize(F_K, v);
+    finalize(F_K, v - ko(F_K));
   }
   // ev_DIFFphi (bssn.cc:797-820)
-  finalize(F_PHI, (0.1 * ph.a_adj_amp * dt * H - 1.0 / 6.0 * (alpha * (Kd + 2.0 * 0.0) + alphad * bg.K_FRW - (0.0 + 0.0 + 0.0))));
+  finalize(F_PHI, (0.1 * ph.a_adj_amp * dt * H - 1.0 / 6.0 * (alpha * (Kd + 2.0 * 0.0) + alphad * bg.K_FRW - (0.0 + 0.0 + 0.0))) -
+                      ko(F_PHI));
   // ev_DIFFalpha (bssn.cc:822-831)
-  finalize(F_ALPHA, ev_lapse(ph, bg, alpha, K, Kd, phi));
+  finalize(F_ALPHA, ev_lapse(ph, bg, alpha, K, Kd, phi) - ko(F_ALPHA));
   if (MATTER == kDust) {
 #pragma unroll
     for (int m = 0; m < 4; ++m) finalize(F_D + m, rhs_m[m]);
@@ -928,11 +983,11 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
 }
 
 // One box: one CTA per brick.
-template <int O, int MATTER, int MODE>
+template <int O, int MATTER, int MODE, bool KO = false>
 __global__ void __launch_bounds__(kThreads, 2)
 stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
-  stage_body<O, MATTER, MODE>(geo, ph, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x,
-                              blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
+  stage_body<O, MATTER, MODE, KO>(geo, ph, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x,
+                                  blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
 }
 
 // A group of boxes of the same order and matter model, one launch per

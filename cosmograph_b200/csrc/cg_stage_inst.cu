@@ -81,6 +81,19 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
   }
   BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
   constexpr size_t smem = sizeof(double) * Slots<M>::value * kThreads;
+  if constexpr (O == 2 || O == 8) {
+    if (b.ph.ko_coeff != 0.0) {  // Kreiss-Oliger dissipation: its own instantiation
+      static bool configured_ko = false;
+      if (!configured_ko) {
+        cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M, kEvolve, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured_ko = true;
+      }
+      stage_kernel<O, M, kEvolve, true><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage);
+      return cudaGetLastError();
+    }
+  }
   static bool configured = false;  // per instantiation
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M, kEvolve>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

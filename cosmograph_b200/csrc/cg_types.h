@@ -40,6 +40,7 @@ struct Physics {
   double lambda;          // rho_Lambda
   double a_adj_amp, k_damping_amp, gd_c, dw_mu_l, dw_p;
   double pot_const, pot_mass;
+  double ko_coeff;        // KO_damping_coefficient (orders 2 and 8)
 };
 
 // Background values for one substep (FRW stage values, grid averages).

@@ -90,7 +90,7 @@ typedef struct {
   int reserved0;
   double dx, dt;           /* grid spacing and time step                          */
   double lambda;           /* rho_Lambda (Lambda::setLambda)                      */
-  double ko_coeff;         /* KO_damping_coefficient; must be 0 here              */
+  double ko_coeff;         /* KO_damping_coefficient (orders 2 and 8; FP64 only)   */
   double a_adj_amp;        /* config a_adj_amp                                    */
   double k_damping_amp;    /* config k_damping_amp                                */
   double gd_c;             /* config gd_c (OnePlusLog), default 1                 */

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from cosmograph_b200 import ics, state as S
-from cosmograph_b200.evolution import BoxConfig, Evolution
+from cosmograph_b200.evolution import BoxConfig, Evolution, evolve
 
 pytestmark = pytest.mark.gpu
 
@@ -92,3 +92,19 @@ def test_substeps_and_mixed_matter_groups():
     ref, _ = run(states, cfg, 1, batch=0)
     for a, b in zip(got, ref):
         assert np.array_equal(a, b)
+
+
+def test_every_box_is_stepped_with_mixed_options():
+    """Boxes with Kreiss-Oliger dissipation keep their own launches; the others
+    of the same kind still form a group; every box advances."""
+    shapes = [(16, 16, 16), (16, 16, 32), (20, 16, 16)]
+    states = ensemble(shapes, seed0=80)
+    cfgs = [BoxConfig(order=8, ko_coeff=0.2), BoxConfig(order=8), BoxConfig(order=8)]
+    with Evolution(states, cfgs) as ev:
+        assert [g["boxes"] for g in ev.groups()] == [2]
+        ev.step(2)
+        ev.synchronize()
+        got = [ev.download(q) for q in range(3)]
+    for q, (st, cfg) in enumerate(zip(states, cfgs)):
+        ref = evolve(st, 2, cfg)
+        assert got[q].step == 2 and np.array_equal(got[q].fields, ref.fields), q

@@ -82,6 +82,23 @@ def test_against_restatement(matter, shape, order, lapse, steps):
     assert worst(errs)[1] <= TOL["fp64"], worst(errs)
 
 
+@pytest.mark.parametrize("matter,shape,order", [(S.DUST, (20, 18, 22), 8), (S.VACUUM, (12, 14, 16), 2),
+                                                 (S.SCALAR, (16, 16, 16), 8), (S.DUST, (16, 16, 16), 4)])
+def test_kreiss_oliger_against_restatement(matter, shape, order):
+    """KO_damping_coefficient != 0 (utils/math.h:36-72: orders 2 and 8; a no-op
+    at order 4)."""
+    st = ics.perturbed(shape, matter, seed=31, amp=2e-2)
+    ref = oracle.evolve(st, 4, order, ko_coeff=0.3)
+    got = evolve(st, 4, BoxConfig(order=order, ko_coeff=0.3))
+    errs = field_errors(got.fields, ref.fields, st.names, floor=1e-18)
+    assert worst(errs)[1] <= TOL["fp64"], worst(errs)
+    plain = evolve(st, 4, BoxConfig(order=order))
+    if order in (2, 8):
+        assert not np.array_equal(plain.fields, got.fields)
+    else:
+        assert np.array_equal(plain.fields, got.fields)
+
+
 def test_sinusoid_100_steps():
     """Single-mode dust box, 32^3, 4th order, dt = 0.1 dx, 100 RK4 steps."""
     st = ics.sinusoid_dust(32)
