@@ -253,7 +253,8 @@ class CosmoSim {
   void run();
   void runCommonStepTasks();
   void outputStateInformation();
-  void outputCommon();  // constraint and FRW time series at their intervals
+  void outputCommon();     // snapshots, constraint and FRW time series at their intervals
+  void outputSnapshots();  // 3-D / 2-D / 1-D field dumps (io_bssn_fields_snapshot)
   idx_t getStep() const { return step; }
   BSSN* bssn() { return bssnSim; }
 

@@ -498,7 +498,66 @@ void CosmoSim::runCommonStepTasks() {
   if (step % 100 == 0) std::cout << "step " << step << " / " << num_steps << "\n" << std::flush;
 }
 
+// Field snapshots (io_bssn_fields_snapshot, IO/io.cc:106-158): for every
+// field register named by a true "IO_3D_<name>" / "IO_2D_<name>" /
+// "IO_1D_<name>" key, at the matching interval.  HDF5 is not available here:
+// 3-D grids (all points) and 2-D grids (the first ny*nz points, the x = 0
+// plane) are gz-compressed raw little-endian FP64 in the box's memory order
+// (x-major, z fastest), named like the reference's files with ".f64.gz" for
+// ".h5.gz"; 1-D strips are the reference's gz text rows (IO/io.cc:730-770).
+void CosmoSim::outputSnapshots() {
+  const std::string step_str = std::to_string(step);
+  const cg_box_desc& d = bssnSim->desc();
+  auto due = [&](const char* key) {
+    const int iv = std::stoi((*cfg)(key, "0"));
+    return iv > 0 && step % iv == 0;
+  };
+  const bool d3 = due("IO_3D_grid_interval"), d2 = due("IO_2D_grid_interval"), d1 = due("IO_1D_grid_interval");
+  if (!d3 && !d2 && !d1) return;
+  for (const auto& kv : bssnSim->fields) {
+    const std::string& name = kv.first;
+    const bool w3 = d3 && std::stoi((*cfg)("IO_3D_" + name, "0"));
+    const bool w2 = d2 && std::stoi((*cfg)("IO_2D_" + name, "0"));
+    const bool w1 = d1 && std::stoi((*cfg)("IO_1D_" + name, "0"));
+    if (!w3 && !w2 && !w1) continue;
+    const std::vector<double> v = kv.second->values();
+    auto dump_raw = [&](const std::string& fn, size_t count) {
+      gzFile f = gzopen(fn.c_str(), "wb");
+      if (!f) {
+        iodata->log("Error opening file: " + fn);
+        return;
+      }
+      gzwrite(f, v.data(), (unsigned)(count * sizeof(double)));
+      gzclose(f);
+    };
+    if (w3) dump_raw(iodata->dir() + "3D_" + name + step_str + ".3d_grid.f64.gz", v.size());
+    if (w2) dump_raw(iodata->dir() + "2D_" + name + step_str + ".2d_grid.f64.gz", (size_t)d.ny * d.nz);
+    if (w1) {
+      const int axis = std::stoi((*cfg)("IO_1D_" + name + "_axis", "1"));
+      const long n1 = std::stol((*cfg)("IO_1D_" + name + "_xoffset", "0"));
+      const long n2 = std::stol((*cfg)("IO_1D_" + name + "_yoffset", "0"));
+      const std::string fn = iodata->dir() + "1D_" + name + ".strip.dat.gz";
+      gzFile f = gzopen(fn.c_str(), "ab");
+      if (!f) {
+        iodata->log("Error opening file: " + fn);
+        continue;
+      }
+      auto at = [&](long i, long j, long k) { return v[((size_t)i * d.ny + j) * d.nz + k]; };
+      std::string row;
+      const long len = axis == 1 ? d.nx : (axis == 2 ? d.ny : d.nz);
+      for (long q = 0; q < len; ++q) {
+        const double x = axis == 1 ? at(q, n1, n2) : (axis == 2 ? at(n1, q, n2) : at(n1, n2, q));
+        row += fmt15(x) + "\t";
+      }
+      row += "\n";
+      gzwrite(f, row.data(), (unsigned)row.size());
+      gzclose(f);
+    }
+  }
+}
+
 void CosmoSim::outputCommon() {
+  outputSnapshots();
   const int ci = std::stoi((*cfg)("IO_constraint_interval", "0"));
   if (ci > 0 && step % ci == 0) {
     real_t H[8] = {0}, M[8] = {0}, G[7] = {0}, A[7] = {0}, S[7] = {0};

@@ -117,3 +117,24 @@ def test_dust_run_with_gpu_initial_data(tmp_path):
     assert got.step == 5 and np.isfinite(got.fields).all()
     h = rows(tmp_path / "out" / "H_violations.dat.gz")
     assert len(h) == 5 and all(np.isfinite(r).all() for r in h)
+
+
+def test_field_snapshots(tmp_path):
+    """IO_3D / IO_2D / IO_1D keys (the reference's io_bssn_fields_snapshot) for
+    the _a register after stepInit at the output steps."""
+    st = ics.grf_dust(16, seed=23, rms_delta=1e-4, order=4)
+    st.save(tmp_path / "ic.bin")
+    run_driver(tmp_path, "\n".join([
+        "simulation_type = dust", "steps = 2", "stencil_order = 4", "lapse = Harmonic", "ic_file = ic.bin",
+        "output_dir = out", "IO_3D_grid_interval = 2", "IO_3D_DIFFphi_a = 1", "IO_2D_grid_interval = 2",
+        "IO_2D_D_a = 1", "IO_1D_grid_interval = 1", "IO_1D_DIFFK_a = 1", "IO_1D_DIFFK_a_axis = 3",
+        "IO_1D_DIFFK_a_xoffset = 2", "IO_1D_DIFFK_a_yoffset = 5", ""]))
+    out = tmp_path / "out"
+    phi0 = np.frombuffer(gzip.open(out / "3D_DIFFphi_a0.3d_grid.f64.gz").read(), dtype="<f8").reshape(16, 16, 16)
+    assert np.array_equal(phi0, st.field("DIFFphi"))
+    D0 = np.frombuffer(gzip.open(out / "2D_D_a0.2d_grid.f64.gz").read(), dtype="<f8").reshape(16, 16)
+    assert np.array_equal(D0, st.field("D")[0])
+    assert (out / "3D_DIFFphi_a2.3d_grid.f64.gz").exists() and not (out / "3D_DIFFphi_a1.3d_grid.f64.gz").exists()
+    strip = rows(out / "1D_DIFFK_a.strip.dat.gz")
+    assert len(strip) == 3 and len(strip[0]) == 16
+    np.testing.assert_allclose(strip[0], st.field("DIFFK")[2, 5, :], rtol=1e-14)
