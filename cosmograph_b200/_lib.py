@@ -25,7 +25,7 @@ LAPSE = {
 }
 PRECISION = {"fp64": 0, "fp64_fma": 1, "mixed": 2}
 POTENTIAL = {"const": 0, "quadratic": 1}
-STATUS_NAN, STATUS_NONFINITE = 1, 2
+STATUS_NAN, STATUS_NONFINITE, STATUS_TILE_TIMEOUT = 1, 2, 4
 
 # every symbol include/cosmograph_b200.h declares
 EXPORTS = (
@@ -37,7 +37,7 @@ EXPORTS = (
     "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints",
     "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust",
 )
-OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID = 1, 2, 3, 4
+OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID, OPT_TMA = 1, 2, 3, 4, 5
 
 
 class BoxDesc(ctypes.Structure):

@@ -113,7 +113,7 @@ struct cg_ctx {
   std::vector<Group> groups;
   std::vector<int> singles;  // boxes launched on their own
   bool grouped = false;      // groups and singles are current
-  int opt_batch = 1, opt_graph = 0, opt_autotune = 1, opt_group_grid = 0;
+  int opt_batch = 1, opt_graph = 0, opt_autotune = 1, opt_group_grid = 0, opt_tma = 1;
   cudaGraphExec_t gexec = nullptr;
   int gexec_steps = 0;
   cudaStream_t stream = nullptr;
@@ -670,6 +670,10 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
       const size_t reg32 = sizeof(float) * (size_t)b.dev.nfields * b.dev.pts;
       if (e == cudaSuccess) e = cudaMalloc(&m.X, reg32);
       if (e == cudaSuccess) e = cudaMalloc(&m.Y, reg32);
+      if (e == cudaSuccess) {
+        cg::mixed::make_tile_maps(m);  // TMA tile copies where the layout allows
+        m.tma = m.tma && ctx->opt_tma;
+      }
       if (e == cudaSuccess && d.matter == CG_MATTER_DUST) {
         const size_t fp = sizeof(float) * (size_t)cg::P_N * b.dev.pts;
         e = cudaMalloc(&m.FP0, fp);
@@ -851,6 +855,9 @@ int write_table(cg_ctx* ctx, Group& g) {
       e.dt = b.mdev.dt;
       e.P = b.mdev.P; e.F = b.mdev.F; e.X = b.mdev.X; e.Y = b.mdev.Y; e.FP0 = b.mdev.FP0; e.FP1 = b.mdev.FP1;
       e.status = b.mdev.status;
+      e.mapX = b.mdev.mapX;
+      e.mapY = b.mdev.mapY;
+      e.tma = b.mdev.tma;
       e.nbx = bricks_along<Br>(e.nx, Br::BX); e.nby = bricks_along<Br>(e.ny, Br::BY); e.nbz = bricks_along<Br>(e.nz, Br::BZ);
       e.first = first;
       first += e.nbx * e.nby * e.nbz;
@@ -1178,6 +1185,14 @@ int cg_set_option(cg_ctx* ctx, int option, int value) {
         ctx->grouped = false;
       }
       return CG_OK;
+    case CG_OPT_TMA:
+      for (Box& b : ctx->boxes)
+        if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "change CG_OPT_TMA between steps");
+      ctx->opt_tma = value != 0;
+      for (Box& b : ctx->boxes)
+        if (b.mixed) b.mdev.tma = b.mdev.maps && ctx->opt_tma;
+      ctx->grouped = false;  // the group tables carry the flag
+      return CG_OK;
     case CG_OPT_GRAPH: ctx->opt_graph = value != 0; return CG_OK;
     case CG_OPT_AUTOTUNE: ctx->opt_autotune = value != 0; return CG_OK;
     case CG_OPT_GROUP_GRID:
@@ -1227,6 +1242,7 @@ int cg_synchronize(cg_ctx* ctx) {
   uint32_t f = 0;
   int rc = cg_status(ctx, &f);
   if (rc) return rc;
+  if (f & CG_STATUS_TILE_TIMEOUT) return fail(ctx, CG_ERR_CUDA, "a TMA tile copy timed out");
   if (f & CG_STATUS_NAN) return fail(ctx, CG_ERR_NAN, "NaN detected in DIFFphi");
   return CG_OK;
 }

@@ -1,6 +1,7 @@
 // cg_internal.h -- host-side declarations shared by the CUDA translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -30,6 +31,9 @@ struct BoxDev {
 // Device storage of one box evolved in the FP32-mixed form: FP64 _p and _f,
 // FP32 perturbation substep inputs and dust flux primitives.
 struct MixedBox {
+  CUtensorMap mapX, mapY;  // TMA maps of X and Y (4-D {nz, ny, nx, field}); valid when maps != 0
+  int maps;                // the maps are encoded
+  int tma;                 // interior tiles are copied by TMA (maps != 0 and the option on)
   int nx, ny, nz, pts, nfields, order, matter, lapse, normalize;
   double dx, dt;
   double* P;
@@ -46,6 +50,8 @@ struct GroupBox;
 struct GroupBg;
 cudaError_t launch_stage(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st);
 cudaError_t launch_init(const MixedBox& b, const Bg& bg, cudaStream_t st);
+// encode b.mapX / b.mapY and set b.maps = b.tma = 1 when the box allows TMA tile copies
+void make_tile_maps(MixedBox& b);
 // one launch for substep `stage` of every box of a mixed group (as launch_group)
 cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
                          cudaStream_t st);

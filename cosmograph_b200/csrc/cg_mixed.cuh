@@ -22,7 +22,9 @@
 #pragma once
 
 #include "cg_group.h"
+#include "cosmograph_b200.h"
 #include "cg_tile.cuh"
+#include "cg_tma.cuh"
 #include "cg_types.h"
 
 namespace cg {
@@ -30,9 +32,13 @@ namespace mixed {
 
 using Brick = tile::Brick32;
 constexpr int kBX = Brick::BX, kBY = Brick::BY, kBZ = Brick::BZ, kThreads = Brick::THREADS;
-// FP32 tiles with a 24-float row pitch: conflict-free taps (cg_tile.cuh)
+// FP32 tiles with a 24-float row pitch (conflict-free taps, cg_tile.cuh)
+// whose column 0 is z0 - 4: a TMA box {24, TY, TX} starts at an aligned z
+// for every stencil order
 template <int O>
-using TileG = tile::Geom<O, Brick, 24>;
+using TileG = tile::Geom<O, Brick, 24, 4>;
+constexpr unsigned kStatusTileTimeout = CG_STATUS_TILE_TIMEOUT;  // a TMA tile copy did not complete
+constexpr long long kTmaWaitCycles = 2000000000;  // about a second
 
 struct Ptrs {
   const float* in;     // delta of a^n
@@ -69,6 +75,7 @@ __host__ __device__ inline double bgv(const double* a, int f) { return bgi(f) < 
 // One box of a mixed launch group (device table) and the per-substep
 // backgrounds of a group (kernel parameter); as the FP64 GroupBox / GroupBg.
 struct GroupBox {
+  CUtensorMap mapX, mapY;  // TMA maps of the FP32 inputs (valid when tma != 0)
   int nx, ny, nz, pts, lapse, normalize;
   float idx;
   double dt;
@@ -77,6 +84,7 @@ struct GroupBox {
   unsigned* status;
   int nbx, nby, nbz;
   int first;
+  int tma;
 };
 struct GroupBg {
   int nboxes, total;
@@ -207,21 +215,11 @@ __device__ __forceinline__ int phase1_field(int it) {
                 : (it == 6 ? F_PHI : (it == 7 ? F_ALPHA : (it == 8 ? F_K : (it < 12 ? F_GAM1 + it - 9 : F_SPHI + it - 12))));
 }
 
-template <int O, int MATTER>
-__device__ __forceinline__ void derivatives(const float* __restrict__ a, int N, float idx, float idx2,
-                                            const float gi[6], float* sl, float* tl, const int* rowoff, int tid,
-                                            int z0, int nz, int cc) {
-  tile::Loader<TileG<O>, Brick, float> ld;
-  ld.init(tid, z0, nz);
-  ld.fetch(a + (size_t)phase1_field(0) * N, rowoff);
-  const tile::Taps<TileG<O>, float> t{tl, cc};
-  constexpr int NIT = 8;  // fields with second derivatives; first-derivative-only fields use global taps
-#pragma unroll 1
-  for (int it = 0; it < NIT; ++it) {
-    __syncthreads();
-    ld.store(tl);
-    __syncthreads();
-    if (it + 1 < NIT) ld.fetch(a + (size_t)phase1_field(it + 1) * N, rowoff);
+// first and second derivatives of phase-1 field `it` from its tile
+template <int O, class T>
+__device__ __forceinline__ void field_derivatives(int it, const T& t, float idx, float idx2, const float gi[6],
+                                                  float* sl) {
+  {
     if (it < 8) {
       const float g1 = d1<O>(t, 0, idx), g2 = d1<O>(t, 1, idx), g3 = d1<O>(t, 2, idx);
       const float h11 = d2<O>(t, 0, idx2), h22 = d2<O>(t, 1, idx2), h33 = d2<O>(t, 2, idx2);
@@ -244,13 +242,52 @@ __device__ __forceinline__ void derivatives(const float* __restrict__ a, int N, 
         sl[(b2 + 4) * kThreads] = h23;
         sl[(b2 + 5) * kThreads] = h33;
       }
-    } else {
-      const int b = it == 8 ? S_DK : (it < 12 ? S_DGAM + 3 * (it - 9) : S_MAT + 3 * (it - 12));
-      sl[(b + 0) * kThreads] = d1<O>(t, 0, idx);
-      sl[(b + 1) * kThreads] = d1<O>(t, 1, idx);
-      sl[(b + 2) * kThreads] = d1<O>(t, 2, idx);
     }
   }
+}
+
+// The tile copies: by TMA (tmap != null, a brick whose halo lies inside the
+// box) or by the threads' own loads with periodic wrap.  Returns false (the
+// same value in every thread) when a TMA copy did not complete within
+// kTmaWaitCycles; the status word then carries kStatusTileTimeout.
+template <int O, int MATTER>
+__device__ __forceinline__ bool derivatives(const float* __restrict__ a, int N, float idx, float idx2,
+                                            const float gi[6], float* sl, float* tl, const int* rowoff, int tid,
+                                            int x0, int y0, int z0, int nz, int cc, const CUtensorMap* tmap,
+                                            uint64_t* bar, unsigned& phase, unsigned* status) {
+  using G = TileG<O>;
+  const tile::Taps<G, float> t{tl, cc};
+  constexpr int NIT = 8;  // fields with second derivatives; first-derivative-only fields use global taps
+  if (tmap) {
+    bool ok = true;
+#pragma unroll 1
+    for (int it = 0; it < NIT; ++it) {
+      tma::fence_proxy_async();  // this thread's shared-memory accesses come before the copy's writes
+      __syncthreads();           // the previous tile has been read
+      if (tid == 0) {
+        tma::arrive_expect_tx(bar, (unsigned)(G::SIZE * sizeof(float)));
+        tma::load_4d(tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, phase1_field(it), bar);
+      }
+      if (ok && !tma::wait(bar, phase, kTmaWaitCycles)) ok = false;
+      phase ^= 1u;
+      field_derivatives<O>(it, t, idx, idx2, gi, sl);
+    }
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == 0) atomicOr(status, kStatusTileTimeout);
+    return ok;
+  }
+  tile::Loader<G, Brick, float> ld;
+  ld.init(tid, z0, nz);
+  ld.fetch(a + (size_t)phase1_field(0) * N, rowoff);
+#pragma unroll 1
+  for (int it = 0; it < NIT; ++it) {
+    __syncthreads();
+    ld.store(tl);
+    __syncthreads();
+    if (it + 1 < NIT) ld.fetch(a + (size_t)phase1_field(it + 1) * N, rowoff);
+    field_derivatives<O>(it, t, idx, idx2, gi, sl);
+  }
+  return true;
 }
 
 // dust flux divergences from the stored FP32 flux primitives (global taps)
@@ -270,11 +307,13 @@ __device__ __forceinline__ void flux_divergences(const T& t, const float* __rest
 // The FP32-mixed substep for the brick at brick coordinates (cx, cy, cz).
 template <int O, int MATTER>
 __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt,
-                                           const Bg& bg, const Ptrs& P, int stage, int cx, int cy, int cz) {
+                                           const Bg& bg, const Ptrs& P, int stage, int cx, int cy, int cz,
+                                           const CUtensorMap* tmap, uint64_t* bar, unsigned& phase,
+                                           bool& tma_ok) {
   constexpr int NFLD = MATTER == kDust ? 22 : (MATTER == kScalar ? 23 : 18);
   constexpr int R = O / 2;
   constexpr float kPif = 3.14159265358979f;
-  extern __shared__ float smf[];
+  extern __shared__ __align__(128) float smf[];  // 128-byte aligned: TMA destinations
   const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
   float* sl = smf + tid;
   auto S = [&](int s) -> float& { return sl[s * kThreads]; };
@@ -308,12 +347,20 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
     static_assert(TileG<O>::SIZE * sizeof(float) + TileG<O>::ROWS * sizeof(int) <=
                       (size_t)kTileSlots * kThreads * sizeof(float),
                   "tile and row offsets fit the phase-2-only slots");
+    using G = TileG<O>;
     float* tl = smf + kTileSlot * kThreads;
-    int* rowoff = reinterpret_cast<int*>(tl + TileG<O>::SIZE);
-    tile::row_offsets<TileG<O>, Brick>(x0, y0, nx, ny, nz, tid, rowoff);
-    __syncthreads();  // every warp reads every row offset
-    derivatives<O, MATTER>(a, N, idx, idx2, gi, sl, tl, rowoff, tid, z0, nz,
-                   tile::centre<TileG<O>>(threadIdx.z, threadIdx.y, threadIdx.x));
+    int* rowoff = reinterpret_cast<int*>(tl + G::SIZE);
+    // TMA when the brick's halo lies inside the box (no wrap)
+    const bool by_tma = tmap && tma_ok && x0 >= G::R && x0 + kBX + G::R <= nx && y0 >= G::R && y0 + kBY + G::R <= ny &&
+                        z0 >= G::ZO && z0 + kBZ + G::R <= nz;
+    if (!by_tma) {
+      tile::row_offsets<G, Brick>(x0, y0, nx, ny, nz, tid, rowoff);
+      __syncthreads();  // every warp reads every row offset
+    }
+    // after a copy timed out the CTA copies by threads (the barrier's phase is unknown)
+    tma_ok = derivatives<O, MATTER>(a, N, idx, idx2, gi, sl, tl, rowoff, tid, x0, y0, z0, nz,
+                                    tile::centre<G>(threadIdx.z, threadIdx.y, threadIdx.x), by_tma ? tmap : nullptr,
+                                    bar, phase, P.status) && tma_ok;
     __syncthreads();
   }
   if (!live) return;
@@ -703,11 +750,27 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
   }
 }
 
-// One box: one CTA per brick.
+// the TMA barrier of a CTA: initialised once, before any copy
+__device__ __forceinline__ void init_tile_barrier(uint64_t* bar, bool use) {
+  if (use && threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+    tma::bar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+// One box: one CTA per brick.  tmap: the TMA map of this substep's input
+// (use_tma = 0: every tile is copied by the threads).
 template <int O, int MATTER>
 __global__ void __launch_bounds__(kThreads, 4)
-mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt, Bg bg, Ptrs P, int stage) {
-  mixed_body<O, MATTER>(nx, ny, nz, lapse, normalize, idx, dt, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x);
+mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt, Bg bg, Ptrs P, int stage,
+             const __grid_constant__ CUtensorMap tmap, int use_tma) {
+  __shared__ __align__(8) uint64_t bar;
+  init_tile_barrier(&bar, use_tma != 0);
+  unsigned phase = 0;
+  bool tma_ok = true;
+  mixed_body<O, MATTER>(nx, ny, nz, lapse, normalize, idx, dt, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x,
+                        use_tma ? &tmap : nullptr, &bar, phase, tma_ok);
 }
 
 // Register roles of substep n (X/Y ping-pong, as in the single-box launcher).
@@ -734,7 +797,12 @@ mixed_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
   __shared__ GroupBox sb;
   __shared__ Ptrs sp;
   __shared__ Bg sbg;
+  __shared__ const CUtensorMap* stm;
+  __shared__ __align__(8) uint64_t bar;
   const bool lead = threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0;
+  init_tile_barrier(&bar, true);
+  unsigned phase = 0;
+  bool tma_ok = true;
   for (int w = blockIdx.x; w < gb.total; w += gridDim.x) {
     __syncthreads();  // the previous brick is finished with the slots, the tile and sb
     if (lead) {
@@ -746,11 +814,15 @@ mixed_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
       sb = boxes[lo];
       sp = group_ptrs(sb, stage);
       sbg = gb.bg[lo];
+      // the map is read from global memory (a TMA map cannot live in shared memory)
+      stm = boxes[lo].tma ? (stage == 1 || stage == 3 ? &boxes[lo].mapX : &boxes[lo].mapY) : nullptr;
+      if (stm) tma::acquire_map(stm);  // the host wrote the map into the table
     }
     __syncthreads();
     const int l = w - sb.first;
     const int cz = l % sb.nbz, cy = (l / sb.nbz) % sb.nby, cx = l / (sb.nbz * sb.nby);
-    mixed_body<O, MATTER>(sb.nx, sb.ny, sb.nz, sb.lapse, sb.normalize, sb.idx, sb.dt, sbg, sp, stage, cx, cy, cz);
+    mixed_body<O, MATTER>(sb.nx, sb.ny, sb.nz, sb.lapse, sb.normalize, sb.idx, sb.dt, sbg, sp, stage, cx, cy, cz, stm,
+                          &bar, phase, tma_ok);
   }
 }
 

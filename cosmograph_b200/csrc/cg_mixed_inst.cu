@@ -1,4 +1,8 @@
 // cg_mixed_inst.cu -- instantiation and launchers of the FP32-mixed kernels.
+#include <cudaTypedefs.h>
+
+#include <cstring>
+
 #include "cg_internal.h"
 #include "cg_mixed.cuh"
 
@@ -40,8 +44,9 @@ cudaError_t go(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
   static bool done = false;
   cudaError_t e = allow_smem(mixed_kernel<O, M>, smem, done);
   if (e != cudaSuccess) return e;
+  const CUtensorMap& map = (stage == 1 || stage == 3) ? b.mapX : b.mapY;  // the substep's input
   mixed_kernel<O, M><<<grid3(b.nx, b.ny, b.nz), dim3(kBZ, kBY, kBX), smem, st>>>(
-      b.nx, b.ny, b.nz, b.lapse, b.normalize, (float)(1.0 / b.dx), b.dt, bg, P, stage);
+      b.nx, b.ny, b.nz, b.lapse, b.normalize, (float)(1.0 / b.dx), b.dt, bg, P, stage, map, b.tma);
   return cudaGetLastError();
 }
 template <int O>
@@ -89,7 +94,58 @@ int ctas_m(int matter) {
     default: return ctas<O, kVacuum>();
   }
 }
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+template <int O>
+bool encode_maps(MixedBox& b) {
+  using G = TileG<O>;
+  auto enc = encode_fn();
+  if (!enc) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)b.nz, (cuuint64_t)b.ny, (cuuint64_t)b.nx, (cuuint64_t)b.nfields};
+  const cuuint64_t strides[3] = {(cuuint64_t)b.nz * sizeof(float), (cuuint64_t)b.ny * b.nz * sizeof(float),
+                                 (cuuint64_t)b.pts * sizeof(float)};
+  const cuuint32_t box[4] = {(cuuint32_t)G::TZ, (cuuint32_t)G::TY, (cuuint32_t)G::TX, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  for (int r = 0; r < 2; ++r) {
+    CUtensorMap* m = r == 0 ? &b.mapX : &b.mapY;
+    float* base = r == 0 ? b.X : b.Y;
+    if (enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  return true;
+}
 }  // namespace
+
+void make_tile_maps(MixedBox& b) {
+  std::memset(&b.mapX, 0, sizeof(b.mapX));
+  std::memset(&b.mapY, 0, sizeof(b.mapY));
+  b.maps = b.tma = 0;
+  // row strides must be multiples of 16 bytes; the bases are cudaMalloc'd
+  if (b.nz % 4 != 0 || !b.X || !b.Y) return;
+  bool ok = false;
+  switch (b.order) {
+    case 2: ok = encode_maps<2>(b); break;
+    case 4: ok = encode_maps<4>(b); break;
+    case 6: ok = encode_maps<6>(b); break;
+    case 8: ok = encode_maps<8>(b); break;
+    default: break;
+  }
+  b.maps = b.tma = ok ? 1 : 0;
+}
 
 cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
                          cudaStream_t st) {

@@ -29,19 +29,25 @@ struct Brick {
 using Brick64 = Brick<4, 2, 16>;
 using Brick32 = Brick<4, 4, 8>;
 
-// PITCH: row pitch in elements (0: the used row length)
-template <int O, class B, int PITCH = 0>
+// PITCH: row pitch in elements (0: the copied row length).  ZOFF: tile
+// column 0 holds z = z0 - ZOFF (default r); the copy fills columns
+// CO = ZOFF - r ... CO + BZ + 2r - 1.  A tile filled by a TMA box starts at
+// an aligned z, below the halo.
+template <int O, class B, int PITCH = 0, int ZOFF = -1>
 struct Geom {
   static constexpr int R = O / 2;
+  static constexpr int ZO = ZOFF < 0 ? R : ZOFF;          // tile column 0: z = z0 - ZO
+  static constexpr int CO = ZO - R;                        // first copied column
   static constexpr int TX = B::BX + 2 * R, TY = B::BY + 2 * R;
-  static constexpr int TZU = B::BZ + 2 * R;               // used z values per row
-  static constexpr int TZ = PITCH ? PITCH : TZU;          // row pitch
+  static constexpr int TZU = B::BZ + 2 * R;                // z values copied per row
+  static constexpr int TZ = PITCH ? PITCH : TZU;           // row pitch
+  static_assert(CO >= 0 && CO + TZU <= TZ, "a row holds the brick and its halo");
   static constexpr int ROWS = TX * TY;
   static constexpr int SIZE = ROWS * TZ;
   static constexpr int SY = TZ, SX = TY * TZ;
   static constexpr int RPP = 32 / TZU;                    // rows per warp instruction
   static constexpr int NPW = (ROWS + B::WARPS * RPP - 1) / (B::WARPS * RPP);  // instructions per warp
-  static_assert(TZU <= 32 && TZ >= TZU, "one warp copies at least one tile row");
+  static_assert(TZU <= 32, "one warp copies at least one tile row");
 };
 
 // v mod n in [0, n) for any v (tile coordinates reach past one period on
@@ -88,7 +94,7 @@ struct Loader {
 #pragma unroll
     for (int q = 0; q < G::NPW; ++q) {
       const int r = row0 + B::WARPS * G::RPP * q;
-      if (zoff >= 0 && r < G::ROWS) tl[r * G::TZ + col] = buf[q];
+      if (zoff >= 0 && r < G::ROWS) tl[r * G::TZ + G::CO + col] = buf[q];
     }
   }
 };
@@ -107,7 +113,7 @@ struct Taps {
 // tile index of the centre of thread (tx, ty, tz) = (threadIdx.z, .y, .x)
 template <class G>
 __device__ __forceinline__ int centre(int tx, int ty, int tz) {
-  return ((tx + G::R) * G::TY + (ty + G::R)) * G::TZ + (tz + G::R);
+  return ((tx + G::R) * G::TY + (ty + G::R)) * G::TZ + (tz + G::ZO);
 }
 
 }  // namespace tile

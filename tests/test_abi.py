@@ -27,6 +27,15 @@ def test_header_declares_what_the_binding_knows():
     assert declared_symbols() == sorted(_lib.EXPORTS)
 
 
+def test_header_constants_match_the_binding():
+    """Every CG_OPT_* / CG_STATUS_* value of the header is the binding's."""
+    text = HEADER.read_text()
+    consts = dict(re.findall(r"#define CG_((?:OPT|STATUS)_[A-Z_]+)\s+(\d+)u?", text))
+    assert consts, "no constants parsed"
+    for name, value in consts.items():
+        assert getattr(_lib, name) == int(value), name
+
+
 def test_library_exports_every_declared_symbol(L):
     for name in declared_symbols():
         assert hasattr(L, name), name
