@@ -38,6 +38,7 @@ UNITS = [
     ("noalloc.o", "cg_noalloc.cu", []),
     ("mixed.o", "cg_mixed_inst.cu", []),
     ("ics.o", "cg_ics.cu", []),
+    ("tma_host.o", "cg_tma_host.cu", []),
 ]
 
 

@@ -659,6 +659,11 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
       }
       for (double* p : {b.dev.P, b.dev.F, b.dev.X, b.dev.Y})
         if (e == cudaSuccess) e = cudaMemset(p, 0, reg);
+      if (e == cudaSuccess) {  // TMA tile copies where the layout allows
+        if (b.variant == cg::kFast) cg::fast::make_tile_maps(b.dev);
+        else cg::exact::make_tile_maps(b.dev);
+        b.dev.tma = b.dev.tma && ctx->opt_tma;
+      }
     } else {
       cg::MixedBox& m = b.mdev;
       m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.pts = b.dev.pts; m.nfields = b.dev.nfields;
@@ -876,6 +881,9 @@ int write_table(cg_ctx* ctx, Group& g) {
       e.kavg = b.dev.kavg;
       e.P = b.dev.P; e.F = b.dev.F; e.X = b.dev.X; e.Y = b.dev.Y; e.FP0 = b.dev.FP0; e.FP1 = b.dev.FP1;
       e.status = b.dev.status;
+      e.mapX = b.dev.mapX;
+      e.mapY = b.dev.mapY;
+      e.tma = b.dev.tma;
       e.nbx = bricks_along<Br>(e.nx, Br::BX); e.nby = bricks_along<Br>(e.ny, Br::BY); e.nbz = bricks_along<Br>(e.nz, Br::BZ);
       e.first = first;
       first += e.nbx * e.nby * e.nbz;
@@ -1189,8 +1197,10 @@ int cg_set_option(cg_ctx* ctx, int option, int value) {
       for (Box& b : ctx->boxes)
         if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "change CG_OPT_TMA between steps");
       ctx->opt_tma = value != 0;
-      for (Box& b : ctx->boxes)
+      for (Box& b : ctx->boxes) {
         if (b.mixed) b.mdev.tma = b.mdev.maps && ctx->opt_tma;
+        else b.dev.tma = b.dev.maps && ctx->opt_tma;
+      }
       ctx->grouped = false;  // the group tables carry the flag
       return CG_OK;
     case CG_OPT_GRAPH: ctx->opt_graph = value != 0; return CG_OK;

@@ -2,6 +2,8 @@
 // arithmetic advanced by one launch per substep (host and device types).
 #pragma once
 
+#include <cuda.h>
+
 #include "cg_types.h"
 
 namespace cg {
@@ -10,6 +12,8 @@ namespace cg {
 // brick counts along x, y, z and the index of its first brick in the launch's
 // work list.  Device table, written once when the group is formed.
 struct GroupBox {
+  CUtensorMap mapX, mapY;  // TMA maps of X and Y (valid when tma != 0)
+  int tma;
   int nx, ny, nz, pts;
   Physics ph;
   const double* kavg;

@@ -16,6 +16,9 @@ namespace cg {
 // nfields arrays of pts doubles (field f at offset f*pts), x-major with z
 // fastest like the reference's CosmoArray (utils/Array.h:47-61).
 struct BoxDev {
+  CUtensorMap mapX, mapY;  // TMA maps of X and Y (4-D {nz, ny, nx, field}); valid when maps != 0
+  int maps;                // the maps are encoded
+  int tma;                 // interior tiles are copied by TMA (maps != 0 and the option on)
   int nx, ny, nz, pts, nfields, order, matter;
   Physics ph;
   double* P;    // the reference's _p register (state at the start of a step)
@@ -62,7 +65,16 @@ int group_ctas_per_sm(int order, int matter);
 // FMA contraction.
 enum Variant : int { kExact = 0, kFast = 1 };
 
+namespace tma_host {
+// 4-D tensor map {nz, ny, nx, nfields} of elem-byte floats (4 or 8) at base,
+// box {bz, by, bx, 1}; false (map zeroed) when the layout or the driver does
+// not allow it
+bool encode(CUtensorMap* map, void* base, int elem, int nx, int ny, int nz, int nfields, int bz, int by, int bx);
+}  // namespace tma_host
+
 namespace exact {
+// encode b.mapX / b.mapY and set b.maps = b.tma = 1 when the box allows TMA tile copies
+void make_tile_maps(BoxDev& b);
 cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
 cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
 // constraint statistics pass 1 on the first-substep input X: per-point values
@@ -71,6 +83,7 @@ cudaError_t launch_constraints(const BoxDev& b, const StageBg& bg, double* cvals
 int constraint_blocks(const BoxDev& b);
 }  // namespace exact
 namespace fast {
+void make_tile_maps(BoxDev& b);
 cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
 cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
 }  // namespace fast

@@ -1,6 +1,4 @@
 // cg_mixed_inst.cu -- instantiation and launchers of the FP32-mixed kernels.
-#include <cudaTypedefs.h>
-
 #include <cstring>
 
 #include "cg_internal.h"
@@ -94,39 +92,11 @@ int ctas_m(int matter) {
     default: return ctas<O, kVacuum>();
   }
 }
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  }
-  return fn;
-}
-
 template <int O>
 bool encode_maps(MixedBox& b) {
   using G = TileG<O>;
-  auto enc = encode_fn();
-  if (!enc) return false;
-  const cuuint64_t dims[4] = {(cuuint64_t)b.nz, (cuuint64_t)b.ny, (cuuint64_t)b.nx, (cuuint64_t)b.nfields};
-  const cuuint64_t strides[3] = {(cuuint64_t)b.nz * sizeof(float), (cuuint64_t)b.ny * b.nz * sizeof(float),
-                                 (cuuint64_t)b.pts * sizeof(float)};
-  const cuuint32_t box[4] = {(cuuint32_t)G::TZ, (cuuint32_t)G::TY, (cuuint32_t)G::TX, 1};
-  const cuuint32_t estr[4] = {1, 1, 1, 1};
-  for (int r = 0; r < 2; ++r) {
-    CUtensorMap* m = r == 0 ? &b.mapX : &b.mapY;
-    float* base = r == 0 ? b.X : b.Y;
-    if (enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return false;
-  }
-  return true;
+  return tma_host::encode(&b.mapX, b.X, sizeof(float), b.nx, b.ny, b.nz, b.nfields, G::TZ, G::TY, G::TX) &&
+         tma_host::encode(&b.mapY, b.Y, sizeof(float), b.nx, b.ny, b.nz, b.nfields, G::TZ, G::TY, G::TX);
 }
 }  // namespace
 

@@ -36,6 +36,8 @@
 #include "cg_group.h"
 #include "cg_point.cuh"
 #include "cg_tile.cuh"
+#include "cg_tma.cuh"
+#include "cosmograph_b200.h"
 
 namespace cg {
 
@@ -61,6 +63,8 @@ struct BoxGeom {
 
 constexpr unsigned kStatusNaN = 1u;
 constexpr unsigned kStatusNonFinite = 2u;
+constexpr unsigned kStatusTileTimeout64 = CG_STATUS_TILE_TIMEOUT;  // a TMA tile copy did not complete
+constexpr long long kTmaWaitCycles64 = 2000000000LL;               // about a second
 
 template <int MATTER>
 struct NF {
@@ -70,8 +74,14 @@ struct NF {
 // CTA brick and field tiles (cg_tile.cuh)
 using Brick = tile::Brick64;
 constexpr int kBX = Brick::BX, kBY = Brick::BY, kBZ = Brick::BZ, kThreads = Brick::THREADS;
+// A tile starts at an even z (z0 - ZO, ZO = r rounded up to even) and its row
+// pitch is even, so that rows and TMA boxes start on 16-byte boundaries.
 template <int O>
-using TileG = tile::Geom<O, Brick>;
+struct TileShape {
+  static constexpr int R = O / 2, ZO = (R + 1) / 2 * 2, PITCH = (ZO - R + kBZ + 2 * R + 1) / 2 * 2;
+};
+template <int O>
+using TileG = tile::Geom<O, Brick, TileShape<O>::PITCH, TileShape<O>::ZO>;
 
 // Per-thread shared-memory slots (one column of kThreads doubles per slot).
 enum : int {
@@ -257,21 +267,61 @@ struct Phase1 {
 // Phase 1: every derivative the point needs, parked in shared memory.  One
 // field at a time is copied into the tile (the next one is fetched into
 // registers meanwhile); all threads of the CTA take part.
+//
+// The copies: by TMA when tmap is set (a brick whose halo lies inside the
+// box), else by the threads' own loads with periodic wrap.  Returns false (the
+// same value in every thread) when a TMA copy did not complete within
+// kTmaWaitCycles64; the status word then carries kStatusTileTimeout64.
 template <int O, int MATTER, int MODE>
-__device__ __forceinline__ void derivatives(const double* __restrict__ a, int N, const Physics& ph, const double gi[6],
-                                            double* sl, double* tl, const int* rowoff, int tid, int z0, int nz,
-                                            int cc) {
+__device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG<O>, double>& t, const Physics& ph,
+                                                  const double gi[6], double* sl);
+
+template <int O, int MATTER, int MODE>
+__device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N, const Physics& ph, const double gi[6],
+                                            double* sl, double* tl, const int* rowoff, int tid, int x0, int y0,
+                                            int z0, int nz, int cc, const CUtensorMap* tmap, uint64_t* bar,
+                                            unsigned& phase, unsigned* status) {
   using PF = Phase1<MATTER, MODE>;
-  tile::Loader<TileG<O>, Brick, double> ld;
+  using G = TileG<O>;
+  const tile::Taps<G, double> t{tl, cc};
+  if (tmap) {
+    bool ok = true;
+#pragma unroll 1
+    for (int it = 0; it < PF::N; ++it) {
+      tma::fence_proxy_async();  // this thread's shared-memory accesses come before the copy's writes
+      __syncthreads();           // the previous tile has been read
+      if (tid == 0) {
+        tma::arrive_expect_tx(bar, (unsigned)(G::SIZE * sizeof(double)));
+        tma::load_4d(tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it), bar);
+      }
+      if (ok && !tma::wait(bar, phase, kTmaWaitCycles64)) ok = false;
+      phase ^= 1u;
+      field_derivatives<O, MATTER, MODE>(it, t, ph, gi, sl);
+    }
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == 0) atomicOr(status, kStatusTileTimeout64);
+    return ok;
+  }
+  tile::Loader<G, Brick, double> ld;
   ld.init(tid, z0, nz);
   ld.fetch(a + (size_t)PF::field(0) * N, rowoff);
-  const tile::Taps<TileG<O>, double> t{tl, cc};
 #pragma unroll 1
   for (int it = 0; it < PF::N; ++it) {
     __syncthreads();  // the previous tile has been read
     ld.store(tl);
     __syncthreads();
     if (it + 1 < PF::N) ld.fetch(a + (size_t)PF::field(it + 1) * N, rowoff);
+    field_derivatives<O, MATTER, MODE>(it, t, ph, gi, sl);
+  }
+  return true;
+}
+
+// the derivatives of phase-1 field `it` from its tile, into the slots
+template <int O, int MATTER, int MODE>
+__device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG<O>, double>& t, const Physics& ph,
+                                                  const double gi[6], double* sl) {
+  using PF = Phase1<MATTER, MODE>;
+  {
     if (it < PF::NA) {
       // d_d A_q for the momentum constraint (BSSN_MI, bssn_macros.h:498-500)
       const int q = it;
@@ -417,7 +467,8 @@ __device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part, int cta
 // common case carries none of their code).
 template <int O, int MATTER, int MODE, bool KO = false>
 __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph, StageBg bg, const StagePtrs& P,
-                                           int stage, int cx, int cy, int cz, int cta) {
+                                           int stage, int cx, int cy, int cz, int cta, const CUtensorMap* tmap,
+                                           uint64_t* bar, unsigned& phase, bool& tma_ok) {
   constexpr int NFLD = NF<MATTER>::value;
   constexpr int NSLOT = MODE == kConstraints ? SlotsC<MATTER>::value : Slots<MATTER>::value;
   static_assert(NSLOT >= S_MAT, "the tile region lies inside the slot array");
@@ -425,7 +476,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
                     (size_t)kTileSlots * kThreads * sizeof(double),
                 "tile and row offsets fit the phase-2-only slots");
   constexpr int R = O / 2;
-  extern __shared__ double smem[];
+  extern __shared__ __align__(128) double smem[];  // 128-byte aligned: TMA destinations
   const int tid = threadIdx.x + kBZ * (threadIdx.y + kBY * threadIdx.z);
   double* sl = smem + tid;  // this thread's slot column
   auto S = [&](int s) -> double& { return sl[s * kThreads]; };
@@ -464,12 +515,21 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   // ---- phase 1: derivatives into shared memory ---------------------------------
   const int x0 = cx * kBX, y0 = cy * kBY, z0 = cz * kBZ;
   {
+    using G = TileG<O>;
     double* tl = smem + kTileSlot * kThreads;
-    int* rowoff = reinterpret_cast<int*>(tl + TileG<O>::SIZE);
-    tile::row_offsets<TileG<O>, Brick>(x0, y0, geo.nx, geo.ny, geo.nz, tid, rowoff);
-    __syncthreads();  // every warp reads every row offset
-    derivatives<O, MATTER, MODE>(a, N, ph, gi, sl, tl, rowoff, tid, z0, geo.nz,
-                                 tile::centre<TileG<O>>(threadIdx.z, threadIdx.y, threadIdx.x));
+    int* rowoff = reinterpret_cast<int*>(tl + G::SIZE);
+    // TMA when the brick's halo lies inside the box (no wrap)
+    const bool by_tma = tmap && tma_ok && x0 >= G::R && x0 + kBX + G::R <= geo.nx && y0 >= G::R &&
+                        y0 + kBY + G::R <= geo.ny && z0 >= G::ZO && z0 + kBZ + G::R <= geo.nz;
+    if (!by_tma) {
+      tile::row_offsets<G, Brick>(x0, y0, geo.nx, geo.ny, geo.nz, tid, rowoff);
+      __syncthreads();  // every warp reads every row offset
+    }
+    // after a copy timed out the CTA copies by threads (the barrier's phase is unknown)
+    tma_ok = derivatives<O, MATTER, MODE>(a, N, ph, gi, sl, tl, rowoff, tid, x0, y0, z0, geo.nz,
+                                          tile::centre<G>(threadIdx.z, threadIdx.y, threadIdx.x),
+                                          by_tma ? tmap : nullptr, bar, phase, P.status) &&
+             tma_ok;
     __syncthreads();  // the tile region becomes slots again
   }
   if (MODE == kEvolve && !live) return;  // no CTA-wide synchronisation after this point
@@ -982,12 +1042,28 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   }
 }
 
-// One box: one CTA per brick.
+// the TMA barrier of a CTA: initialised once, before any copy
+__device__ __forceinline__ void init_tile_barrier(uint64_t* bar, bool use) {
+  if (use && threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+    tma::bar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+// One box: one CTA per brick.  tmap: the TMA map of this substep's input
+// (use_tma = 0: every tile is copied by the threads).
 template <int O, int MATTER, int MODE, bool KO = false>
 __global__ void __launch_bounds__(kThreads, 2)
-stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage) {
+stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage, const __grid_constant__ CUtensorMap tmap,
+             int use_tma) {
+  __shared__ __align__(8) uint64_t bar;
+  init_tile_barrier(&bar, use_tma != 0);
+  unsigned phase = 0;
+  bool tma_ok = true;
   stage_body<O, MATTER, MODE, KO>(geo, ph, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x,
-                                  blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z));
+                                  blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
+                                  use_tma ? &tmap : nullptr, &bar, phase, tma_ok);
 }
 
 // A group of boxes of the same order and matter model, one launch per
@@ -1001,7 +1077,12 @@ stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
   __shared__ GroupBox sb;
   __shared__ StagePtrs sp;
   __shared__ StageBg sbg;
+  __shared__ const CUtensorMap* stm;
+  __shared__ __align__(8) uint64_t bar;
   const bool lead = threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0;
+  init_tile_barrier(&bar, true);
+  unsigned phase = 0;
+  bool tma_ok = true;
   for (int w = blockIdx.x; w < gb.total; w += gridDim.x) {
     __syncthreads();  // the previous brick is finished with the slots, the tile and sb
     if (lead) {
@@ -1013,12 +1094,15 @@ stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
       sb = boxes[lo];
       sp = group_ptrs(sb, stage);
       sbg = gb.bg[lo];
+      // the map is read from global memory (a TMA map cannot live in shared memory)
+      stm = boxes[lo].tma ? (stage == 1 || stage == 3 ? &boxes[lo].mapX : &boxes[lo].mapY) : nullptr;
+      if (stm) tma::acquire_map(stm);  // the host wrote the map into the table
     }
     __syncthreads();
     const int l = w - sb.first;
     const int cz = l % sb.nbz, cy = (l / sb.nbz) % sb.nby, cx = l / (sb.nbz * sb.nby);
     const BoxGeom geo{sb.nx, sb.ny, sb.nz, sb.pts};
-    stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0);
+    stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0, stm, &bar, phase, tma_ok);
   }
 }
 

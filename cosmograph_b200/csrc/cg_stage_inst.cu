@@ -80,6 +80,7 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
     default: P.in = b.Y; P.prev = b.X; P.out = b.P; P.norm = b.X; P.fp_in = b.FP1; P.fp_out = b.FP0; break;
   }
   BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
+  const CUtensorMap& map = (stage == 1 || stage == 3) ? b.mapX : b.mapY;  // the substep's input
   constexpr size_t smem = sizeof(double) * Slots<M>::value * kThreads;
   if constexpr (O == 2 || O == 8) {
     if (b.ph.ko_coeff != 0.0) {  // Kreiss-Oliger dissipation: its own instantiation
@@ -90,7 +91,8 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
         if (e != cudaSuccess) return e;
         configured_ko = true;
       }
-      stage_kernel<O, M, kEvolve, true><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage);
+      stage_kernel<O, M, kEvolve, true><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage, map,
+                                                                                    b.tma);
       return cudaGetLastError();
     }
   }
@@ -100,7 +102,7 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  stage_kernel<O, M, kEvolve><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage);
+  stage_kernel<O, M, kEvolve><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage, map, b.tma);
   return cudaGetLastError();
 }
 
@@ -123,7 +125,7 @@ cudaError_t go_constraints(const BoxDev& b, const StageBg& bg, double* cvals, do
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  stage_kernel<O, M, kConstraints><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, 1);
+  stage_kernel<O, M, kConstraints><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, 1, b.mapX, b.tma);
   return cudaGetLastError();
 }
 
@@ -187,7 +189,25 @@ cudaError_t go_stage_m(const BoxDev& b, const StageBg& bg, int stage, cudaStream
     default: return go_stage<O, kVacuum>(b, bg, stage, st);
   }
 }
+template <int O>
+bool encode_maps(BoxDev& b) {
+  using G = TileG<O>;
+  return tma_host::encode(&b.mapX, b.X, sizeof(double), b.nx, b.ny, b.nz, b.nfields, G::TZ, G::TY, G::TX) &&
+         tma_host::encode(&b.mapY, b.Y, sizeof(double), b.nx, b.ny, b.nz, b.nfields, G::TZ, G::TY, G::TX);
+}
 }  // namespace
+
+void make_tile_maps(BoxDev& b) {
+  bool ok = false;
+  switch (b.order) {
+    case 2: ok = encode_maps<2>(b); break;
+    case 4: ok = encode_maps<4>(b); break;
+    case 6: ok = encode_maps<6>(b); break;
+    case 8: ok = encode_maps<8>(b); break;
+    default: break;
+  }
+  b.maps = b.tma = ok ? 1 : 0;
+}
 
 cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
   switch (b.order) {

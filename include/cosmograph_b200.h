@@ -74,8 +74,8 @@ extern "C" {
 #define CG_STATUS_NAN 1u        /* NaN in DIFFphi after a step          */
 #define CG_STATUS_NONFINITE 2u  /* NaN or Inf in any evolved field      */
 #define CG_STATUS_TILE_TIMEOUT 4u /* a TMA tile copy did not complete in
-                                     about a second (mixed kernel); the
-                                     substep's output is not valid       */
+                                     about a second; the substep's output
+                                     is not valid                        */
 
 typedef struct cg_ctx cg_ctx;
 
@@ -199,11 +199,12 @@ int cg_ic_grf_dust(cg_ctx *ctx, int box, const double *delta, uint64_t seed, dou
  *   CG_OPT_GROUP_GRID the launch shape of groups the autotuner has not set:
  *                    0 (default) one CTA per brick, n > 0 a persistent grid of
  *                    n CTAs, -1 one launch per box.
- *   CG_OPT_TMA       1 (default): the FP32-mixed kernel copies the halo tiles
- *                    of bricks away from the periodic wrap with the tensor
- *                    memory accelerator (boxes with nz a multiple of 4);
- *                    0: every tile is copied by the CTA's threads.  Results
- *                    are identical.  Change it between steps only. */
+ *   CG_OPT_TMA       1 (default): the substep kernels copy the halo tiles of
+ *                    bricks away from the periodic wrap with the tensor memory
+ *                    accelerator (FP64 boxes with even nz, mixed boxes with nz
+ *                    a multiple of 4); 0: every tile is copied by the CTA's
+ *                    threads.  Results are identical.  Change it between
+ *                    steps only. */
 #define CG_OPT_BATCH 1
 #define CG_OPT_GRAPH 2
 #define CG_OPT_AUTOTUNE 3

@@ -130,33 +130,3 @@ def test_grf_dust_128_order8_500_steps():
     assert delta_err < 1e-4 * 1e-4  # below 1e-4 of the density-contrast amplitude
     assert hmx <= 2.0 * h64 and mmx <= 2.0 * m64
 
-
-@pytest.mark.parametrize("matter", [S.DUST, S.SCALAR, S.VACUUM])
-@pytest.mark.parametrize("order", [2, 4, 6, 8])
-def test_tma_tile_copies_match_thread_copies(matter, order):
-    """Interior halo tiles copied by the tensor memory accelerator hold the
-    same values as tiles copied by the threads: identical fields after a few
-    steps, on a non-cubic box, one box and a launch group (the group kernel
-    reads the maps from its table; the 18-point box has no maps)."""
-    shapes = [(24, 20, 32), (20, 28, 16), (12, 16, 18)]
-    states = [ics.perturbed(sh, matter, seed=5 + q, amp=1e-3) for q, sh in enumerate(shapes)]
-    cfg = BoxConfig(order=order, precision="mixed")
-    res = {}
-    for tma in (1, 0):
-        with Evolution(states[0], cfg) as ev:
-            ev.set_option("tma", tma)
-            ev.step(3)
-            ev.synchronize()
-            one = ev.download(0).fields
-        with Evolution(states, [cfg] * len(states)) as ev:
-            ev.set_option("tma", tma)
-            ev.set_option("autotune", 0)
-            ev.step(3)
-            ev.synchronize()
-            assert ev.groups()[0]["boxes"] == len(states)
-            group = [ev.download(q).fields for q in range(len(states))]
-        res[tma] = (one, group)
-    assert np.array_equal(res[1][0], res[0][0])
-    for q in range(len(states)):
-        assert np.array_equal(res[1][1][q], res[0][1][q]), q
-    assert np.array_equal(res[1][0], res[1][1][0])
