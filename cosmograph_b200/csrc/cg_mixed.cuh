@@ -267,6 +267,8 @@ __device__ __forceinline__ bool derivatives(const float* __restrict__ a, int N, 
       if (tid == 0) {
         tma::arrive_expect_tx(bar, (unsigned)(G::SIZE * sizeof(float)));
         tma::load_4d(tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, phase1_field(it), bar);
+        // the next field's tile into L2 while this one is used
+        if (it + 1 < NIT) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, phase1_field(it + 1));
       }
       if (ok && !tma::wait(bar, phase, kTmaWaitCycles)) ok = false;
       phase ^= 1u;

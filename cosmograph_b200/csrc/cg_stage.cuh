@@ -152,14 +152,6 @@ struct Taps {
   }
 };
 
-// taps of one field read from global memory through index taps T
-template <class T>
-struct GTaps {
-  const double* f;
-  T t;
-  __device__ __forceinline__ double ax(int a, int n) const { return __ldg(f + t.ax(a, n)); }
-};
-
 // first derivative (utils/math.h:74-100, 231-263, 412-450, 554-586)
 template <int O, class T>
 __device__ __forceinline__ double d1(const T& t, int a, const Physics& ph) {
@@ -241,32 +233,28 @@ __device__ __forceinline__ double d1p(const double* __restrict__ fa, const doubl
 
 // Fields copied into tiles in phase 1, in order: (constraint mode) A_q with
 // first derivatives; the metric components, phi and alpha with first and
-// second derivatives; (constraint mode) K and Gamma^i with first derivatives;
-// (constraint mode, scalar) phi, Pi, psi_i with first derivatives.  In evolve
-// mode K, Gamma^i and the scalar fields take their first-derivative taps
-// straight from global memory (cheaper than a tile copy for first
-// derivatives only).
+// second derivatives; K and Gamma^i with first derivatives; (scalar) phi, Pi,
+// psi_i with first derivatives.
 template <int MATTER, int MODE>
 struct Phase1 {
   static constexpr int NA = MODE == kConstraints ? 6 : 0;
-  static constexpr int NS = (MATTER == kScalar && MODE != kEvolve) ? 5 : 0;
-  static constexpr int N = NA + 8 + (MODE == kEvolve ? 0 : 4) + NS;
+  static constexpr int NS = MATTER == kScalar ? 5 : 0;
+  static constexpr int N = NA + 8 + 4 + NS;
   __device__ __forceinline__ static int field(int it) {
     if (it < NA) return F_A11 + it;
     it -= NA;
     if (it < 8) return it < 6 ? F_G11 + it : (it == 6 ? F_PHI : F_ALPHA);
     it -= 8;
-    if (MODE != kEvolve) {
-      if (it < 4) return it == 0 ? F_K : F_GAM1 + it - 1;
-      it -= 4;
-    }
+    if (it < 4) return it == 0 ? F_K : F_GAM1 + it - 1;
+    it -= 4;
     return F_SPHI + it;
   }
 };
 
 // Phase 1: every derivative the point needs, parked in shared memory.  One
 // field at a time is copied into the tile (the next one is fetched into
-// registers meanwhile); all threads of the CTA take part.
+// registers, or into L2 on the TMA path, meanwhile); all threads of the CTA
+// take part.
 //
 // The copies: by TMA when tmap is set (a brick whose halo lies inside the
 // box), else by the threads' own loads with periodic wrap.  Returns false (the
@@ -293,6 +281,8 @@ __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N,
       if (tid == 0) {
         tma::arrive_expect_tx(bar, (unsigned)(G::SIZE * sizeof(double)));
         tma::load_4d(tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it), bar);
+        // the next field's tile into L2 while this one is used
+        if (it + 1 < PF::N) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it + 1));
       }
       if (ok && !tma::wait(bar, phase, kTmaWaitCycles64)) ok = false;
       phase ^= 1u;
@@ -363,7 +353,7 @@ __device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG
         sl[(b2 + 4) * kThreads] = h23;
         sl[(b2 + 5) * kThreads] = h33;
       }
-    } else if (MODE != kEvolve && it < PF::NA + 12) {
+    } else if (it < PF::NA + 12) {
       // K and Gamma^K: first derivatives (calculate_dK, bssn.cc:529-535; the
       // d_J Gamma^K of BSSN_CALCULATE_RICCI_UNITARY_TERM2, bssn_macros.h:251-252)
       const int q = it - PF::NA - 8;
@@ -373,7 +363,7 @@ __device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG
       sl[(b + 2) * kThreads] = d1<O>(t, 2, ph);
     } else {
       // Scalar::getScalarData derivatives (scalar.cc:109-127): d_d of phi, Pi, psi1..3
-      const int m = it - PF::NA - (MODE == kEvolve ? 8 : 12);
+      const int m = it - PF::NA - 12;
       sl[(S_MAT + 3 * m + 0) * kThreads] = d1<O>(t, 0, ph);
       sl[(S_MAT + 3 * m + 1) * kThreads] = d1<O>(t, 1, ph);
       sl[(S_MAT + 3 * m + 2) * kThreads] = d1<O>(t, 2, ph);
@@ -536,26 +526,13 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   {
     const bool interior = x0 >= R && x0 + kBX + R <= geo.nx && y0 >= R && y0 + kBY + R <= geo.ny && z0 >= R &&
                           z0 + kBZ + R <= geo.nz;
-    // K and Gamma^K first derivatives (calculate_dK, bssn.cc:529-535; the
-    // d_J Gamma^K of BSSN_CALCULATE_RICCI_UNITARY_TERM2, bssn_macros.h:251-252)
-    // and the dust flux divergences, taps from global memory
-    auto gpass = [&](auto t) {
-      if (MODE == kEvolve) {
-        constexpr int NG = MATTER == kScalar ? 9 : 4;  // K, Gamma^i (and phi_s, Pi, psi_i)
-#pragma unroll 1
-        for (int q = 0; q < NG; ++q) {
-          const int fld = q == 0 ? F_K : (q < 4 ? F_GAM1 + q - 1 : F_SPHI + q - 4);
-          const int b = q == 0 ? S_DK : (q < 4 ? S_DGAM + 3 * (q - 1) : S_MAT + 3 * (q - 4));
-          const GTaps<decltype(t)> gt{a + (size_t)fld * N, t};
-          S(b + 0) = d1<O>(gt, 0, ph);
-          S(b + 1) = d1<O>(gt, 1, ph);
-          S(b + 2) = d1<O>(gt, 2, ph);
-        }
-      }
-      if (MATTER == kDust) flux_divergences<O>(t, P.fp_in, N, ph, sl);
-    };
-    if (interior) gpass(Taps<false>{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c});
-    else gpass(Taps<true>{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c});
+    // the dust flux divergences, taps from global memory
+    if (MATTER == kDust) {
+      if (interior) flux_divergences<O>(Taps<false>{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c},
+                                        P.fp_in, N, ph, sl);
+      else flux_divergences<O>(Taps<true>{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c}, P.fp_in, N,
+                               ph, sl);
+    }
   }
 
   // ---- phase 2: the algebra of set_bd_values (bssn.cc:361-421) ----------------

@@ -51,6 +51,14 @@ __device__ __forceinline__ void load_4d(void* dst, const CUtensorMap* map, int c
       : "memory");
 }
 
+// prefetch a 4-D tile of `map` at {c0, c1, c2, c3} into L2 (no completion to wait for)
+__device__ __forceinline__ void prefetch_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3) {
+  asm volatile("cp.async.bulk.prefetch.tensor.4d.L2.global.tile [%0, {%1, %2, %3, %4}];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+               : "memory");
+}
+
 // Wait until the barrier completes the phase with parity `phase`; gives up
 // after `limit` clock cycles and returns false.
 __device__ __forceinline__ bool wait(uint64_t* bar, unsigned phase, long long limit) {
