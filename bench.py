@@ -12,7 +12,9 @@ and Hamiltonian-constraint error against the FP64 run after the same steps.
 
 Printed JSON (rank 0, one line): value = whole-job updates/s with the state
 resident in HBM; e2e = the same through the C ABI with the full state copied
-host->device and device->host around every step; roofline = the substep
+host->device and device->host around every step (pinned buffers; each step's
+result goes out while the next step's input comes in, cg_exchange_state_async);
+roofline = the substep
 kernel's algorithmic HBM bytes against the measured copy bandwidth;
 cpu_baseline = the reference's own sources (oracle/_ref) on the host cores.
 
@@ -62,7 +64,7 @@ def parse():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--order", type=int, default=8)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma", "mixed"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference CPU build (rank 0)")
     ap.add_argument("--ncu", action="store_true", help="short run for profiler capture (no JSON extras)")
     ap.add_argument("--variants", default="fp64_fma,mixed", help="comma list of extra precisions timed alongside")
@@ -293,12 +295,17 @@ def run_ensemble(a, world, rank, local):
     torch.cuda.synchronize()
     q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     q0.record(stream)
-    for _ in range(a.e2e_steps):
-        for b, h in enumerate(h_in):
-            ev._check(L.cg_upload_state_async(ev.ctx, b, ctypes.cast(h.data_ptr(), dp), h.numel()))
+    for b, h in enumerate(h_in):
+        ev._check(L.cg_upload_state_async(ev.ctx, b, ctypes.cast(h.data_ptr(), dp), h.numel()))
+    ev.step(1)
+    for _ in range(a.e2e_steps - 1):
+        # the step's result out and the next step's input in, overlapped
+        for b, (hi, ho) in enumerate(zip(h_in, h_out)):
+            ev._check(L.cg_exchange_state_async(ev.ctx, b, ctypes.cast(ho.data_ptr(), dp),
+                                                ctypes.cast(hi.data_ptr(), dp), hi.numel()))
         ev.step(1)
-        for b, h in enumerate(h_out):
-            ev._check(L.cg_download_state_async(ev.ctx, b, ctypes.cast(h.data_ptr(), dp), h.numel()))
+    for b, h in enumerate(h_out):
+        ev._check(L.cg_download_state_async(ev.ctx, b, ctypes.cast(h.data_ptr(), dp), h.numel()))
     q1.record(stream)
     torch.cuda.synchronize()
     ev.synchronize()
@@ -530,10 +537,13 @@ def main():
     t0 = time.perf_counter()
     q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     q0.record(stream)
-    for _ in range(a.e2e_steps):
-        ev._check(L.cg_upload_state_async(ev.ctx, 0, pin, cnt))
+    ev._check(L.cg_upload_state_async(ev.ctx, 0, pin, cnt))
+    ev.step(1)
+    for _ in range(a.e2e_steps - 1):
+        # the step's result out and the next step's input in, overlapped
+        ev._check(L.cg_exchange_state_async(ev.ctx, 0, pout, pin, cnt))
         ev.step(1)
-        ev._check(L.cg_download_state_async(ev.ctx, 0, pout, cnt))
+    ev._check(L.cg_download_state_async(ev.ctx, 0, pout, cnt))
     q1.record(stream)
     torch.cuda.synchronize()
     ev.synchronize()

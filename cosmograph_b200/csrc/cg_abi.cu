@@ -118,6 +118,10 @@ struct cg_ctx {
   int gexec_steps = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
+  // cg_exchange_state_async: the device-to-host stream and one event per field
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t copy_start = nullptr;
+  std::vector<cudaEvent_t> copy_done;
   unsigned* status = nullptr;
   double* red = nullptr;   // reduction scratch for cg_conformal_average
   int red_blocks = 0;
@@ -716,6 +720,12 @@ int cg_destroy(cg_ctx* ctx) {
   for (Box& b : ctx->boxes) free_box(b);
   cudaFree(ctx->red);
   cudaFree(ctx->status);
+  if (ctx->copy_stream) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
+  }
+  if (ctx->copy_start) cudaEventDestroy(ctx->copy_start);
+  for (cudaEvent_t ev : ctx->copy_done) cudaEventDestroy(ev);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return CG_OK;
@@ -763,6 +773,41 @@ int cg_upload_state_async(cg_ctx* ctx, int box, const double* host, size_t count
 }
 int cg_download_state_async(cg_ctx* ctx, int box, double* host, size_t count) {
   return state_copy(ctx, box, host, count, false, true);
+}
+
+// The download runs on a second stream, field by field, after the work queued
+// so far on the context's stream; the context's stream uploads field f once
+// field f has been downloaded.  Opposite copy directions overlap, so the pair
+// takes about as long as the longer of the two.
+int cg_exchange_state_async(cg_ctx* ctx, int box, double* host_out, const double* host_in, size_t count) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  Box& b = ctx->boxes[box];
+  const size_t n = (size_t)b.dev.nfields * b.dev.pts;
+  if (!host_out || !host_in || count != n)
+    return fail(ctx, CG_ERR_INVALID, "count must be nfields*nx*ny*nz = " + std::to_string(n));
+  if (!ctx->copy_stream) CG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  if (!ctx->copy_start) CG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->copy_start, cudaEventDisableTiming));
+  while ((int)ctx->copy_done.size() < b.dev.nfields) {
+    cudaEvent_t ev = nullptr;
+    CG_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    ctx->copy_done.push_back(ev);
+  }
+  const size_t pts = (size_t)b.dev.pts, fbytes = pts * sizeof(double);
+  CG_CUDA(ctx, cudaEventRecord(ctx->copy_start, ctx->stream));
+  CG_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_start, 0));
+  for (int f = 0; f < b.dev.nfields; ++f) {
+    CG_CUDA(ctx, cudaMemcpyAsync(host_out + f * pts, b.dev.P + f * pts, fbytes, cudaMemcpyDeviceToHost,
+                                 ctx->copy_stream));
+    CG_CUDA(ctx, cudaEventRecord(ctx->copy_done[f], ctx->copy_stream));
+  }
+  for (int f = 0; f < b.dev.nfields; ++f) {
+    CG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->copy_done[f], 0));
+    CG_CUDA(ctx, cudaMemcpyAsync(b.dev.P + f * pts, host_in + f * pts, fbytes, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  b.stage_next = 0;
+  b.steps = 0;
+  return CG_OK;
 }
 
 static int field_copy(cg_ctx* ctx, int box, int field, char reg, double* host, size_t n, bool upload) {

@@ -138,6 +138,17 @@ int cg_download_state(cg_ctx *ctx, int box, double *host, size_t count);
 int cg_upload_state_async(cg_ctx *ctx, int box, const double *host, size_t count);
 int cg_download_state_async(cg_ctx *ctx, int box, double *host, size_t count);
 
+/* Download the box's "_p" registers into host_out and upload host_in as the
+ * new "_p", asynchronously: the download follows the work queued so far on
+ * the context's stream and runs field by field on a second stream, and each
+ * field is uploaded (on the context's stream) as soon as it has been
+ * downloaded, so the two directions overlap.  Both buffers pinned, count as
+ * for cg_upload_state; work queued afterwards on the context's stream sees
+ * the new state, and host_out is complete once that stream reaches it (e.g.
+ * cg_synchronize).  No reference counterpart: streaming boxes through one
+ * GPU (the reference evolves one box per process). */
+int cg_exchange_state_async(cg_ctx *ctx, int box, double *host_out, const double *host_in, size_t count);
+
 /* One register of one field: reg = 'p', 'a' (current substep input), 'f'.
  * Replaces BSSN::fields["<name>_<reg>"] access (bssn.cc:30-39). Synchronous.
  * On a CG_PREC_MIXED box 'a' is held as an FP32 perturbation about a uniform
