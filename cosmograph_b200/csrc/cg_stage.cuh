@@ -113,6 +113,22 @@ struct SlotsC {
   static constexpr int dA = Slots<MATTER>::value;
   static constexpr int value = dA + 18;
 };
+// A second tile buffer after the slot array lets the TMA copy of the next
+// field overlap the derivatives of the current one.  Evolve mode, dust and
+// vacuum: two CTAs per SM still fit in shared memory.
+template <int O, int MATTER, int MODE>
+struct TileBuffers {
+  static constexpr bool kTwo = MODE == kEvolve && MATTER != kScalar;
+  static constexpr size_t kBytes = (TileG<O>::SIZE * sizeof(double) + 127) / 128 * 128;
+};
+// dynamic shared memory of a substep launch
+template <int O, int MATTER, int MODE>
+constexpr size_t stage_smem() {
+  return sizeof(double) * kThreads * (MODE == kConstraints ? SlotsC<MATTER>::value : Slots<MATTER>::value) +
+         (TileBuffers<O, MATTER, MODE>::kTwo ? TileBuffers<O, MATTER, MODE>::kBytes : 0);
+}
+// two CTAs per SM (228 KB, 1 KB reserved per CTA, up to 1 KB of static shared memory)
+static_assert(2 * (stage_smem<8, kDust, kEvolve>() + 2048) <= 228 * 1024, "two dust CTAs fit on an SM");
 // per-block partial results of the constraint pass (see constraint_reduce)
 constexpr int kCPart = 27;
 
@@ -264,29 +280,45 @@ template <int O, int MATTER, int MODE>
 __device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG<O>, double>& t, const Physics& ph,
                                                   const double gi[6], double* sl);
 
+//
+// bar[0] (and bar[1] with two buffers) are the buffers' mbarriers; bit b of
+// phase is the parity bar[b] completes next.
 template <int O, int MATTER, int MODE>
 __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N, const Physics& ph, const double gi[6],
-                                            double* sl, double* tl, const int* rowoff, int tid, int x0, int y0,
-                                            int z0, int nz, int cc, const CUtensorMap* tmap, uint64_t* bar,
+                                            double* sl, double* tl, double* tl2, const int* rowoff, int tid, int x0,
+                                            int y0, int z0, int nz, int cc, const CUtensorMap* tmap, uint64_t* bar,
                                             unsigned& phase, unsigned* status) {
   using PF = Phase1<MATTER, MODE>;
   using G = TileG<O>;
+  constexpr bool TWO = TileBuffers<O, MATTER, MODE>::kTwo;
   const tile::Taps<G, double> t{tl, cc};
   if (tmap) {
     bool ok = true;
+    constexpr unsigned kBytes = (unsigned)(G::SIZE * sizeof(double));
+    // field it into buffer it % 2 (one buffer: 0), field it + 1 into L2
+    auto issue = [&](int it) {
+      const int b = TWO ? (it & 1) : 0;
+      tma::arrive_expect_tx(bar + b, kBytes);
+      tma::load_4d(b ? tl2 : tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it), bar + b);
+      if (it + 1 < PF::N) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it + 1));
+    };
+    if (TWO) {
+      tma::fence_proxy_async();  // this thread's shared-memory accesses come before the copy's writes
+      __syncthreads();
+      if (tid == 0) issue(0);
+    }
 #pragma unroll 1
     for (int it = 0; it < PF::N; ++it) {
-      tma::fence_proxy_async();  // this thread's shared-memory accesses come before the copy's writes
-      __syncthreads();           // the previous tile has been read
+      tma::fence_proxy_async();
+      __syncthreads();  // the buffer the next copy writes has been read
       if (tid == 0) {
-        tma::arrive_expect_tx(bar, (unsigned)(G::SIZE * sizeof(double)));
-        tma::load_4d(tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it), bar);
-        // the next field's tile into L2 while this one is used
-        if (it + 1 < PF::N) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it + 1));
+        if (!TWO) issue(it);
+        else if (it + 1 < PF::N) issue(it + 1);
       }
-      if (ok && !tma::wait(bar, phase, kTmaWaitCycles64)) ok = false;
-      phase ^= 1u;
-      field_derivatives<O, MATTER, MODE>(it, t, ph, gi, sl);
+      const int b = TWO ? (it & 1) : 0;
+      if (ok && !tma::wait(bar + b, (phase >> b) & 1u, kTmaWaitCycles64)) ok = false;
+      phase ^= 1u << b;
+      field_derivatives<O, MATTER, MODE>(it, tile::Taps<G, double>{b ? tl2 : tl, cc}, ph, gi, sl);
     }
     ok = __syncthreads_and(ok);
     if (!ok && tid == 0) atomicOr(status, kStatusTileTimeout64);
@@ -516,7 +548,8 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       __syncthreads();  // every warp reads every row offset
     }
     // after a copy timed out the CTA copies by threads (the barrier's phase is unknown)
-    tma_ok = derivatives<O, MATTER, MODE>(a, N, ph, gi, sl, tl, rowoff, tid, x0, y0, z0, geo.nz,
+    double* tl2 = TileBuffers<O, MATTER, MODE>::kTwo ? smem + NSLOT * kThreads : nullptr;
+    tma_ok = derivatives<O, MATTER, MODE>(a, N, ph, gi, sl, tl, tl2, rowoff, tid, x0, y0, z0, geo.nz,
                                           tile::centre<G>(threadIdx.z, threadIdx.y, threadIdx.x),
                                           by_tma ? tmap : nullptr, bar, phase, P.status) &&
              tma_ok;
@@ -1019,10 +1052,11 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   }
 }
 
-// the TMA barrier of a CTA: initialised once, before any copy
-__device__ __forceinline__ void init_tile_barrier(uint64_t* bar, bool use) {
+// the two TMA barriers of a CTA: initialised once, before any copy
+__device__ __forceinline__ void init_tile_barriers(uint64_t* bar, bool use) {
   if (use && threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
     tma::bar_init(bar, 1);
+    tma::bar_init(bar + 1, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -1034,13 +1068,13 @@ template <int O, int MATTER, int MODE, bool KO = false>
 __global__ void __launch_bounds__(kThreads, 2)
 stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage, const __grid_constant__ CUtensorMap tmap,
              int use_tma) {
-  __shared__ __align__(8) uint64_t bar;
-  init_tile_barrier(&bar, use_tma != 0);
+  __shared__ __align__(8) uint64_t bar[2];
+  init_tile_barriers(bar, use_tma != 0);
   unsigned phase = 0;
   bool tma_ok = true;
   stage_body<O, MATTER, MODE, KO>(geo, ph, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x,
                                   blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
-                                  use_tma ? &tmap : nullptr, &bar, phase, tma_ok);
+                                  use_tma ? &tmap : nullptr, bar, phase, tma_ok);
 }
 
 // A group of boxes of the same order and matter model, one launch per
@@ -1055,9 +1089,9 @@ stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
   __shared__ StagePtrs sp;
   __shared__ StageBg sbg;
   __shared__ const CUtensorMap* stm;
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar[2];
   const bool lead = threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0;
-  init_tile_barrier(&bar, true);
+  init_tile_barriers(bar, true);
   unsigned phase = 0;
   bool tma_ok = true;
   for (int w = blockIdx.x; w < gb.total; w += gridDim.x) {
@@ -1079,7 +1113,7 @@ stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
     const int l = w - sb.first;
     const int cz = l % sb.nbz, cy = (l / sb.nbz) % sb.nby, cx = l / (sb.nbz * sb.nby);
     const BoxGeom geo{sb.nx, sb.ny, sb.nz, sb.pts};
-    stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0, stm, &bar, phase, tma_ok);
+    stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0, stm, bar, phase, tma_ok);
   }
 }
 

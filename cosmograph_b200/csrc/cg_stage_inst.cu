@@ -81,7 +81,7 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
   }
   BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
   const CUtensorMap& map = (stage == 1 || stage == 3) ? b.mapX : b.mapY;  // the substep's input
-  constexpr size_t smem = sizeof(double) * Slots<M>::value * kThreads;
+  constexpr size_t smem = stage_smem<O, M, kEvolve>();
   if constexpr (O == 2 || O == 8) {
     if (b.ph.ko_coeff != 0.0) {  // Kreiss-Oliger dissipation: its own instantiation
       static bool configured_ko = false;
@@ -117,7 +117,7 @@ cudaError_t go_constraints(const BoxDev& b, const StageBg& bg, double* cvals, do
   P.cvals = cvals;
   P.cpart = cpart;
   BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
-  constexpr size_t smem = sizeof(double) * SlotsC<M>::value * kThreads;
+  constexpr size_t smem = stage_smem<O, M, kConstraints>();
   static bool configured = false;
   if (!configured) {
     cudaError_t e =
@@ -140,7 +140,7 @@ cudaError_t go_constraints_m(const BoxDev& b, const StageBg& bg, double* cvals, 
 
 template <int O, int M>
 cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, cudaStream_t st) {
-  constexpr size_t smem = sizeof(double) * Slots<M>::value * kThreads;
+  constexpr size_t smem = stage_smem<O, M, kEvolve>();
   static bool configured = false;
   if (!configured) {
     cudaError_t e = cudaFuncSetAttribute(stage_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -154,7 +154,7 @@ cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int gr
 
 template <int O, int M>
 int ctas_per_sm() {
-  constexpr size_t smem = sizeof(double) * Slots<M>::value * kThreads;
+  constexpr size_t smem = stage_smem<O, M, kEvolve>();
   if (cudaFuncSetAttribute(stage_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return 1;
