@@ -12,8 +12,9 @@ and Hamiltonian-constraint error against the FP64 run after the same steps.
 
 Printed JSON (rank 0, one line): value = whole-job updates/s with the state
 resident in HBM; e2e = the same through the C ABI with the full state copied
-host->device and device->host around every step (pinned buffers; each step's
-result goes out while the next step's input comes in, cg_exchange_state_async);
+host->device and device->host around every step (pinned buffers; the next
+step's input comes in and the previous step's result goes out while a step
+runs: cg_prefetch_state_async + cg_exchange_state_async);
 roofline = the substep
 kernel's algorithmic HBM bytes against the measured copy bandwidth;
 cpu_baseline = the reference's own sources (oracle/_ref) on the host cores.
@@ -64,7 +65,7 @@ def parse():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--order", type=int, default=8)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma", "mixed"])
-    ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--e2e-steps", type=int, default=6)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference CPU build (rank 0)")
     ap.add_argument("--ncu", action="store_true", help="short run for profiler capture (no JSON extras)")
     ap.add_argument("--variants", default="fp64_fma,mixed", help="comma list of extra precisions timed alongside")
@@ -291,18 +292,29 @@ def run_ensemble(a, world, rank, local):
     h_out = [torch.empty_like(h).pin_memory() for h in h_in]
     dp = ctypes.POINTER(ctypes.c_double)
     L = ev.L
+
+    def p(h):
+        return ctypes.cast(h.data_ptr(), dp)
+
+    def exchange_all():
+        for b, (hi, ho) in enumerate(zip(h_in, h_out)):
+            ev._check(L.cg_prefetch_state_async(ev.ctx, b, p(hi), hi.numel()))
+        for b, (hi, ho) in enumerate(zip(h_in, h_out)):
+            ev._check(L.cg_exchange_state_async(ev.ctx, b, p(ho), p(hi), hi.numel()))
+
+    exchange_all()  # untimed warm-up: allocates the staging buffers
+    ev.synchronize()
     barrier()
     torch.cuda.synchronize()
     q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     q0.record(stream)
     for b, h in enumerate(h_in):
-        ev._check(L.cg_upload_state_async(ev.ctx, b, ctypes.cast(h.data_ptr(), dp), h.numel()))
+        ev._check(L.cg_upload_state_async(ev.ctx, b, p(h), h.numel()))
     ev.step(1)
     for _ in range(a.e2e_steps - 1):
-        # the step's result out and the next step's input in, overlapped
-        for b, (hi, ho) in enumerate(zip(h_in, h_out)):
-            ev._check(L.cg_exchange_state_async(ev.ctx, b, ctypes.cast(ho.data_ptr(), dp),
-                                                ctypes.cast(hi.data_ptr(), dp), hi.numel()))
+        # the next step's inputs come in while this step runs, and this step's
+        # results go out while the next one runs
+        exchange_all()
         ev.step(1)
     for b, h in enumerate(h_out):
         ev._check(L.cg_download_state_async(ev.ctx, b, ctypes.cast(h.data_ptr(), dp), h.numel()))
@@ -532,6 +544,10 @@ def main():
     pin = ctypes.cast(h_in.data_ptr(), dp)
     pout = ctypes.cast(h_out.data_ptr(), dp)
     cnt = h_in.numel()
+    # untimed warm-up: the first staged exchange allocates the staging buffers
+    ev._check(L.cg_prefetch_state_async(ev.ctx, 0, pin, cnt))
+    ev._check(L.cg_exchange_state_async(ev.ctx, 0, pout, pin, cnt))
+    ev.synchronize()
     barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -540,7 +556,9 @@ def main():
     ev._check(L.cg_upload_state_async(ev.ctx, 0, pin, cnt))
     ev.step(1)
     for _ in range(a.e2e_steps - 1):
-        # the step's result out and the next step's input in, overlapped
+        # the next step's input comes in while this step runs, and this
+        # step's result goes out while the next one runs
+        ev._check(L.cg_prefetch_state_async(ev.ctx, 0, pin, cnt))
         ev._check(L.cg_exchange_state_async(ev.ctx, 0, pout, pin, cnt))
         ev.step(1)
     ev._check(L.cg_download_state_async(ev.ctx, 0, pout, cnt))

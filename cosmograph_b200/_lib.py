@@ -31,7 +31,7 @@ STATUS_NAN, STATUS_NONFINITE, STATUS_TILE_TIMEOUT = 1, 2, 4
 EXPORTS = (
     "cg_box_desc_default", "cg_create", "cg_destroy", "cg_set_stream", "cg_get_stream",
     "cg_num_fields", "cg_field_name", "cg_upload_state", "cg_download_state",
-    "cg_upload_state_async", "cg_download_state_async", "cg_exchange_state_async",
+    "cg_upload_state_async", "cg_download_state_async", "cg_exchange_state_async", "cg_prefetch_state_async",
     "cg_upload_field", "cg_download_field",
     "cg_device_register", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
     "cg_status", "cg_frw_state", "cg_step_count", "cg_last_error", "cg_version",
@@ -85,6 +85,7 @@ def load() -> ctypes.CDLL:
         "cg_upload_state_async": (i, [vp, i, dp, sz]),
         "cg_download_state_async": (i, [vp, i, dp, sz]),
         "cg_exchange_state_async": (i, [vp, i, dp, dp, sz]),
+        "cg_prefetch_state_async": (i, [vp, i, dp, sz]),
         "cg_upload_field": (i, [vp, i, i, ctypes.c_char, dp, sz]),
         "cg_download_field": (i, [vp, i, i, ctypes.c_char, dp, sz]),
         "cg_device_register": (i, [vp, i, ctypes.c_char, ctypes.POINTER(dp)]),

@@ -89,6 +89,14 @@ struct Box {
   bool mixed = false;
   cg::MixedBox mdev{};
   double bp[23] = {}, bf[23] = {}, ba[23] = {}, bprev[23] = {};  // uniform background registers
+  // staged state copies (cg_prefetch_state_async): device copies of the
+  // next input and of the last result, the prefetched host buffer, and the
+  // events that order the staging buffers' producers and consumers
+  double* stage_in = nullptr;
+  double* stage_out = nullptr;
+  const double* pre_host = nullptr;
+  size_t pre_count = 0;
+  cudaEvent_t in_ready = nullptr, in_free = nullptr, out_ready = nullptr, out_free = nullptr;
 };
 
 }  // namespace
@@ -118,8 +126,10 @@ struct cg_ctx {
   int gexec_steps = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
-  // cg_exchange_state_async: the device-to-host stream and one event per field
+  // cg_exchange_state_async: the device-to-host stream and one event per field;
+  // cg_prefetch_state_async: the host-to-device stream
   cudaStream_t copy_stream = nullptr;
+  cudaStream_t up_stream = nullptr;
   cudaEvent_t copy_start = nullptr;
   std::vector<cudaEvent_t> copy_done;
   unsigned* status = nullptr;
@@ -553,6 +563,13 @@ void free_box(Box& b) {
   cudaFree(b.kavg_partial);
   b.dev.P = b.dev.F = b.dev.X = b.dev.Y = b.dev.FP0 = b.dev.FP1 = nullptr;
   b.kavg_partial = nullptr;
+  cudaFree(b.stage_in);
+  cudaFree(b.stage_out);
+  b.stage_in = b.stage_out = nullptr;
+  for (cudaEvent_t* ev : {&b.in_ready, &b.in_free, &b.out_ready, &b.out_free}) {
+    if (*ev) cudaEventDestroy(*ev);
+    *ev = nullptr;
+  }
 }
 
 }  // namespace
@@ -720,10 +737,11 @@ int cg_destroy(cg_ctx* ctx) {
   for (Box& b : ctx->boxes) free_box(b);
   cudaFree(ctx->red);
   cudaFree(ctx->status);
-  if (ctx->copy_stream) {
-    cudaStreamSynchronize(ctx->copy_stream);
-    cudaStreamDestroy(ctx->copy_stream);
-  }
+  for (cudaStream_t* cs : {&ctx->copy_stream, &ctx->up_stream})
+    if (*cs) {
+      cudaStreamSynchronize(*cs);
+      cudaStreamDestroy(*cs);
+    }
   if (ctx->copy_start) cudaEventDestroy(ctx->copy_start);
   for (cudaEvent_t ev : ctx->copy_done) cudaEventDestroy(ev);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -756,6 +774,8 @@ static int state_copy(cg_ctx* ctx, int box, double* host, size_t count, bool upl
     b.stage_next = 0;
     b.steps = 0;
   } else {
+    // after the staged download of an earlier exchange (it may write the same host buffer)
+    if (b.out_free) CG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, b.out_free, 0));
     CG_CUDA(ctx, cudaMemcpyAsync(host, b.dev.P, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   }
   if (!async) CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -779,6 +799,72 @@ int cg_download_state_async(cg_ctx* ctx, int box, double* host, size_t count) {
 // so far on the context's stream; the context's stream uploads field f once
 // field f has been downloaded.  Opposite copy directions overlap, so the pair
 // takes about as long as the longer of the two.
+static int ensure_event(cg_ctx* ctx, cudaEvent_t* ev) {
+  if (!*ev) CG_CUDA(ctx, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+  return CG_OK;
+}
+
+// The input is copied into the box's staging buffer on its own stream, at
+// once; the exchange that names the same host buffer moves it into the
+// registers by a device copy.
+int cg_prefetch_state_async(cg_ctx* ctx, int box, const double* host_in, size_t count) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  Box& b = ctx->boxes[box];
+  const size_t n = (size_t)b.dev.nfields * b.dev.pts;
+  if (!host_in || count != n)
+    return fail(ctx, CG_ERR_INVALID, "count must be nfields*nx*ny*nz = " + std::to_string(n));
+  if (!ctx->up_stream) CG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->up_stream, cudaStreamNonBlocking));
+  for (cudaEvent_t* ev : {&b.in_ready, &b.in_free})
+    if ((rc = ensure_event(ctx, ev))) return rc;
+  if (!b.stage_in) {
+    const cudaError_t e = cudaMalloc(&b.stage_in, n * sizeof(double));
+    if (e != cudaSuccess) {
+      b.stage_in = nullptr;
+      return fail(ctx, e == cudaErrorMemoryAllocation ? CG_ERR_MEMORY : CG_ERR_CUDA,
+                  std::string("staging buffer: ") + cudaGetErrorString(e));
+    }
+  }
+  // the previous staged input has been moved into the registers
+  CG_CUDA(ctx, cudaStreamWaitEvent(ctx->up_stream, b.in_free, 0));
+  CG_CUDA(ctx, cudaMemcpyAsync(b.stage_in, host_in, n * sizeof(double), cudaMemcpyHostToDevice, ctx->up_stream));
+  CG_CUDA(ctx, cudaEventRecord(b.in_ready, ctx->up_stream));
+  b.pre_host = host_in;
+  b.pre_count = count;
+  return CG_OK;
+}
+
+// staged exchange: the result leaves through stage_out (its download overlaps
+// later work on the context's stream), the input comes from stage_in
+static int exchange_staged(cg_ctx* ctx, Box& b, double* host_out, size_t n) {
+  int rc = CG_OK;
+  for (cudaEvent_t* ev : {&b.out_ready, &b.out_free})
+    if ((rc = ensure_event(ctx, ev))) return rc;
+  if (!b.stage_out) {
+    const cudaError_t e = cudaMalloc(&b.stage_out, n * sizeof(double));
+    if (e != cudaSuccess) {
+      b.stage_out = nullptr;
+      return fail(ctx, e == cudaErrorMemoryAllocation ? CG_ERR_MEMORY : CG_ERR_CUDA,
+                  std::string("staging buffer: ") + cudaGetErrorString(e));
+    }
+  }
+  const size_t bytes = n * sizeof(double);
+  CG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, b.out_free, 0));  // the previous staged download is done
+  CG_CUDA(ctx, cudaMemcpyAsync(b.stage_out, b.dev.P, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  CG_CUDA(ctx, cudaEventRecord(b.out_ready, ctx->stream));
+  CG_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, b.out_ready, 0));
+  CG_CUDA(ctx, cudaMemcpyAsync(host_out, b.stage_out, bytes, cudaMemcpyDeviceToHost, ctx->copy_stream));
+  CG_CUDA(ctx, cudaEventRecord(b.out_free, ctx->copy_stream));
+  CG_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, b.in_ready, 0));  // the prefetched input has arrived
+  CG_CUDA(ctx, cudaMemcpyAsync(b.dev.P, b.stage_in, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  CG_CUDA(ctx, cudaEventRecord(b.in_free, ctx->stream));
+  b.pre_host = nullptr;
+  b.pre_count = 0;
+  b.stage_next = 0;
+  b.steps = 0;
+  return CG_OK;
+}
+
 int cg_exchange_state_async(cg_ctx* ctx, int box, double* host_out, const double* host_in, size_t count) {
   int rc = check_box(ctx, box);
   if (rc) return rc;
@@ -787,6 +873,9 @@ int cg_exchange_state_async(cg_ctx* ctx, int box, double* host_out, const double
   if (!host_out || !host_in || count != n)
     return fail(ctx, CG_ERR_INVALID, "count must be nfields*nx*ny*nz = " + std::to_string(n));
   if (!ctx->copy_stream) CG_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+  if (b.pre_host == host_in && b.pre_count == count && b.stage_in) return exchange_staged(ctx, b, host_out, n);
+  // after the staged download of an earlier exchange (it may write the same host buffer)
+  if (b.out_free) CG_CUDA(ctx, cudaStreamWaitEvent(ctx->copy_stream, b.out_free, 0));
   if (!ctx->copy_start) CG_CUDA(ctx, cudaEventCreateWithFlags(&ctx->copy_start, cudaEventDisableTiming));
   while ((int)ctx->copy_done.size() < b.dev.nfields) {
     cudaEvent_t ev = nullptr;
@@ -1296,6 +1385,7 @@ int cg_status(cg_ctx* ctx, uint32_t* flags) {
 int cg_synchronize(cg_ctx* ctx) {
   uint32_t f = 0;
   int rc = cg_status(ctx, &f);
+  if (!rc && ctx->copy_stream) CG_CUDA(ctx, cudaStreamSynchronize(ctx->copy_stream));  // staged downloads
   if (rc) return rc;
   if (f & CG_STATUS_TILE_TIMEOUT) return fail(ctx, CG_ERR_CUDA, "a TMA tile copy timed out");
   if (f & CG_STATUS_NAN) return fail(ctx, CG_ERR_NAN, "NaN detected in DIFFphi");

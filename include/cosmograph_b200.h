@@ -146,8 +146,23 @@ int cg_download_state_async(cg_ctx *ctx, int box, double *host, size_t count);
  * for cg_upload_state; work queued afterwards on the context's stream sees
  * the new state, and host_out is complete once that stream reaches it (e.g.
  * cg_synchronize).  No reference counterpart: streaming boxes through one
- * GPU (the reference evolves one box per process). */
+ * GPU (the reference evolves one box per process).
+ *
+ * When host_in was handed to cg_prefetch_state_async for this box before,
+ * the exchange is staged instead: the state is copied on the device into a
+ * staging buffer and downloaded from there on the second stream while later
+ * work runs, and the prefetched input is copied on the device into the
+ * registers.  host_out is then complete after cg_synchronize. */
 int cg_exchange_state_async(cg_ctx *ctx, int box, double *host_out, const double *host_in, size_t count);
+
+/* Start copying host_in (pinned, count as for cg_upload_state) into a device
+ * staging buffer of the box at once, on a stream of its own, so that the copy
+ * overlaps the work queued on the context's stream.  The next
+ * cg_exchange_state_async of this box with the same host_in takes its input
+ * from there.  host_in must stay unchanged until the context's stream has
+ * passed that exchange.  The first call allocates the staging buffers (two
+ * copies of the state).  No reference counterpart. */
+int cg_prefetch_state_async(cg_ctx *ctx, int box, const double *host_in, size_t count);
 
 /* One register of one field: reg = 'p', 'a' (current substep input), 'f'.
  * Replaces BSSN::fields["<name>_<reg>"] access (bssn.cc:30-39). Synchronous.
@@ -231,7 +246,8 @@ int cg_set_option(cg_ctx *ctx, int option, int value);
 int cg_num_groups(cg_ctx *ctx, int *n);
 int cg_group_info(cg_ctx *ctx, int group, int *info, int n);
 
-/* Wait for queued work; returns CG_ERR_NAN if a NaN appeared in DIFFphi. */
+/* Wait for queued work (and staged downloads); returns CG_ERR_NAN if a NaN
+ * appeared in DIFFphi. */
 int cg_synchronize(cg_ctx *ctx);
 
 /* Sticky error flags (CG_STATUS_*), OR-reduced on the device. */

@@ -23,7 +23,7 @@ def ptr(t: torch.Tensor):
     return ctypes.cast(t.data_ptr(), DP)
 
 
-def stream_states(states, cfg, exchange: bool):
+def stream_states(states, cfg, exchange: bool, prefetch: bool = False):
     """One step per state, each state uploaded in turn; returns each step's result."""
     ins = [pinned(s.fields) for s in states]
     outs = [torch.zeros_like(ins[0]).pin_memory() for _ in states]
@@ -32,6 +32,8 @@ def stream_states(states, cfg, exchange: bool):
         ev._check(ev.L.cg_upload_state_async(ev.ctx, 0, ptr(ins[0]), n))
         ev.step(1)
         for q in range(1, len(states)):
+            if prefetch:
+                ev._check(ev.L.cg_prefetch_state_async(ev.ctx, 0, ptr(ins[q]), n))
             if exchange:
                 ev._check(ev.L.cg_exchange_state_async(ev.ctx, 0, ptr(outs[q - 1]), ptr(ins[q]), n))
             else:
@@ -44,11 +46,14 @@ def stream_states(states, cfg, exchange: bool):
     return [o.numpy().copy() for o in outs], steps
 
 
+@pytest.mark.parametrize("prefetch", [False, True])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_exchange_equals_download_then_upload(precision):
+def test_exchange_equals_download_then_upload(precision, prefetch):
+    """Plain exchange (field-by-field overlap) and staged exchange (prefetched
+    input, download from a device copy while the next step runs)."""
     cfg = BoxConfig(order=8, precision=precision)
     states = [ics.perturbed((16, 20, 32), S.DUST, seed=q, amp=1e-3) for q in range(4)]
-    got, steps_x = stream_states(states, cfg, exchange=True)
+    got, steps_x = stream_states(states, cfg, exchange=True, prefetch=prefetch)
     want, steps_s = stream_states(states, cfg, exchange=False)
     for q in range(len(states)):
         assert np.array_equal(got[q], want[q]), q
@@ -64,3 +69,24 @@ def test_exchange_rejects_bad_arguments():
         assert b"count" in ev.L.cg_last_error(ev.ctx)
         assert ev.L.cg_exchange_state_async(ev.ctx, 0, None, ptr(h), h.numel()) == -1
         assert ev.L.cg_exchange_state_async(ev.ctx, 3, ptr(h), ptr(h), h.numel()) == -1
+
+
+def test_prefetch_then_plain_copies_keep_order():
+    """A staged exchange followed by a plain download into the same host
+    buffer: the plain download lands last."""
+    cfg = BoxConfig(order=4)
+    a = ics.perturbed((16, 16, 16), S.DUST, seed=1, amp=1e-3)
+    b = ics.perturbed((16, 16, 16), S.DUST, seed=2, amp=1e-3)
+    h_b = pinned(b.fields)
+    h_out = torch.zeros_like(h_b).pin_memory()
+    with Evolution(a, cfg) as ev:
+        n = h_b.numel()
+        ev.step(1)
+        ev._check(ev.L.cg_prefetch_state_async(ev.ctx, 0, ptr(h_b), n))
+        ev._check(ev.L.cg_exchange_state_async(ev.ctx, 0, ptr(h_out), ptr(h_b), n))
+        ev._check(ev.L.cg_download_state_async(ev.ctx, 0, ptr(h_out), n))
+        ev.synchronize()
+    assert np.array_equal(h_out.numpy(), h_b.numpy())
+    with Evolution(a, cfg) as ev:
+        assert ev.L.cg_prefetch_state_async(ev.ctx, 0, ptr(h_b), n + 1) == -1
+        assert ev.L.cg_prefetch_state_async(ev.ctx, 0, None, n) == -1
