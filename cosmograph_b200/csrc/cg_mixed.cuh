@@ -258,10 +258,17 @@ __device__ __forceinline__ bool derivatives(const float* __restrict__ a, int N, 
   using G = TileG<O>;
   const tile::Taps<G, float> t{tl, cc};
   constexpr int NIT = 8;  // fields with second derivatives; first-derivative-only fields use global taps
-  if (tmap) {
-    bool ok = true;
+  const bool by_tma = tmap != nullptr;
+  bool ok = true;
+  tile::Loader<G, Brick, float> ld;
+  if (!by_tma) {
+    ld.init(tid, z0, nz);
+    ld.fetch(a + (size_t)phase1_field(0) * N, rowoff);
+  }
+  // one loop (and one copy of the derivative code) for both kinds of copy
 #pragma unroll 1
-    for (int it = 0; it < NIT; ++it) {
+  for (int it = 0; it < NIT; ++it) {
+    if (by_tma) {
       tma::fence_proxy_async();  // this thread's shared-memory accesses come before the copy's writes
       __syncthreads();           // the previous tile has been read
       if (tid == 0) {
@@ -272,24 +279,19 @@ __device__ __forceinline__ bool derivatives(const float* __restrict__ a, int N, 
       }
       if (ok && !tma::wait(bar, phase, kTmaWaitCycles)) ok = false;
       phase ^= 1u;
-      field_derivatives<O>(it, t, idx, idx2, gi, sl);
+    } else {
+      __syncthreads();
+      ld.store(tl);
+      __syncthreads();
+      if (it + 1 < NIT) ld.fetch(a + (size_t)phase1_field(it + 1) * N, rowoff);
     }
-    ok = __syncthreads_and(ok);
-    if (!ok && tid == 0) atomicOr(status, kStatusTileTimeout);
-    return ok;
-  }
-  tile::Loader<G, Brick, float> ld;
-  ld.init(tid, z0, nz);
-  ld.fetch(a + (size_t)phase1_field(0) * N, rowoff);
-#pragma unroll 1
-  for (int it = 0; it < NIT; ++it) {
-    __syncthreads();
-    ld.store(tl);
-    __syncthreads();
-    if (it + 1 < NIT) ld.fetch(a + (size_t)phase1_field(it + 1) * N, rowoff);
     field_derivatives<O>(it, t, idx, idx2, gi, sl);
   }
-  return true;
+  if (by_tma) {
+    ok = __syncthreads_and(ok);
+    if (!ok && tid == 0) atomicOr(status, kStatusTileTimeout);
+  }
+  return ok;
 }
 
 // dust flux divergences from the stored FP32 flux primitives (global taps)

@@ -291,51 +291,54 @@ __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N,
   using PF = Phase1<MATTER, MODE>;
   using G = TileG<O>;
   constexpr bool TWO = TileBuffers<O, MATTER, MODE>::kTwo;
-  const tile::Taps<G, double> t{tl, cc};
-  if (tmap) {
-    bool ok = true;
-    constexpr unsigned kBytes = (unsigned)(G::SIZE * sizeof(double));
-    // field it into buffer it % 2 (one buffer: 0), field it + 1 into L2
-    auto issue = [&](int it) {
-      const int b = TWO ? (it & 1) : 0;
-      tma::arrive_expect_tx(bar + b, kBytes);
-      tma::load_4d(b ? tl2 : tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it), bar + b);
-      if (it + 1 < PF::N) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it + 1));
-    };
+  constexpr unsigned kBytes = (unsigned)(G::SIZE * sizeof(double));
+  // TMA: field it into buffer it % 2 (one buffer: 0), field it + 1 into L2
+  auto issue = [&](int it) {
+    const int b = TWO ? (it & 1) : 0;
+    tma::arrive_expect_tx(bar + b, kBytes);
+    tma::load_4d(b ? tl2 : tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it), bar + b);
+    if (it + 1 < PF::N) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it + 1));
+  };
+  const bool by_tma = tmap != nullptr;
+  bool ok = true;
+  tile::Loader<G, Brick, double> ld;
+  if (by_tma) {
     if (TWO) {
       tma::fence_proxy_async();  // this thread's shared-memory accesses come before the copy's writes
       __syncthreads();
       if (tid == 0) issue(0);
     }
+  } else {
+    ld.init(tid, z0, nz);
+    ld.fetch(a + (size_t)PF::field(0) * N, rowoff);
+  }
+  // one loop (and one copy of the derivative code) for both kinds of copy
 #pragma unroll 1
-    for (int it = 0; it < PF::N; ++it) {
+  for (int it = 0; it < PF::N; ++it) {
+    int b = 0;
+    if (by_tma) {
       tma::fence_proxy_async();
       __syncthreads();  // the buffer the next copy writes has been read
       if (tid == 0) {
         if (!TWO) issue(it);
         else if (it + 1 < PF::N) issue(it + 1);
       }
-      const int b = TWO ? (it & 1) : 0;
+      b = TWO ? (it & 1) : 0;
       if (ok && !tma::wait(bar + b, (phase >> b) & 1u, kTmaWaitCycles64)) ok = false;
       phase ^= 1u << b;
-      field_derivatives<O, MATTER, MODE>(it, tile::Taps<G, double>{b ? tl2 : tl, cc}, ph, gi, sl);
+    } else {
+      __syncthreads();  // the previous tile has been read
+      ld.store(tl);
+      __syncthreads();
+      if (it + 1 < PF::N) ld.fetch(a + (size_t)PF::field(it + 1) * N, rowoff);
     }
+    field_derivatives<O, MATTER, MODE>(it, tile::Taps<G, double>{b ? tl2 : tl, cc}, ph, gi, sl);
+  }
+  if (by_tma) {
     ok = __syncthreads_and(ok);
     if (!ok && tid == 0) atomicOr(status, kStatusTileTimeout64);
-    return ok;
   }
-  tile::Loader<G, Brick, double> ld;
-  ld.init(tid, z0, nz);
-  ld.fetch(a + (size_t)PF::field(0) * N, rowoff);
-#pragma unroll 1
-  for (int it = 0; it < PF::N; ++it) {
-    __syncthreads();  // the previous tile has been read
-    ld.store(tl);
-    __syncthreads();
-    if (it + 1 < PF::N) ld.fetch(a + (size_t)PF::field(it + 1) * N, rowoff);
-    field_derivatives<O, MATTER, MODE>(it, t, ph, gi, sl);
-  }
-  return true;
+  return ok;
 }
 
 // the derivatives of phase-1 field `it` from its tile, into the slots
