@@ -35,7 +35,7 @@ EXPORTS = (
     "cg_upload_field", "cg_download_field",
     "cg_device_register", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
     "cg_status", "cg_frw_state", "cg_step_count", "cg_last_error", "cg_version",
-    "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints",
+    "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints", "cg_field_statistics",
     "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust",
 )
 OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID, OPT_TMA = 1, 2, 3, 4, 5
@@ -100,6 +100,7 @@ def load() -> ctypes.CDLL:
         "cg_conformal_average": (i, [vp, vp, vp, sz, ctypes.c_double, dp]),
         "cg_conformal_average_noalloc": (i, [vp, vp, sz, ctypes.c_double, vp, vp]),
         "cg_constraints": (i, [vp, i, dp, dp, dp, dp, dp]),
+        "cg_field_statistics": (i, [vp, i, dp, i]),
         "cg_set_option": (i, [vp, i, i]),
         "cg_ic_grf_dust": (i, [vp, i, dp, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
         "cg_num_groups": (i, [vp, ctypes.POINTER(i)]),

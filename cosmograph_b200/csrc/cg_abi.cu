@@ -287,6 +287,58 @@ __global__ void constraint_stdev_kernel(const double* cvals, int n, const double
     for (int m = 0; m < 10; ++m) part[(size_t)blockIdx.x * 10 + m] = s[m][0];
 }
 
+// Volume-weighted statistics of io_bssn_dump_statistics (IO/io.cc:8-14):
+// pass 1, per CTA, sum_q w f_m (m < 4) and sum_q w, w = exp(6 (phi + phi_FRW))
+// (conformal_average / volume_average, utils/math.h:1382-1415).
+__global__ void wstats_sum_kernel(const double* f0, const double* f1, const double* f2, const double* f3,
+                                  const double* __restrict__ phi, int n, double phi_frw, double* part) {
+  __shared__ double s[5][256];
+  double a[5] = {0, 0, 0, 0, 0};
+  const double* f[4] = {f0, f1, f2, f3};
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const double w = exp(6.0 * (phi[q] + phi_frw));
+    for (int m = 0; m < 4; ++m) a[m] += w * f[m][q];
+    a[4] += w;
+  }
+  for (int m = 0; m < 5; ++m) s[m][threadIdx.x] = a[m];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int m = 0; m < 5; ++m) s[m][threadIdx.x] += s[m][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int m = 0; m < 5; ++m) part[(size_t)blockIdx.x * 5 + m] = s[m][0];
+}
+
+// pass 2: sum_q w (avg_m - f_m)^2 with avg_m = sum w f_m / sum w from pass 1
+// (conformal_standard_deviation, utils/math.h:1455-1470)
+__global__ void wstats_var_kernel(const double* f0, const double* f1, const double* f2, const double* f3,
+                                  const double* __restrict__ phi, int n, double phi_frw, const double* r1,
+                                  double* part) {
+  __shared__ double s[4][256];
+  double a[4] = {0, 0, 0, 0}, avg[4];
+  const double* f[4] = {f0, f1, f2, f3};
+  const double vol = r1[4] / n;
+  for (int m = 0; m < 4; ++m) avg[m] = r1[m] / n / vol;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const double w = exp(6.0 * (phi[q] + phi_frw));
+    for (int m = 0; m < 4; ++m) {
+      const double d = avg[m] - f[m][q];
+      a[m] += w * (d * d);
+    }
+  }
+  for (int m = 0; m < 4; ++m) s[m][threadIdx.x] = a[m];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o)
+      for (int m = 0; m < 4; ++m) s[m][threadIdx.x] += s[m][threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int m = 0; m < 4; ++m) part[(size_t)blockIdx.x * 4 + m] = s[m][0];
+}
+
 }  // namespace
 
 namespace cg {
@@ -363,14 +415,21 @@ void pack_bg(const double* full, double* compact) {
   for (int f : {(int)cg::F_K, (int)cg::F_PHI, (int)cg::F_ALPHA, 18, 19}) compact[cg::mixed::bgi(f)] = full[f];
 }
 
+// Constraint / statistics scratch of a box: per-point values (12 arrays),
+// per-CTA partials of the two constraint passes, their results, and the
+// field-statistics partials (5 + 4 per block) and results (9).
+size_t cscratch_doubles(const Box& b) {
+  const size_t n = (size_t)b.dev.pts;
+  const size_t nblk1 = (size_t)cg::exact::constraint_blocks(b.dev);
+  const size_t nblk2 = std::min<size_t>(1024, (n + 255) / 256);
+  return 12 * n + 27 * nblk1 + 10 * nblk2 + 37 + 9 * nblk2 + 9;
+}
+
 int mixed_init(cg_ctx* ctx, Box& b) {
   // background registers from the means of _p (K, phi, alpha, D)
   const int n = b.dev.pts;
   const int nblk = std::min(1024, (n + 255) / 256);
-  if (!b.cscratch) {
-    const size_t need = (size_t)10 * n + 27 * (size_t)cg::exact::constraint_blocks(b.dev) + 10 * (size_t)nblk + 37;
-    CG_CUDA(ctx, cudaMalloc(&b.cscratch, sizeof(double) * need));
-  }
+  if (!b.cscratch) CG_CUDA(ctx, cudaMalloc(&b.cscratch, sizeof(double) * cscratch_doubles(b)));
   double* part = b.cscratch;
   double* res = part + 5 * (size_t)nblk;
   const double* P = b.mdev.P;
@@ -1411,71 +1470,136 @@ int cg_step_count(cg_ctx* ctx, int box, int64_t* steps) {
   return CG_OK;
 }
 
+// Scratch layout of the constraint pass (cscratch_doubles): cvals (12 n) |
+// part1 (27 nblk1) | part2 (10 nblk2) | r1 (27) | r2 (10) | wpart (9 nblk2) | wres (9)
+struct CScratch {
+  double *cvals, *part1, *part2, *r1, *r2, *wpart, *wres;
+  int n, nblk1, nblk2;
+};
+
+static CScratch cscratch_layout(const Box& b) {
+  CScratch c{};
+  c.n = b.dev.pts;
+  c.nblk1 = cg::exact::constraint_blocks(b.dev);
+  c.nblk2 = std::min(1024, (c.n + 255) / 256);
+  c.cvals = b.cscratch;
+  c.part1 = c.cvals + (size_t)12 * c.n;
+  c.part2 = c.part1 + (size_t)27 * c.nblk1;
+  c.r1 = c.part2 + (size_t)10 * c.nblk2;
+  c.r2 = c.r1 + 27;
+  c.wpart = c.r2 + 10;
+  c.wres = c.wpart + (size_t)9 * c.nblk2;
+  return c;
+}
+
+// The constraint pass (BSSN::setConstraintCalcs, bssn.cc:965-1071) on the
+// box's state between steps: per-point values and both reduction passes, on
+// the context's stream.  dev gets the FP64 first-substep input; for a mixed
+// box it is built in *xtmp, which the caller frees after the last use.
+static int constraint_pass(cg_ctx* ctx, Box& b, cg::BoxDev& dev, double** xtmp) {
+  *xtmp = nullptr;
+  if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "constraints are taken between steps");
+  if (b.stage_next == 0) {
+    const int rc = do_init(ctx, b);
+    if (rc) return rc;
+  }
+  const int n = b.dev.pts;
+  if (!b.cscratch) CG_CUDA(ctx, cudaMalloc(&b.cscratch, sizeof(double) * cscratch_doubles(b)));
+  dev = b.dev;
+  if (b.mixed) {
+    // FP64 first-substep input of the current _p for the FP64 constraint pass
+    const size_t nx64 = (size_t)b.dev.nfields * n + (size_t)cg::P_N * n;
+    CG_CUDA(ctx, cudaMalloc(xtmp, sizeof(double) * nx64));
+    dev.X = *xtmp;
+    dev.FP0 = *xtmp + (size_t)b.dev.nfields * n;
+    StageBg bg0 = bg_for(b, 1, b.frw.get_phi);
+    cudaError_t ei = cg::launch_init(cg::kExact, dev, bg0, ctx->stream);
+    if (ei != cudaSuccess) return cuda_fail(ctx, ei, "init");
+  }
+  const CScratch c = cscratch_layout(b);
+  StageBg bg = bg_for(b, 1, b.frw.get_phi);
+  cudaError_t ec = cg::exact::launch_constraints(dev, bg, c.cvals, c.part1, ctx->stream);
+  if (ec != cudaSuccess) return cuda_fail(ctx, ec, "constraints");
+  part_final_kernel<<<1, 256, 0, ctx->stream>>>(c.part1, c.nblk1, 27, 17, c.r1);
+  constraint_stdev_kernel<<<c.nblk2, 256, 0, ctx->stream>>>(c.cvals, n, c.r1, c.part2);
+  part_final_kernel<<<1, 256, 0, ctx->stream>>>(c.part2, c.nblk2, 10, 10, c.r2);
+  CG_CUDA(ctx, cudaGetLastError());
+  return CG_OK;
+}
+
 int cg_constraints(cg_ctx* ctx, int box, double* H, double* M, double* G, double* A, double* S) {
   int rc = check_box(ctx, box);
   if (rc) return rc;
   if (!H || !M || !G || !A || !S) return fail(ctx, CG_ERR_INVALID, "null output array");
   Box& b = ctx->boxes[box];
-  if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "constraints are taken between steps");
-  if (b.stage_next == 0) {
-    rc = do_init(ctx, b);
-    if (rc) return rc;
-  }
-  const int n = b.dev.pts;
-  const int nblk1 = cg::exact::constraint_blocks(b.dev);
-  const int nblk2 = std::min(1024, (n + 255) / 256);
-  // layout: cvals (10 n) | part1 (27 nblk1) | part2 (10 nblk2) | r1 (27) | r2 (10)
-  const size_t need = (size_t)10 * n + 27 * (size_t)nblk1 + 10 * (size_t)nblk2 + 37;
-  if (!b.cscratch) CG_CUDA(ctx, cudaMalloc(&b.cscratch, sizeof(double) * need));
-  cg::BoxDev dev = b.dev;
+  cg::BoxDev dev{};
   double* xtmp = nullptr;
-  if (b.mixed) {
-    // FP64 first-substep input of the current _p for the FP64 constraint pass
-    const size_t nx64 = (size_t)b.dev.nfields * n + (size_t)cg::P_N * n;
-    CG_CUDA(ctx, cudaMalloc(&xtmp, sizeof(double) * nx64));
-    dev.X = xtmp;
-    dev.FP0 = xtmp + (size_t)b.dev.nfields * n;
-    StageBg bg0 = bg_for(b, 1, b.frw.get_phi);
-    cudaError_t ei = cg::launch_init(cg::kExact, dev, bg0, ctx->stream);
-    if (ei != cudaSuccess) {
-      cudaFree(xtmp);
-      return cuda_fail(ctx, ei, "init");
-    }
-  }
-  double* cvals = b.cscratch;
-  double* part1 = cvals + (size_t)10 * n;
-  double* part2 = part1 + (size_t)27 * nblk1;
-  double* r1 = part2 + (size_t)10 * nblk2;
-  double* r2 = r1 + 27;
-  StageBg bg = bg_for(b, 1, b.frw.get_phi);
-  cudaError_t ec = cg::exact::launch_constraints(dev, bg, cvals, part1, ctx->stream);
-  if (ec != cudaSuccess) {
+  rc = constraint_pass(ctx, b, dev, &xtmp);
+  if (rc) {
     cudaFree(xtmp);
-    return cuda_fail(ctx, ec, "constraints");
+    return rc;
   }
-  part_final_kernel<<<1, 256, 0, ctx->stream>>>(part1, nblk1, 27, 17, r1);
-  constraint_stdev_kernel<<<nblk2, 256, 0, ctx->stream>>>(cvals, n, r1, part2);
-  part_final_kernel<<<1, 256, 0, ctx->stream>>>(part2, nblk2, 10, 10, r2);
-  CG_CUDA(ctx, cudaGetLastError());
+  const CScratch c = cscratch_layout(b);
+  const int n = c.n;
   double h1[27], h2[10];
-  CG_CUDA(ctx, cudaMemcpyAsync(h1, r1, sizeof(h1), cudaMemcpyDeviceToHost, ctx->stream));
-  CG_CUDA(ctx, cudaMemcpyAsync(h2, r2, sizeof(h2), cudaMemcpyDeviceToHost, ctx->stream));
+  CG_CUDA(ctx, cudaMemcpyAsync(h1, c.r1, sizeof(h1), cudaMemcpyDeviceToHost, ctx->stream));
+  CG_CUDA(ctx, cudaMemcpyAsync(h2, c.r2, sizeof(h2), cudaMemcpyDeviceToHost, ctx->stream));
   CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   cudaFree(xtmp);
   // BSSN_NORMALIZE_MEAN / _STDEV and BSSN_STORE_CONSTRAINT_STAT_VARS (bssn_macros.h:539-560)
   double* outs[5] = {H, M, G, A, S};
-  for (int c = 0; c < 5; ++c) {
-    double* o = outs[c];
-    o[0] = h1[c] / n;
-    o[1] = std::sqrt(h2[2 * c] / (n - 1.0));
-    o[2] = h1[17 + c];
-    o[3] = h1[5 + c];
-    o[4] = h1[10 + c] / n;
-    o[5] = std::sqrt(h2[2 * c + 1] / (n - 1.0));
-    o[6] = h1[22 + c];
+  for (int k = 0; k < 5; ++k) {
+    double* o = outs[k];
+    o[0] = h1[k] / n;
+    o[1] = std::sqrt(h2[2 * k] / (n - 1.0));
+    o[2] = h1[17 + k];
+    o[3] = h1[5 + k];
+    o[4] = h1[10 + k] / n;
+    o[5] = std::sqrt(h2[2 * k + 1] / (n - 1.0));
+    o[6] = h1[22 + k];
   }
   H[7] = std::sqrt(h1[15]);
   M[7] = std::sqrt(h1[16]);
+  return CG_OK;
+}
+
+int cg_field_statistics(cg_ctx* ctx, int box, double* out, int n_out) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  if (!out || n_out < 9) return fail(ctx, CG_ERR_INVALID, "out needs 9 entries");
+  Box& b = ctx->boxes[box];
+  cg::BoxDev dev{};
+  double* xtmp = nullptr;
+  rc = constraint_pass(ctx, b, dev, &xtmp);  // ricci_a and DIFFr_a per point
+  if (rc) {
+    cudaFree(xtmp);
+    return rc;
+  }
+  const CScratch c = cscratch_layout(b);
+  const int n = c.n;
+  const double* phi = dev.X + (size_t)cg::F_PHI * n;
+  const double* K = dev.X + (size_t)cg::F_K * n;
+  const double* ricci = c.cvals + (size_t)10 * n;
+  const double* rho = c.cvals + (size_t)11 * n;
+  const double phi_frw = b.frw.get_phi;
+  wstats_sum_kernel<<<c.nblk2, 256, 0, ctx->stream>>>(phi, K, rho, ricci, phi, n, phi_frw, c.wpart);
+  part_final_kernel<<<1, 256, 0, ctx->stream>>>(c.wpart, c.nblk2, 5, 5, c.wres);
+  wstats_var_kernel<<<c.nblk2, 256, 0, ctx->stream>>>(phi, K, rho, ricci, phi, n, phi_frw, c.wres,
+                                                      c.wpart + (size_t)5 * c.nblk2);
+  part_final_kernel<<<1, 256, 0, ctx->stream>>>(c.wpart + (size_t)5 * c.nblk2, c.nblk2, 4, 4, c.wres + 5);
+  cudaError_t e = cudaGetLastError();
+  double h[9];
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, c.wres, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(xtmp);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "field statistics");
+  // DETAILS(field) for DIFFphi, DIFFK, DIFFr, ricci, then the volume average
+  const double vol = h[4] / n;
+  for (int m = 0; m < 4; ++m) {
+    out[2 * m] = h[m] / n / vol;
+    out[2 * m + 1] = std::sqrt(h[5 + m] / (n - 1.0) / vol);
+  }
+  out[8] = vol;
   return CG_OK;
 }
 

@@ -52,7 +52,8 @@ struct StagePtrs {
   double* fp_out;        // flux primitives of the output state
   unsigned* status;      // error flags (bit 0: NaN in DIFFphi, bit 1: non-finite field)
   const double* kavg;    // device-side K_avg of a^n, or null (bssn.cc:168)
-  double* cvals;         // constraint mode: per-point value and scaled value of H, M, G, A, S (10 arrays)
+  double* cvals;         // constraint mode: per-point value and scaled value of H, M, G, A, S (10 arrays),
+                         // then the Ricci scalar and DIFFr (arrays 10, 11)
   double* cpart;         // constraint mode: kCPart partial results per CTA
 };
 
@@ -901,6 +902,11 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
         P.cvals[(size_t)(2 * m) * N + c] = v[m];
         P.cvals[(size_t)(2 * m + 1) * N + c] = sd;
       }
+    }
+    if (live) {
+      // ricci_a (bssn.cc:663) and DIFFr_a at this point, for io_bssn_dump_statistics
+      P.cvals[(size_t)10 * N + c] = ricci;
+      P.cvals[(size_t)11 * N + c] = S(S_SRC + Q_R);
     }
     q[15] = live ? v[0] * v[0] * dx * dx * dx : 0.0;
     q[16] = live ? v[1] * v[1] * dx * dx * dx : 0.0;

@@ -144,6 +144,14 @@ class Evolution:
         self._check(self.L.cg_constraints(self.ctx, box, *(_dptr(arrs[k]) for k in "HMGAS")))
         return arrs
 
+    def field_statistics(self, box: int = 0) -> np.ndarray:
+        """io_bssn_dump_statistics columns of the current state (between steps):
+        volume-weighted mean and stdev of DIFFphi, DIFFK, DIFFr, ricci, then the
+        volume average."""
+        out = np.zeros(9)
+        self._check(self.L.cg_field_statistics(self.ctx, box, _dptr(out), out.size))
+        return out
+
     def synchronize(self) -> None:
         self._check(self.L.cg_synchronize(self.ctx))
 

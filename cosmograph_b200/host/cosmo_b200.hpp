@@ -145,6 +145,9 @@ class BSSN {
 
   // statistics of the current state (bssn.cc:965-1071): H[8], M[8], G/A/S[7]
   void setConstraintCalcs(real_t H[8], real_t M[8], real_t G[7], real_t A[7], real_t S[7]);
+  // the columns of io_bssn_dump_statistics (IO/io.cc:8-14, 386-403): volume-
+  // weighted mean and stdev of DIFFphi, DIFFK, DIFFr, ricci; volume average
+  void fieldStatistics(real_t out[9]);
 
   // fields["DIFFphi_a"], fields["D_p"], ... (bssn.cc:30-39)
   map_t fields;

@@ -328,6 +328,8 @@ void BSSN::setConstraintCalcs(real_t H[8], real_t M[8], real_t G[7], real_t A[7]
   check(cg_constraints(ctx(), 0, H, M, G, A, S), "setConstraintCalcs");
 }
 
+void BSSN::fieldStatistics(real_t out[9]) { check(cg_field_statistics(ctx(), 0, out, 9), "fieldStatistics"); }
+
 bool BSSN::nan_seen() {
   if (!c) return false;
   const int rc = cg_synchronize(c);
@@ -597,6 +599,21 @@ void CosmoSim::outputCommon() {
       row += "\n";
       gzwrite(f, row.data(), (unsigned)row.size());
       gzclose(f);
+    }
+    // field statistics (IO/io.cc:378-403): DETAILS of DIFFphi, DIFFK, DIFFr,
+    // ricci, then the volume average
+    const std::string fs = iodata->dir() + (*cfg)["dump_file"] + ".dat.gz";
+    gzFile g = gzopen(fs.c_str(), "ab");
+    if (!g) {
+      iodata->log("Error opening file: " + fs);
+    } else {
+      real_t st[9];
+      bssnSim->fieldStatistics(st);
+      std::string row;
+      for (double v : st) row += fmt15(v) + "\t";
+      row += "\n";
+      gzwrite(g, row.data(), (unsigned)row.size());
+      gzclose(g);
     }
   }
 }

@@ -271,6 +271,15 @@ int cg_step_count(cg_ctx *ctx, int box, int64_t *steps);
  * Synchronous. */
 int cg_constraints(cg_ctx *ctx, int box, double *H, double *M, double *G, double *A, double *S);
 
+/* Field statistics of one box between steps, the columns of the reference's
+ * "<dump_file>.dat.gz" (io_bssn_dump_statistics, IO/io.cc:8-14, 386-403): out
+ * = {avg, stdev} of DIFFphi, DIFFK, DIFFr (the density source) and the Ricci
+ * scalar (ricci_a, bssn.cc:663), each volume-weighted by exp(6 (DIFFphi +
+ * phi_FRW)) (conformal_average / conformal_standard_deviation, utils/math.h:
+ * 1403-1470), then volume_average(DIFFphi) (math.h:1382-1393); n_out >= 9.
+ * Same state and sources as cg_constraints.  Synchronous. */
+int cg_field_statistics(cg_ctx *ctx, int box, double *out, int n_out);
+
 /* Volume-weighted grid average of a device array, the reference's
  * conformal_average (utils/math.h:1403-1415) used by BSSN::setExtraFieldData
  * (components/bssn/bssn.cc:165-170):

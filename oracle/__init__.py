@@ -70,13 +70,13 @@ _lib = None
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
-            build_lib()
+        build_lib()  # no-op when the library is newer than its sources
         L = ctypes.CDLL(str(LIB_PATH))
         dp = ctypes.POINTER(ctypes.c_double)
         L.cgo_evolve.argtypes = [ctypes.POINTER(CgoParams), dp, ctypes.c_int, dp]
         L.cgo_rhs.argtypes = [ctypes.POINTER(CgoParams), dp, dp]
         L.cgo_constraints.argtypes = [ctypes.POINTER(CgoParams), dp, dp, dp, dp, dp, dp]
+        L.cgo_field_statistics.argtypes = [ctypes.POINTER(CgoParams), dp, dp]
         L.cgo_frw_evolve.argtypes = [dp, dp, ctypes.c_int, ctypes.c_double, ctypes.c_int]
         L.cgo_frw_evolve.restype = None
         L.cgo_set_threads.argtypes = [ctypes.c_int]
@@ -149,6 +149,20 @@ def constraints(state, order: int, **kw) -> dict:
     if rc != 0:
         raise RuntimeError(f"cgo_constraints failed: {rc}")
     return {"H": H, "M": M, "G": G, "A": A, "S": S}
+
+
+def field_statistics(state, order: int, **kw) -> np.ndarray:
+    """io_bssn_dump_statistics columns after the step initialisation:
+    volume-weighted mean and stdev of DIFFphi, DIFFK, DIFFr, ricci; volume
+    average (cgo_field_statistics)."""
+    L = lib()
+    p = make_params(state, order, **kw)
+    f = np.ascontiguousarray(state.fields, dtype=np.float64)
+    out = np.zeros(9)
+    rc = L.cgo_field_statistics(ctypes.byref(p), _ptr(f), _ptr(out))
+    if rc != 0:
+        raise RuntimeError(f"cgo_field_statistics failed: {rc}")
+    return out
 
 
 def frw_evolve(phi: float, K: float, fluids, h: float, steps: int):

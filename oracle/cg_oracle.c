@@ -995,6 +995,53 @@ static void momentum(const sim_t *s, long i, long j, long k, const bd_t *bd, int
                  fabs(2.0 / 3.0 * 2.0 * theta_d) + 6.0 * fabs(t6) + fabs(tD));
 }
 
+/* io_bssn_dump_statistics (IO/io.cc:8-14, 386-403) after the step
+ * initialisation: volume-weighted mean and standard deviation of DIFFphi,
+ * DIFFK, DIFFr and ricci (conformal_average / conformal_standard_deviation,
+ * utils/math.h:1403-1470, weights exp(6 (DIFFphi + phi_FRW))), then
+ * volume_average (math.h:1382-1393).  ricci as set_bd_values computes it for
+ * prepBSSNOutput (sims/sim.cc:214-225). */
+int cgo_field_statistics(const cgo_params *p, const double *fields, double *out) {
+  sim_t s;
+  int rc = sim_init(&s, p);
+  if (rc) {
+    sim_free(&s);
+    return rc;
+  }
+  memcpy(s.reg_p, fields, sizeof(double) * s.nf * s.pts);
+  step_init(&s);
+  const long N = s.pts;
+  double *ricci = (double *)malloc(sizeof(double) * N);
+  long ii;
+#pragma omp parallel for schedule(static)
+  for (ii = 0; ii < s.nx; ++ii) {
+    bd_t bd;
+    for (long j = 0; j < s.ny; ++j)
+      for (long k = 0; k < s.nz; ++k) {
+        set_bd(&s, ii, j, k, &bd);
+        ricci[IDX(&s, ii, j, k)] = bd.ricci;
+      }
+  }
+  const double *f[4] = {s.reg_a + F_PHI * N, s.reg_a + F_K * N, s.src + Q_R * N, ricci};
+  const double *phi = s.reg_a + F_PHI * N;
+  double vol = 0.0;
+  for (long q = 0; q < N; ++q) vol += exp(6.0 * (phi[q] + s.frw_phi));
+  vol /= N;
+  for (int m = 0; m < 4; ++m) {
+    double sum = 0.0;
+    for (long q = 0; q < N; ++q) sum += exp(6.0 * (phi[q] + s.frw_phi)) * f[m][q];
+    const double avg = sum / N / vol;
+    double var = 0.0;
+    for (long q = 0; q < N; ++q) var += exp(6.0 * (phi[q] + s.frw_phi)) * PW2(avg - f[m][q]);
+    out[2 * m] = avg;
+    out[2 * m + 1] = sqrt(var / (N - 1) / vol);
+  }
+  out[8] = vol;
+  free(ricci);
+  sim_free(&s);
+  return 0;
+}
+
 int cgo_constraints(const cgo_params *p, const double *fields, double *Hv, double *Mv, double *Gv, double *Av,
                     double *Sv) {
   sim_t s;

@@ -75,6 +75,11 @@ int cgo_evolve(const cgo_params *p, double *fields, int steps, double *frw_out);
  * rhs_out receives the "_c" register of every field (nfields*N^3). */
 int cgo_rhs(const cgo_params *p, const double *fields, double *rhs_out);
 
+/* io_bssn_dump_statistics columns (IO/io.cc:8-14, 386-403) after the step
+ * initialisation: {avg, stdev} of DIFFphi, DIFFK, DIFFr, ricci (volume
+ * weighted), then the volume average; out[9]. */
+int cgo_field_statistics(const cgo_params *p, const double *fields, double *out);
+
 /* Step initialisation, then the constraint statistics of
  * BSSN::setConstraintCalcs (bssn.cc:965-1071): H[8], M[8], G[7], A[7], S[7]. */
 int cgo_constraints(const cgo_params *p, const double *fields, double *H,

@@ -19,7 +19,12 @@
  *                        RKEvolve, write every field's "_c" register (the RHS)
  *          constraints : step initialisation, then BSSN::setConstraintCalcs
  *                        (components/bssn/bssn.cc:965-1071); write the H, M,
- *                        G, A, S statistics as text to <out>
+ *                        G, A, S statistics as text to <out>, and the field
+ *                        statistics of io_bssn_dump_statistics (IO/io.cc:8-14,
+ *                        386-403: conformal average and standard deviation of
+ *                        DIFFphi, DIFFK, DIFFr, ricci after the
+ *                        set_bd_values sweep of prepBSSNOutput, sims/sim.cc:
+ *                        214-225; volume average) as the row STATS
  * The last stdout line is "CGRESULT {json}" with the timing of the step loop.
  */
 #include "cosmo_includes.h"
@@ -29,6 +34,7 @@
 #include "components/dust_fluid/dust.h"
 #include "components/scalar/scalar.h"
 #include "components/Lambda/lambda.h"
+#include "utils/math.h"
 #include "cg_state.h"
 
 #include <time.h>
@@ -232,6 +238,26 @@ int main(int argc, char **argv) {
     row("G", G, 7);
     row("A", A, 7);
     row("S", S, 7);
+    // CosmoSim::prepBSSNOutput: ricci_a at every point
+    {
+      idx_t i, j, k;
+#pragma omp parallel for default(shared) private(i, j, k)
+      LOOP3(i, j, k) {
+        BSSNData b_data = {0};
+        sim.bssn->set_bd_values(i, j, k, &b_data);
+      }
+    }
+    map_t &F = sim.bssn->fields;
+    const real_t phi_frw = sim.bssn->frw->get_phi();
+    real_t st[9];
+    const char *names[4] = {"DIFFphi_a", "DIFFK_a", "DIFFr_a", "ricci_a"};
+    for (int q = 0; q < 4; ++q) {
+      arr_t &f = *F[names[q]];
+      st[2 * q] = conformal_average(f, *F["DIFFphi_a"], phi_frw);
+      st[2 * q + 1] = conformal_standard_deviation(f, *F["DIFFphi_a"], phi_frw, st[2 * q]);
+    }
+    st[8] = volume_average(*F["DIFFphi_a"], phi_frw);
+    row("STATS", st, 9);
     fclose(fo);
   } else {
     die("unknown mode");

@@ -6,7 +6,7 @@ by the reference's BSSN / Dust / Scalar / Lambda classes compiled unmodified
 Needs the reference checkout, so it runs only where that exists; the
 resulting .npz files are committed and need nothing at test time.
 
-Usage: python tests/golden/make_golden.py
+Usage: python tests/golden/make_golden.py [case ...]   (default: every case)
 """
 from __future__ import annotations
 
@@ -35,6 +35,7 @@ CASES = [
      {"lapse": "OnePlusLog", "a_adj_amp": 0.2, "k_damping_amp": 0.1}),
     ("dust_o4_rhs", S.DUST, (8, 10, 12), 4, 11, 2e-2, "rhs", 0, {"lapse": "Harmonic"}),
     ("dust_o8_constraints", S.DUST, (10, 9, 11), 8, 12, 2e-2, "constraints", 0, {"lapse": "Harmonic"}),
+    ("scalar_o6_constraints", S.SCALAR, (8, 8, 10), 6, 13, 2e-2, "constraints", 0, {"lapse": "Harmonic"}),
     ("sinusoid_o4", S.DUST, (16, 4, 4), 4, 0, 0.0, "evolve", 20, {"lapse": "Harmonic"}),
     ("grf_dust_o4", S.DUST, (8, 8, 8), 4, 9, 0.0, "evolve", 5, {"lapse": "Harmonic"}),
 ]
@@ -54,8 +55,12 @@ def main() -> int:
     if not build_ref.reference_available():
         print("reference checkout not found; nothing to do")
         return 1
-    index = {}
+    only = set(sys.argv[1:])
+    index_path = OUT / "index.json"
+    index = json.loads(index_path.read_text()) if only and index_path.exists() else {}
     for name, matter, shape, order, seed, amp, mode, steps, cfg in CASES:
+        if only and name not in only:
+            continue
         st = make_input(name, matter, shape, order, seed, amp)
         binp = build_ref.build(*shape, order, "strict")
         res, info = oracle.run_reference(binp, mode, st, steps=steps, threads=1, **cfg)
@@ -71,7 +76,7 @@ def main() -> int:
                        "steps": steps, "config": cfg, "generator": "reference sources, strict build",
                        "binary": binp.name}
         print(name, mode, info)
-    (OUT / "index.json").write_text(json.dumps(index, indent=1, sort_keys=True) + "\n")
+    index_path.write_text(json.dumps(index, indent=1, sort_keys=True) + "\n")
     return 0
 
 

@@ -26,12 +26,32 @@ def assert_close(got, ref, tol):
         assert rel.max() <= tol, (c, got[c], ref[c])
 
 
-def test_constraints_match_reference_fixture():
-    inp, _, ref, meta = load_golden("dust_o8_constraints")
+@pytest.mark.parametrize("name", ["dust_o8_constraints", "scalar_o6_constraints"])
+def test_constraints_match_reference_fixture(name):
+    inp, _, ref, meta = load_golden(name)
     with Evolution(inp, BoxConfig(order=meta["order"], **meta["config"])) as ev:
         got = ev.constraints(0)
     # fixed-order GPU reductions vs OpenMP reductions: last-bits differences
     assert_close(got, ref, 1e-11)
+
+
+@pytest.mark.parametrize("name", ["dust_o8_constraints", "scalar_o6_constraints"])
+def test_field_statistics_match_reference_fixture(name):
+    """The io_bssn_dump_statistics columns (volume-weighted mean and stdev of
+    DIFFphi, DIFFK, DIFFr, ricci; volume average) against the reference's
+    own functions on the same state (STATS row of the fixture)."""
+    inp, _, ref, meta = load_golden(name)
+    with Evolution(inp, BoxConfig(order=meta["order"], **meta["config"])) as ev:
+        got = ev.field_statistics(0)
+        again = ev.field_statistics(0)
+        ev.step(1)
+        after = ev.field_statistics(0)
+    want = ref["STATS"]
+    rel = np.abs(got - want) / np.abs(want)
+    print(name, "field statistics, max relative error", rel.max())
+    assert rel.max() < 1e-11, (got, want)
+    assert np.array_equal(got, again)  # deterministic reductions
+    assert np.all(np.isfinite(after)) and not np.array_equal(after, got)
 
 
 @pytest.mark.parametrize("matter,shape,order", [

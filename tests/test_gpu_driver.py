@@ -47,9 +47,11 @@ def test_dust_run_matches_python_front_end(tmp_path):
 
     h = rows(tmp_path / "out" / "H_violations.dat.gz")
     m = rows(tmp_path / "out" / "M_violations.dat.gz")
+    fs = rows(tmp_path / "out" / "calculated.dat.gz")
     assert len(h) == 2 and len(m) == 2 and all(len(r) == 5 for r in h)
+    assert len(fs) == 2 and all(len(r) == 9 for r in fs)
     with Evolution(st, BoxConfig(order=4, lapse="Harmonic")) as ev:
-        for row_h, row_m, steps in zip(h, m, (0, 5)):
+        for row_h, row_m, row_s, steps in zip(h, m, fs, (0, 5)):
             if steps:
                 ev.step(steps)
             c = ev.constraints(0)
@@ -57,6 +59,7 @@ def test_dust_run_matches_python_front_end(tmp_path):
             want_m = [c["M"][4], c["M"][5], c["M"][6], c["M"][2], c["M"][7]]
             np.testing.assert_allclose(row_h, want_h, rtol=1e-14, atol=0)
             np.testing.assert_allclose(row_m, want_m, rtol=1e-14, atol=0)
+            np.testing.assert_allclose(row_s, ev.field_statistics(0), rtol=1e-14, atol=0)
     frw = rows(tmp_path / "out" / "calculated.frwdat.gz")
     assert len(frw) == 2 and frw[0][0] == st.frw_phi
     log = (tmp_path / "out" / "log.txt").read_text()
