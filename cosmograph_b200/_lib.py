@@ -33,7 +33,7 @@ EXPORTS = (
     "cg_num_fields", "cg_field_name", "cg_upload_state", "cg_download_state",
     "cg_upload_state_async", "cg_download_state_async", "cg_exchange_state_async", "cg_prefetch_state_async",
     "cg_upload_field", "cg_download_field",
-    "cg_device_register", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
+    "cg_device_register", "cg_substep_input", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
     "cg_status", "cg_frw_state", "cg_step_count", "cg_last_error", "cg_version",
     "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints", "cg_field_statistics",
     "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust",
@@ -47,7 +47,7 @@ class BoxDesc(ctypes.Structure):
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
         ("stencil_order", ctypes.c_int), ("matter", ctypes.c_int), ("lapse", ctypes.c_int),
         ("precision", ctypes.c_int), ("normalize_metric", ctypes.c_int),
-        ("potential", ctypes.c_int), ("reserved0", ctypes.c_int),
+        ("potential", ctypes.c_int), ("x_ghost", ctypes.c_int),
         ("dx", ctypes.c_double), ("dt", ctypes.c_double), ("lam", ctypes.c_double),
         ("ko_coeff", ctypes.c_double), ("a_adj_amp", ctypes.c_double),
         ("k_damping_amp", ctypes.c_double), ("gd_c", ctypes.c_double),
@@ -89,6 +89,7 @@ def load() -> ctypes.CDLL:
         "cg_upload_field": (i, [vp, i, i, ctypes.c_char, dp, sz]),
         "cg_download_field": (i, [vp, i, i, ctypes.c_char, dp, sz]),
         "cg_device_register": (i, [vp, i, ctypes.c_char, ctypes.POINTER(dp)]),
+        "cg_substep_input": (i, [vp, i, ctypes.POINTER(dp), ctypes.POINTER(dp)]),
         "cg_step_init": (i, [vp]),
         "cg_rk_stage": (i, [vp, i]),
         "cg_step": (i, [vp, i]),

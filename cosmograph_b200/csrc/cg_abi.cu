@@ -261,8 +261,10 @@ __global__ void field_sums_kernel(const double* f0, const double* f1, const doub
 
 // Second pass of BSSN::setConstraintCalcs (bssn.cc:1026-1054): squared
 // deviations from the means of pass 1 (r1: sums of value in [0,5), of scaled
-// value in [10,15)), per CTA, 10 partial sums.
-__global__ void constraint_stdev_kernel(const double* cvals, int n, const double* r1, double* part) {
+// value in [10,15)), per CTA, 10 partial sums, over the n points from index
+// off of arrays `stride` apart.
+__global__ void constraint_stdev_kernel(const double* cvals, size_t stride, int off, int n, const double* r1,
+                                        double* part) {
   __shared__ double s[10][256];
   double acc[10];
   double mean[10];
@@ -273,7 +275,7 @@ __global__ void constraint_stdev_kernel(const double* cvals, int n, const double
   for (int m = 0; m < 10; ++m) acc[m] = 0.0;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
     for (int m = 0; m < 10; ++m) {
-      const double d = cvals[(size_t)m * n + q] - mean[m];
+      const double d = cvals[(size_t)m * stride + off + q] - mean[m];
       acc[m] += d * d;
     }
   for (int m = 0; m < 10; ++m) s[m][threadIdx.x] = acc[m];
@@ -593,6 +595,29 @@ int validate(const cg_box_desc& d, std::string& why) {
   }
   if (d.nfluids < 0 || d.nfluids > 4) { why = "at most 4 FRW fluids"; return CG_ERR_INVALID; }
   if (!(d.dx > 0.0) || !std::isfinite(d.dt)) { why = "dx must be positive and dt finite"; return CG_ERR_INVALID; }
+  if (d.x_ghost != 0) {
+    // an x-slab: interior bricks only, ghost planes refreshed by the caller
+    const int g = d.x_ghost;
+    const int reach = d.ko_coeff != 0.0 && (d.stencil_order == 2 || d.stencil_order == 8)
+                          ? (d.stencil_order == 8 ? 5 : 2)
+                          : d.stencil_order / 2;
+    if (g < 0 || g % 4 != 0 || g < reach) {
+      why = "x_ghost must be a multiple of 4 and at least the stencil (and Kreiss-Oliger) radius";
+      return CG_ERR_INVALID;
+    }
+    if (d.nx - 2 * g < 4 || (d.nx - 2 * g) % 4 != 0) {
+      why = "an x-slab needs nx - 2 x_ghost interior planes, a positive multiple of 4";
+      return CG_ERR_INVALID;
+    }
+    if (d.precision == CG_PREC_MIXED) {
+      why = "x-slabs (x_ghost > 0) are FP64 only";
+      return CG_ERR_INVALID;
+    }
+    if (lapse_needs_kavg(d.lapse)) {
+      why = "x-slabs (x_ghost > 0) support lapses without the grid average of K";
+      return CG_ERR_INVALID;
+    }
+  }
   return CG_OK;
 }
 
@@ -693,6 +718,7 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
     const cg_box_desc& d = b.desc;
     b.variant = d.precision == CG_PREC_FP64_FMA ? cg::kFast : cg::kExact;
     b.dev.nx = d.nx;
+    b.dev.xg = d.x_ghost;
     b.dev.ny = d.ny;
     b.dev.nz = d.nz;
     b.dev.pts = d.nx * d.ny * d.nz;
@@ -1006,6 +1032,19 @@ int cg_download_field(cg_ctx* ctx, int box, int field, char reg, double* host, s
   return field_copy(ctx, box, field, reg, host, n, false);
 }
 
+int cg_substep_input(cg_ctx* ctx, int box, double** input, double** flux) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  if (!input) return fail(ctx, CG_ERR_INVALID, "input is null");
+  Box& b = ctx->boxes[box];
+  if (b.mixed) return fail(ctx, CG_ERR_INVALID, "the substep input of an FP64 box only");
+  if (b.stage_next == 0) return fail(ctx, CG_ERR_STATE, "the substep input exists after cg_step_init");
+  const bool even = b.stage_next == 2 || b.stage_next == 4;
+  *input = even ? b.dev.Y : b.dev.X;
+  if (flux) *flux = b.desc.matter == CG_MATTER_DUST ? (even ? b.dev.FP1 : b.dev.FP0) : nullptr;
+  return CG_OK;
+}
+
 int cg_device_register(cg_ctx* ctx, int box, char reg, double** dptr) {
   int rc = check_box(ctx, box);
   if (rc) return rc;
@@ -1109,13 +1148,13 @@ int ensure_groups(cg_ctx* ctx) {
     g.matter = ba.desc.matter;
     g.members.push_back((int)a);
     used[a] = true;
-    // boxes with Kreiss-Oliger dissipation keep their own launches
-    for (size_t b = a + 1; ba.desc.ko_coeff == 0.0 && b < ctx->boxes.size() &&
+    // boxes with Kreiss-Oliger dissipation and x-slabs keep their own launches
+    for (size_t b = a + 1; ba.desc.ko_coeff == 0.0 && ba.desc.x_ghost == 0 && b < ctx->boxes.size() &&
                            g.members.size() < (size_t)cg::kMaxGroupBoxes;
          ++b) {
       const Box& bb = ctx->boxes[b];
       if (used[b] || bb.mixed != g.mixed || bb.variant != g.variant || bb.desc.stencil_order != g.order ||
-          bb.desc.matter != g.matter || bb.desc.ko_coeff != 0.0)
+          bb.desc.matter != g.matter || bb.desc.ko_coeff != 0.0 || bb.desc.x_ghost != 0)
         continue;
       g.members.push_back((int)b);
       used[b] = true;
@@ -1331,8 +1370,12 @@ int cg_rk_stage(cg_ctx* ctx, int n) {
 int cg_step(cg_ctx* ctx, int nsteps) {
   if (!ctx) return CG_ERR_INVALID;
   if (nsteps < 0) return fail(ctx, CG_ERR_INVALID, "nsteps must be >= 0");
-  for (Box& b : ctx->boxes)
+  for (Box& b : ctx->boxes) {
     if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "a step is in progress; finish it with cg_rk_stage");
+    if (b.desc.x_ghost != 0)
+      return fail(ctx, CG_ERR_STATE,
+                  "x-slab boxes step through cg_step_init / cg_rk_stage with a halo exchange before every substep");
+  }
   if (nsteps == 0) return CG_OK;
   for (Box& b : ctx->boxes)
     if (b.stage_next == 0) {
@@ -1475,6 +1518,7 @@ int cg_step_count(cg_ctx* ctx, int box, int64_t* steps) {
 struct CScratch {
   double *cvals, *part1, *part2, *r1, *r2, *wpart, *wres;
   int n, nblk1, nblk2;
+  int off, nin;  // the points the kernels update: from index off, nin of them (x-slabs skip ghost planes)
 };
 
 static CScratch cscratch_layout(const Box& b) {
@@ -1489,6 +1533,8 @@ static CScratch cscratch_layout(const Box& b) {
   c.r2 = c.r1 + 27;
   c.wpart = c.r2 + 10;
   c.wres = c.wpart + (size_t)9 * c.nblk2;
+  c.off = b.dev.xg * b.dev.ny * b.dev.nz;
+  c.nin = (b.dev.nx - 2 * b.dev.xg) * b.dev.ny * b.dev.nz;
   return c;
 }
 
@@ -1521,7 +1567,7 @@ static int constraint_pass(cg_ctx* ctx, Box& b, cg::BoxDev& dev, double** xtmp) 
   cudaError_t ec = cg::exact::launch_constraints(dev, bg, c.cvals, c.part1, ctx->stream);
   if (ec != cudaSuccess) return cuda_fail(ctx, ec, "constraints");
   part_final_kernel<<<1, 256, 0, ctx->stream>>>(c.part1, c.nblk1, 27, 17, c.r1);
-  constraint_stdev_kernel<<<c.nblk2, 256, 0, ctx->stream>>>(c.cvals, n, c.r1, c.part2);
+  constraint_stdev_kernel<<<c.nblk2, 256, 0, ctx->stream>>>(c.cvals, (size_t)n, c.off, c.nin, c.r1, c.part2);
   part_final_kernel<<<1, 256, 0, ctx->stream>>>(c.part2, c.nblk2, 10, 10, c.r2);
   CG_CUDA(ctx, cudaGetLastError());
   return CG_OK;
@@ -1540,7 +1586,7 @@ int cg_constraints(cg_ctx* ctx, int box, double* H, double* M, double* G, double
     return rc;
   }
   const CScratch c = cscratch_layout(b);
-  const int n = c.n;
+  const int n = c.nin;  // statistics over the updated points
   double h1[27], h2[10];
   CG_CUDA(ctx, cudaMemcpyAsync(h1, c.r1, sizeof(h1), cudaMemcpyDeviceToHost, ctx->stream));
   CG_CUDA(ctx, cudaMemcpyAsync(h2, c.r2, sizeof(h2), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1576,11 +1622,11 @@ int cg_field_statistics(cg_ctx* ctx, int box, double* out, int n_out) {
     return rc;
   }
   const CScratch c = cscratch_layout(b);
-  const int n = c.n;
-  const double* phi = dev.X + (size_t)cg::F_PHI * n;
-  const double* K = dev.X + (size_t)cg::F_K * n;
-  const double* ricci = c.cvals + (size_t)10 * n;
-  const double* rho = c.cvals + (size_t)11 * n;
+  const int N = c.n, n = c.nin;  // statistics over the updated points
+  const double* phi = dev.X + (size_t)cg::F_PHI * N + c.off;
+  const double* K = dev.X + (size_t)cg::F_K * N + c.off;
+  const double* ricci = c.cvals + (size_t)10 * N + c.off;
+  const double* rho = c.cvals + (size_t)11 * N + c.off;
   const double phi_frw = b.frw.get_phi;
   wstats_sum_kernel<<<c.nblk2, 256, 0, ctx->stream>>>(phi, K, rho, ricci, phi, n, phi_frw, c.wpart);
   part_final_kernel<<<1, 256, 0, ctx->stream>>>(c.wpart, c.nblk2, 5, 5, c.wres);

@@ -20,6 +20,7 @@ struct BoxDev {
   int maps;                // the maps are encoded
   int tma;                 // interior tiles are copied by TMA (maps != 0 and the option on)
   int nx, ny, nz, pts, nfields, order, matter;
+  int xg;  // ghost planes on each x face (0: periodic box)
   Physics ph;
   double* P;    // the reference's _p register (state at the start of a step)
   double* F;    // the reference's _f register (RK accumulator)

@@ -60,6 +60,7 @@ struct StagePtrs {
 struct BoxGeom {
   int nx, ny, nz;
   int pts;
+  int bx0;  // first x brick of the launch (x-slab boxes skip their ghost planes)
 };
 
 constexpr unsigned kStatusNaN = 1u;
@@ -1081,7 +1082,7 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage, const 
   init_tile_barriers(bar, use_tma != 0);
   unsigned phase = 0;
   bool tma_ok = true;
-  stage_body<O, MATTER, MODE, KO>(geo, ph, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x,
+  stage_body<O, MATTER, MODE, KO>(geo, ph, bg, P, stage, blockIdx.z + geo.bx0, blockIdx.y, blockIdx.x,
                                   blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
                                   use_tma ? &tmap : nullptr, bar, phase, tma_ok);
 }
@@ -1121,7 +1122,7 @@ stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
     __syncthreads();
     const int l = w - sb.first;
     const int cz = l % sb.nbz, cy = (l / sb.nbz) % sb.nby, cx = l / (sb.nbz * sb.nby);
-    const BoxGeom geo{sb.nx, sb.ny, sb.nz, sb.pts};
+    const BoxGeom geo{sb.nx, sb.ny, sb.nz, sb.pts, 0};
     stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0, stm, bar, phase, tma_ok);
   }
 }

@@ -62,8 +62,9 @@ dim3 grid_dims(const BoxDev& b) {
   return dim3((b.nz + 31) / 32, (b.ny + 3) / 4, b.nx);
 }
 dim3 stage_block() { return dim3(kBZ, kBY, kBX); }
+// bricks of the points a substep updates: x-slab boxes skip their ghost planes
 dim3 stage_grid(const BoxDev& b) {
-  return dim3((b.nz + kBZ - 1) / kBZ, (b.ny + kBY - 1) / kBY, (b.nx + kBX - 1) / kBX);
+  return dim3((b.nz + kBZ - 1) / kBZ, (b.ny + kBY - 1) / kBY, (b.nx - 2 * b.xg + kBX - 1) / kBX);
 }
 
 template <int O, int M>
@@ -79,7 +80,7 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
     case 3: P.in = b.X; P.prev = b.Y; P.out = b.Y; P.fp_in = b.FP0; P.fp_out = b.FP1; break;
     default: P.in = b.Y; P.prev = b.X; P.out = b.P; P.norm = b.X; P.fp_in = b.FP1; P.fp_out = b.FP0; break;
   }
-  BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
+  BoxGeom geo{b.nx, b.ny, b.nz, b.pts, b.xg / kBX};
   const CUtensorMap& map = (stage == 1 || stage == 3) ? b.mapX : b.mapY;  // the substep's input
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
   if constexpr (O == 2 || O == 8) {
@@ -116,7 +117,7 @@ cudaError_t go_constraints(const BoxDev& b, const StageBg& bg, double* cvals, do
   P.kavg = b.kavg;
   P.cvals = cvals;
   P.cpart = cpart;
-  BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
+  BoxGeom geo{b.nx, b.ny, b.nz, b.pts, b.xg / kBX};
   constexpr size_t smem = stage_smem<O, M, kConstraints>();
   static bool configured = false;
   if (!configured) {
@@ -255,7 +256,7 @@ int constraint_blocks(const BoxDev& b) {
 }
 
 cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st) {
-  BoxGeom geo{b.nx, b.ny, b.nz, b.pts};
+  BoxGeom geo{b.nx, b.ny, b.nz, b.pts, b.xg / kBX};
   switch (b.matter) {
     case kDust: init_kernel<kDust><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
     case kScalar: init_kernel<kScalar><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;

@@ -33,6 +33,7 @@ class BoxConfig:
     gd_c: float = 1.0
     dw_mu_l: float = 0.0
     dw_p: float = 0.0
+    x_ghost: int = 0  # > 0: the box is an x-slab with this many ghost planes per face (cosmograph_b200.slab)
 
 
 def make_desc(state: BoxState, cfg: BoxConfig) -> _lib.BoxDesc:
@@ -48,6 +49,7 @@ def make_desc(state: BoxState, cfg: BoxConfig) -> _lib.BoxDesc:
     d.ko_coeff, d.a_adj_amp, d.k_damping_amp = cfg.ko_coeff, cfg.a_adj_amp, cfg.k_damping_amp
     d.gd_c, d.dw_mu_l, d.dw_p = cfg.gd_c, cfg.dw_mu_l, cfg.dw_p
     d.pot_const, d.pot_mass = cfg.pot_const, cfg.pot_mass
+    d.x_ghost = cfg.x_ghost
     d.frw_phi, d.frw_K = state.frw_phi, state.frw_K
     d.nfluids = len(state.fluids)
     for n, (rho, w) in enumerate(state.fluids):

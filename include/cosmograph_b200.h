@@ -90,7 +90,15 @@ typedef struct {
   int precision;           /* CG_PREC_*                                          */
   int normalize_metric;    /* config normalize_metric (default 1)                */
   int potential;           /* CG_POT_* (scalar matter only)                      */
-  int reserved0;
+  int x_ghost;             /* 0: periodic box.  g > 0: an x-slab of a larger
+                              box; its first and last g planes are ghost planes
+                              that the caller refreshes from the neighbouring
+                              slabs before every substep (cg_substep_input);
+                              kernels update the nx - 2g interior planes only.
+                              FP64 arithmetic, lapses without K_avg; g a
+                              multiple of 4, >= the stencil radius (and the
+                              Kreiss-Oliger radius), nx - 2g a positive
+                              multiple of 4.                                   */
   double dx, dt;           /* grid spacing and time step                          */
   double lambda;           /* rho_Lambda (Lambda::setLambda)                      */
   double ko_coeff;         /* KO_damping_coefficient (orders 2 and 8; FP64 only)   */
@@ -259,6 +267,17 @@ int cg_frw_state(cg_ctx *ctx, int box, double *out, int n);
 
 /* Steps completed by a box since creation or the last upload. */
 int cg_step_count(cg_ctx *ctx, int box, int64_t *steps);
+
+/* Device arrays that the next cg_rk_stage of an FP64 box reads with
+ * stencils: the substep input (nfields arrays of nx*ny*nz doubles, field-major,
+ * x slowest) and, for dust, its flux primitives (7 arrays: alpha*D,
+ * alpha*S_1..3, v^1..3; NULL otherwise).  Valid after cg_step_init and after
+ * each cg_rk_stage, until the next one.  For an x-slab box (x_ghost = g) the
+ * caller refreshes planes [0, g) and [nx-g, nx) of every array from the
+ * neighbouring slabs' interior planes before each substep (and before
+ * cg_constraints / cg_field_statistics).  No reference counterpart: the
+ * reference evolves one box per process. */
+int cg_substep_input(cg_ctx *ctx, int box, double **input, double **flux);
 
 /* Constraint statistics of one box between steps (after cg_step_init or a
  * whole step), BSSN::setConstraintCalcs (components/bssn/bssn.cc:965-1071)

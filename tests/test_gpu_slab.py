@@ -1,0 +1,67 @@
+"""A box cut into x-slabs (x_ghost > 0), all slabs in one context on one GPU
+with the ghost planes refreshed by device copies before every substep, must
+evolve exactly as the undivided box: the assembled interiors equal the
+single-box run bit for bit (FP64; every point sees the same taps and the same
+arithmetic).  The exchange between GPUs uses the same planes
+(tests/test_slab.py checks it on CPU ranks)."""
+import numpy as np
+import pytest
+
+from cosmograph_b200 import ics, slab, state as S
+from cosmograph_b200.evolution import BoxConfig, Evolution, evolve
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("matter,order,nslabs,precision", [
+    (S.DUST, 4, 2, "fp64"), (S.DUST, 8, 4, "fp64"), (S.SCALAR, 6, 2, "fp64"),
+    (S.VACUUM, 2, 3, "fp64_fma"), (S.DUST, 8, 2, "fp64_fma"),
+])
+def test_slabs_evolve_like_the_whole_box(matter, order, nslabs, precision):
+    shape = (8 * nslabs, 20, 48)  # nz = 48: interior z bricks take the TMA path
+    st = ics.perturbed(shape, matter, seed=31 + order, amp=1e-3)
+    cfg = BoxConfig(order=order, precision=precision)
+    g = slab.ghost_width(order)
+    with slab.SlabEvolution(slab.split(st, nslabs, g), cfg, g) as se:
+        se.step(3)
+        se.ev.synchronize()
+        got = slab.assemble(se.download(), g)
+    want = evolve(st, 3, cfg)
+    assert np.array_equal(got.fields, want.fields)
+    assert got.frw_phi == want.frw_phi and got.frw_K == want.frw_K
+
+
+def test_slabs_with_kreiss_oliger():
+    st = ics.perturbed((32, 12, 16), S.DUST, seed=5, amp=1e-3)
+    cfg = BoxConfig(order=8, ko_coeff=0.05)
+    g = slab.ghost_width(8, ko=True)
+    with slab.SlabEvolution(slab.split(st, 2, g), cfg, g) as se:
+        se.step(2)
+        got = slab.assemble(se.download(), g)
+    assert np.array_equal(got.fields, evolve(st, 2, cfg).fields)
+
+
+def test_slab_constraints_cover_the_interior():
+    """Constraint statistics of one slab after a ghost refresh equal those of
+    the same planes inside the whole box: the means of the slab interiors
+    average to the box's mean."""
+    st = ics.perturbed((16, 16, 16), S.DUST, seed=8, amp=1e-3)
+    cfg = BoxConfig(order=4)
+    g = slab.ghost_width(4)
+    with slab.SlabEvolution(slab.split(st, 2, g), cfg, g) as se:
+        se.step(1)
+        se.refresh()
+        parts = [se.ev.constraints(b)["H"] for b in range(2)]
+    with Evolution(st, cfg) as ev:
+        ev.step(1)
+        whole = ev.constraints(0)["H"]
+    mean = 0.5 * (parts[0][0] + parts[1][0])
+    assert abs(mean - whole[0]) <= 1e-12 * max(abs(whole[0]), 1e-300) + 1e-18
+    assert max(parts[0][2], parts[1][2]) == pytest.approx(whole[2], rel=1e-13)
+
+
+def test_cg_step_refuses_slabs():
+    st = ics.perturbed((16, 8, 8), S.DUST, seed=2, amp=1e-3)
+    with Evolution(slab.split(st, 1, 4)[0], BoxConfig(order=4, x_ghost=4)) as ev:
+        with pytest.raises(RuntimeError, match="x-slab"):
+            ev.step(1)
