@@ -69,8 +69,9 @@ def parse():
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference CPU build (rank 0)")
     ap.add_argument("--ncu", action="store_true", help="short run for profiler capture (no JSON extras)")
     ap.add_argument("--variants", default="fp64_fma,mixed", help="comma list of extra precisions timed alongside")
-    ap.add_argument("--workload", choices=["box", "ensemble"], default="box",
-                    help="box: one 256^3 box per GPU; ensemble: 48 boxes of 32^3/64^3/96^3 split over the GPUs")
+    ap.add_argument("--workload", choices=["box", "ensemble", "slab"], default="box",
+                    help="box: one 256^3 box per GPU; ensemble: 48 boxes of 32^3/64^3/96^3 split over the GPUs; "
+                         "slab: one (256 N) x 256 x 256 box cut into N x-slabs with a ghost exchange per substep")
     return ap.parse_args()
 
 
@@ -369,6 +370,62 @@ def run_ensemble(a, world, rank, local):
     print(json.dumps(line))
 
 
+def run_slab(a, world, rank, local):
+    """One box of (n*world) x n x n points cut into `world` x-slabs, one per
+    rank, ghost planes exchanged before every substep (NCCL point-to-point;
+    on one GPU the periodic self-exchange).  The box is the n^3 GRF box
+    repeated along x, so every slab starts from the same n^3 state with its
+    own periodic planes as ghosts, as the undivided box would give it."""
+    import torch
+    import torch.distributed as dist
+
+    from cosmograph_b200 import slab
+    from cosmograph_b200.evolution import BoxConfig
+
+    n, g = a.n, slab.ghost_width(a.order)
+    mine = slab.split(make_state(n, seed=1, order=a.order), 1, g)[0]
+    halo = slab.DistHalo(g) if world > 1 else None
+    cfg = BoxConfig(order=a.order, lapse="Harmonic", precision=a.precision)
+    se = slab.SlabEvolution([mine], cfg, g, halo=halo)  # one rank: its own periodic planes as ghosts
+    for _ in range(max(a.warmup, 0)):
+        se.step(1)
+    se.ev.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(se.stream)
+        se.step(a.steps)
+        e1.record(se.stream)
+        torch.cuda.synchronize()
+    se.ev.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    pts = n ** 3
+    value = world * pts * a.steps / (ms / 1e3)
+    peak, peak_kind = measured_peaks()
+    achieved = algo_bytes(a.precision) * pts / 4 / (ms / a.steps / 4 / 1e3) / 1e9
+    se.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "grid-pt RK4 updates/s (BSSN+dust)", "value": value, "unit": "grid-pt RK4 updates/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"bssn_dust_{n * world}x{n}x{n}_o{a.order}_xslabs", "slab_planes": n,
+                       "ghost_planes": g, "stencil_order": a.order, "lapse": "Harmonic",
+                       "precision": a.precision, "parallelism": f"x-slabs x{world}, ghost exchange per substep",
+                       "l2": "inputs larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind},
+            "e2e": None, "gpu_launches": 4 * a.steps, "clocks": clk.summary(), "cpu_baseline": None,
+        }))
+
+
 def run_reference_arm(a, world, rank):
     """--impl reference: the reference's CPU implementation (oracle/_ref) of the
     same workload, all host threads, rank 0 only."""
@@ -437,8 +494,8 @@ def main():
         int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0)
     if a.impl == "reference":
         return run_reference_arm(a, world, rank)
-    if a.workload == "ensemble":
-        run_ensemble(a, world, rank, local)
+    if a.workload in ("ensemble", "slab"):
+        (run_ensemble if a.workload == "ensemble" else run_slab)(a, world, rank, local)
         if world > 1:
             import torch.distributed as dist
 
