@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--order", type=int, default=8)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp64_fma", "mixed"])
-    ap.add_argument("--e2e-steps", type=int, default=6)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference CPU build (rank 0)")
     ap.add_argument("--ncu", action="store_true", help="short run for profiler capture (no JSON extras)")
     ap.add_argument("--variants", default="fp64_fma,mixed", help="comma list of extra precisions timed alongside")
