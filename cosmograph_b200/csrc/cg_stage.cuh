@@ -304,12 +304,17 @@ __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N,
   const bool by_tma = tmap != nullptr;
   bool ok = true;
   tile::Loader<G, Brick, double> ld;
+  tile::AsyncLoader<G, Brick> ald;
   if (by_tma) {
     if (TWO) {
       tma::fence_proxy_async();  // this thread's shared-memory accesses come before the copy's writes
       __syncthreads();
       if (tid == 0) issue(0);
     }
+  } else if (TWO) {
+    // two buffers: cp.async copies of field it + 1 run while field it is differentiated
+    ald.init(tid, z0, nz);
+    ald.issue(tl, a + (size_t)PF::field(0) * N, rowoff);
   } else {
     ld.init(tid, z0, nz);
     ld.fetch(a + (size_t)PF::field(0) * N, rowoff);
@@ -328,6 +333,16 @@ __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N,
       b = TWO ? (it & 1) : 0;
       if (ok && !tma::wait(bar + b, (phase >> b) & 1u, kTmaWaitCycles64)) ok = false;
       phase ^= 1u << b;
+    } else if (TWO) {
+      __syncthreads();  // the buffer the next copies write has been read
+      if (it + 1 < PF::N) {
+        ald.issue((it + 1) & 1 ? tl2 : tl, a + (size_t)PF::field(it + 1) * N, rowoff);
+        tile::cp_async_wait<1>();  // this thread's copies of field it have landed
+      } else {
+        tile::cp_async_wait<0>();
+      }
+      __syncthreads();  // and every other thread's
+      b = it & 1;
     } else {
       __syncthreads();  // the previous tile has been read
       ld.store(tl);

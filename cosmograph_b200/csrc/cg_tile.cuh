@@ -16,7 +16,9 @@
 //         wavefront.
 //
 // The copy is software-pipelined by the caller: the next field's elements are
-// fetched into registers while the current tile is being read.
+// fetched into registers while the current tile is being read (Loader), or,
+// with a second tile buffer, copied by cp.async straight into it
+// (AsyncLoader).
 #pragma once
 
 namespace cg {
@@ -96,6 +98,38 @@ struct Loader {
       const int r = row0 + B::WARPS * G::RPP * q;
       if (zoff >= 0 && r < G::ROWS) tl[r * G::TZ + G::CO + col] = buf[q];
     }
+  }
+};
+
+// Asynchronous copy of one field's tile (cp.async, global to shared memory,
+// no register staging), with the lane/row mapping of Loader.  issue() starts
+// this thread's copies and commits them as one group; the caller waits for
+// its groups (cp_async_wait) and synchronises the CTA before reading.
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <class G, class B>
+struct AsyncLoader {
+  int row0, col, zoff;  // zoff < 0: lane without a column
+  __device__ __forceinline__ void init(int tid, int z0, int nz) {
+    const int warp = tid >> 5, lane = tid & 31;
+    const int sub = lane / G::TZU;
+    col = lane - sub * G::TZU;
+    row0 = warp * G::RPP + sub;
+    zoff = sub < G::RPP ? pmod(z0 - G::R + col, nz) : -1;
+  }
+  __device__ __forceinline__ void issue(double* tl, const double* __restrict__ f, const int* rowoff) const {
+#pragma unroll
+    for (int q = 0; q < G::NPW; ++q) {
+      const int r = row0 + B::WARPS * G::RPP * q;
+      if (zoff >= 0 && r < G::ROWS) cp_async(tl + r * G::TZ + G::CO + col, f + rowoff[r] + zoff);
+    }
+    cp_async_commit();
   }
 };
 
