@@ -97,6 +97,10 @@ struct Box {
   const double* pre_host = nullptr;
   size_t pre_count = 0;
   cudaEvent_t in_ready = nullptr, in_free = nullptr, out_ready = nullptr, out_free = nullptr;
+  // FP32-mixed background means set by the caller (cg_set_background) for
+  // the next initialisation instead of this box's own means (x-slabs of one box)
+  bool bg_set = false;
+  double bg_means[5] = {};
 };
 
 }  // namespace
@@ -427,31 +431,50 @@ size_t cscratch_doubles(const Box& b) {
   return 12 * n + 27 * nblk1 + 10 * nblk2 + 37 + 9 * nblk2 + 9;
 }
 
-int mixed_init(cg_ctx* ctx, Box& b) {
-  // background registers from the means of _p (K, phi, alpha, D)
-  const int n = b.dev.pts;
+// Sums over the updated points of _p of the fields with a uniform
+// background in the FP32-mixed form: K, phi, alpha, field 18 (D or the scalar
+// field) and field 19 (Pi); into h[5].  Synchronous.
+int background_sums(cg_ctx* ctx, Box& b, double h[5]) {
+  const int N = b.dev.pts;
+  const int off = b.dev.xg * b.dev.ny * b.dev.nz, n = (b.dev.nx - 2 * b.dev.xg) * b.dev.ny * b.dev.nz;
   const int nblk = std::min(1024, (n + 255) / 256);
   if (!b.cscratch) CG_CUDA(ctx, cudaMalloc(&b.cscratch, sizeof(double) * cscratch_doubles(b)));
   double* part = b.cscratch;
   double* res = part + 5 * (size_t)nblk;
-  const double* P = b.mdev.P;
+  const double* P = b.dev.P + off;
   const bool dust = b.desc.matter == CG_MATTER_DUST, scalar = b.desc.matter == CG_MATTER_SCALAR;
   // D (dust) or the scalar phi and Pi (fields 18, 19) have a background
-  field_sums_kernel<<<nblk, 256, 0, ctx->stream>>>(P + (size_t)cg::F_K * n, P + (size_t)cg::F_PHI * n,
-                                                   P + (size_t)cg::F_ALPHA * n,
-                                                   dust || scalar ? P + (size_t)18 * n : nullptr,
-                                                   scalar ? P + (size_t)19 * n : nullptr, n, part);
+  field_sums_kernel<<<nblk, 256, 0, ctx->stream>>>(P + (size_t)cg::F_K * N, P + (size_t)cg::F_PHI * N,
+                                                   P + (size_t)cg::F_ALPHA * N,
+                                                   dust || scalar ? P + (size_t)18 * N : nullptr,
+                                                   scalar ? P + (size_t)19 * N : nullptr, n, part);
   part_final_kernel<<<1, 256, 0, ctx->stream>>>(part, nblk, 5, 5, res);
   CG_CUDA(ctx, cudaGetLastError());
-  double h[5];
-  CG_CUDA(ctx, cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  CG_CUDA(ctx, cudaMemcpyAsync(h, res, sizeof(double) * 5, cudaMemcpyDeviceToHost, ctx->stream));
   CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return CG_OK;
+}
+
+int mixed_init(cg_ctx* ctx, Box& b) {
+  // background registers from the means of _p (K, phi, alpha, D), or the
+  // means the caller set for the whole decomposed box
+  const int n = (b.dev.nx - 2 * b.dev.xg) * b.dev.ny * b.dev.nz;
+  const bool dust = b.desc.matter == CG_MATTER_DUST, scalar = b.desc.matter == CG_MATTER_SCALAR;
+  double mean[5];
+  if (b.bg_set) {
+    for (int q = 0; q < 5; ++q) mean[q] = b.bg_means[q];
+  } else {
+    double h[5];
+    int rc = background_sums(ctx, b, h);
+    if (rc) return rc;
+    for (int q = 0; q < 5; ++q) mean[q] = h[q] / n;
+  }
   for (int f = 0; f < 23; ++f) b.bp[f] = b.ba[f] = b.bprev[f] = b.bf[f] = 0.0;
-  b.bp[cg::F_K] = h[0] / n;
-  b.bp[cg::F_PHI] = h[1] / n;
-  b.bp[cg::F_ALPHA] = h[2] / n;
-  if (dust || scalar) b.bp[18] = h[3] / n;
-  if (scalar) b.bp[19] = h[4] / n;
+  b.bp[cg::F_K] = mean[0];
+  b.bp[cg::F_PHI] = mean[1];
+  b.bp[cg::F_ALPHA] = mean[2];
+  if (dust || scalar) b.bp[18] = mean[3];
+  if (scalar) b.bp[19] = mean[4];
   for (int f = 0; f < 23; ++f) b.ba[f] = b.bprev[f] = b.bp[f];
   cg::mixed::Bg bg{};
   pack_bg(b.ba, bg.in);
@@ -607,10 +630,6 @@ int validate(const cg_box_desc& d, std::string& why) {
     }
     if (d.nx - 2 * g < 4 || (d.nx - 2 * g) % 4 != 0) {
       why = "an x-slab needs nx - 2 x_ghost interior planes, a positive multiple of 4";
-      return CG_ERR_INVALID;
-    }
-    if (d.precision == CG_PREC_MIXED) {
-      why = "x-slabs (x_ghost > 0) are FP64 only";
       return CG_ERR_INVALID;
     }
     if (lapse_needs_kavg(d.lapse)) {
@@ -774,6 +793,7 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
       cg::MixedBox& m = b.mdev;
       m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.pts = b.dev.pts; m.nfields = b.dev.nfields;
       m.order = d.stencil_order; m.matter = d.matter; m.lapse = d.lapse; m.normalize = d.normalize_metric;
+      m.xg = d.x_ghost;
       m.dx = d.dx; m.dt = d.dt;
       m.P = b.dev.P;
       m.F = b.dev.F;
@@ -1032,16 +1052,48 @@ int cg_download_field(cg_ctx* ctx, int box, int field, char reg, double* host, s
   return field_copy(ctx, box, field, reg, host, n, false);
 }
 
-int cg_substep_input(cg_ctx* ctx, int box, double** input, double** flux) {
+int cg_substep_input(cg_ctx* ctx, int box, void** input, void** flux) {
   int rc = check_box(ctx, box);
   if (rc) return rc;
   if (!input) return fail(ctx, CG_ERR_INVALID, "input is null");
   Box& b = ctx->boxes[box];
-  if (b.mixed) return fail(ctx, CG_ERR_INVALID, "the substep input of an FP64 box only");
   if (b.stage_next == 0) return fail(ctx, CG_ERR_STATE, "the substep input exists after cg_step_init");
-  const bool even = b.stage_next == 2 || b.stage_next == 4;
-  *input = even ? b.dev.Y : b.dev.X;
-  if (flux) *flux = b.desc.matter == CG_MATTER_DUST ? (even ? b.dev.FP1 : b.dev.FP0) : nullptr;
+  const bool even = b.stage_next == 2 || b.stage_next == 4, dust = b.desc.matter == CG_MATTER_DUST;
+  if (b.mixed) {
+    *input = even ? b.mdev.Y : b.mdev.X;
+    if (flux) *flux = dust ? (even ? b.mdev.FP1 : b.mdev.FP0) : nullptr;
+  } else {
+    *input = even ? b.dev.Y : b.dev.X;
+    if (flux) *flux = dust ? (even ? b.dev.FP1 : b.dev.FP0) : nullptr;
+  }
+  return CG_OK;
+}
+
+int cg_background_sums(cg_ctx* ctx, int box, double* out, int n) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  if (!out || n < 6) return fail(ctx, CG_ERR_INVALID, "out needs 6 entries");
+  Box& b = ctx->boxes[box];
+  rc = background_sums(ctx, b, out);
+  if (rc) return rc;
+  out[5] = (double)(b.dev.nx - 2 * b.dev.xg) * b.dev.ny * b.dev.nz;
+  return CG_OK;
+}
+
+int cg_set_background(cg_ctx* ctx, int box, const double* means, int n) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  Box& b = ctx->boxes[box];
+  if (!b.mixed) return fail(ctx, CG_ERR_INVALID, "the background belongs to FP32-mixed boxes");
+  if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "set the background between steps");
+  if (!means) {
+    b.bg_set = false;  // back to the box's own means
+  } else {
+    if (n < 5) return fail(ctx, CG_ERR_INVALID, "means needs 5 entries");
+    for (int q = 0; q < 5; ++q) b.bg_means[q] = means[q];
+    b.bg_set = true;
+  }
+  b.stage_next = 0;  // the next step starts from the initialisation
   return CG_OK;
 }
 
@@ -1544,6 +1596,8 @@ static CScratch cscratch_layout(const Box& b) {
 // box it is built in *xtmp, which the caller frees after the last use.
 static int constraint_pass(cg_ctx* ctx, Box& b, cg::BoxDev& dev, double** xtmp) {
   *xtmp = nullptr;
+  if (b.mixed && b.desc.x_ghost != 0)
+    return fail(ctx, CG_ERR_INVALID, "constraints of an FP32-mixed x-slab would read stale ghost planes of _p");
   if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "constraints are taken between steps");
   if (b.stage_next == 0) {
     const int rc = do_init(ctx, b);

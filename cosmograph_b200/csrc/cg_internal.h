@@ -39,6 +39,7 @@ struct MixedBox {
   int maps;                // the maps are encoded
   int tma;                 // interior tiles are copied by TMA (maps != 0 and the option on)
   int nx, ny, nz, pts, nfields, order, matter, lapse, normalize;
+  int xg;  // ghost planes on each x face (0: periodic box)
   double dx, dt;
   double* P;
   double* F;

@@ -763,17 +763,18 @@ __device__ __forceinline__ void init_tile_barrier(uint64_t* bar, bool use) {
   __syncthreads();
 }
 
-// One box: one CTA per brick.  tmap: the TMA map of this substep's input
-// (use_tma = 0: every tile is copied by the threads).
+// One box: one CTA per updated brick.  tmap: the TMA map of this substep's
+// input (use_tma = 0: every tile is copied by the threads).
 template <int O, int MATTER>
 __global__ void __launch_bounds__(kThreads, 4)
 mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt, Bg bg, Ptrs P, int stage,
-             const __grid_constant__ CUtensorMap tmap, int use_tma) {
+             const __grid_constant__ CUtensorMap tmap, int use_tma, int bx0) {
   __shared__ __align__(8) uint64_t bar;
   init_tile_barrier(&bar, use_tma != 0);
   unsigned phase = 0;
   bool tma_ok = true;
-  mixed_body<O, MATTER>(nx, ny, nz, lapse, normalize, idx, dt, bg, P, stage, blockIdx.z, blockIdx.y, blockIdx.x,
+  // bx0: first x brick (x-slab boxes skip their ghost planes)
+  mixed_body<O, MATTER>(nx, ny, nz, lapse, normalize, idx, dt, bg, P, stage, blockIdx.z + bx0, blockIdx.y, blockIdx.x,
                         use_tma ? &tmap : nullptr, &bar, phase, tma_ok);
 }
 

@@ -43,8 +43,8 @@ cudaError_t go(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
   cudaError_t e = allow_smem(mixed_kernel<O, M>, smem, done);
   if (e != cudaSuccess) return e;
   const CUtensorMap& map = (stage == 1 || stage == 3) ? b.mapX : b.mapY;  // the substep's input
-  mixed_kernel<O, M><<<grid3(b.nx, b.ny, b.nz), dim3(kBZ, kBY, kBX), smem, st>>>(
-      b.nx, b.ny, b.nz, b.lapse, b.normalize, (float)(1.0 / b.dx), b.dt, bg, P, stage, map, b.tma);
+  mixed_kernel<O, M><<<grid3(b.nx - 2 * b.xg, b.ny, b.nz), dim3(kBZ, kBY, kBX), smem, st>>>(
+      b.nx, b.ny, b.nz, b.lapse, b.normalize, (float)(1.0 / b.dx), b.dt, bg, P, stage, map, b.tma, b.xg / kBX);
   return cudaGetLastError();
 }
 template <int O>

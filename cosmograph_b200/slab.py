@@ -19,8 +19,11 @@ Two exchanges:
 * ``DistHalo``: one slab per rank; ghost planes travel as point-to-point
   messages through ``torch.distributed`` (NCCL between GPUs, gloo on CPU).
 
-Only FP64 boxes whose lapse does not use the grid average of K
-(the C ABI rejects the others for slabs).
+Lapses that use the grid average of K are not available for slabs (the C ABI
+rejects them).  FP32-mixed slabs hold FP32 perturbations about one uniform
+background, which must be the whole box's: the slabs' sums of the background
+fields are added up (across ranks: an all-reduce) and every slab gets the
+same means (``cg_set_background``) before the first step.
 """
 from __future__ import annotations
 
@@ -71,22 +74,36 @@ def assemble(slabs: list[BoxState], ghost: int) -> BoxState:
 class _CudaArray:
     """__cuda_array_interface__ view of library-owned device memory."""
 
-    def __init__(self, ptr: int, shape: tuple[int, ...]):
-        self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f8", "data": (ptr, False),
+    def __init__(self, ptr: int, shape: tuple[int, ...], typestr: str):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (ptr, False),
                                          "version": 2, "strides": None}
 
 
-def _substep_arrays(ev: Evolution, box: int, nfields: int, shape) -> list:
-    """torch views of the arrays the next substep of `box` reads with stencils."""
+def _substep_arrays(ev: Evolution, box: int, nfields: int, shape, mixed: bool) -> list:
+    """torch views of the arrays the next substep of `box` reads with stencils
+    (FP32 perturbations for a mixed box)."""
     import torch
 
-    inp, flux = ctypes.POINTER(ctypes.c_double)(), ctypes.POINTER(ctypes.c_double)()
+    inp, flux = ctypes.c_void_p(), ctypes.c_void_p()
     ev._check(ev.L.cg_substep_input(ev.ctx, box, ctypes.byref(inp), ctypes.byref(flux)))
-    addr = lambda p: ctypes.cast(p, ctypes.c_void_p).value  # noqa: E731  (device address, not read here)
-    out = [torch.as_tensor(_CudaArray(addr(inp), (nfields, *shape)), device="cuda")]
-    if flux:
-        out.append(torch.as_tensor(_CudaArray(addr(flux), (FLUX_ARRAYS, *shape)), device="cuda"))
+    t = "<f4" if mixed else "<f8"
+    out = [torch.as_tensor(_CudaArray(inp.value, (nfields, *shape), t), device="cuda")]
+    if flux.value:
+        out.append(torch.as_tensor(_CudaArray(flux.value, (FLUX_ARRAYS, *shape), t), device="cuda"))
     return out
+
+
+def background_sums(ev: Evolution, box: int) -> np.ndarray:
+    """Sums of K, phi, alpha, field 18 and field 19 of _p over the box's
+    updated points, and their count (cg_background_sums)."""
+    out = np.zeros(6)
+    ev._check(ev.L.cg_background_sums(ev.ctx, box, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 6))
+    return out
+
+
+def set_background(ev: Evolution, box: int, sums: np.ndarray) -> None:
+    means = np.ascontiguousarray(sums[:5] / sums[5])
+    ev._check(ev.L.cg_set_background(ev.ctx, box, means.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 5))
 
 
 def fill_ghosts(arrays_by_slab: list[list], ghost: int) -> None:
@@ -105,13 +122,19 @@ def fill_ghosts(arrays_by_slab: list[list], ghost: int) -> None:
 class LocalHalo:
     """Ghost planes among slabs that are boxes of one context (one GPU)."""
 
-    def __init__(self, ev: Evolution, ghost: int):
-        self.ev, self.ghost = ev, ghost
+    def __init__(self, ev: Evolution, ghost: int, mixed: bool = False):
+        self.ev, self.ghost, self.mixed = ev, ghost, mixed
 
     def exchange(self) -> None:
         ev = self.ev
-        arrays = [_substep_arrays(ev, b, t.fields.shape[0], t.shape) for b, t in enumerate(ev.templates)]
+        arrays = [_substep_arrays(ev, b, t.fields.shape[0], t.shape, self.mixed) for b, t in enumerate(ev.templates)]
         fill_ghosts(arrays, self.ghost)
+
+    def background(self) -> None:
+        """One background for every slab: the whole box's means."""
+        total = sum(background_sums(self.ev, b) for b in range(len(self.ev.templates)))
+        for b in range(len(self.ev.templates)):
+            set_background(self.ev, b, total)
 
 
 class DistHalo:
@@ -153,9 +176,20 @@ class DistHalo:
             a[:, :g].copy_(from_left)
             a[:, nx - g:].copy_(from_right)
 
-    def exchange(self, ev: Evolution) -> None:
+    def exchange(self, ev: Evolution, mixed: bool = False) -> None:
         t = ev.templates[0]
-        self.exchange_arrays(_substep_arrays(ev, 0, t.fields.shape[0], t.shape))
+        self.exchange_arrays(_substep_arrays(ev, 0, t.fields.shape[0], t.shape, mixed))
+
+    def background(self, ev: Evolution) -> None:
+        """One background for every rank's slab: the all-reduced sums."""
+        import torch
+
+        sums = torch.from_numpy(background_sums(ev, 0))
+        if self.size > 1:
+            if self.dist.get_backend(self.group) == "nccl":
+                sums = sums.cuda()
+            self.dist.all_reduce(sums, group=self.group)
+        set_background(ev, 0, sums.cpu().numpy())
 
 
 class SlabEvolution:
@@ -179,8 +213,14 @@ class SlabEvolution:
         self.ev.set_stream(self.stream.cuda_stream)
         self.ghost = ghost
         self.halo = halo
-        self.local = LocalHalo(self.ev, ghost) if halo is None else None
+        self.mixed = cfg.precision == "mixed"
+        self.local = LocalHalo(self.ev, ghost, self.mixed) if halo is None else None
         self.started = False
+        if self.mixed:  # the whole box's uniform background in every slab
+            if self.local is not None:
+                self.local.background()
+            else:
+                self.halo.background(self.ev)
 
     def _exchange(self) -> None:
         import torch
@@ -189,7 +229,7 @@ class SlabEvolution:
             if self.local is not None:
                 self.local.exchange()
             else:
-                self.halo.exchange(self.ev)
+                self.halo.exchange(self.ev, self.mixed)
 
     def step(self, nsteps: int = 1) -> None:
         for _ in range(nsteps):
@@ -220,5 +260,5 @@ class SlabEvolution:
         self.close()
 
 
-__all__ = ["ghost_width", "slab_bounds", "split", "assemble", "fill_ghosts", "LocalHalo", "DistHalo",
-           "SlabEvolution", "FLUX_ARRAYS"]
+__all__ = ["ghost_width", "slab_bounds", "split", "assemble", "fill_ghosts", "background_sums", "set_background",
+           "LocalHalo", "DistHalo", "SlabEvolution", "FLUX_ARRAYS"]

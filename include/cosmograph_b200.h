@@ -95,7 +95,8 @@ typedef struct {
                               that the caller refreshes from the neighbouring
                               slabs before every substep (cg_substep_input);
                               kernels update the nx - 2g interior planes only.
-                              FP64 arithmetic, lapses without K_avg; g a
+                              Lapses without K_avg; FP32-mixed slabs of one
+                              box share a background (cg_set_background); g a
                               multiple of 4, >= the stencil radius (and the
                               Kreiss-Oliger radius), nx - 2g a positive
                               multiple of 4.                                   */
@@ -268,16 +269,26 @@ int cg_frw_state(cg_ctx *ctx, int box, double *out, int n);
 /* Steps completed by a box since creation or the last upload. */
 int cg_step_count(cg_ctx *ctx, int box, int64_t *steps);
 
-/* Device arrays that the next cg_rk_stage of an FP64 box reads with
- * stencils: the substep input (nfields arrays of nx*ny*nz doubles, field-major,
- * x slowest) and, for dust, its flux primitives (7 arrays: alpha*D,
- * alpha*S_1..3, v^1..3; NULL otherwise).  Valid after cg_step_init and after
- * each cg_rk_stage, until the next one.  For an x-slab box (x_ghost = g) the
- * caller refreshes planes [0, g) and [nx-g, nx) of every array from the
- * neighbouring slabs' interior planes before each substep (and before
- * cg_constraints / cg_field_statistics).  No reference counterpart: the
- * reference evolves one box per process. */
-int cg_substep_input(cg_ctx *ctx, int box, double **input, double **flux);
+/* Device arrays that the next cg_rk_stage of a box reads with stencils: the
+ * substep input (nfields arrays of nx*ny*nz values, field-major, x slowest;
+ * double, or float perturbations for CG_PREC_MIXED) and, for dust, its flux
+ * primitives (7 arrays of the same type: alpha*D, alpha*S_1..3, v^1..3; NULL
+ * otherwise).  Valid after cg_step_init and after each cg_rk_stage, until the
+ * next one.  For an x-slab box (x_ghost = g) the caller refreshes planes
+ * [0, g) and [nx-g, nx) of every array from the neighbouring slabs' interior
+ * planes before each substep (and, FP64, before cg_constraints /
+ * cg_field_statistics).  No reference counterpart: the reference evolves one
+ * box per process. */
+int cg_substep_input(cg_ctx *ctx, int box, void **input, void **flux);
+
+/* FP32-mixed x-slabs of one box share one uniform background: out[0..4] =
+ * sums over the box's updated points of K, phi, alpha, field 18 (D or the
+ * scalar phi) and field 19 (Pi) of "_p", out[5] = their count (n >= 6);
+ * cg_set_background gives a mixed box the background means (K, phi, alpha,
+ * field 18, field 19; NULL: its own means again) for the next step
+ * initialisation.  Synchronous.  No reference counterpart. */
+int cg_background_sums(cg_ctx *ctx, int box, double *out, int n);
+int cg_set_background(cg_ctx *ctx, int box, const double *means, int n);
 
 /* Constraint statistics of one box between steps (after cg_step_init or a
  * whole step), BSSN::setConstraintCalcs (components/bssn/bssn.cc:965-1071)
