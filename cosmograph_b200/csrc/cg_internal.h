@@ -21,6 +21,8 @@ struct BoxDev {
   int tma;                 // interior tiles are copied by TMA (maps != 0 and the option on)
   int nx, ny, nz, pts, nfields, order, matter;
   int xg;  // ghost planes on each x face (0: periodic box)
+  CUtensorMap fmap0[3], fmap1[3];  // TMA maps of the flux primitives FP0 / FP1 (x, y, z boxes)
+  int fmaps;                       // those maps are encoded
   Physics ph;
   double* P;    // the reference's _p register (state at the start of a step)
   double* F;    // the reference's _f register (RK accumulator)

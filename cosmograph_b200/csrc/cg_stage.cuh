@@ -121,7 +121,15 @@ struct SlotsC {
 template <int O, int MATTER, int MODE>
 struct TileBuffers {
   static constexpr bool kTwo = MODE == kEvolve && MATTER != kScalar;
-  static constexpr size_t kBytes = (TileG<O>::SIZE * sizeof(double) + 127) / 128 * 128;
+  // dust also stages the x and z boxes of its flux primitives here (5 arrays
+  // each, flux_from_tiles)
+  static constexpr size_t kTile = TileG<O>::SIZE * sizeof(double);
+  static constexpr size_t kFluxX = 5 * (kBX + O) * kBY * kBZ * sizeof(double);
+  static constexpr size_t kFluxZ = 5 * kBX * kBY * TileG<O>::TZ * sizeof(double);
+  static constexpr size_t kNeed =
+      MATTER == kDust ? (kTile > kFluxX ? (kTile > kFluxZ ? kTile : kFluxZ) : (kFluxX > kFluxZ ? kFluxX : kFluxZ))
+                      : kTile;
+  static constexpr size_t kBytes = (kNeed + 127) / 128 * 128;
 };
 // dynamic shared memory of a substep launch
 template <int O, int MATTER, int MODE>
@@ -438,7 +446,103 @@ __device__ __forceinline__ void flux_divergences(const T& t, const double* __res
   }
 }
 
-// Kreiss-Oliger dissipation of one field at (i, j, k) (utils/math.h:36-72;
+// TMA boxes of the dust flux primitives for their divergence: for axis a the
+// brick extended by r along a only (x: (4+2r) x 2 x 16, y: 4 x (2+2r) x 16,
+// z: 4 x 2 x the tile row of the field tiles, starting at an aligned z).
+template <int O>
+struct FluxBox {
+  static constexpr int R = O / 2;
+  static constexpr int XB = (kBX + 2 * R) * kBY * kBZ;
+  static constexpr int YB = kBX * (kBY + 2 * R) * kBZ;
+  static constexpr int ZP = TileG<O>::TZ, ZB = kBX * kBY * ZP;
+};
+struct FluxMaps {
+  CUtensorMap m[3];  // x, y and z boxes of the substep input's 7 flux-primitive arrays
+};
+
+// divergence term along one axis from box tiles: u (4 arrays, the m-th at
+// u + m*len) and v^a (at u + 4*len); the product at each tap as d1p forms it
+template <int O>
+__device__ __forceinline__ double d1p_tile(const double* u, const double* v, int c, int s, const Physics& ph) {
+  auto V = [&](int n) { return u[c + n * s] * v[c + n * s]; };
+  double r;
+  if (O == 2) {
+    r = (-1.0 / 2.0 * V(-1) + 1.0 / 2.0 * V(1));
+  } else if (O == 4) {
+    r = (+1.0 / 12.0 * V(-2) - 2.0 / 3.0 * V(-1) + 2.0 / 3.0 * V(1) - 1.0 / 12.0 * V(2));
+  } else if (O == 6) {
+    r = (-1.0 / 60.0 * V(-3) + 3.0 / 20.0 * V(-2) - 3.0 / 4.0 * V(-1) + 3.0 / 4.0 * V(1) -
+         3.0 / 20.0 * V(2) + 1.0 / 60.0 * V(3));
+  } else {
+    r = ((1.0 / 280.0 * V(-4) - 1.0 / 280.0 * V(4)) - (4.0 / 105.0 * V(-3) - 4.0 / 105.0 * V(3)) +
+         (1.0 / 5.0 * V(-2) - 1.0 / 5.0 * V(2)) - (4.0 / 5.0 * V(-1) - 4.0 / 5.0 * V(1)));
+  }
+  return divdx(r, ph);
+}
+
+// Dust flux divergences of a brick inside the box from TMA boxes: x boxes
+// into tl2, y boxes into tl, then z boxes into tl2; the sum over axes in the
+// order of flux_divergences.  All threads of the CTA take part.
+template <int O>
+__device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, double* tl2, int tid, int x0, int y0,
+                                                int z0, const Physics& ph, double* sl, uint64_t* bar,
+                                                unsigned& phase) {
+  using FB = FluxBox<O>;
+  constexpr int R = FB::R;
+  // every staging area fits its buffer: x and z boxes in the second tile
+  // buffer, y boxes in the first (the phase-2-only slot columns)
+  static_assert(5 * FB::XB * sizeof(double) <= TileBuffers<O, kDust, kEvolve>::kBytes, "x boxes fit");
+  static_assert(5 * FB::ZB * sizeof(double) <= TileBuffers<O, kDust, kEvolve>::kBytes, "z boxes fit");
+  static_assert(5 * FB::YB * sizeof(double) <= (size_t)kTileSlots * kThreads * sizeof(double), "y boxes fit");
+  bool ok = true;
+  auto wait = [&](int b) {
+    if (ok && !tma::wait(bar + b, (phase >> b) & 1u, kTmaWaitCycles64)) ok = false;
+    phase ^= 1u << b;
+  };
+  auto load5 = [&](int a, double* dst, uint64_t* b, int len) {
+    tma::arrive_expect_tx(b, (unsigned)(5 * len * sizeof(double)));
+    const int cx = x0 - (a == 0 ? R : 0), cy = y0 - (a == 1 ? R : 0);
+    const int cz = z0 - (a == 2 ? TileG<O>::ZO : 0);
+    for (int q = 0; q < 5; ++q)  // alpha*D, alpha*S_1..3, then v^a
+      tma::load_4d(dst + (size_t)q * len, &fm->m[a], cz, cy, cx, q < 4 ? P_AD + q : P_V1 + a, b);
+  };
+  const int tx = threadIdx.z, ty = threadIdx.y, tz = threadIdx.x;
+  tma::fence_proxy_async();
+  __syncthreads();  // the field tiles have been read
+  if (tid == 0) {
+    load5(0, tl2, bar + 1, FB::XB);
+    load5(1, tl, bar, FB::YB);
+  }
+  wait(1);
+  {
+    const int c = ((tx + R) * kBY + ty) * kBZ + tz;
+#pragma unroll 1
+    for (int m = 0; m < 4; ++m)
+      sl[(S_MAT + m) * kThreads] = d1p_tile<O>(tl2 + (size_t)m * FB::XB, tl2 + (size_t)4 * FB::XB, c, kBY * kBZ, ph);
+  }
+  tma::fence_proxy_async();
+  __syncthreads();  // the x boxes have been read
+  if (tid == 0) load5(2, tl2, bar + 1, FB::ZB);
+  wait(0);
+  {
+    const int c = (tx * (kBY + 2 * R) + ty + R) * kBZ + tz;
+#pragma unroll 1
+    for (int m = 0; m < 4; ++m)
+      sl[(S_MAT + m) * kThreads] =
+          sl[(S_MAT + m) * kThreads] + d1p_tile<O>(tl + (size_t)m * FB::YB, tl + (size_t)4 * FB::YB, c, kBZ, ph);
+  }
+  wait(1);
+  {
+    const int c = (tx * kBY + ty) * FB::ZP + tz + TileG<O>::ZO;
+#pragma unroll 1
+    for (int m = 0; m < 4; ++m)
+      sl[(S_MAT + m) * kThreads] =
+          sl[(S_MAT + m) * kThreads] + d1p_tile<O>(tl2 + (size_t)m * FB::ZB, tl2 + (size_t)4 * FB::ZB, c, 1, ph);
+  }
+  return __syncthreads_and(ok);
+}
+
+// Kreiss-Oliger dissipation of one field at (i, j, k)// Kreiss-Oliger dissipation of one field at (i, j, k) (utils/math.h:36-72;
 // the reference defines it for stencil orders 2 and 8 only): the sixth
 // (order 2: fourth) undivided difference along each axis, taps from global
 // memory, plain offsets when the taps stay inside the box.
@@ -510,7 +614,8 @@ __device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part, int cta
 template <int O, int MATTER, int MODE, bool KO = false>
 __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph, StageBg bg, const StagePtrs& P,
                                            int stage, int cx, int cy, int cz, int cta, const CUtensorMap* tmap,
-                                           uint64_t* bar, unsigned& phase, bool& tma_ok) {
+                                           uint64_t* bar, unsigned& phase, bool& tma_ok,
+                                           const FluxMaps* fmaps = nullptr) {
   constexpr int NFLD = NF<MATTER>::value;
   constexpr int NSLOT = MODE == kConstraints ? SlotsC<MATTER>::value : Slots<MATTER>::value;
   static_assert(NSLOT >= S_MAT, "the tile region lies inside the slot array");
@@ -556,6 +661,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
 
   // ---- phase 1: derivatives into shared memory ---------------------------------
   const int x0 = cx * kBX, y0 = cy * kBY, z0 = cz * kBZ;
+  bool flux_tiles = false;  // the dust flux divergences came from TMA boxes
   {
     using G = TileG<O>;
     double* tl = smem + kTileSlot * kThreads;
@@ -573,13 +679,21 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
                                           tile::centre<G>(threadIdx.z, threadIdx.y, threadIdx.x),
                                           by_tma ? tmap : nullptr, bar, phase, P.status) &&
              tma_ok;
+    if constexpr (MATTER == kDust && MODE == kEvolve && TileBuffers<O, MATTER, MODE>::kTwo) {
+      flux_tiles = fmaps && by_tma && tma_ok;
+      if (flux_tiles) {
+        tma_ok = flux_from_tiles<O>(fmaps, tl, tl2, tid, x0, y0, z0, ph, sl, bar, phase);
+        if (!tma_ok && tid == 0) atomicOr(P.status, kStatusTileTimeout64);
+      }
+    }
     __syncthreads();  // the tile region becomes slots again
   }
   if (MODE == kEvolve && !live) return;  // no CTA-wide synchronisation after this point
-  {
+  if (!flux_tiles) {
     const bool interior = x0 >= R && x0 + kBX + R <= geo.nx && y0 >= R && y0 + kBY + R <= geo.ny && z0 >= R &&
                           z0 + kBZ + R <= geo.nz;
-    // the dust flux divergences, taps from global memory
+    // the dust flux divergences of bricks that did not take them from TMA
+    // boxes: taps from global memory
     if (MATTER == kDust) {
       if (interior) flux_divergences<O>(Taps<false>{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c},
                                         P.fp_in, N, ph, sl);
@@ -1092,14 +1206,15 @@ __device__ __forceinline__ void init_tile_barriers(uint64_t* bar, bool use) {
 template <int O, int MATTER, int MODE, bool KO = false>
 __global__ void __launch_bounds__(kThreads, 2)
 stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage, const __grid_constant__ CUtensorMap tmap,
-             int use_tma) {
+             int use_tma, const __grid_constant__ FluxMaps fmaps, int use_fmaps) {
   __shared__ __align__(8) uint64_t bar[2];
   init_tile_barriers(bar, use_tma != 0);
   unsigned phase = 0;
   bool tma_ok = true;
   stage_body<O, MATTER, MODE, KO>(geo, ph, bg, P, stage, blockIdx.z + geo.bx0, blockIdx.y, blockIdx.x,
                                   blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
-                                  use_tma ? &tmap : nullptr, bar, phase, tma_ok);
+                                  use_tma ? &tmap : nullptr, bar, phase, tma_ok,
+                                  use_tma && use_fmaps ? &fmaps : nullptr);
 }
 
 // A group of boxes of the same order and matter model, one launch per

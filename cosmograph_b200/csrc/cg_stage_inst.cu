@@ -82,6 +82,9 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
   }
   BoxGeom geo{b.nx, b.ny, b.nz, b.pts, b.xg / kBX};
   const CUtensorMap& map = (stage == 1 || stage == 3) ? b.mapX : b.mapY;  // the substep's input
+  FluxMaps fm;
+  const CUtensorMap* fsrc = (stage == 1 || stage == 3) ? b.fmap0 : b.fmap1;
+  for (int a = 0; a < 3; ++a) fm.m[a] = fsrc[a];
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
   if constexpr (O == 2 || O == 8) {
     if (b.ph.ko_coeff != 0.0) {  // Kreiss-Oliger dissipation: its own instantiation
@@ -93,7 +96,7 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
         configured_ko = true;
       }
       stage_kernel<O, M, kEvolve, true><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage, map,
-                                                                                    b.tma);
+                                                                                    b.tma, fm, b.fmaps);
       return cudaGetLastError();
     }
   }
@@ -103,7 +106,8 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  stage_kernel<O, M, kEvolve><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage, map, b.tma);
+  stage_kernel<O, M, kEvolve><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage, map, b.tma,
+                                                                            fm, b.fmaps);
   return cudaGetLastError();
 }
 
@@ -126,7 +130,9 @@ cudaError_t go_constraints(const BoxDev& b, const StageBg& bg, double* cvals, do
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  stage_kernel<O, M, kConstraints><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, 1, b.mapX, b.tma);
+  FluxMaps fm{};
+  stage_kernel<O, M, kConstraints><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, 1, b.mapX, b.tma,
+                                                                                fm, 0);
   return cudaGetLastError();
 }
 
@@ -193,8 +199,23 @@ cudaError_t go_stage_m(const BoxDev& b, const StageBg& bg, int stage, cudaStream
 template <int O>
 bool encode_maps(BoxDev& b) {
   using G = TileG<O>;
-  return tma_host::encode(&b.mapX, b.X, sizeof(double), b.nx, b.ny, b.nz, b.nfields, G::TZ, G::TY, G::TX) &&
-         tma_host::encode(&b.mapY, b.Y, sizeof(double), b.nx, b.ny, b.nz, b.nfields, G::TZ, G::TY, G::TX);
+  b.fmaps = 0;
+  if (!(tma_host::encode(&b.mapX, b.X, sizeof(double), b.nx, b.ny, b.nz, b.nfields, G::TZ, G::TY, G::TX) &&
+        tma_host::encode(&b.mapY, b.Y, sizeof(double), b.nx, b.ny, b.nz, b.nfields, G::TZ, G::TY, G::TX)))
+    return false;
+  if (b.FP0 && b.FP1) {  // dust: x, y, z boxes of the flux primitives
+    constexpr int R = O / 2;
+    const int box[3][3] = {{kBZ, kBY, kBX + 2 * R}, {kBZ, kBY + 2 * R, kBX}, {G::TZ, kBY, kBX}};
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) {
+      ok = ok && tma_host::encode(&b.fmap0[a], b.FP0, sizeof(double), b.nx, b.ny, b.nz, P_N, box[a][0], box[a][1],
+                                  box[a][2]);
+      ok = ok && tma_host::encode(&b.fmap1[a], b.FP1, sizeof(double), b.nx, b.ny, b.nz, P_N, box[a][0], box[a][1],
+                                  box[a][2]);
+    }
+    b.fmaps = ok ? 1 : 0;
+  }
+  return true;
 }
 }  // namespace
 
