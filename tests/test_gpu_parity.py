@@ -133,6 +133,24 @@ def test_translation_equivariance_full_size():
     assert np.array_equal(np.roll(a.fields, (5, -7, 3), axis=(1, 2, 3)), b.fields)
 
 
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("fp64_fma", 1e-13), ("mixed", 1e-10)])
+def test_dust_mass_is_conserved_full_size(precision, tol):
+    """The dust density evolves in flux-divergence form (dust.cc:203-224),
+    and a centred difference summed over a periodic grid vanishes, so the sum
+    of D over the box is conserved up to roundoff -- a size-independent check
+    at the bench's size (256^3, order 8, GRF initial data built on the GPU)."""
+    st = ics.grf_dust_gpu(256, seed=3, rms_delta=1e-4, order=8)
+    d = st.names.index("D")
+    mass0 = st.fields[d].sum()
+    with Evolution(st, BoxConfig(order=8, precision=precision)) as ev:
+        ev.step(3)
+        ev.synchronize()
+        after = ev.download_field(0, d)
+    moved = np.abs(after - st.fields[d]).max() / np.abs(st.fields[d] - st.fields[d].mean()).max()
+    assert moved > 1e-6  # the density did evolve
+    assert abs(after.sum() - mass0) / mass0 < tol, (after.sum(), mass0)
+
+
 def test_uniform_box_stays_uniform_full_size():
     st = ics.perturbed((256, 64, 64), S.DUST, amp=0.0)
     got = evolve(st, 3, BoxConfig(order=8))

@@ -92,3 +92,15 @@ def test_rk4_known_answer_uniform_vacuum():
         # stencils of a uniform field leave ulp-level residues (e.g. 1/12 - 2/3
         # + 2/3 - 1/12 of a constant), so the grid is an ODE only to ~1e-15/step
         assert abs(arr.flat[0] - v) <= 1e-13 * max(1.0, abs(v)), (f_, arr.flat[0], v)
+
+
+def test_restatement_conserves_dust_mass():
+    """sum D over the periodic grid is conserved by the flux-divergence form
+    (the property the GPU full-size test checks at 256^3)."""
+    from cosmograph_b200 import ics, state as S
+
+    st = ics.perturbed((12, 10, 8), S.DUST, seed=6, amp=2e-2)
+    d = st.names.index("D")
+    out = oracle.evolve(st, 3, 4, lapse="Harmonic")
+    assert not np.array_equal(out.fields[d], st.fields[d])
+    assert abs(out.fields[d].sum() - st.fields[d].sum()) / st.fields[d].sum() < 1e-14
