@@ -33,7 +33,8 @@ EXPORTS = (
     "cg_num_fields", "cg_field_name", "cg_upload_state", "cg_download_state",
     "cg_upload_state_async", "cg_download_state_async", "cg_exchange_state_async", "cg_prefetch_state_async",
     "cg_upload_field", "cg_download_field",
-    "cg_device_register", "cg_substep_input", "cg_background_sums", "cg_set_background", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
+    "cg_device_register", "cg_substep_input", "cg_background_sums", "cg_set_background",
+    "cg_kavg_sums", "cg_set_kavg", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
     "cg_status", "cg_frw_state", "cg_step_count", "cg_last_error", "cg_version",
     "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints", "cg_field_statistics",
     "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust",
@@ -92,6 +93,8 @@ def load() -> ctypes.CDLL:
         "cg_substep_input": (i, [vp, i, ctypes.POINTER(vp), ctypes.POINTER(vp)]),
         "cg_background_sums": (i, [vp, i, dp, i]),
         "cg_set_background": (i, [vp, i, dp, i]),
+        "cg_kavg_sums": (i, [vp, i, ctypes.POINTER(vp)]),
+        "cg_set_kavg": (i, [vp, i, vp]),
         "cg_step_init": (i, [vp]),
         "cg_rk_stage": (i, [vp, i]),
         "cg_step": (i, [vp, i]),

@@ -83,6 +83,8 @@ struct Box {
   bool needs_kavg = false;
   double* kavg_partial = nullptr;  // per-block partial sums for K_avg
   double* kavg = nullptr;          // device K_avg
+  double* kavg_sums = nullptr;     // device sums of exp(6 phi) K and exp(6 phi) (x-slabs: cg_kavg_sums)
+  bool kavg_set = false;           // x-slab: the caller set K_avg for the next substep (cg_set_kavg)
   int kavg_blocks = 0;
   double* cscratch = nullptr;      // constraint statistics scratch (allocated on first use)
   // FP32-mixed boxes
@@ -382,8 +384,20 @@ StageBg bg_for(const Box& b, int stage, double phi_next) {
   return bg;
 }
 
+// K_avg from two device sums: sum exp(6 (phi + phi_FRW)) K over sum exp(6 (phi + phi_FRW))
+__global__ void kavg_from_sums_kernel(const double* sums, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) out[0] = sums[0] / sums[1];
+}
+
 int launch_kavg(cg_ctx* ctx, Box& b, const double* in) {
   if (!b.needs_kavg) return CG_OK;
+  if (b.desc.x_ghost != 0) {
+    // an x-slab's K_avg is the whole box's: the caller set it (cg_set_kavg)
+    if (!b.kavg_set)
+      return fail(ctx, CG_ERR_STATE, "an x-slab with this lapse needs cg_kavg_sums / cg_set_kavg before each substep");
+    b.kavg_set = false;
+    return CG_OK;
+  }
   const double* K = in + (size_t)cg::F_K * b.dev.pts;
   const double* phi = in + (size_t)cg::F_PHI * b.dev.pts;
   kavg_partial_kernel<<<b.kavg_blocks, 256, 0, ctx->stream>>>(K, phi, b.dev.pts, b.frw.get_phi, b.kavg_partial);
@@ -632,8 +646,8 @@ int validate(const cg_box_desc& d, std::string& why) {
       why = "an x-slab needs nx - 2 x_ghost interior planes, a positive multiple of 4";
       return CG_ERR_INVALID;
     }
-    if (lapse_needs_kavg(d.lapse)) {
-      why = "x-slabs (x_ghost > 0) support lapses without the grid average of K";
+    if (lapse_needs_kavg(d.lapse) && d.precision == CG_PREC_MIXED) {
+      why = "the FP32-mixed form supports the Harmonic and Static lapses";
       return CG_ERR_INVALID;
     }
   }
@@ -817,8 +831,9 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
     b.needs_kavg = lapse_needs_kavg(d.lapse);
     if (e == cudaSuccess && b.needs_kavg) {
       b.kavg_blocks = std::min(1024, (b.dev.pts + 255) / 256);
-      e = cudaMalloc(&b.kavg_partial, sizeof(double) * (2 * b.kavg_blocks + 1));
+      e = cudaMalloc(&b.kavg_partial, sizeof(double) * (2 * b.kavg_blocks + 3));
       b.kavg = b.kavg_partial + 2 * b.kavg_blocks;
+      b.kavg_sums = b.kavg + 1;
       b.dev.kavg = b.kavg;
     }
   }
@@ -1066,6 +1081,38 @@ int cg_substep_input(cg_ctx* ctx, int box, void** input, void** flux) {
     *input = even ? b.dev.Y : b.dev.X;
     if (flux) *flux = dust ? (even ? b.dev.FP1 : b.dev.FP0) : nullptr;
   }
+  return CG_OK;
+}
+
+int cg_kavg_sums(cg_ctx* ctx, int box, double** dsums) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  if (!dsums) return fail(ctx, CG_ERR_INVALID, "dsums is null");
+  Box& b = ctx->boxes[box];
+  if (!b.needs_kavg || b.mixed) return fail(ctx, CG_ERR_INVALID, "the box's lapse does not use K_avg");
+  if (b.stage_next == 0) return fail(ctx, CG_ERR_STATE, "K_avg sums exist after cg_step_init");
+  // over the updated points of the next substep's input
+  const int N = b.dev.pts, off = b.dev.xg * b.dev.ny * b.dev.nz;
+  const int n = (b.dev.nx - 2 * b.dev.xg) * b.dev.ny * b.dev.nz;
+  const double* in = current_a(b);
+  kavg_partial_kernel<<<b.kavg_blocks, 256, 0, ctx->stream>>>(in + (size_t)cg::F_K * N + off,
+                                                               in + (size_t)cg::F_PHI * N + off, n, b.frw.get_phi,
+                                                               b.kavg_partial);
+  part_final_kernel<<<1, 256, 0, ctx->stream>>>(b.kavg_partial, b.kavg_blocks, 2, 2, b.kavg_sums);
+  CG_CUDA(ctx, cudaGetLastError());
+  *dsums = b.kavg_sums;
+  return CG_OK;
+}
+
+int cg_set_kavg(cg_ctx* ctx, int box, const double* dsums) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  if (!dsums) return fail(ctx, CG_ERR_INVALID, "dsums is null");
+  Box& b = ctx->boxes[box];
+  if (!b.needs_kavg || b.mixed) return fail(ctx, CG_ERR_INVALID, "the box's lapse does not use K_avg");
+  kavg_from_sums_kernel<<<1, 32, 0, ctx->stream>>>(dsums, b.kavg);
+  CG_CUDA(ctx, cudaGetLastError());
+  b.kavg_set = true;
   return CG_OK;
 }
 

@@ -19,8 +19,10 @@ Two exchanges:
 * ``DistHalo``: one slab per rank; ghost planes travel as point-to-point
   messages through ``torch.distributed`` (NCCL between GPUs, gloo on CPU).
 
-Lapses that use the grid average of K are not available for slabs (the C ABI
-rejects them).  FP32-mixed slabs hold FP32 perturbations about one uniform
+Lapses that use the grid average of K need the whole box's K_avg before every
+substep: each slab's two sums (``cg_kavg_sums``) are added up (across ranks:
+an all-reduce) and handed back (``cg_set_kavg``).  FP32-mixed slabs hold FP32
+perturbations about one uniform
 background, which must be the whole box's: the slabs' sums of the background
 fields are added up (across ranks: an all-reduce) and every slab gets the
 same means (``cg_set_background``) before the first step.
@@ -101,6 +103,22 @@ def background_sums(ev: Evolution, box: int) -> np.ndarray:
     return out
 
 
+KAVG_LAPSES = ("ConformalFLRW", "Anharmonic", "OnePlusLog")
+
+
+def _kavg_sums(ev: Evolution, box: int):
+    """torch view of the box's two K_avg sums over its updated points (queued)."""
+    import torch
+
+    p = ctypes.c_void_p()
+    ev._check(ev.L.cg_kavg_sums(ev.ctx, box, ctypes.byref(p)))
+    return torch.as_tensor(_CudaArray(p.value, (2,), "<f8"), device="cuda")
+
+
+def _set_kavg(ev: Evolution, box: int, sums) -> None:
+    ev._check(ev.L.cg_set_kavg(ev.ctx, box, ctypes.c_void_p(sums.data_ptr())))
+
+
 def set_background(ev: Evolution, box: int, sums: np.ndarray) -> None:
     means = np.ascontiguousarray(sums[:5] / sums[5])
     ev._check(ev.L.cg_set_background(ev.ctx, box, means.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 5))
@@ -129,6 +147,13 @@ class LocalHalo:
         ev = self.ev
         arrays = [_substep_arrays(ev, b, t.fields.shape[0], t.shape, self.mixed) for b, t in enumerate(ev.templates)]
         fill_ghosts(arrays, self.ghost)
+
+    def kavg(self) -> None:
+        """The whole box's K_avg for every slab's next substep."""
+        ev = self.ev
+        total = sum(_kavg_sums(ev, b) for b in range(len(ev.templates)))
+        for b in range(len(ev.templates)):
+            _set_kavg(ev, b, total)
 
     def background(self) -> None:
         """One background for every slab: the whole box's means."""
@@ -180,6 +205,14 @@ class DistHalo:
         t = ev.templates[0]
         self.exchange_arrays(_substep_arrays(ev, 0, t.fields.shape[0], t.shape, mixed))
 
+    def kavg(self, ev: Evolution) -> None:
+        """The whole box's K_avg for this rank's next substep: the slabs' sums
+        all-reduced in place (the same call on every rank)."""
+        sums = _kavg_sums(ev, 0)
+        if self.size > 1:
+            self.dist.all_reduce(sums, group=self.group)
+        _set_kavg(ev, 0, sums)
+
     def background(self, ev: Evolution) -> None:
         """One background for every rank's slab: the all-reduced sums."""
         import torch
@@ -214,6 +247,7 @@ class SlabEvolution:
         self.ghost = ghost
         self.halo = halo
         self.mixed = cfg.precision == "mixed"
+        self.needs_kavg = cfg.lapse in KAVG_LAPSES
         self.local = LocalHalo(self.ev, ghost, self.mixed) if halo is None else None
         self.started = False
         if self.mixed:  # the whole box's uniform background in every slab
@@ -230,6 +264,8 @@ class SlabEvolution:
                 self.local.exchange()
             else:
                 self.halo.exchange(self.ev, self.mixed)
+            if self.needs_kavg:
+                (self.local.kavg() if self.local is not None else self.halo.kavg(self.ev))
 
     def step(self, nsteps: int = 1) -> None:
         for _ in range(nsteps):
@@ -261,4 +297,4 @@ class SlabEvolution:
 
 
 __all__ = ["ghost_width", "slab_bounds", "split", "assemble", "fill_ghosts", "background_sums", "set_background",
-           "LocalHalo", "DistHalo", "SlabEvolution", "FLUX_ARRAYS"]
+           "LocalHalo", "DistHalo", "SlabEvolution", "FLUX_ARRAYS", "KAVG_LAPSES"]

@@ -95,8 +95,9 @@ typedef struct {
                               that the caller refreshes from the neighbouring
                               slabs before every substep (cg_substep_input);
                               kernels update the nx - 2g interior planes only.
-                              Lapses without K_avg; FP32-mixed slabs of one
-                              box share a background (cg_set_background); g a
+                              Lapses with K_avg take it from the caller
+                              (cg_set_kavg); FP32-mixed slabs of one box share
+                              a background (cg_set_background); g a
                               multiple of 4, >= the stencil radius (and the
                               Kreiss-Oliger radius), nx - 2g a positive
                               multiple of 4.                                   */
@@ -288,6 +289,18 @@ int cg_substep_input(cg_ctx *ctx, int box, void **input, void **flux);
  * field 18, field 19; NULL: its own means again) for the next step
  * initialisation.  Synchronous.  No reference counterpart. */
 int cg_background_sums(cg_ctx *ctx, int box, double *out, int n);
+
+/* x-slabs whose lapse uses the grid average of K (ConformalFLRW, Anharmonic,
+ * OnePlusLog; BSSN::setExtraFieldData, bssn.cc:165-213) take the whole box's
+ * K_avg = sum w K / sum w, w = exp(6 (DIFFphi + phi_FRW)).  Before each
+ * substep: cg_kavg_sums queues this slab's two sums over its updated points
+ * of the next substep's input into device memory and returns their address;
+ * the caller adds up every slab's sums (e.g. an all-reduce on the context's
+ * stream) and passes the device address of the totals to cg_set_kavg, which
+ * queues K_avg for the next cg_rk_stage (which refuses to run without it).
+ * FP64 boxes.  No reference counterpart. */
+int cg_kavg_sums(cg_ctx *ctx, int box, double **dsums);
+int cg_set_kavg(cg_ctx *ctx, int box, const double *dsums);
 int cg_set_background(cg_ctx *ctx, int box, const double *means, int n);
 
 /* Constraint statistics of one box between steps (after cg_step_init or a

@@ -95,3 +95,30 @@ def test_mixed_slab_constraints_are_refused():
         se.step(1)
         with pytest.raises(RuntimeError, match="x-slab"):
             se.ev.constraints(0)
+
+
+@pytest.mark.parametrize("lapse", ["OnePlusLog", "ConformalFLRW"])
+def test_slabs_with_a_kavg_lapse(lapse):
+    """Lapses that use the grid average of K: every slab takes the whole box's
+    K_avg (the slabs' sums added up) before each substep.  The sums run in a
+    different order than the undivided box's, so the agreement is to
+    roundoff, not bit for bit."""
+    st = ics.perturbed((24, 16, 32), S.DUST, seed=12, amp=1e-3)
+    cfg = BoxConfig(order=4, lapse=lapse)
+    g = slab.ghost_width(4)
+    with slab.SlabEvolution(slab.split(st, 3, g), cfg, g) as se:
+        se.step(3)
+        got = slab.assemble(se.download(), g)
+    want = evolve(st, 3, cfg)
+    for f in range(want.fields.shape[0]):
+        scale = max(np.abs(want.fields[f]).max(), 1e-300)
+        assert np.abs(got.fields[f] - want.fields[f]).max() <= 1e-12 * scale, want.names[f]
+
+
+def test_kavg_slab_refuses_a_substep_without_kavg():
+    st = ics.perturbed((16, 8, 8), S.DUST, seed=2, amp=1e-3)
+    part = slab.split(st, 1, 4)[0]
+    with Evolution(part, BoxConfig(order=4, lapse="OnePlusLog", x_ghost=4)) as ev:
+        ev.step_init()
+        with pytest.raises(RuntimeError, match="cg_set_kavg"):
+            ev.rk_stage(1)
