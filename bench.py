@@ -476,7 +476,7 @@ def run_reference_arm(a, world, rank):
     line = dict(base, value=rate, unit="grid-pt RK4 updates/s", n_gpus=a.gpus, steps=len(step_s),
                 warmup=warm, ms_per_step=1e3 * tot / len(step_s), higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="f64", data="synthetic",
-                config={"workload": (f"bssn_dust_{n}cubed_o{order}" if a.workload == "box" else
+                config={"workload": (f"bssn_dust_{n}cubed_o{order}" if a.workload != "ensemble" else
                                      "ensemble_48_boxes_16x32c_16x64c_16x96c_o4_mixed"),
                         "n": n, "stencil_order": order, "lapse": "Harmonic", "parallelism": "host threads"},
                 cpu_baseline={"value": rate, "unit": "grid-pt RK4 updates/s", "cores": threads,
