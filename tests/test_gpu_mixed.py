@@ -130,3 +130,30 @@ def test_grf_dust_128_order8_500_steps():
     assert delta_err < 1e-4 * 1e-4  # below 1e-4 of the density-contrast amplitude
     assert hmx <= 2.0 * h64 and mmx <= 2.0 * m64
 
+
+
+def test_grf_scalar_256_order8_200_steps():
+    """256^3, 8th order, BSSN + scalar field with V = m^2 phi^2 / 2 (m = 1),
+    phi_0 = 1e-2 plus a k^-3 random fluctuation of rms 1e-5, 200 RK4 steps:
+    the mixed form against the FP64 run.  The scalar field's error is stated
+    against the fluctuation amplitude; every field against its spread; the
+    Hamiltonian constraint norm no worse than twice FP64's."""
+    st = ics.grf_scalar(256, seed=4, phi0=1e-2, rms=1e-5, order=8)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        cfg = BoxConfig(order=8, precision=prec, potential="quadratic", pot_mass=1.0)
+        with Evolution(st, cfg) as ev:
+            ev.step(200)
+            ev.synchronize()
+            res[prec] = (ev.download(0), ev.constraints(0))
+    ref, got = res["fp64"][0], res["mixed"][0]
+    errs = perturbation_errors(got.fields, ref.fields, st.names)
+    worst = max(errs, key=errs.get)
+    f = st.names.index("phi")
+    phi_err = float(np.abs(got.fields[f] - ref.fields[f]).max()) / 1e-5
+    h64, hmx = res["fp64"][1]["H"][7], res["mixed"][1]["H"][7]
+    print("256^3 scalar o8 200 steps: worst field", worst, errs[worst], "phi error / fluctuation rms", phi_err,
+          "H L2", hmx, h64)
+    assert errs[worst] < 1e-4, errs
+    assert phi_err < 1e-6
+    assert hmx <= 2.0 * h64
