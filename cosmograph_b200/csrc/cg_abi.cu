@@ -1219,8 +1219,21 @@ int write_table(cg_ctx* ctx, Group& g) {
       e.first = first;
       first += e.nbx * e.nby * e.nbz;
     }
-    if (!g.table) CG_CUDA(ctx, cudaMalloc(&g.table, sizeof(cg::GroupBox) * m));
-    CG_CUDA(ctx, cudaMemcpyAsync(g.table, t.data(), sizeof(cg::GroupBox) * m, cudaMemcpyHostToDevice, ctx->stream));
+    // the members' flux-primitive maps follow the GroupBox entries
+    std::vector<cg::GroupFluxMaps> fm(m);
+    for (size_t q = 0; q < m; ++q) {
+      const Box& b = ctx->boxes[order[q]];
+      for (int a = 0; a < 3; ++a) {
+        fm[q].fp0[a] = b.dev.fmap0[a];
+        fm[q].fp1[a] = b.dev.fmap1[a];
+      }
+      fm[q].valid = b.dev.fmaps && b.dev.tma;
+    }
+    const size_t tb = sizeof(cg::GroupBox) * m;
+    if (!g.table) CG_CUDA(ctx, cudaMalloc(&g.table, tb + sizeof(cg::GroupFluxMaps) * m));
+    CG_CUDA(ctx, cudaMemcpyAsync(g.table, t.data(), tb, cudaMemcpyHostToDevice, ctx->stream));
+    CG_CUDA(ctx, cudaMemcpyAsync(static_cast<char*>(g.table) + tb, fm.data(), sizeof(cg::GroupFluxMaps) * m,
+                                 cudaMemcpyHostToDevice, ctx->stream));
     CG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   g.total = first;

@@ -22,6 +22,14 @@ struct GroupBox {
   int nbx, nby, nbz;
   int first;
 };
+// TMA maps of a member's dust flux primitives (FP0, FP1; the x, y and z boxes
+// of the divergence), stored after the GroupBox entries in the same device
+// table (entry q at (GroupFluxMaps*)(table + nboxes) + q).
+struct GroupFluxMaps {
+  CUtensorMap fp0[3], fp1[3];
+  int valid;
+};
+static_assert(sizeof(GroupBox) % alignof(GroupFluxMaps) == 0, "the flux maps after the GroupBox entries stay aligned");
 constexpr int kMaxGroupBoxes = 64;
 // Per-substep values of every box of an FP64 group (kernel parameter, by value).
 struct GroupBg {

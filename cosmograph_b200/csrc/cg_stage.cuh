@@ -1229,6 +1229,7 @@ stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
   __shared__ StagePtrs sp;
   __shared__ StageBg sbg;
   __shared__ const CUtensorMap* stm;
+  __shared__ const FluxMaps* sfm;
   __shared__ __align__(8) uint64_t bar[2];
   const bool lead = threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0;
   init_tile_barriers(bar, true);
@@ -1248,12 +1249,20 @@ stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
       // the map is read from global memory (a TMA map cannot live in shared memory)
       stm = boxes[lo].tma ? (stage == 1 || stage == 3 ? &boxes[lo].mapX : &boxes[lo].mapY) : nullptr;
       if (stm) tma::acquire_map(stm);  // the host wrote the map into the table
+      sfm = nullptr;
+      if (MATTER == kDust && stm) {  // the flux-primitive boxes, after the GroupBox entries
+        const GroupFluxMaps& fx = reinterpret_cast<const GroupFluxMaps*>(boxes + gb.nboxes)[lo];
+        if (fx.valid) {
+          sfm = reinterpret_cast<const FluxMaps*>(stage == 1 || stage == 3 ? fx.fp0 : fx.fp1);
+          for (int a = 0; a < 3; ++a) tma::acquire_map(&sfm->m[a]);
+        }
+      }
     }
     __syncthreads();
     const int l = w - sb.first;
     const int cz = l % sb.nbz, cy = (l / sb.nbz) % sb.nby, cx = l / (sb.nbz * sb.nby);
     const BoxGeom geo{sb.nx, sb.ny, sb.nz, sb.pts, 0};
-    stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0, stm, bar, phase, tma_ok);
+    stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0, stm, bar, phase, tma_ok, sfm);
   }
 }
 
