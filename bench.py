@@ -184,9 +184,45 @@ def accuracy(ref, got, h_ref, h_got) -> dict:
             "M_L2": float(h_got["M"][7]), "M_L2_fp64": float(h_ref["M"][7])}
 
 
-def cpu_baseline(st, order: int, budget_s: float = 30.0):
-    """The reference's own sources on the host cores (oracle/_ref, fast build);
-    one RK4 step of the same box, all host threads."""
+def box_config(n: int, order: int, precision: str, world: int) -> dict:
+    """The workload description both arms print (ours and --impl reference)."""
+    state_gb = 22 * n ** 3 * 8 / 1e9
+    return {"workload": f"bssn_dust_{n}cubed_o{order}", "n": n, "stencil_order": order, "lapse": "Harmonic",
+            "precision": precision, "boxes_per_gpu": 1, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (state %.1f GB per box)" % state_gb}
+
+
+def ensemble_config(specs, world: int, groups=None) -> dict:
+    all_pts = sum(s.points for s in specs)
+    state_gb = 22 * all_pts * 8 / 1e9
+    d = {"workload": "ensemble_48_boxes_16x32c_16x64c_16x96c_o4_mixed", "boxes": len(specs),
+         "points": all_pts, "stencil_order": 4, "lapse": "Harmonic", "precision": "mixed",
+         "seeds": f"{specs[0].seed}..{specs[-1].seed}", "parallelism": f"boxes split over {world} ranks",
+         "l2": "inputs larger than L2 (ensemble state %.1f GB)" % state_gb}
+    return d
+
+
+def _reference_steps(binp: Path, st, steps: int, threads: int, timeout: float = 1800.0):
+    """Runs an oracle/_ref binary for `steps` RK4 steps of `st`; returns the
+    per-step seconds of its step loop (timed like _timer["RK_steps"])."""
+    with tempfile.TemporaryDirectory(prefix="cg_bench_cpu_") as tmp:
+        tmp = Path(tmp)
+        (tmp / "config.txt").write_text("lapse = Harmonic\n")
+        st.save(tmp / "in.bin")
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        proc = subprocess.run([str(binp), "evolve", str(tmp / "config.txt"), str(tmp / "in.bin"),
+                               str(tmp / "out.bin"), str(steps)], capture_output=True, text=True, env=env,
+                              timeout=timeout)
+    if proc.returncode != 0:
+        raise RuntimeError(f"{binp.name} failed ({proc.returncode}): {proc.stderr[-300:]}")
+    return [float(l.split()[2]) for l in proc.stdout.splitlines() if l.startswith("CGSTEP")]
+
+
+def cpu_baseline(st, order: int, steps: int = 3):
+    """The reference's own sources on the host cores (oracle/_ref, fast build):
+    `steps` RK4 steps of the same box on all host threads, plus the 1-thread
+    rate of the same physics on a 64^3 box of the same order (a full 256^3
+    step on one thread takes minutes)."""
     from oracle import build_ref
 
     nx, ny, nz = st.shape
@@ -194,26 +230,26 @@ def cpu_baseline(st, order: int, budget_s: float = 30.0):
     threads = os.cpu_count() or 1
     if not binp.exists():
         return None
-    with tempfile.TemporaryDirectory(prefix="cg_bench_cpu_") as tmp:
-        tmp = Path(tmp)
-        (tmp / "config.txt").write_text("lapse = Harmonic\n")
-        st.save(tmp / "in.bin")
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-        t0 = time.time()
-        proc = subprocess.run([str(binp), "evolve", str(tmp / "config.txt"), str(tmp / "in.bin"),
-                               str(tmp / "out.bin"), "1"], capture_output=True, text=True, env=env,
-                              timeout=600)
-        wall = time.time() - t0
-    if proc.returncode != 0:
-        return None
-    step_s = [float(l.split()[2]) for l in proc.stdout.splitlines() if l.startswith("CGSTEP")]
+    t0 = time.time()
+    step_s = _reference_steps(binp, st, steps, threads)
+    wall = time.time() - t0
     if not step_s:
         return None
     rate = nx * ny * nz * len(step_s) / sum(step_s)
-    return {"value": rate, "unit": "grid-pt RK4 updates/s", "cores": threads, "kind": "reference",
-            "sample": f"1 RK4 step of the same {nx}x{ny}x{nz} order-{order} BSSN+dust box, reference "
-                      f"sources built -O3 -ffast-math -march=x86-64-v3 -fopenmp ({binp.name}); "
-                      f"{sum(step_s):.2f} s of step loop, {wall:.1f} s wall"}
+    out = {"value": rate, "unit": "grid-pt RK4 updates/s", "cores": threads, "kind": "reference",
+           "sample": f"{len(step_s)} RK4 steps of the same {nx}x{ny}x{nz} order-{order} BSSN+dust box, reference "
+                     f"sources built -O3 -ffast-math -march=x86-64-v3 -fopenmp ({binp.name}); "
+                     f"{sum(step_s):.2f} s of step loop, {wall:.1f} s wall; per step "
+                     + ", ".join(f"{s:.2f}" for s in step_s) + " s"}
+    one = build_ref.binary_path(64, 64, 64, order, "fast")
+    if one.exists():
+        small = make_state(64, seed=1, order=order, gpu=False)
+        s1 = _reference_steps(one, small, 2, 1)
+        if s1:
+            out["one_thread"] = {"value": 64 ** 3 * len(s1) / sum(s1), "unit": "grid-pt RK4 updates/s",
+                                 "cores": 1, "sample": f"{len(s1)} RK4 steps of a 64^3 order-{order} BSSN+dust "
+                                                       f"GRF box on one thread ({one.name})"}
+    return out
 
 
 def run_ensemble(a, world, rank, local):
@@ -347,11 +383,8 @@ def run_ensemble(a, world, rank, local):
         "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic",
-        "config": {"workload": "ensemble_48_boxes_16x32c_16x64c_16x96c_o4_mixed", "boxes": len(specs),
-                   "points": all_pts, "stencil_order": 4, "lapse": "Harmonic", "precision": "mixed",
-                   "seeds": f"{specs[0].seed}..{specs[-1].seed}", "parallelism": f"boxes split over {world} ranks",
-                   "l2": "inputs larger than L2 (ensemble state %.1f GB)" % (state_bytes * world / 1e9),
-                   "groups": groups},
+        "config": ensemble_config(specs, world),
+        "groups": groups,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_update": ALGO_BYTES_MIXED_DUST},
         "e2e": {"value": all_pts * a.e2e_steps / (e2e_ms / 1e3), "unit": "grid-pt RK4 updates/s",
@@ -476,9 +509,8 @@ def run_reference_arm(a, world, rank):
     line = dict(base, value=rate, unit="grid-pt RK4 updates/s", n_gpus=a.gpus, steps=len(step_s),
                 warmup=warm, ms_per_step=1e3 * tot / len(step_s), higher_is_better=True, scaling="weak",
                 vs_baseline=None, dtype="f64", data="synthetic",
-                config={"workload": (f"bssn_dust_{n}cubed_o{order}" if a.workload != "ensemble" else
-                                     "ensemble_48_boxes_16x32c_16x64c_16x96c_o4_mixed"),
-                        "n": n, "stencil_order": order, "lapse": "Harmonic", "parallelism": "host threads"},
+                config=(box_config(n, order, a.precision, world) if a.workload != "ensemble" else
+                        ensemble_config(ensemble.standard_ensemble(), world)),
                 cpu_baseline={"value": rate, "unit": "grid-pt RK4 updates/s", "cores": threads,
                               "kind": "reference",
                               "sample": f"{len(step_s)} RK4 steps (of {a.steps} requested) of one "
@@ -653,10 +685,7 @@ def main():
             "vs_baseline": None,
             "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"bssn_dust_{n}cubed_o{a.order}", "n": n, "stencil_order": a.order,
-                       "lapse": "Harmonic", "precision": a.precision, "boxes_per_gpu": 1,
-                       "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (state %.1f GB per box)" % (state_bytes / 1e9)},
+            "config": box_config(n, a.order, a.precision, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": algo},

@@ -175,7 +175,7 @@ __global__ void kavg_partial_kernel(const double* __restrict__ K, const double* 
                                     double phi_FRW, double* partial) {
   __shared__ double sK[256], sV[256];
   double aK = 0.0, aV = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < pts; q += gridDim.x * blockDim.x) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < pts; q += (long long)gridDim.x * blockDim.x) {
     const double e = exp(6.0 * (phi[q] + phi_FRW));
     aK += e * K[q];
     aV += e;
@@ -247,7 +247,7 @@ __global__ void field_sums_kernel(const double* f0, const double* f1, const doub
                                   const double* f4, int n, double* part) {
   __shared__ double s[5][256];
   double a[5] = {0, 0, 0, 0, 0};
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     a[0] += f0[q];
     a[1] += f1[q];
     a[2] += f2[q];
@@ -279,7 +279,7 @@ __global__ void constraint_stdev_kernel(const double* cvals, size_t stride, int 
     mean[2 * m + 1] = r1[10 + m] / n;
   }
   for (int m = 0; m < 10; ++m) acc[m] = 0.0;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
     for (int m = 0; m < 10; ++m) {
       const double d = cvals[(size_t)m * stride + off + q] - mean[m];
       acc[m] += d * d;
@@ -303,7 +303,7 @@ __global__ void wstats_sum_kernel(const double* f0, const double* f1, const doub
   __shared__ double s[5][256];
   double a[5] = {0, 0, 0, 0, 0};
   const double* f[4] = {f0, f1, f2, f3};
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     const double w = exp(6.0 * (phi[q] + phi_frw));
     for (int m = 0; m < 4; ++m) a[m] += w * f[m][q];
     a[4] += w;
@@ -329,7 +329,7 @@ __global__ void wstats_var_kernel(const double* f0, const double* f1, const doub
   const double* f[4] = {f0, f1, f2, f3};
   const double vol = r1[4] / n;
   for (int m = 0; m < 4; ++m) avg[m] = r1[m] / n / vol;
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     const double w = exp(6.0 * (phi[q] + phi_frw));
     for (int m = 0; m < 4; ++m) {
       const double d = avg[m] - f[m][q];
@@ -354,11 +354,17 @@ void set_global_error(const char* msg) { g_create_error = msg; }
 
 // Conformal average of `field` weighted by exp(6 (phi + phi_FRW)) into
 // out[0] on the device, using `partial` (2*nblk doubles) as scratch.
+// The status is that of these two launches alone (cudaLaunchKernel returns
+// the launch's own error), so an error left pending by an earlier, unrelated
+// launch on the calling thread is neither reported nor cleared here.
 cudaError_t launch_conformal_average(const double* field, const double* phi, int n, double phi_frw,
                                      double* partial, int nblk, double* out, cudaStream_t st) {
-  kavg_partial_kernel<<<nblk, 256, 0, st>>>(field, phi, n, phi_frw, partial);
-  kavg_final_kernel<<<1, 256, 0, st>>>(partial, nblk, n, out);
-  return cudaGetLastError();
+  void* a1[] = {(void*)&field, (void*)&phi, (void*)&n, (void*)&phi_frw, (void*)&partial};
+  cudaError_t e = cudaLaunchKernel((const void*)kavg_partial_kernel, dim3(nblk), dim3(256), a1, 0, st);
+  if (e != cudaSuccess) return e;
+  const double* cpartial = partial;
+  void* a2[] = {(void*)&cpartial, (void*)&nblk, (void*)&n, (void*)&out};
+  return cudaLaunchKernel((const void*)kavg_final_kernel, dim3(1), dim3(256), a2, 0, st);
 }
 }  // namespace cg
 

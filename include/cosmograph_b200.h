@@ -343,7 +343,12 @@ int cg_conformal_average(cg_ctx *ctx, const double *d_field, const double *d_phi
  *     (a cudaStream_t, NULL = legacy default stream), no host synchronisation.
  *   - The first call on a device looks up the scratch array's device address
  *     with that device current; make that first call before any stream
- *     capture begins.
+ *     capture begins.  The address is then kept per device index for the
+ *     rest of the process: after a cudaDeviceReset of that device the kept
+ *     address is stale, so do not call this entry point again in that
+ *     process.
+ *   - Only errors of this call's own launches are returned; an error left
+ *     pending by earlier work on the calling thread is not cleared.
  *   - All calls on a GPU share the scratch: calls whose kernels overlap on the
  *     GPU (different streams, concurrent threads) race; serialise them. */
 #define CG_NOALLOC_MAX_BLOCKS 1024

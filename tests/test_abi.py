@@ -72,3 +72,19 @@ def test_create_rejects_bad_descriptors(L, field, value, msg):
     rc = L.cg_create(ctypes.byref(d), 1, ctypes.byref(h))
     assert rc == -1 and not h.value
     assert msg in L.cg_last_error(None).decode()
+
+
+@pytest.mark.parametrize("n", [0, (1 << 30) + 1, 1 << 31, (1 << 32) + 5])
+def test_noalloc_average_rejects_sizes_before_touching_cuda(L, n):
+    """The allocation-free average checks n against its fixed scratch (at most
+    CG_NOALLOC_MAX_POINTS = 2^30 points) before any CUDA call, so the check
+    runs without a GPU."""
+    rc = L.cg_conformal_average_noalloc(ctypes.c_void_p(16), ctypes.c_void_p(16), n, 0.0, ctypes.c_void_p(16), None)
+    assert rc == -1
+    assert b"n must be in 1.." in L.cg_last_error(None)
+
+
+def test_conformal_average_rejects_a_null_context(L):
+    rc = L.cg_conformal_average(None, ctypes.c_void_p(16), ctypes.c_void_p(16), 1 << 31, 0.0,
+                                ctypes.byref(ctypes.c_double()))
+    assert rc == -1

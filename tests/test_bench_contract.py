@@ -30,5 +30,9 @@ def test_reference_arm_prints_one_contract_line():
     assert KEYS <= set(d), KEYS - set(d)
     assert d["impl"] == "reference" and d["value"] > 0 and d["higher_is_better"] is True
     assert d["config"]["workload"] == "bssn_dust_16cubed_o4"
+    # the same workload description as the GPU arm prints
+    import bench
+
+    assert d["config"] == bench.box_config(16, 4, "fp64", 1)
     assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]

@@ -82,6 +82,26 @@ def test_against_restatement(matter, shape, order, lapse, steps):
     assert worst(errs)[1] <= TOL["fp64"], worst(errs)
 
 
+@pytest.mark.parametrize("order,shape,steps", [(4, (20, 16, 24), 12), (8, (24, 24, 24), 8)])
+def test_quadratic_potential_against_restatement(order, shape, steps):
+    """V(phi) = m^2 phi^2 / 2 (m = 1) on the scalar field's GRF initial data
+    (phi_0 = 1e-2, rms delta phi 1e-5, k^-3 spectrum cut at N/4).  The
+    reference has only a constant potential (scalar.cc:262-274); the
+    restatement's dV term (oracle/cg_oracle.c, pot_dV) is the checker here.
+    The potential must make a difference: the same run with the constant
+    potential differs from it."""
+    st = ics.grf_scalar(shape, seed=7, phi0=1e-2, rms=1e-5, mass=1.0, order=order)
+    kw = dict(lapse="Harmonic", potential="quadratic", pot_mass=1.0)
+    ref = oracle.evolve(st, steps, order, **kw)
+    got = evolve(st, steps, BoxConfig(order=order, **kw))
+    errs = field_errors(got.fields, ref.fields, st.names, floor=1e-18)
+    print("quadratic potential order", order, "worst", worst(errs))
+    assert worst(errs)[1] <= TOL["fp64"], worst(errs)
+    const = evolve(st, steps, BoxConfig(order=order, lapse="Harmonic"))
+    pi = st.names.index("Pi")
+    assert np.abs(const.fields[pi] - got.fields[pi]).max() > 1e3 * np.abs(got.fields[pi] - ref.fields[pi]).max()
+
+
 @pytest.mark.parametrize("matter,shape,order", [(S.DUST, (20, 18, 22), 8), (S.VACUUM, (12, 14, 16), 2),
                                                  (S.SCALAR, (16, 16, 16), 8), (S.DUST, (16, 16, 16), 4)])
 def test_kreiss_oliger_against_restatement(matter, shape, order):
