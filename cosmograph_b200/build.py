@@ -32,7 +32,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *ARCH, f"-I{I
 
 # (object name, source, extra flags)
 UNITS = [
-    ("stage_exact.o", "cg_stage_inst.cu", ["--fmad=false", "-DCG_VARIANT_NS=exact"]),
+    ("stage_exact.o", "cg_stage_inst.cu", ["--fmad=false", "-DCG_VARIANT_NS=exact", "-DCG_REFERENCE_ORDER=1"]),
     ("stage_fast.o", "cg_stage_inst.cu", ["--fmad=true", "-DCG_VARIANT_NS=fast"]),
     ("abi.o", "cg_abi.cu", []),
     ("noalloc.o", "cg_noalloc.cu", []),

@@ -7,8 +7,8 @@
 // scalar-field terms (components/scalar/scalar.cc:132-260), evaluated for one
 // point by one thread.  Operand order inside every expression follows the
 // reference so that, compiled without FMA contraction, the FP64 kernel
-// reproduces the reference's rounding except where CUDA's exp/log1p/expm1
-// differ from the host libm by an ulp.
+// reproduces the reference's rounding (with e^x, expm1 and log1p correctly
+// rounded, as an exact C library returns them).
 //
 // Finite differences use the reference's centred stencils of order 2/4/6/8
 // (utils/math.h:74-1085): first derivatives on the 2r axis points, second
@@ -19,6 +19,7 @@
 // units compiled with and without FMA contraction never share a symbol.
 #pragma once
 
+#include "cg_crmath.h"
 #include "cg_types.h"
 
 #ifndef CG_VARIANT_NS
@@ -27,6 +28,28 @@
 
 namespace cg {
 namespace CG_VARIANT_NS {
+
+// The parity build (compiled with -DCG_REFERENCE_ORDER=1 and without FMA
+// contraction) evaluates every expression in the reference's operand order
+// and takes e^x, expm1 and log1p correctly rounded (cg_crmath.h), the values
+// any exact C library returns; the FMA build uses CUDA's functions.
+#ifndef CG_REFERENCE_ORDER
+#define CG_REFERENCE_ORDER 0
+#endif
+constexpr bool kReferenceOrder = CG_REFERENCE_ORDER != 0;
+
+__device__ __forceinline__ double xexp(double x) {
+  if constexpr (kReferenceOrder) return crm::exp(x);
+  else return ::exp(x);
+}
+__device__ __forceinline__ double xexpm1(double x) {
+  if constexpr (kReferenceOrder) return crm::expm1(x);
+  else return ::expm1(x);
+}
+__device__ __forceinline__ double xlog1p(double x) {
+  if constexpr (kReferenceOrder) return crm::log1p(x);
+  else return ::log1p(x);
+}
 
 __device__ __forceinline__ int wrap(int v, int n) {
   v = v < 0 ? v + n : v;
@@ -147,7 +170,7 @@ __device__ __forceinline__ void normalize_point(double g[6], double A[6]) {
   double omd = -1.0 * (g[0] + g[3] + g[5] - g[1] * g[1] - g[2] * g[2] - g[4] * g[4] + g[0] * g[3] +
                        g[0] * g[5] + g[3] * g[5] - g[4] * g[4] * g[0] - g[2] * g[2] * g[3] -
                        g[1] * g[1] * g[5] + 2.0 * g[1] * g[2] * g[4] + g[0] * g[3] * g[5]);
-  double t = -1.0 * expm1(log1p(-1.0 * omd) / 3.0);
+  double t = -1.0 * xexpm1(xlog1p(-1.0 * omd) / 3.0);
   g[0] = (g[0] + t) / (1.0 - t);
   g[3] = (g[3] + t) / (1.0 - t);
   g[5] = (g[5] + t) / (1.0 - t);
@@ -173,8 +196,8 @@ struct DustPrim {
 __device__ __forceinline__ DustPrim dust_prim(const double gi[6], double phi, double D,
                                               const double S[3]) {
   DustPrim d;
-  const double em4phi = exp(-4.0 * phi);
-  const double e6phi = exp(6.0 * phi);
+  const double em4phi = xexp(-4.0 * phi);
+  const double e6phi = xexp(6.0 * phi);
   const double giIJSISJ = em4phi * (gi[0] * S[0] * S[0] + gi[3] * S[1] * S[1] + gi[5] * S[2] * S[2] +
                                     2.0 * (gi[1] * S[0] * S[1] + gi[2] * S[0] * S[2] + gi[4] * S[1] * S[2]));
   d.W = sqrt(1.0 + giIJSISJ / D / D);

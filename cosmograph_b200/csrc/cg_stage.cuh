@@ -711,7 +711,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   double gm[6];
   gm[0] = g[0] + 1.0; gm[1] = g[1]; gm[2] = g[2];
   gm[3] = g[3] + 1.0; gm[4] = g[4]; gm[5] = g[5] + 1.0;
-  const double em4phi = exp(-4.0 * phi);
+  const double em4phi = xexp(-4.0 * phi);
 
   // -- sources and matter centre quantities --
   double rhs_m[5] = {0, 0, 0, 0, 0};
@@ -723,8 +723,8 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       // the stepInit populate used this same state (sims/dust.cc:56-62)
       const DustPrim dp = dust_prim(gi, phi, D, Sv);
       Wl = dp.W;
-      const double e4 = exp(4.0 * phi);
-      detgl = exp(6.0 * phi);
+      const double e4 = xexp(4.0 * phi);
+      detgl = xexp(6.0 * phi);
 #pragma unroll
       for (int m = 0; m < 6; ++m) gph[m] = e4 * gm[m];
     } else {
@@ -738,8 +738,8 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       inv_metric(gp, gip);
       const DustPrim dp = dust_prim(gip, phip, Dp, Sp);
       Wl = dp.W;
-      const double e4 = exp(4.0 * phip);
-      detgl = exp(6.0 * phip);
+      const double e4 = xexp(4.0 * phip);
+      detgl = xexp(6.0 * phip);
       gph[0] = e4 * (gp[0] + 1.0); gph[1] = e4 * gp[1]; gph[2] = e4 * gp[2];
       gph[3] = e4 * (gp[3] + 1.0); gph[4] = e4 * gp[4]; gph[5] = e4 * (gp[5] + 1.0);
     }
@@ -749,7 +749,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     for (int m = 0; m < Q_N; ++m) S(S_SRC + m) = q[m];
     // momentum source S_m^src (dust.cc:135-146) with the current W, v
     const DustPrim cur = dust_prim(gi, phi, D, Sv);
-    const double e4 = exp(4.0 * phi);
+    const double e4 = xexp(4.0 * phi);
     rhs_m[0] = S(S_MAT + 0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -886,9 +886,32 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   // t4_IJ = sum_{K,M} (H^K_{MI} G_{J,KM} + H^K_{MJ} G_{I,KM})
   //       + sum_{K,L} (H^K_{LI} G_{K,LJ} + H^K_{LJ} G_{K,LI}) / 2.
   // A third of the reference's multiplications, in a different summation
-  // order (the one departure from the reference's operand order in this
-  // kernel; the parity tests hold it to the same bound).
+  // order: the FMA build uses it.  The parity build (kReferenceOrder) sums
+  // the reference's terms in the reference's order, so that its rounding is
+  // the reference's.
   double t4[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if constexpr (kReferenceOrder) {
+    // the parity build: the reference's 27 terms per component, summed over
+    // (K, L, M) with M fastest, each term formed as the macro forms it
+#pragma unroll
+    for (int I = 0; I < 3; ++I)
+#pragma unroll
+      for (int J = I; J < 3; ++J) {
+        double acc = 0.0;
+#pragma unroll
+        for (int Kx = 0; Kx < 3; ++Kx)
+#pragma unroll
+          for (int L = 0; L < 3; ++L)
+#pragma unroll
+            for (int M = 0; M < 3; ++M) {
+              const double u =
+                  gi[sym(L, M)] * (G(Kx, sym(L, I)) * GL(J, sym(Kx, M)) + G(Kx, sym(L, J)) * GL(I, sym(Kx, M)) +
+                                   0.5 * (G(Kx, sym(I, M)) * GL(Kx, sym(L, J)) + G(Kx, sym(J, M)) * GL(Kx, sym(L, I))));
+              acc = (Kx == 0 && L == 0 && M == 0) ? u : acc + u;
+            }
+        t4[sym(I, J)] = acc;
+      }
+  } else {
 #pragma unroll
   for (int Kx = 0; Kx < 3; ++Kx) {
     double Hm[3][3];  // H^K_{MX} = sum_L g^{LM} G^K_{LX}
@@ -910,6 +933,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
         t4[sym(I, J)] = t4[sym(I, J)] + (u + 0.5 * w);
       }
   }
+  }
 #pragma unroll
   for (int I = 0; I < 3; ++I)
 #pragma unroll
@@ -926,7 +950,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   auto Ric = [&](int qq) { return S(S_T1 + qq); };  // full Ricci R_ij (bssn.cc:650-655)
   const double ricci = em4phi * (Ric(0) * gi[0] + Ric(3) * gi[3] + Ric(5) * gi[5] +
                                  2.0 * (Ric(1) * gi[1] + Ric(2) * gi[2] + Ric(4) * gi[4]));
-  const double e4phi = exp(4.0 * phi);
+  const double e4phi = xexp(4.0 * phi);
 
   // -- A^ij, A_ij A^ij (calculate_Acont, bssn.cc:463-472) --
   double A[6], Ac[6];
@@ -950,18 +974,18 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   const double AijAij = Ac[0] * A[0] + Ac[3] * A[3] + Ac[5] * A[5] + 2.0 * (Ac[1] * A[1] + Ac[2] * A[2] + Ac[4] * A[4]);
   const double r = S(S_SRC + Q_R) + bg.rho_FRW;
   // Hamiltonian constraint, bssn.cc:1073-1084 (theta = 0)
-  const double H = -exp(5.0 * phi) / 8.0 * (ricci + 2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0)) - AijAij - 16.0 * kPi * r);
+  const double H = -xexp(5.0 * phi) / 8.0 * (ricci + 2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0)) - AijAij - 16.0 * kPi * r);
 
   if constexpr (MODE == kConstraints) {
     // BSSN::setConstraintCalcs per point (bssn.cc:983-1006)
     double v[5], sc[5];
     v[0] = H;  // hamiltonianConstraintCalc / Scale, bssn.cc:1073-1100
-    sc[0] = (exp(5.0 * phi) / 8.0) * sqrt(ricci * ricci + AijAij * AijAij +
+    sc[0] = (xexp(5.0 * phi) / 8.0) * sqrt(ricci * ricci + AijAij * AijAij +
                                           (2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0))) *
                                               (2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0))) +
                                           (16.0 * kPi * r) * (16.0 * kPi * r));
     {  // momentum, BSSN_MI / BSSN_MI_SCALE (bssn_macros.h:487-527)
-      const double e6 = exp(6.0 * phi);
+      const double e6 = xexp(6.0 * phi);
       double mv[3], ms[3];
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
@@ -1132,7 +1156,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   {
     double v = (-DDaTR + alpha * (1.0 / 3.0 * (Kd + 2.0 * 0.0) * (Kd + 2.0 * 0.0 + 2.0 * bg.K_FRW) + AijAij) +
                 4.0 * kPi * alpha * (S(S_SRC + Q_R) + S(S_SRC + Q_S)) + 4.0 * kPi * alphad * (bg.rho_FRW + bg.S_FRW));
-    if (ph.k_damping_amp != 0.0) v = v - 1.0 * ph.k_damping_amp * H * exp(-5.0 * phi);
+    if (ph.k_damping_amp != 0.0) v = v - 1.0 * ph.k_damping_amp * H * xexp(-5.0 * phi);
     finalize(F_K, v - ko(F_K));
   }
   // ev_DIFFphi (bssn.cc:797-820)

@@ -24,6 +24,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 BUILD_DIR = HERE / "_build"
 LIB_PATH = BUILD_DIR / "libcg_oracle.so"
+# the same restatement with correctly rounded exp, expm1, log1p (cr_libm.h)
+LIB_CR_PATH = BUILD_DIR / "libcg_oracle_cr.so"
 
 LAPSES = {
     "Static": 0, "Harmonic": 1, "ConformalFLRW": 2, "ConformalSync": 3,
@@ -50,28 +52,31 @@ class CgoParams(ctypes.Structure):
 
 
 def build_lib(force: bool = False) -> Path:
-    """Compile the C restatement (strict FP: no FMA contraction)."""
+    """Compile the C restatement (strict FP: no FMA contraction), with the C
+    library's exp/expm1/log1p (libcg_oracle.so) and with correctly rounded
+    ones (libcg_oracle_cr.so)."""
     src = HERE / "cg_oracle.c"
     hdr = HERE / "cg_oracle.h"
-    newest = max(src.stat().st_mtime, hdr.stat().st_mtime)
-    if LIB_PATH.exists() and not force and LIB_PATH.stat().st_mtime >= newest:
-        return LIB_PATH
+    newest = max(src.stat().st_mtime, hdr.stat().st_mtime, (HERE / "cr_libm.h").stat().st_mtime)
     BUILD_DIR.mkdir(exist_ok=True)
-    tmp = LIB_PATH.with_suffix(".so.tmp")
-    subprocess.run(["gcc", "-std=c11", "-O2", "-ffp-contract=off", "-fopenmp", "-fPIC",
-                    "-shared", "-o", str(tmp), str(src), "-lm"], check=True)
-    os.replace(tmp, LIB_PATH)
+    for path, extra in ((LIB_PATH, []), (LIB_CR_PATH, ["-include", str(HERE / "cr_libm.h")])):
+        if path.exists() and not force and path.stat().st_mtime >= newest:
+            continue
+        tmp = path.with_suffix(".so.tmp")
+        subprocess.run(["gcc", "-std=gnu11", "-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", *extra,
+                        "-shared", "-o", str(tmp), str(src), "-lquadmath", "-lm"], check=True)
+        os.replace(tmp, path)
     return LIB_PATH
 
 
-_lib = None
+_libs = {}
 
 
-def lib() -> ctypes.CDLL:
-    global _lib
-    if _lib is None:
-        build_lib()  # no-op when the library is newer than its sources
-        L = ctypes.CDLL(str(LIB_PATH))
+def lib(cr: bool = False) -> ctypes.CDLL:
+    """The restatement; cr=True: with correctly rounded exp, expm1, log1p."""
+    if cr not in _libs:
+        build_lib()  # no-op when the libraries are newer than their sources
+        L = ctypes.CDLL(str(LIB_CR_PATH if cr else LIB_PATH))
         dp = ctypes.POINTER(ctypes.c_double)
         L.cgo_evolve.argtypes = [ctypes.POINTER(CgoParams), dp, ctypes.c_int, dp]
         L.cgo_rhs.argtypes = [ctypes.POINTER(CgoParams), dp, dp]
@@ -81,8 +86,8 @@ def lib() -> ctypes.CDLL:
         L.cgo_frw_evolve.restype = None
         L.cgo_set_threads.argtypes = [ctypes.c_int]
         L.cgo_set_threads.restype = None
-        _lib = L
-    return _lib
+        _libs[cr] = L
+    return _libs[cr]
 
 
 def _ptr(a: np.ndarray):
@@ -109,9 +114,10 @@ def make_params(state, order: int, lapse: str = "Harmonic", normalize_metric: in
     return p
 
 
-def evolve(state, steps: int, order: int, threads: int = 0, **kw):
-    """Run the C restatement for `steps` RK4 steps; returns a new state."""
-    L = lib()
+def evolve(state, steps: int, order: int, threads: int = 0, cr: bool = False, **kw):
+    """Run the C restatement for `steps` RK4 steps; returns a new state.
+    cr=True: with correctly rounded exp, expm1 and log1p."""
+    L = lib(cr)
     if threads:
         L.cgo_set_threads(threads)
     p = make_params(state, order, **kw)

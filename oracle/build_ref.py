@@ -11,6 +11,8 @@ no reference checkout exists.
 Flavours:
   strict : -O2 -ffp-contract=off          (parity oracle; no FMA contraction,
                                             no reassociation)
+  strict_cr : strict, with the C library's exp, expm1 and log1p replaced by
+           correctly rounded ones (cr_libm.c) at link time
   fast   : -O3 -ffast-math -march=x86-64-v3 (the reference's own optimisation
            flags, cmake/optimization.cmake:18, with a portable -march so the
            binary also runs on the GPU machine's host CPU; CPU-baseline timing)
@@ -44,8 +46,12 @@ REF_SOURCES = [
 
 FLAVOURS = {
     "strict": ["-O2", "-ffp-contract=off"],
+    "strict_cr": ["-O2", "-ffp-contract=off"],
     "fast": ["-O3", "-ffast-math", "-march=x86-64-v3"],
 }
+# strict_cr: the strict build linked with correctly rounded exp, expm1 and
+# log1p (cr_libm.c, in place of the C library's) -- the reference as a
+# correctly rounded C library runs it
 
 
 def binary_name(nx: int, ny: int, nz: int, order: int, flavour: str) -> str:
@@ -65,7 +71,8 @@ def build(nx: int, ny: int, nz: int, order: int, flavour: str = "strict",
     """Compile one oracle binary; returns its path (skips if up to date)."""
     out = binary_path(nx, ny, nz, order, flavour)
     driver = HERE / "ref_driver.cc"
-    if out.exists() and not force and out.stat().st_mtime >= driver.stat().st_mtime:
+    newest = max(driver.stat().st_mtime, (HERE / "cr_libm.c").stat().st_mtime, (HERE / "cr_libm.h").stat().st_mtime)
+    if out.exists() and not force and out.stat().st_mtime >= newest:
         return out
     if not reference_available():
         raise FileNotFoundError(f"reference sources not found under {REF_ROOT}")
@@ -89,8 +96,15 @@ def build(nx: int, ny: int, nz: int, order: int, flavour: str = "strict",
 
         with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
             list(ex.map(cc, zip(srcs, objs)))
+        libs = ["-lz"]
+        if flavour == "strict_cr":
+            crobj = Path(tmp) / "cr_libm.o"
+            subprocess.run(["gcc", "-std=gnu11", "-O2", "-ffp-contract=off", f"-I{HERE}", "-c",
+                            str(HERE / "cr_libm.c"), "-o", str(crobj)], check=True)
+            objs.append(crobj)
+            libs.append("-lquadmath")
         tmp_out = Path(tmp) / out.name
-        subprocess.run([*common, *map(str, objs), "-lz", "-o", str(tmp_out)], check=True)
+        subprocess.run([*common, *map(str, objs), *libs, "-o", str(tmp_out)], check=True)
         shutil.move(str(tmp_out), out)
     return out
 
