@@ -39,7 +39,7 @@ EXPORTS = (
     "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints", "cg_field_statistics",
     "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust",
 )
-OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID, OPT_TMA = 1, 2, 3, 4, 5
+OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID, OPT_TMA, OPT_PAIR = 1, 2, 3, 4, 5, 6
 
 
 class BoxDesc(ctypes.Structure):

@@ -127,7 +127,7 @@ struct cg_ctx {
   std::vector<Group> groups;
   std::vector<int> singles;  // boxes launched on their own
   bool grouped = false;      // groups and singles are current
-  int opt_batch = 1, opt_graph = 0, opt_autotune = 1, opt_group_grid = 0, opt_tma = 1;
+  int opt_batch = 1, opt_graph = 0, opt_autotune = 1, opt_group_grid = 0, opt_tma = 1, opt_pair = 1;
   cudaGraphExec_t gexec = nullptr;
   int gexec_steps = 0;
   cudaStream_t stream = nullptr;
@@ -809,6 +809,7 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
         else cg::exact::make_tile_maps(b.dev);
         b.dev.tma = b.dev.tma && ctx->opt_tma;
       }
+      b.dev.pair = ctx->opt_pair;
     } else {
       cg::MixedBox& m = b.mdev;
       m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.pts = b.dev.pts; m.nfields = b.dev.nfields;
@@ -1326,7 +1327,7 @@ int group_launch(cg_ctx* ctx, Group& g, std::vector<Box>& boxes, int n) {
       if (rc) return rc;
     }
     CG_CUDA(ctx, cg::launch_group(g.variant, static_cast<const cg::GroupBox*>(g.table), gb, g.order, g.matter, n,
-                                  g.grid, ctx->stream));
+                                  g.grid, ctx->opt_pair, ctx->stream));
   }
   return CG_OK;
 }
@@ -1367,7 +1368,7 @@ int tune_groups(cg_ctx* ctx) {
     for (int q : g.members) ready = ready && ctx->boxes[q].stage_next == 1;
     if (!ready) continue;
     const int per_sm = g.mixed ? cg::mixed::group_ctas_per_sm(g.order, g.matter)
-                               : cg::group_ctas_per_sm(g.variant, g.order, g.matter);
+                               : cg::group_ctas_per_sm(g.variant, g.order, g.matter, ctx->opt_pair);
     float best = 1e30f;
     int best_lpt = 0, best_grid = 0;
     for (int lpt = 0; lpt < 2 && rc == CG_OK; ++lpt) {
@@ -1556,6 +1557,13 @@ int cg_set_option(cg_ctx* ctx, int option, int value) {
         else b.dev.tma = b.dev.maps && ctx->opt_tma;
       }
       ctx->grouped = false;  // the group tables carry the flag
+      return CG_OK;
+    case CG_OPT_PAIR:
+      for (Box& b : ctx->boxes)
+        if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "change CG_OPT_PAIR between steps");
+      ctx->opt_pair = value != 0;
+      for (Box& b : ctx->boxes) b.dev.pair = ctx->opt_pair;
+      for (Group& g : ctx->groups) g.tuned = false;  // the launch shapes change
       return CG_OK;
     case CG_OPT_GRAPH: ctx->opt_graph = value != 0; return CG_OK;
     case CG_OPT_AUTOTUNE: ctx->opt_autotune = value != 0; return CG_OK;

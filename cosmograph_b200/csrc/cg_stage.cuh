@@ -435,12 +435,12 @@ __device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG
 // from the stored flux primitives, taps read from global memory.
 template <int O, class T>
 __device__ __forceinline__ void flux_divergences(const T& t, const double* __restrict__ fp, int N, const Physics& ph,
-                                                 double* sl) {
+                                                 double* sl, int m0 = 0, int m1 = 4) {
   const double* v1 = fp + (size_t)P_V1 * N;
   const double* v2 = fp + (size_t)P_V2 * N;
   const double* v3 = fp + (size_t)P_V3 * N;
 #pragma unroll 1
-  for (int m = 0; m < 4; ++m) {
+  for (int m = m0; m < m1; ++m) {
     const double* u = fp + (size_t)(P_AD + m) * N;
     sl[(S_MAT + m) * kThreads] = d1p<O>(u, v1, t, 0, ph) + d1p<O>(u, v2, t, 1, ph) + d1p<O>(u, v3, t, 2, ph);
   }
@@ -483,10 +483,12 @@ __device__ __forceinline__ double d1p_tile(const double* u, const double* v, int
 // Dust flux divergences of a brick inside the box from TMA boxes: x boxes
 // into tl2, y boxes into tl, then z boxes into tl2; the sum over axes in the
 // order of flux_divergences.  All threads of the CTA take part.
+// (tx, ty, tz): the thread's point in the brick; it computes the divergences
+// m0 <= m < m1 (alpha*D, alpha*S_1..3)
 template <int O>
 __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, double* tl2, int tid, int x0, int y0,
                                                 int z0, const Physics& ph, double* sl, uint64_t* bar,
-                                                unsigned& phase) {
+                                                unsigned& phase, int tx, int ty, int tz, int m0 = 0, int m1 = 4) {
   using FB = FluxBox<O>;
   constexpr int R = FB::R;
   // every staging area fits its buffer: x and z boxes in the second tile
@@ -506,7 +508,6 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
     for (int q = 0; q < 5; ++q)  // alpha*D, alpha*S_1..3, then v^a
       tma::load_4d(dst + (size_t)q * len, &fm->m[a], cz, cy, cx, q < 4 ? P_AD + q : P_V1 + a, b);
   };
-  const int tx = threadIdx.z, ty = threadIdx.y, tz = threadIdx.x;
   tma::fence_proxy_async();
   __syncthreads();  // the field tiles have been read
   if (tid == 0) {
@@ -517,7 +518,7 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
   {
     const int c = ((tx + R) * kBY + ty) * kBZ + tz;
 #pragma unroll 1
-    for (int m = 0; m < 4; ++m)
+    for (int m = m0; m < m1; ++m)
       sl[(S_MAT + m) * kThreads] = d1p_tile<O>(tl2 + (size_t)m * FB::XB, tl2 + (size_t)4 * FB::XB, c, kBY * kBZ, ph);
   }
   tma::fence_proxy_async();
@@ -527,7 +528,7 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
   {
     const int c = (tx * (kBY + 2 * R) + ty + R) * kBZ + tz;
 #pragma unroll 1
-    for (int m = 0; m < 4; ++m)
+    for (int m = m0; m < m1; ++m)
       sl[(S_MAT + m) * kThreads] =
           sl[(S_MAT + m) * kThreads] + d1p_tile<O>(tl + (size_t)m * FB::YB, tl + (size_t)4 * FB::YB, c, kBZ, ph);
   }
@@ -535,7 +536,7 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
   {
     const int c = (tx * kBY + ty) * FB::ZP + tz + TileG<O>::ZO;
 #pragma unroll 1
-    for (int m = 0; m < 4; ++m)
+    for (int m = m0; m < m1; ++m)
       sl[(S_MAT + m) * kThreads] =
           sl[(S_MAT + m) * kThreads] + d1p_tile<O>(tl2 + (size_t)m * FB::ZB, tl2 + (size_t)4 * FB::ZB, c, 1, ph);
   }
@@ -682,7 +683,8 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     if constexpr (MATTER == kDust && MODE == kEvolve && TileBuffers<O, MATTER, MODE>::kTwo) {
       flux_tiles = fmaps && by_tma && tma_ok;
       if (flux_tiles) {
-        tma_ok = flux_from_tiles<O>(fmaps, tl, tl2, tid, x0, y0, z0, ph, sl, bar, phase);
+        tma_ok = flux_from_tiles<O>(fmaps, tl, tl2, tid, x0, y0, z0, ph, sl, bar, phase, threadIdx.z, threadIdx.y,
+                                    threadIdx.x);
         if (!tma_ok && tid == 0) atomicOr(P.status, kStatusTileTimeout64);
       }
     }
@@ -1289,6 +1291,8 @@ stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
     stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0, stm, bar, phase, tma_ok, sfm);
   }
 }
+
+#include "cg_stage_pair.cuh"
 
 }  // namespace CG_VARIANT_NS
 }  // namespace cg

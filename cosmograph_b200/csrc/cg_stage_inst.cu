@@ -85,6 +85,32 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
   FluxMaps fm;
   const CUtensorMap* fsrc = (stage == 1 || stage == 3) ? b.fmap0 : b.fmap1;
   for (int a = 0; a < 3; ++a) fm.m[a] = fsrc[a];
+  if (b.pair) {  // two threads per point
+    constexpr size_t psmem = pair_smem<O, M>();
+    const dim3 block(kPairThreads);
+    if constexpr (O == 2 || O == 8) {
+      if (b.ph.ko_coeff != 0.0) {
+        static bool configured_ko = false;
+        if (!configured_ko) {
+          cudaError_t e = cudaFuncSetAttribute(stage_pair_kernel<O, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)psmem);
+          if (e != cudaSuccess) return e;
+          configured_ko = true;
+        }
+        stage_pair_kernel<O, M, true><<<stage_grid(b), block, psmem, st>>>(geo, b.ph, bg, P, stage, map, b.tma, fm,
+                                                                           b.fmaps);
+        return cudaGetLastError();
+      }
+    }
+    static bool configured_pair = false;
+    if (!configured_pair) {
+      cudaError_t e = cudaFuncSetAttribute(stage_pair_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+      if (e != cudaSuccess) return e;
+      configured_pair = true;
+    }
+    stage_pair_kernel<O, M><<<stage_grid(b), block, psmem, st>>>(geo, b.ph, bg, P, stage, map, b.tma, fm, b.fmaps);
+    return cudaGetLastError();
+  }
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
   if constexpr (O == 2 || O == 8) {
     if (b.ph.ko_coeff != 0.0) {  // Kreiss-Oliger dissipation: its own instantiation
@@ -146,7 +172,20 @@ cudaError_t go_constraints_m(const BoxDev& b, const StageBg& bg, double* cvals, 
 }
 
 template <int O, int M>
-cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, cudaStream_t st) {
+cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, int pair, cudaStream_t st) {
+  const int g = grid > 0 ? grid : gb.total;
+  if (pair) {
+    constexpr size_t psmem = pair_smem<O, M>();
+    static bool configured_pair = false;
+    if (!configured_pair) {
+      cudaError_t e =
+          cudaFuncSetAttribute(stage_pair_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+      if (e != cudaSuccess) return e;
+      configured_pair = true;
+    }
+    stage_pair_group_kernel<O, M><<<g, kPairThreads, psmem, st>>>(table, gb, stage);
+    return cudaGetLastError();
+  }
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
   static bool configured = false;
   if (!configured) {
@@ -154,13 +193,23 @@ cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int gr
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  const int g = grid > 0 ? grid : gb.total;
   stage_group_kernel<O, M><<<g, stage_block(), smem, st>>>(table, gb, stage);
   return cudaGetLastError();
 }
 
 template <int O, int M>
-int ctas_per_sm() {
+int ctas_per_sm(int pair) {
+  if (pair) {
+    constexpr size_t psmem = pair_smem<O, M>();
+    if (cudaFuncSetAttribute(stage_pair_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem) !=
+        cudaSuccess)
+      return 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_pair_group_kernel<O, M>, kPairThreads, psmem) !=
+        cudaSuccess)
+      return 1;
+    return n > 0 ? n : 1;
+  }
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
   if (cudaFuncSetAttribute(stage_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
@@ -172,19 +221,20 @@ int ctas_per_sm() {
 }
 
 template <int O>
-cudaError_t go_group_m(const GroupBox* table, const GroupBg& gb, int matter, int stage, int grid, cudaStream_t st) {
+cudaError_t go_group_m(const GroupBox* table, const GroupBg& gb, int matter, int stage, int grid, int pair,
+                       cudaStream_t st) {
   switch (matter) {
-    case kDust: return go_group<O, kDust>(table, gb, stage, grid, st);
-    case kScalar: return go_group<O, kScalar>(table, gb, stage, grid, st);
-    default: return go_group<O, kVacuum>(table, gb, stage, grid, st);
+    case kDust: return go_group<O, kDust>(table, gb, stage, grid, pair, st);
+    case kScalar: return go_group<O, kScalar>(table, gb, stage, grid, pair, st);
+    default: return go_group<O, kVacuum>(table, gb, stage, grid, pair, st);
   }
 }
 template <int O>
-int ctas_m(int matter) {
+int ctas_m(int matter, int pair) {
   switch (matter) {
-    case kDust: return ctas_per_sm<O, kDust>();
-    case kScalar: return ctas_per_sm<O, kScalar>();
-    default: return ctas_per_sm<O, kVacuum>();
+    case kDust: return ctas_per_sm<O, kDust>(pair);
+    case kScalar: return ctas_per_sm<O, kScalar>(pair);
+    default: return ctas_per_sm<O, kVacuum>(pair);
   }
 }
 
@@ -252,22 +302,22 @@ cudaError_t launch_constraints(const BoxDev& b, const StageBg& bg, double* cvals
 }
 
 cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
-                         cudaStream_t st) {
+                         int pair, cudaStream_t st) {
   switch (order) {
-    case 2: return go_group_m<2>(table, gb, matter, stage, grid, st);
-    case 4: return go_group_m<4>(table, gb, matter, stage, grid, st);
-    case 6: return go_group_m<6>(table, gb, matter, stage, grid, st);
-    case 8: return go_group_m<8>(table, gb, matter, stage, grid, st);
+    case 2: return go_group_m<2>(table, gb, matter, stage, grid, pair, st);
+    case 4: return go_group_m<4>(table, gb, matter, stage, grid, pair, st);
+    case 6: return go_group_m<6>(table, gb, matter, stage, grid, pair, st);
+    case 8: return go_group_m<8>(table, gb, matter, stage, grid, pair, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
-int group_ctas_per_sm(int order, int matter) {
+int group_ctas_per_sm(int order, int matter, int pair) {
   switch (order) {
-    case 2: return ctas_m<2>(matter);
-    case 4: return ctas_m<4>(matter);
-    case 6: return ctas_m<6>(matter);
-    default: return ctas_m<8>(matter);
+    case 2: return ctas_m<2>(matter, pair);
+    case 4: return ctas_m<4>(matter, pair);
+    case 6: return ctas_m<6>(matter, pair);
+    default: return ctas_m<8>(matter, pair);
   }
 }
 

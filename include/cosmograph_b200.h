@@ -240,12 +240,17 @@ int cg_ic_grf_dust(cg_ctx *ctx, int box, const double *delta, uint64_t seed, dou
  *                    accelerator (FP64 boxes with even nz, mixed boxes with nz
  *                    a multiple of 4); 0: every tile is copied by the CTA's
  *                    threads.  Results are identical.  Change it between
- *                    steps only. */
+ *                    steps only.
+ *   CG_OPT_PAIR      1 (default): the FP64 substep kernels run two threads
+ *                    per grid point (256-thread CTAs, twice the warps per
+ *                    SM); 0: one thread per point.  Results are identical.
+ *                    Change it between steps only. */
 #define CG_OPT_BATCH 1
 #define CG_OPT_GRAPH 2
 #define CG_OPT_AUTOTUNE 3
 #define CG_OPT_GROUP_GRID 4
 #define CG_OPT_TMA 5
+#define CG_OPT_PAIR 6
 int cg_set_option(cg_ctx *ctx, int option, int value);
 
 /* Launch groups of the context (formed on first use), and for group g:
