@@ -38,10 +38,8 @@
 
 #if defined(__CUDACC__)
 #define CRM_FN __host__ __device__ __forceinline__
-#define CRM_SLOW static __host__ __device__ __noinline__
 #else
 #define CRM_FN static inline
-#define CRM_SLOW static __attribute__((noinline))
 #endif
 
 namespace cg {
@@ -215,25 +213,50 @@ CRM_FN int reduce(double x, double& rh, double& rl) {
   return (int)kd;
 }
 
+// 1/(n+1)!, n = 0..11: hi parts, and the lo parts of n <= 5 (the terms
+// evaluated in double-double)
+#define CG_CRM_COEF_HI 1.0, 0.5, 0x1.5555555555555p-3, 0x1.5555555555555p-5, 0x1.1111111111111p-7, \
+    0x1.6c16c16c16c17p-10, 0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-16, 0x1.71de3a556c734p-19,      \
+    0x1.27e4fb7789f5cp-22, 0x1.ae64567f544e4p-26, 0x1.1eed8eff8d898p-29
+#define CG_CRM_COEF_LO 0.0, 0.0, 0x1.5555555555555p-57, 0x1.5555555555555p-59, 0x1.1111111111111p-63, \
+    -0x1.f49f49f49f49fp-65
+#if defined(__CUDACC__)
+static __constant__ const double kCoefHiDev[12] = {CG_CRM_COEF_HI};
+static __constant__ const double kCoefLoDev[6] = {CG_CRM_COEF_LO};
+#endif
+static const double kCoefHiHost[12] = {CG_CRM_COEF_HI};
+static const double kCoefLoHost[6] = {CG_CRM_COEF_LO};
+#undef CG_CRM_COEF_HI
+#undef CG_CRM_COEF_LO
+CRM_FN double coef_hi(int n) {
+#if defined(__CUDA_ARCH__)
+  return kCoefHiDev[n];
+#else
+  return kCoefHiHost[n];
+#endif
+}
+CRM_FN double coef_lo(int n) {
+#if defined(__CUDA_ARCH__)
+  return kCoefLoDev[n];
+#else
+  return kCoefLoHost[n];
+#endif
+}
+
 // e^r - 1 = r * P(r), P(r) = sum r^n/(n+1)!, r = rh + rl, in double-double
-// (error below 2^-103 relative for |r| <= 0.0055).
+// (error below 2^-103 relative for |r| <= 0.0055).  Rolled loops: this is
+// the accurate phase, which runs rarely, and a small body keeps the code of
+// every call site small.
 CRM_FN DD expm1_small_dd(double rh, double rl) {
-  // tail n = 6..11 in double: |r^6/7!| < 2^-61, so its rounding stays below 2^-110
-  double t = 0x1.1eed8eff8d898p-29;            // 1/12!
-  t = fma_(t, rh, 0x1.ae64567f544e4p-26);      // 1/11!
-  t = fma_(t, rh, 0x1.27e4fb7789f5cp-22);      // 1/10!
-  t = fma_(t, rh, 0x1.71de3a556c734p-19);      // 1/9!
-  t = fma_(t, rh, 0x1.a01a01a01a01ap-16);      // 1/8!
-  t = fma_(t, rh, 0x1.a01a01a01a01ap-13);      // 1/7!
+  // tail n = 11..6 in double: |r^6/7!| < 2^-61, so its rounding stays below 2^-110
+  double t = coef_hi(11);
+#pragma unroll 1
+  for (int n = 10; n >= 6; --n) t = fma_(t, rh, coef_hi(n));
   // n = 5..0 in double-double: P = P * r + 1/(n+1)!
   const DD r{rh, rl};
   DD P{t, 0.0};
-  P = dd_add(dd_mul(P, r), DD{0x1.6c16c16c16c17p-10, -0x1.f49f49f49f49fp-65});  // 1/6!
-  P = dd_add(dd_mul(P, r), DD{0x1.1111111111111p-7, 0x1.1111111111111p-63});    // 1/5!
-  P = dd_add(dd_mul(P, r), DD{0x1.5555555555555p-5, 0x1.5555555555555p-59});    // 1/4!
-  P = dd_add(dd_mul(P, r), DD{0x1.5555555555555p-3, 0x1.5555555555555p-57});    // 1/3!
-  P = dd_add(dd_mul(P, r), DD{0.5, 0.0});
-  P = dd_add(dd_mul(P, r), DD{1.0, 0.0});
+#pragma unroll 1
+  for (int n = 5; n >= 0; --n) P = dd_add(dd_mul(P, r), DD{coef_hi(n), coef_lo(n)});
   return dd_mul(P, r);
 }
 
@@ -314,15 +337,11 @@ CRM_FN DD exp_dd_reduced(int k, double rh, double rl) {
   return table_times(k & 63, expm1_small_dd(rh, rl));
 }
 
-// e^x when the fast evaluation of exp() cannot decide the rounding, or for
-// subnormal results (a call, so that call sites inline only the fast part)
-CRM_SLOW double exp_accurate(double x, int k, double rh, double rl) {
+// e^x when the fast evaluation cannot decide the rounding, and for
+// subnormal results.  Inline (a call in a kernel's straight-line code costs
+// more than this rarely taken code).
+CRM_FN double exp_accurate(double x, int k, double rh, double rl) {
   const int j = k & 63, m = k >> 6;
-  if (x < kExpSub) {
-    const DD z = exp_dd_reduced(k, rh, rl);
-    return round_subnormal(z.hi, z.lo, m);
-  }
-  // 2^(j/64) (1 + s) with s = e^r - 1 in double-double
   const double ax = x < 0.0 ? -x : x;
   if (ax < kTiny) {  // 1 + x + x^2/2 + x^3/6 + x^4/24
     const DD h2 = half_square(x);
@@ -331,46 +350,117 @@ CRM_SLOW double exp_accurate(double x, int k, double rh, double rl) {
     return round_sum(z.hi, DD{z.lo, h2.hi},
                      add(h2.lo, add(h3.hi, add(h3.lo, mul(mul(h2.hi, h2.hi), 0x1.5555555555555p-3)))));
   }
+  // 2^(j/64) (1 + s) with s = e^r - 1 in double-double
   const double* T = exp2_table();
   const double Th = T[2 * j], Tl = T[2 * j + 1];
   const DD sd = expm1_small_dd(rh, rl);
   const DD pp = two_prod(Th, sd.hi);
-  return scale2(round_sum(Th, pp, add(mul(Th, sd.lo), fma_(Tl, sd.hi, Tl))), m);
+  const double rest = add(mul(Th, sd.lo), fma_(Tl, sd.hi, Tl));
+  if (x < kExpSub) {
+    const DD z = two_sum(Th, pp.hi);
+    return round_subnormal(z.hi, add(z.lo, add(pp.lo, rest)), m);
+  }
+  return scale2(round_sum(Th, pp, rest), m);
+}
+
+// Accept y.hi + y.lo (|y.lo| <= ulp/2, within e of the exact value) when
+// every value within e of it rounds to y.hi.
+CRM_FN bool decided(DD y, double e) {
+  const int64_t b = bits(y.hi);
+  const double up = from_bits(b + 1), dn = from_bits(b - 1);
+  const double gap_up = mul(sub(up, y.hi), 0.5), gap_dn = mul(sub(y.hi, dn), 0.5);  // exact
+  return add(y.lo, e) < gap_up && sub(y.lo, e) > -gap_dn;
+}
+
+// The fast evaluation of e^x.  Returns false when it cannot decide the
+// rounding (then exp_full decides); special values are decided here.
+CRM_FN bool exp_fast(double x, double& y) {
+  if (!(x == x)) { y = add(x, x); return true; }  // NaN
+  if (x > kExpMax) { y = from_bits(0x7ff0000000000000LL); return true; }
+  if (x < kExpMin) { y = 0.0; return true; }
+  const double ax = x < 0.0 ? -x : x;
+  if (ax <= 0.0054) {
+    // |x| <= ln2/128 (k = 0): e^x = 1 + x + c with |error of c| < 2^-67
+    double p = 0x1.a01a01a01a01ap-13;
+    p = fma_(p, x, 0x1.6c16c16c16c17p-10);
+    p = fma_(p, x, 0x1.1111111111111p-7);
+    p = fma_(p, x, 0x1.5555555555555p-5);
+    p = fma_(p, x, 0x1.5555555555555p-3);
+    p = fma_(p, x, 0.5);
+    const double c = mul(mul(x, x), p);
+    const DD s = two_sum(x, c);
+    DD z = two_sum(1.0, s.hi);
+    z.lo = add(z.lo, s.lo);
+    z = two_sum(z.hi, z.lo);
+    y = z.hi;
+    return decided(z, 0x1p-63);
+  }
+  if (x < kExpSub) return false;
+  double rh, rl;
+  const int k = reduce(x, rh, rl);
+  const int j = k & 63, m = k >> 6;  // arithmetic shift: floor(k / 64)
+  // e^r - 1 = rh + c, |error of c| < 2^-67 (|rh| <= 0.0055)
+  double p = 0x1.a01a01a01a01ap-13;            // 1/7!
+  p = fma_(p, rh, 0x1.6c16c16c16c17p-10);      // 1/6!
+  p = fma_(p, rh, 0x1.1111111111111p-7);       // 1/5!
+  p = fma_(p, rh, 0x1.5555555555555p-5);       // 1/4!
+  p = fma_(p, rh, 0x1.5555555555555p-3);       // 1/3!
+  p = fma_(p, rh, 0.5);
+  const double c = add(mul(mul(rh, rh), p), fma_(rl, rh, rl));
+  const DD s = two_sum(rh, c);
+  const double* T = exp2_table();
+  const double Th = T[2 * j], Tl = T[2 * j + 1];
+  const DD ps = two_prod(Th, s.hi);
+  DD z = two_sum(Th, ps.hi);
+  z.lo = add(z.lo, add(ps.lo, add(mul(Th, s.lo), fma_(Tl, s.hi, Tl))));
+  z = two_sum(z.hi, z.lo);
+  // z is within 2^-64 (absolute; z < 2.02) of 2^(j/64) e^r
+  y = scale2(z.hi, m);
+  return decided(z, 0x1p-63);
+}
+
+// The accurate phase of e^x for any finite x in [kExpMin, kExpMax].
+CRM_FN double exp_full(double x) {
+  const double ax = x < 0.0 ? -x : x;
+  if (ax <= 0.0054) return exp_accurate(x, 0, x, 0.0);
+  double rh, rl;
+  const int k = reduce(x, rh, rl);
+  return exp_accurate(x, k, rh, rl);
 }
 
 // Correctly rounded e^x.
 CRM_FN double exp(double x) {
-  if (!(x == x)) return add(x, x);  // NaN
-  if (x > kExpMax) return from_bits(0x7ff0000000000000LL);
-  if (x < kExpMin) return 0.0;
-  double rh, rl;
-  const int k = reduce(x, rh, rl);
-  if (x >= kExpSub) {
-    const int j = k & 63, m = k >> 6;  // arithmetic shift: floor(k / 64)
-    // fast evaluation: e^r - 1 = rh + c, |error of c| < 2^-67 (|rh| <= 0.0055)
-    double p = 0x1.a01a01a01a01ap-13;            // 1/7!
-    p = fma_(p, rh, 0x1.6c16c16c16c17p-10);      // 1/6!
-    p = fma_(p, rh, 0x1.1111111111111p-7);       // 1/5!
-    p = fma_(p, rh, 0x1.5555555555555p-5);       // 1/4!
-    p = fma_(p, rh, 0x1.5555555555555p-3);       // 1/3!
-    p = fma_(p, rh, 0.5);
-    const double c = add(mul(mul(rh, rh), p), fma_(rl, rh, rl));
-    const DD s = two_sum(rh, c);
-    const double* T = exp2_table();
-    const double Th = T[2 * j], Tl = T[2 * j + 1];
-    const DD ps = two_prod(Th, s.hi);
-    DD y = two_sum(Th, ps.hi);
-    y.lo = add(y.lo, add(ps.lo, add(mul(Th, s.lo), fma_(Tl, s.hi, Tl))));
-    y = two_sum(y.hi, y.lo);
-    // y is within 2^-64 (absolute; y < 2.02) of 2^(j/64) e^r.  Accept y.hi if
-    // both ends of that interval round to it.
-    const double e = 0x1p-63;
-    const int64_t b = bits(y.hi);
-    const double up = from_bits(b + 1), dn = from_bits(b - 1);
-    const double gap_up = mul(sub(up, y.hi), 0.5), gap_dn = mul(sub(y.hi, dn), 0.5);  // exact
-    if (add(y.lo, e) < gap_up && sub(y.lo, e) > -gap_dn) return scale2(y.hi, m);
+  double y;
+  if (exp_fast(x, y)) return y;
+  return exp_full(x);
+}
+
+// Correctly rounded e^x of N arguments: the fast evaluation of each inline,
+// the accurate phase (needed for about 0.15 % of arguments) in one rolled
+// loop for all N, so that a kernel carries one copy of its code per batch.
+template <int N>
+CRM_FN void exp_n(const double (&x)[N], double (&y)[N]) {
+  unsigned bad = 0;
+#pragma unroll
+  for (int n = 0; n < N; ++n)
+    if (!exp_fast(x[n], y[n])) bad |= 1u << n;
+  // one argument at a time, picked and stored by compare-and-select, so that
+  // neither a call nor an indexed (local-memory) array enters the kernel
+#pragma unroll 1
+  while (bad) {
+#if defined(__CUDA_ARCH__)
+    const int q = __ffs(bad) - 1;
+#else
+    const int q = __builtin_ctz(bad);
+#endif
+    bad &= bad - 1u;
+    double v = x[0];
+#pragma unroll
+    for (int n = 1; n < N; ++n) v = q == n ? x[n] : v;
+    v = exp_full(v);
+#pragma unroll
+    for (int n = 0; n < N; ++n) y[n] = q == n ? v : y[n];
   }
-  return exp_accurate(x, k, rh, rl);
 }
 
 // e^x - 1 in double-double with the same reduction (error about 2^-100
@@ -388,7 +478,7 @@ CRM_FN DD expm1_dd(double x) {
 }
 
 // Correctly rounded e^x - 1.
-CRM_SLOW double expm1(double x) {
+CRM_FN double expm1(double x) {
   if (!(x == x)) return add(x, x);
   if (x > 709.78) return exp(x);  // e^x - 1 and e^x round alike (they differ by 2^-1022 relative)
   if (x < -40.0) return -1.0;     // e^x < 2^-57: -1 + e^x rounds to -1
@@ -407,7 +497,7 @@ CRM_SLOW double expm1(double x) {
 // start value z0 within a few ulp, with t = (1 + y) e^{-z0} - 1 formed in
 // double-double (as y + q + y q, q = expm1(-z0), where the result is small,
 // so that the error stays relative to the result).
-CRM_SLOW double log1p(double y) {
+CRM_FN double log1p(double y) {
   if (!(y == y)) return add(y, y);
   if (y < -1.0) return from_bits(0x7ff8000000000000LL);
   if (y == -1.0) return from_bits((int64_t)0xfff0000000000000ULL);

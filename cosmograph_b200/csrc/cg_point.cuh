@@ -38,6 +38,16 @@ namespace CG_VARIANT_NS {
 #endif
 constexpr bool kReferenceOrder = CG_REFERENCE_ORDER != 0;
 
+// e^x of N arguments at once (one copy of the accurate phase per batch)
+template <int N>
+__device__ __forceinline__ void xexp_n(const double (&x)[N], double (&y)[N]) {
+  if constexpr (kReferenceOrder) {
+    crm::exp_n<N>(x, y);
+  } else {
+#pragma unroll
+    for (int n = 0; n < N; ++n) y[n] = ::exp(x[n]);
+  }
+}
 __device__ __forceinline__ double xexp(double x) {
   if constexpr (kReferenceOrder) return crm::exp(x);
   else return ::exp(x);
@@ -193,11 +203,10 @@ __device__ __forceinline__ void normalize_point(double g[6], double A[6]) {
 struct DustPrim {
   double W, v[3];
 };
-__device__ __forceinline__ DustPrim dust_prim(const double gi[6], double phi, double D,
+// em4phi = exp(-4 phi), e6phi = exp(6 phi) of the point's phi
+__device__ __forceinline__ DustPrim dust_prim(const double gi[6], double em4phi, double e6phi, double D,
                                               const double S[3]) {
   DustPrim d;
-  const double em4phi = xexp(-4.0 * phi);
-  const double e6phi = xexp(6.0 * phi);
   const double giIJSISJ = em4phi * (gi[0] * S[0] * S[0] + gi[3] * S[1] * S[1] + gi[5] * S[2] * S[2] +
                                     2.0 * (gi[1] * S[0] * S[1] + gi[2] * S[0] * S[2] + gi[4] * S[1] * S[2]));
   d.W = sqrt(1.0 + giIJSISJ / D / D);

@@ -713,7 +713,17 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   double gm[6];
   gm[0] = g[0] + 1.0; gm[1] = g[1]; gm[2] = g[2];
   gm[3] = g[3] + 1.0; gm[4] = g[4]; gm[5] = g[5] + 1.0;
-  const double em4phi = xexp(-4.0 * phi);
+  // every e^x this point's substep takes, in one batch: of phi and, for dust
+  // after the first substep, of the previous substep's phi (the lagged sources)
+  double phip = phi;
+  if (MATTER == kDust && stage > 1) phip = __ldcs(&P.prev[(size_t)F_PHI * N + c]) + bg.phi_FRW_prev;
+  double ex[8];
+  {
+    const double xa[8] = {-4.0 * phi, 4.0 * phi, 6.0 * phi, 5.0 * phi, -5.0 * phi, -4.0 * phip, 4.0 * phip, 6.0 * phip};
+    xexp_n<8>(xa, ex);
+  }
+  const double em4phi = ex[0], e4phi = ex[1], e6phi = ex[2], e5phi = ex[3], em5phi = ex[4];
+  const double em4phip = ex[5], e4phip = ex[6], e6phip = ex[7];
 
   // -- sources and matter centre quantities --
   double rhs_m[5] = {0, 0, 0, 0, 0};
@@ -723,10 +733,10 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     double Wl, detgl, gph[6];
     if (stage == 1) {
       // the stepInit populate used this same state (sims/dust.cc:56-62)
-      const DustPrim dp = dust_prim(gi, phi, D, Sv);
+      const DustPrim dp = dust_prim(gi, em4phi, e6phi, D, Sv);
       Wl = dp.W;
-      const double e4 = xexp(4.0 * phi);
-      detgl = xexp(6.0 * phi);
+      const double e4 = e4phi;
+      detgl = e6phi;
 #pragma unroll
       for (int m = 0; m < 6; ++m) gph[m] = e4 * gm[m];
     } else {
@@ -734,14 +744,13 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       double gp[6], gip[6];
 #pragma unroll
       for (int m = 0; m < 6; ++m) gp[m] = __ldcs(&pv[(size_t)(F_G11 + m) * N + c]);
-      const double phip = __ldcs(&pv[(size_t)F_PHI * N + c]) + bg.phi_FRW_prev;
       const double Dp = __ldcs(&pv[(size_t)F_D * N + c]);
       const double Sp[3] = {__ldcs(&pv[(size_t)F_S1 * N + c]), __ldcs(&pv[(size_t)F_S2 * N + c]), __ldcs(&pv[(size_t)F_S3 * N + c])};
       inv_metric(gp, gip);
-      const DustPrim dp = dust_prim(gip, phip, Dp, Sp);
+      const DustPrim dp = dust_prim(gip, em4phip, e6phip, Dp, Sp);
       Wl = dp.W;
-      const double e4 = xexp(4.0 * phip);
-      detgl = xexp(6.0 * phip);
+      const double e4 = e4phip;
+      detgl = e6phip;
       gph[0] = e4 * (gp[0] + 1.0); gph[1] = e4 * gp[1]; gph[2] = e4 * gp[2];
       gph[3] = e4 * (gp[3] + 1.0); gph[4] = e4 * gp[4]; gph[5] = e4 * (gp[5] + 1.0);
     }
@@ -750,8 +759,8 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
 #pragma unroll
     for (int m = 0; m < Q_N; ++m) S(S_SRC + m) = q[m];
     // momentum source S_m^src (dust.cc:135-146) with the current W, v
-    const DustPrim cur = dust_prim(gi, phi, D, Sv);
-    const double e4 = xexp(4.0 * phi);
+    const DustPrim cur = dust_prim(gi, em4phi, e6phi, D, Sv);
+    const double e4 = e4phi;
     rhs_m[0] = S(S_MAT + 0);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -894,25 +903,24 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   double t4[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   if constexpr (kReferenceOrder) {
     // the parity build: the reference's 27 terms per component, summed over
-    // (K, L, M) with M fastest, each term formed as the macro forms it
+    // (K, L, M) with M fastest, each term formed as the macro forms it; the
+    // six components advance together, so the symbols of one K are loaded
+    // once for all of them
 #pragma unroll
-    for (int I = 0; I < 3; ++I)
+    for (int Kx = 0; Kx < 3; ++Kx)
 #pragma unroll
-      for (int J = I; J < 3; ++J) {
-        double acc = 0.0;
+      for (int L = 0; L < 3; ++L)
 #pragma unroll
-        for (int Kx = 0; Kx < 3; ++Kx)
+        for (int M = 0; M < 3; ++M)
 #pragma unroll
-          for (int L = 0; L < 3; ++L)
+          for (int I = 0; I < 3; ++I)
 #pragma unroll
-            for (int M = 0; M < 3; ++M) {
+            for (int J = I; J < 3; ++J) {
               const double u =
                   gi[sym(L, M)] * (G(Kx, sym(L, I)) * GL(J, sym(Kx, M)) + G(Kx, sym(L, J)) * GL(I, sym(Kx, M)) +
                                    0.5 * (G(Kx, sym(I, M)) * GL(Kx, sym(L, J)) + G(Kx, sym(J, M)) * GL(Kx, sym(L, I))));
-              acc = (Kx == 0 && L == 0 && M == 0) ? u : acc + u;
+              t4[sym(I, J)] = (Kx == 0 && L == 0 && M == 0) ? u : t4[sym(I, J)] + u;
             }
-        t4[sym(I, J)] = acc;
-      }
   } else {
 #pragma unroll
   for (int Kx = 0; Kx < 3; ++Kx) {
@@ -952,7 +960,6 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   auto Ric = [&](int qq) { return S(S_T1 + qq); };  // full Ricci R_ij (bssn.cc:650-655)
   const double ricci = em4phi * (Ric(0) * gi[0] + Ric(3) * gi[3] + Ric(5) * gi[5] +
                                  2.0 * (Ric(1) * gi[1] + Ric(2) * gi[2] + Ric(4) * gi[4]));
-  const double e4phi = xexp(4.0 * phi);
 
   // -- A^ij, A_ij A^ij (calculate_Acont, bssn.cc:463-472) --
   double A[6], Ac[6];
@@ -976,18 +983,18 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   const double AijAij = Ac[0] * A[0] + Ac[3] * A[3] + Ac[5] * A[5] + 2.0 * (Ac[1] * A[1] + Ac[2] * A[2] + Ac[4] * A[4]);
   const double r = S(S_SRC + Q_R) + bg.rho_FRW;
   // Hamiltonian constraint, bssn.cc:1073-1084 (theta = 0)
-  const double H = -xexp(5.0 * phi) / 8.0 * (ricci + 2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0)) - AijAij - 16.0 * kPi * r);
+  const double H = -e5phi / 8.0 * (ricci + 2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0)) - AijAij - 16.0 * kPi * r);
 
   if constexpr (MODE == kConstraints) {
     // BSSN::setConstraintCalcs per point (bssn.cc:983-1006)
     double v[5], sc[5];
     v[0] = H;  // hamiltonianConstraintCalc / Scale, bssn.cc:1073-1100
-    sc[0] = (xexp(5.0 * phi) / 8.0) * sqrt(ricci * ricci + AijAij * AijAij +
+    sc[0] = (e5phi / 8.0) * sqrt(ricci * ricci + AijAij * AijAij +
                                           (2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0))) *
                                               (2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0))) +
                                           (16.0 * kPi * r) * (16.0 * kPi * r));
     {  // momentum, BSSN_MI / BSSN_MI_SCALE (bssn_macros.h:487-527)
-      const double e6 = xexp(6.0 * phi);
+      const double e6 = e6phi;
       double mv[3], ms[3];
 #pragma unroll
       for (int I = 0; I < 3; ++I) {
@@ -1158,7 +1165,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   {
     double v = (-DDaTR + alpha * (1.0 / 3.0 * (Kd + 2.0 * 0.0) * (Kd + 2.0 * 0.0 + 2.0 * bg.K_FRW) + AijAij) +
                 4.0 * kPi * alpha * (S(S_SRC + Q_R) + S(S_SRC + Q_S)) + 4.0 * kPi * alphad * (bg.rho_FRW + bg.S_FRW));
-    if (ph.k_damping_amp != 0.0) v = v - 1.0 * ph.k_damping_amp * H * xexp(-5.0 * phi);
+    if (ph.k_damping_amp != 0.0) v = v - 1.0 * ph.k_damping_amp * H * em5phi;
     finalize(F_K, v - ko(F_K));
   }
   // ev_DIFFphi (bssn.cc:797-820)
@@ -1206,7 +1213,13 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     for (int m = 0; m < 6; ++m) go[m] = outv[F_G11 + m];
     inv_metric(go, gio);
     const double So[3] = {outv[F_S1], outv[F_S2], outv[F_S3]};
-    const DustPrim dp = dust_prim(gio, outv[F_PHI] + bg.phi_FRW_next, outv[F_D], So);
+    const double phio = outv[F_PHI] + bg.phi_FRW_next;
+    double eo[2];
+    {
+      const double xo[2] = {-4.0 * phio, 6.0 * phio};
+      xexp_n<2>(xo, eo);
+    }
+    const DustPrim dp = dust_prim(gio, eo[0], eo[1], outv[F_D], So);
     const double alo = outv[F_ALPHA] + 1.0;
     double* fo = P.fp_out;
     __stcs(&fo[(size_t)P_AD * N + c], alo * outv[F_D]);

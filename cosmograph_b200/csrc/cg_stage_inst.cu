@@ -46,7 +46,13 @@ __global__ void __launch_bounds__(128) init_kernel(BoxGeom geo, Physics ph, Stag
     for (int m = 0; m < 6; ++m) g[m] = v[F_G11 + m];
     inv_metric(g, gi);
     const double S[3] = {v[F_S1], v[F_S2], v[F_S3]};
-    const DustPrim dp = dust_prim(gi, v[F_PHI] + bg.phi_FRW, v[F_D], S);
+    const double phi = v[F_PHI] + bg.phi_FRW;
+    double e[2];
+    {
+      const double x[2] = {-4.0 * phi, 6.0 * phi};
+      xexp_n<2>(x, e);
+    }
+    const DustPrim dp = dust_prim(gi, e[0], e[1], v[F_D], S);
     const double al = v[F_ALPHA] + 1.0;
     FP0[(size_t)P_AD * N + c] = al * v[F_D];
 #pragma unroll

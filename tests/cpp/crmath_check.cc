@@ -86,6 +86,19 @@ int main(int argc, char** argv) {
   }
   long mism = 0;
   double first = 0.0;
+  if (fn == "exp") {
+    // the batched form (exp_n) must return the same bits as exp()
+    for (size_t q = 0; q + 4 <= xs.size(); q += 4) {
+      const double in[4] = {xs[q], xs[q + 1], xs[q + 2], xs[q + 3]};
+      double out[4];
+      cg::crm::exp_n<4>(in, out);
+      for (int n = 0; n < 4; ++n)
+        if (!same(out[n], cg::crm::exp(in[n]))) {
+          if (mism == 0) first = in[n];
+          ++mism;
+        }
+    }
+  }
   for (double x : xs) {
     if (fn == "log1p" && x < -1.0) continue;
     const double a = crm(fn, x), b = ref(fn, x);
