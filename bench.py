@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference CPU build (rank 0)")
     ap.add_argument("--ncu", action="store_true", help="short run for profiler capture (no JSON extras)")
     ap.add_argument("--variants", default="fp64_fma,mixed", help="comma list of extra precisions timed alongside")
+    ap.add_argument("--ensemble", type=int, default=1, help="also time the 48-box ensemble (variants.ensemble)")
     ap.add_argument("--workload", choices=["box", "ensemble", "slab"], default="box",
                     help="box: one 256^3 box per GPU; ensemble: 48 boxes of 32^3/64^3/96^3 split over the GPUs; "
                          "slab: one (256 N) x 256 x 256 box cut into N x-slabs with a ghost exchange per substep")
@@ -250,6 +251,61 @@ def cpu_baseline(st, order: int, steps: int = 3):
                                  "cores": 1, "sample": f"{len(s1)} RK4 steps of a 64^3 order-{order} BSSN+dust "
                                                        f"GRF box on one thread ({one.name})"}
     return out
+
+
+def ensemble_variant(a, world, rank, stream):
+    """The 48-box ensemble (16 each of 32^3, 64^3, 96^3
+    BSSN + dust boxes, order 4, FP32-mixed, one autotuned launch per
+    substep) timed beside the default box: updates/s over all ranks, the
+    launch groups the autotuner chose, and every box against an FP64 run of
+    the same steps (worst field error against its spread, Hamiltonian L2
+    ratio)."""
+    import torch
+    import torch.distributed as dist
+
+    from cosmograph_b200 import ensemble
+    from cosmograph_b200.evolution import BoxConfig, Evolution
+
+    specs = ensemble.standard_ensemble()
+    mine = ensemble.local_share(specs, rank, world)
+    states = ensemble.initial_states(mine, order=4, gpu=True)
+    all_pts = sum(s.points for s in specs)
+    cfg = BoxConfig(order=4, lapse="Harmonic", precision="mixed")
+    ev = Evolution(states, [cfg] * len(states))
+    ev.set_stream(stream.cuda_stream)
+    ev.step(max(a.warmup, 0))
+    ev.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ev.step(a.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ev.synchronize()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    fp64 = Evolution(states, [BoxConfig(order=4, lapse="Harmonic")] * len(states))
+    fp64.set_stream(stream.cuda_stream)
+    fp64.step(max(a.warmup, 0) + a.steps)
+    fp64.synchronize()
+    acc = {}
+    for q, sp in enumerate(mine):
+        acc[sp.box_id] = accuracy(fp64.download(q), ev.download(q), fp64.constraints(q), ev.constraints(q))
+    groups = ev.groups()
+    fp64.close()
+    ev.close()
+    acc_all = ensemble.gather(acc, world)
+    return {"workload": ensemble_config(specs, world)["workload"], "value": all_pts * a.steps / (ms / 1e3),
+            "ms_per_step": ms / a.steps, "groups": groups,
+            "accuracy_vs_fp64": {
+                "max_field_err_rel_perturbation": max(v["field_err_rel_perturbation"] for v in acc_all.values()),
+                "max_H_ratio": max(v["H_ratio"] for v in acc_all.values()),
+                "min_H_ratio": min(v["H_ratio"] for v in acc_all.values()), "boxes": len(acc_all)}}
 
 
 def run_ensemble(a, world, rank, local):
@@ -621,6 +677,8 @@ def main():
             variants[prec]["accuracy_vs_fp64"] = accuracy(ref_state, ev_v.download(0), ref_h, ev_v.constraints(0))
         ev_v.close()
     del ref_state
+    if a.ensemble:
+        variants["ensemble"] = ensemble_variant(a, world, rank, stream)
 
     # end to end through the C ABI: pinned host state in, one RK4 step, state out
     state_bytes = st.fields.nbytes

@@ -18,7 +18,7 @@ CG_OK = 0
 ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "out of sequence",
           -10: "NaN detected"}
 
-MATTER = {"vacuum": 0, "dust": 1, "scalar": 2}
+MATTER = {"vacuum": 0, "dust": 1, "scalar": 2, "static": 3}
 LAPSE = {
     "Static": 0, "Harmonic": 1, "ConformalFLRW": 2, "ConformalSync": 3, "Anharmonic": 4,
     "OnePlusLog": 5, "AwAGaugeWave": 6, "AwAShiftedWave": 7, "DampedWave": 8,
@@ -39,7 +39,7 @@ EXPORTS = (
     "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints", "cg_field_statistics",
     "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust",
 )
-OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID, OPT_TMA, OPT_PAIR = 1, 2, 3, 4, 5, 6
+OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID, OPT_TMA = 1, 2, 3, 4, 5
 
 
 class BoxDesc(ctypes.Structure):

@@ -127,7 +127,7 @@ struct cg_ctx {
   std::vector<Group> groups;
   std::vector<int> singles;  // boxes launched on their own
   bool grouped = false;      // groups and singles are current
-  int opt_batch = 1, opt_graph = 0, opt_autotune = 1, opt_group_grid = 0, opt_tma = 1, opt_pair = 1;
+  int opt_batch = 1, opt_graph = 0, opt_autotune = 1, opt_group_grid = 0, opt_tma = 1;
   cudaGraphExec_t gexec = nullptr;
   int gexec_steps = 0;
   cudaStream_t stream = nullptr;
@@ -605,13 +605,22 @@ int validate(const cg_box_desc& d, std::string& why) {
     why = "box too large for 32-bit point indices";
     return CG_ERR_INVALID;
   }
-  if (d.matter < 0 || d.matter > 2) { why = "unknown matter model"; return CG_ERR_INVALID; }
+  if (d.matter < 0 || d.matter > 3) { why = "unknown matter model"; return CG_ERR_INVALID; }
+  if (d.matter == CG_MATTER_STATIC && d.lapse != CG_LAPSE_STATIC && d.lapse != CG_LAPSE_CONFORMAL_FLRW) {
+    // StaticSim::StaticSim (sims/static.cc:11-17)
+    why = "not using a constant lapse gauge: static matter needs the Static or ConformalFLRW lapse";
+    return CG_ERR_INVALID;
+  }
   if (d.lapse < 0 || d.lapse > 8) { why = "unknown lapse gauge"; return CG_ERR_INVALID; }
   if (d.precision != CG_PREC_FP64 && d.precision != CG_PREC_FP64_FMA && d.precision != CG_PREC_MIXED) {
     why = "unknown precision";
     return CG_ERR_INVALID;
   }
   if (d.precision == CG_PREC_MIXED) {
+    if (d.matter == CG_MATTER_STATIC) {
+      why = "the FP32-mixed form evolves vacuum, dust or scalar boxes";
+      return CG_ERR_INVALID;
+    }
     if (d.lapse != CG_LAPSE_HARMONIC && d.lapse != CG_LAPSE_STATIC) {
       why = "the FP32-mixed form supports the Harmonic and Static lapses";
       return CG_ERR_INVALID;
@@ -701,7 +710,9 @@ extern "C" {
 
 int cg_version(void) { return CG_ABI_VERSION; }
 
-int cg_num_fields(int matter) { return matter == CG_MATTER_DUST ? 22 : matter == CG_MATTER_SCALAR ? 23 : 18; }
+int cg_num_fields(int matter) {
+  return matter == CG_MATTER_DUST ? 22 : matter == CG_MATTER_SCALAR ? 23 : matter == CG_MATTER_STATIC ? 19 : 18;
+}
 
 const char* cg_field_name(int matter, int field) {
   static const char* bssn[18] = {"DIFFgamma11", "DIFFgamma12", "DIFFgamma13", "DIFFgamma22", "DIFFgamma23",
@@ -711,6 +722,7 @@ const char* cg_field_name(int matter, int field) {
   static const char* scal[5] = {"phi", "Pi", "psi1", "psi2", "psi3"};
   if (field < 0 || field >= cg_num_fields(matter)) return nullptr;
   if (field < 18) return bssn[field];
+  if (matter == CG_MATTER_STATIC) return "DIFFD";
   return matter == CG_MATTER_DUST ? dust[field - 18] : scal[field - 18];
 }
 
@@ -809,7 +821,6 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
         else cg::exact::make_tile_maps(b.dev);
         b.dev.tma = b.dev.tma && ctx->opt_tma;
       }
-      b.dev.pair = ctx->opt_pair;
     } else {
       cg::MixedBox& m = b.mdev;
       m.nx = d.nx; m.ny = d.ny; m.nz = d.nz; m.pts = b.dev.pts; m.nfields = b.dev.nfields;
@@ -1327,7 +1338,7 @@ int group_launch(cg_ctx* ctx, Group& g, std::vector<Box>& boxes, int n) {
       if (rc) return rc;
     }
     CG_CUDA(ctx, cg::launch_group(g.variant, static_cast<const cg::GroupBox*>(g.table), gb, g.order, g.matter, n,
-                                  g.grid, ctx->opt_pair, ctx->stream));
+                                  g.grid, ctx->stream));
   }
   return CG_OK;
 }
@@ -1368,7 +1379,7 @@ int tune_groups(cg_ctx* ctx) {
     for (int q : g.members) ready = ready && ctx->boxes[q].stage_next == 1;
     if (!ready) continue;
     const int per_sm = g.mixed ? cg::mixed::group_ctas_per_sm(g.order, g.matter)
-                               : cg::group_ctas_per_sm(g.variant, g.order, g.matter, ctx->opt_pair);
+                               : cg::group_ctas_per_sm(g.variant, g.order, g.matter);
     float best = 1e30f;
     int best_lpt = 0, best_grid = 0;
     for (int lpt = 0; lpt < 2 && rc == CG_OK; ++lpt) {
@@ -1557,13 +1568,6 @@ int cg_set_option(cg_ctx* ctx, int option, int value) {
         else b.dev.tma = b.dev.maps && ctx->opt_tma;
       }
       ctx->grouped = false;  // the group tables carry the flag
-      return CG_OK;
-    case CG_OPT_PAIR:
-      for (Box& b : ctx->boxes)
-        if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "change CG_OPT_PAIR between steps");
-      ctx->opt_pair = value != 0;
-      for (Box& b : ctx->boxes) b.dev.pair = ctx->opt_pair;
-      for (Group& g : ctx->groups) g.tuned = false;  // the launch shapes change
       return CG_OK;
     case CG_OPT_GRAPH: ctx->opt_graph = value != 0; return CG_OK;
     case CG_OPT_AUTOTUNE: ctx->opt_autotune = value != 0; return CG_OK;

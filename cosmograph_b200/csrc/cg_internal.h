@@ -21,7 +21,6 @@ struct BoxDev {
   int tma;                 // interior tiles are copied by TMA (maps != 0 and the option on)
   int nx, ny, nz, pts, nfields, order, matter;
   int xg;  // ghost planes on each x face (0: periodic box)
-  int pair;  // substeps with two threads per point (stage_pair_kernel)
   CUtensorMap fmap0[3], fmap1[3];  // TMA maps of the flux primitives FP0 / FP1 (x, y, z boxes)
   int fmaps;                       // those maps are encoded
   Physics ph;
@@ -98,21 +97,21 @@ cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
 // per brick; otherwise a persistent grid of that many CTAs.
 namespace exact {
 cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
-                         int pair, cudaStream_t st);
-int group_ctas_per_sm(int order, int matter, int pair);
+                         cudaStream_t st);
+int group_ctas_per_sm(int order, int matter);
 }  // namespace exact
 namespace fast {
 cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
-                         int pair, cudaStream_t st);
-int group_ctas_per_sm(int order, int matter, int pair);
+                         cudaStream_t st);
+int group_ctas_per_sm(int order, int matter);
 }  // namespace fast
 inline cudaError_t launch_group(int v, const GroupBox* table, const GroupBg& gb, int order, int matter, int stage,
-                                int grid, int pair, cudaStream_t st) {
-  return v == kFast ? fast::launch_group(table, gb, order, matter, stage, grid, pair, st)
-                    : exact::launch_group(table, gb, order, matter, stage, grid, pair, st);
+                                int grid, cudaStream_t st) {
+  return v == kFast ? fast::launch_group(table, gb, order, matter, stage, grid, st)
+                    : exact::launch_group(table, gb, order, matter, stage, grid, st);
 }
-inline int group_ctas_per_sm(int v, int order, int matter, int pair) {
-  return v == kFast ? fast::group_ctas_per_sm(order, matter, pair) : exact::group_ctas_per_sm(order, matter, pair);
+inline int group_ctas_per_sm(int v, int order, int matter) {
+  return v == kFast ? fast::group_ctas_per_sm(order, matter) : exact::group_ctas_per_sm(order, matter);
 }
 
 // Volume-weighted average (utils/math.h:1403-1415) of n values of `field`,

@@ -70,7 +70,7 @@ constexpr long long kTmaWaitCycles64 = 2000000000LL;               // about a se
 
 template <int MATTER>
 struct NF {
-  static constexpr int value = MATTER == kDust ? 22 : (MATTER == kScalar ? 23 : 18);
+  static constexpr int value = MATTER == kDust ? 22 : (MATTER == kScalar ? 23 : (MATTER == kStaticMatter ? 19 : 18));
 };
 
 // CTA brick and field tiles (cg_tile.cuh)
@@ -714,12 +714,14 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   gm[0] = g[0] + 1.0; gm[1] = g[1]; gm[2] = g[2];
   gm[3] = g[3] + 1.0; gm[4] = g[4]; gm[5] = g[5] + 1.0;
   // every e^x this point's substep takes, in one batch: of phi and, for dust
-  // after the first substep, of the previous substep's phi (the lagged sources)
+  // after the first substep, of the previous substep's phi (the lagged
+  // sources); static matter takes e^{-6 phi} in the sixth place
   double phip = phi;
   if (MATTER == kDust && stage > 1) phip = __ldcs(&P.prev[(size_t)F_PHI * N + c]) + bg.phi_FRW_prev;
   double ex[8];
   {
-    const double xa[8] = {-4.0 * phi, 4.0 * phi, 6.0 * phi, 5.0 * phi, -5.0 * phi, -4.0 * phip, 4.0 * phip, 6.0 * phip};
+    const double xa[8] = {-4.0 * phi, 4.0 * phi, 6.0 * phi, 5.0 * phi, -5.0 * phi,
+                          MATTER == kStaticMatter ? -6.0 * phi : -4.0 * phip, 4.0 * phip, 6.0 * phip};
     xexp_n<8>(xa, ex);
   }
   const double em4phi = ex[0], e4phi = ex[1], e6phi = ex[2], e5phi = ex[3], em5phi = ex[4];
@@ -811,6 +813,17 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
                          pot_dV(ph, sphi)));
 #pragma unroll
     for (int m = 0; m < 3; ++m) rhs_m[2 + m] = (-alpha * SD(1, m) - sPi * S(S_DA + m));
+  } else if (MATTER == kStaticMatter) {
+    // BSSN::clearSrc, Static::addBSSNSrc (components/static/static.cc:19-36)
+    // and Lambda::addBSSNSource: the fixed density sources DIFFr only
+#pragma unroll
+    for (int m = 0; m < Q_N; ++m) S(S_SRC + m) = 0.0;
+    const double phid = C(F_PHI);
+    double r = 0.0;
+    r += ex[5] * C(F_DIFFD) + bg.rho_FRW * xexpm1(-6.0 * phid);
+    r += ph.lambda;
+    S(S_SRC + Q_R) = r;
+    S(S_SRC + Q_S) = 0.0 + -3.0 * ph.lambda;
   } else {
 #pragma unroll
     for (int m = 0; m < Q_N; ++m) S(S_SRC + m) = 0.0;
@@ -1179,6 +1192,12 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   } else if (MATTER == kScalar) {
 #pragma unroll
     for (int m = 0; m < 5; ++m) finalize(F_SPHI + m, rhs_m[m]);
+  } else if (MATTER == kStaticMatter) {
+    // the fixed density is no register of the reference: every output keeps it
+    const double pv = __ldcs(&P.p[(size_t)F_DIFFD * N + c]);
+    __stcs(&P.out[(size_t)F_DIFFD * N + c], pv);
+    if (stage == 4) __stcs(&P.norm[(size_t)F_DIFFD * N + c], pv);
+    outv[F_DIFFD] = pv;
   }
 
   // ---- the next substep's inputs -----------------------------------------------
@@ -1304,8 +1323,6 @@ stage_group_kernel(const GroupBox* __restrict__ boxes, GroupBg gb, int stage) {
     stage_body<O, MATTER, kEvolve>(geo, sb.ph, sbg, sp, stage, cx, cy, cz, 0, stm, bar, phase, tma_ok, sfm);
   }
 }
-
-#include "cg_stage_pair.cuh"
 
 }  // namespace CG_VARIANT_NS
 }  // namespace cg

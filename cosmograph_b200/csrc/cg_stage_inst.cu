@@ -91,32 +91,6 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
   FluxMaps fm;
   const CUtensorMap* fsrc = (stage == 1 || stage == 3) ? b.fmap0 : b.fmap1;
   for (int a = 0; a < 3; ++a) fm.m[a] = fsrc[a];
-  if (b.pair) {  // two threads per point
-    constexpr size_t psmem = pair_smem<O, M>();
-    const dim3 block(kPairThreads);
-    if constexpr (O == 2 || O == 8) {
-      if (b.ph.ko_coeff != 0.0) {
-        static bool configured_ko = false;
-        if (!configured_ko) {
-          cudaError_t e = cudaFuncSetAttribute(stage_pair_kernel<O, M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)psmem);
-          if (e != cudaSuccess) return e;
-          configured_ko = true;
-        }
-        stage_pair_kernel<O, M, true><<<stage_grid(b), block, psmem, st>>>(geo, b.ph, bg, P, stage, map, b.tma, fm,
-                                                                           b.fmaps);
-        return cudaGetLastError();
-      }
-    }
-    static bool configured_pair = false;
-    if (!configured_pair) {
-      cudaError_t e = cudaFuncSetAttribute(stage_pair_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
-      if (e != cudaSuccess) return e;
-      configured_pair = true;
-    }
-    stage_pair_kernel<O, M><<<stage_grid(b), block, psmem, st>>>(geo, b.ph, bg, P, stage, map, b.tma, fm, b.fmaps);
-    return cudaGetLastError();
-  }
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
   if constexpr (O == 2 || O == 8) {
     if (b.ph.ko_coeff != 0.0) {  // Kreiss-Oliger dissipation: its own instantiation
@@ -173,25 +147,13 @@ cudaError_t go_constraints_m(const BoxDev& b, const StageBg& bg, double* cvals, 
   switch (b.matter) {
     case kDust: return go_constraints<O, kDust>(b, bg, cvals, cpart, st);
     case kScalar: return go_constraints<O, kScalar>(b, bg, cvals, cpart, st);
+    case kStaticMatter: return go_constraints<O, kStaticMatter>(b, bg, cvals, cpart, st);
     default: return go_constraints<O, kVacuum>(b, bg, cvals, cpart, st);
   }
 }
 
 template <int O, int M>
-cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, int pair, cudaStream_t st) {
-  const int g = grid > 0 ? grid : gb.total;
-  if (pair) {
-    constexpr size_t psmem = pair_smem<O, M>();
-    static bool configured_pair = false;
-    if (!configured_pair) {
-      cudaError_t e =
-          cudaFuncSetAttribute(stage_pair_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
-      if (e != cudaSuccess) return e;
-      configured_pair = true;
-    }
-    stage_pair_group_kernel<O, M><<<g, kPairThreads, psmem, st>>>(table, gb, stage);
-    return cudaGetLastError();
-  }
+cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, cudaStream_t st) {
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
   static bool configured = false;
   if (!configured) {
@@ -199,23 +161,13 @@ cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int gr
     if (e != cudaSuccess) return e;
     configured = true;
   }
+  const int g = grid > 0 ? grid : gb.total;
   stage_group_kernel<O, M><<<g, stage_block(), smem, st>>>(table, gb, stage);
   return cudaGetLastError();
 }
 
 template <int O, int M>
-int ctas_per_sm(int pair) {
-  if (pair) {
-    constexpr size_t psmem = pair_smem<O, M>();
-    if (cudaFuncSetAttribute(stage_pair_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem) !=
-        cudaSuccess)
-      return 1;
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage_pair_group_kernel<O, M>, kPairThreads, psmem) !=
-        cudaSuccess)
-      return 1;
-    return n > 0 ? n : 1;
-  }
+int ctas_per_sm() {
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
   if (cudaFuncSetAttribute(stage_group_kernel<O, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
@@ -227,20 +179,21 @@ int ctas_per_sm(int pair) {
 }
 
 template <int O>
-cudaError_t go_group_m(const GroupBox* table, const GroupBg& gb, int matter, int stage, int grid, int pair,
-                       cudaStream_t st) {
+cudaError_t go_group_m(const GroupBox* table, const GroupBg& gb, int matter, int stage, int grid, cudaStream_t st) {
   switch (matter) {
-    case kDust: return go_group<O, kDust>(table, gb, stage, grid, pair, st);
-    case kScalar: return go_group<O, kScalar>(table, gb, stage, grid, pair, st);
-    default: return go_group<O, kVacuum>(table, gb, stage, grid, pair, st);
+    case kDust: return go_group<O, kDust>(table, gb, stage, grid, st);
+    case kScalar: return go_group<O, kScalar>(table, gb, stage, grid, st);
+    case kStaticMatter: return go_group<O, kStaticMatter>(table, gb, stage, grid, st);
+    default: return go_group<O, kVacuum>(table, gb, stage, grid, st);
   }
 }
 template <int O>
-int ctas_m(int matter, int pair) {
+int ctas_m(int matter) {
   switch (matter) {
-    case kDust: return ctas_per_sm<O, kDust>(pair);
-    case kScalar: return ctas_per_sm<O, kScalar>(pair);
-    default: return ctas_per_sm<O, kVacuum>(pair);
+    case kDust: return ctas_per_sm<O, kDust>();
+    case kScalar: return ctas_per_sm<O, kScalar>();
+    case kStaticMatter: return ctas_per_sm<O, kStaticMatter>();
+    default: return ctas_per_sm<O, kVacuum>();
   }
 }
 
@@ -249,6 +202,7 @@ cudaError_t go_stage_m(const BoxDev& b, const StageBg& bg, int stage, cudaStream
   switch (b.matter) {
     case kDust: return go_stage<O, kDust>(b, bg, stage, st);
     case kScalar: return go_stage<O, kScalar>(b, bg, stage, st);
+    case kStaticMatter: return go_stage<O, kStaticMatter>(b, bg, stage, st);
     default: return go_stage<O, kVacuum>(b, bg, stage, st);
   }
 }
@@ -308,22 +262,22 @@ cudaError_t launch_constraints(const BoxDev& b, const StageBg& bg, double* cvals
 }
 
 cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
-                         int pair, cudaStream_t st) {
+                         cudaStream_t st) {
   switch (order) {
-    case 2: return go_group_m<2>(table, gb, matter, stage, grid, pair, st);
-    case 4: return go_group_m<4>(table, gb, matter, stage, grid, pair, st);
-    case 6: return go_group_m<6>(table, gb, matter, stage, grid, pair, st);
-    case 8: return go_group_m<8>(table, gb, matter, stage, grid, pair, st);
+    case 2: return go_group_m<2>(table, gb, matter, stage, grid, st);
+    case 4: return go_group_m<4>(table, gb, matter, stage, grid, st);
+    case 6: return go_group_m<6>(table, gb, matter, stage, grid, st);
+    case 8: return go_group_m<8>(table, gb, matter, stage, grid, st);
     default: return cudaErrorInvalidValue;
   }
 }
 
-int group_ctas_per_sm(int order, int matter, int pair) {
+int group_ctas_per_sm(int order, int matter) {
   switch (order) {
-    case 2: return ctas_m<2>(matter, pair);
-    case 4: return ctas_m<4>(matter, pair);
-    case 6: return ctas_m<6>(matter, pair);
-    default: return ctas_m<8>(matter, pair);
+    case 2: return ctas_m<2>(matter);
+    case 4: return ctas_m<4>(matter);
+    case 6: return ctas_m<6>(matter);
+    default: return ctas_m<8>(matter);
   }
 }
 
@@ -337,6 +291,7 @@ cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st) {
   switch (b.matter) {
     case kDust: init_kernel<kDust><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
     case kScalar: init_kernel<kScalar><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
+    case kStaticMatter: init_kernel<kStaticMatter><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
     default: init_kernel<kVacuum><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
   }
   return cudaGetLastError();

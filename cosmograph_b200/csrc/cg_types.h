@@ -17,7 +17,8 @@ enum : int {
   F_G11 = 0, F_G12, F_G13, F_G22, F_G23, F_G33, F_PHI, F_A11, F_A12, F_A13,
   F_A22, F_A23, F_A33, F_K, F_GAM1, F_GAM2, F_GAM3, F_ALPHA, F_NBSSN = 18,
   F_D = 18, F_S1 = 19, F_S2 = 20, F_S3 = 21,
-  F_SPHI = 18, F_SPI = 19, F_SPSI1 = 20
+  F_SPHI = 18, F_SPI = 19, F_SPSI1 = 20,
+  F_DIFFD = 18  // static matter: the fixed density, not evolved
 };
 // source slots (bssn_macros.h:101-112)
 enum : int { Q_R = 0, Q_S, Q_S1, Q_S2, Q_S3, Q_STF11, Q_N = 11 };
@@ -25,7 +26,7 @@ enum : int { Q_R = 0, Q_S, Q_S1, Q_S2, Q_S3, Q_STF11, Q_N = 11 };
 // alpha*D, alpha*S_1..3, v^1..3 (dust.cc:121-133 forms the products of these)
 enum : int { P_AD = 0, P_AS1, P_AS2, P_AS3, P_V1, P_V2, P_V3, P_N = 7 };
 
-enum Matter : int { kVacuum = 0, kDust = 1, kScalar = 2 };
+enum Matter : int { kVacuum = 0, kDust = 1, kScalar = 2, kStaticMatter = 3 };
 enum Lapse : int {
   kStatic = 0, kHarmonic, kConformalFLRW, kConformalSync, kAnharmonic, kOnePlusLog,
   kAwAGaugeWave, kAwAShiftedWave, kDampedWave

@@ -175,9 +175,9 @@ class Evolution:
         self._check(self.L.cg_ic_grf_dust(self.ctx, box, dptr, ctypes.c_uint64(seed), rms_delta, ns, cutoff))
 
     def set_option(self, option: str, value: int) -> None:
-        """Launch options: "batch", "graph", "autotune", "group_grid", "tma", "pair" (cg_set_option)."""
+        """Launch options: "batch", "graph", "autotune", "group_grid", "tma" (cg_set_option)."""
         code = {"batch": _lib.OPT_BATCH, "graph": _lib.OPT_GRAPH, "autotune": _lib.OPT_AUTOTUNE,
-                "group_grid": _lib.OPT_GROUP_GRID, "tma": _lib.OPT_TMA, "pair": _lib.OPT_PAIR}[option]
+                "group_grid": _lib.OPT_GROUP_GRID, "tma": _lib.OPT_TMA}[option]
         self._check(self.L.cg_set_option(self.ctx, code, int(value)))
 
     def groups(self) -> list[dict]:

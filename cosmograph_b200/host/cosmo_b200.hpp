@@ -230,6 +230,16 @@ class Scalar {
   BSSN* b = nullptr;
 };
 
+// Static matter (components/static/static.h): a fixed density DIFFD (field
+// 18 of the box) that sources DIFFr; the source is formed inside the substep
+// kernel, this class keeps the reference's call sequence.
+class Static {
+ public:
+  Static() = default;
+  void init() {}
+  void addBSSNSrc(BSSN* bssn);
+};
+
 // Cosmological constant (components/Lambda/lambda.h)
 class Lambda {
  public:
@@ -299,6 +309,22 @@ class ScalarSim : public CosmoSim {
 
  private:
   Scalar* scalarSim = nullptr;
+};
+
+// sims/static.h: static matter, Static or ConformalFLRW lapse
+class StaticSim : public CosmoSim {
+ public:
+  explicit StaticSim(ConfigParser* config);
+  ~StaticSim() override;
+  void init() override;
+  void setICs() override;
+  void runStep() override;
+  void initStaticStep();
+  void runStaticStep();
+
+ private:
+  Static* staticSim = nullptr;
+  Lambda* lambda = nullptr;
 };
 
 class VacuumSim : public CosmoSim {

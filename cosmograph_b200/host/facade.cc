@@ -44,7 +44,8 @@ int matter_code(const std::string& sim) {
   if (sim == "dust") return CG_MATTER_DUST;
   if (sim == "scalar") return CG_MATTER_SCALAR;
   if (sim == "vacuum") return CG_MATTER_VACUUM;
-  raise(2, "simulation_type `" + sim + "` is not on this path (dust, scalar, vacuum)");
+  if (sim == "static") return CG_MATTER_STATIC;
+  raise(2, "simulation_type `" + sim + "` is not on this path (dust, scalar, vacuum, static)");
 }
 
 // state-file header (cosmograph_b200.state: "CGSTATE1", 168 bytes, little endian)
@@ -433,6 +434,11 @@ void Dust::finalize(int n) {
                                              std::to_string(n) + "Finalize");
 }
 
+void Static::addBSSNSrc(BSSN* bssn) {
+  if (!bssn || bssn->matter() != CG_MATTER_STATIC) raise(-1, "the BSSN box was not created with static matter");
+  bssn->note_sources();
+}
+
 void Scalar::stepInit(BSSN* bssn) {
   if (!bssn || bssn->matter() != CG_MATTER_SCALAR) raise(-1, "the BSSN box was not created with a scalar field");
   b = bssn;
@@ -819,6 +825,73 @@ void ScalarSim::runStep() {
   runScalarStep();
 }
 
+StaticSim::StaticSim(ConfigParser* config) : CosmoSim(config) {
+  // sims/static.cc:11-17
+  const std::string lapse = (*config)("lapse", "");
+  if (lapse != "" && lapse != "Static" && lapse != "ConformalFLRW") {
+    iodata->log("Error - not using a constant lapse gauge! You must use it for 'static' sims.");
+    iodata->log("Please change this setting in the config file and re-run.");
+    throw -1;
+  }
+}
+
+StaticSim::~StaticSim() {
+  delete staticSim;
+  delete lambda;
+}
+
+void StaticSim::init() {
+  simInit();
+  iodata->log("Initializing 'static' type simulation.");
+  staticSim = new Static();
+  staticSim->init();
+  lambda = new Lambda();
+}
+
+void StaticSim::setICs() {
+  iodata->log("Setting static initial conditions (ICs).");
+  loadICs();
+  lambda->setLambda(bssnSim->desc().lambda);
+  iodata->log("Finished setting ICs.");
+}
+
+void StaticSim::initStaticStep() {
+  const auto t0 = std::chrono::steady_clock::now();
+  // sims/static.cc:71-80
+  bssnSim->stepInit();
+  bssnSim->clearSrc();
+  staticSim->addBSSNSrc(bssnSim);
+  lambda->addBSSNSource(bssnSim);
+  rk_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void StaticSim::runStaticStep() {
+  const auto t0 = std::chrono::steady_clock::now();
+  // sims/static.cc:131-167 (without the ray sheets)
+  for (int n = 1; n <= 4; ++n) {
+    if (n > 1) {
+      bssnSim->clearSrc();
+      staticSim->addBSSNSrc(bssnSim);
+      lambda->addBSSNSource(bssnSim);
+    }
+    bssnSim->RKEvolve();
+    if (n == 1) bssnSim->K1Finalize();
+    else if (n == 2) bssnSim->K2Finalize();
+    else if (n == 3) bssnSim->K3Finalize();
+    else bssnSim->K4Finalize();
+  }
+  rk_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void StaticSim::runStep() {
+  // sims/static.cc:169-175
+  initStaticStep();
+  runCommonStepTasks();
+  outputCommon();
+  if (step == 0) outputStateInformation();
+  runStaticStep();
+}
+
 void VacuumSim::init() {
   simInit();
   iodata->log("Running 'vacuum' type simulation.");
@@ -850,6 +923,7 @@ int run_config_file(const std::string& fname) {
     if (sim == "dust") s = std::make_unique<DustSim>(&config);
     else if (sim == "scalar") s = std::make_unique<ScalarSim>(&config);
     else if (sim == "vacuum") s = std::make_unique<VacuumSim>(&config);
+    else if (sim == "static") s = std::make_unique<StaticSim>(&config);
     else {
       std::cerr << "Invalid simulation type specified. ";
       throw 2;

@@ -22,7 +22,7 @@ import math
 
 import numpy as np
 
-from .state import BSSN_FIELDS, DUST, SCALAR, VACUUM, BoxState, field_names
+from .state import BSSN_FIELDS, DUST, SCALAR, STATIC, VACUUM, BoxState, field_names
 
 PI = math.pi
 RHO_FRW = 3.0 / PI / 8.0        # dust_ic.cc:29, H0 = 1
@@ -274,14 +274,21 @@ def perturbed(shape, matter: int, seed: int = 1, amp: float = 1.0e-2, modes: int
             v += (a * s1[0])[:, None, None] * s1[1][None, :, None] * s1[2][None, None, :]
         v *= amp / modes
         base = {"DIFFK": -3.0, "D": RHO_FRW, "phi": 0.1}.get(name, 0.0)
-        if name in ("D", "S1", "S2", "S3"):
+        if name in ("D", "S1", "S2", "S3", "DIFFD"):
             v = RHO_FRW * v            # keep the density positive
+        if matter == STATIC and name == "DIFFK":
+            base = 0.0                 # K sits in the FRW background
         st.fields[f] = base + v
-    if matter == DUST:
+    if matter in (DUST, STATIC):
         st.lam = 1.0e-6 * RHO_FRW
+    if matter == STATIC:
+        # the static sims' FRW background: one pressureless fluid at the
+        # density of H = 1, K = -3 (FRW::addFluid, utils/FRW.h:60-76)
+        st.fluids = ((RHO_FRW, 0.0),)
+        st.frw_K = -3.0
     return st
 
 
 __all__ = ["sinusoid_dust", "grf_dust", "grf_scalar", "perturbed", "derivative",
            "double_derivative", "laplacian", "inverse_laplacian", "default_dt",
-           "gaussian_random_field", "BSSN_FIELDS", "VACUUM", "DUST", "SCALAR"]
+           "gaussian_random_field", "BSSN_FIELDS", "VACUUM", "DUST", "SCALAR", "STATIC"]

@@ -10,8 +10,9 @@ path, and a run can be resumed from one.
 
 Field order is the reference's field-list order: BSSN_APPLY_TO_FIELDS
 (components/bssn/bssn_macros.h:77-95), then the dust registers D, S1, S2, S3
-(components/dust_fluid/dust.h:32-35) or the scalar registers phi, Pi, psi1,
-psi2, psi3 (components/scalar/scalar.h:35-39).
+(components/dust_fluid/dust.h:32-35), the scalar registers phi, Pi, psi1,
+psi2, psi3 (components/scalar/scalar.h:35-39), or the static sims' fixed
+density DIFFD (components/static/static.h:17), which no substep changes.
 """
 from __future__ import annotations
 
@@ -24,8 +25,8 @@ import numpy as np
 MAGIC = b"CGSTATE1"
 MAX_FLUIDS = 4
 
-VACUUM, DUST, SCALAR = 0, 1, 2
-MATTER_NAMES = {"vacuum": VACUUM, "dust": DUST, "scalar": SCALAR}
+VACUUM, DUST, SCALAR, STATIC = 0, 1, 2, 3
+MATTER_NAMES = {"vacuum": VACUUM, "dust": DUST, "scalar": SCALAR, "static": STATIC}
 
 BSSN_FIELDS = (
     "DIFFgamma11", "DIFFgamma12", "DIFFgamma13", "DIFFgamma22", "DIFFgamma23",
@@ -34,6 +35,7 @@ BSSN_FIELDS = (
 )
 DUST_FIELDS = ("D", "S1", "S2", "S3")
 SCALAR_FIELDS = ("phi", "Pi", "psi1", "psi2", "psi3")
+STATIC_FIELDS = ("DIFFD",)  # the static sims' fixed density (components/static/static.h:17), not evolved
 
 # header layout (168 bytes); mirrors oracle/cg_state.h
 _HDR = struct.Struct("<8s8i4d4d4dd3d")
@@ -45,6 +47,8 @@ def field_names(matter: int) -> tuple[str, ...]:
         return BSSN_FIELDS + DUST_FIELDS
     if matter == SCALAR:
         return BSSN_FIELDS + SCALAR_FIELDS
+    if matter == STATIC:
+        return BSSN_FIELDS + STATIC_FIELDS
     return BSSN_FIELDS
 
 

@@ -45,6 +45,9 @@ extern "C" {
 #define CG_MATTER_VACUUM 0
 #define CG_MATTER_DUST 1
 #define CG_MATTER_SCALAR 2
+#define CG_MATTER_STATIC 3  /* the static sims' matter: a fixed density DIFFD that
+                               sources DIFFr (components/static/static.cc:19-36,
+                               sims/static.cc); Static or ConformalFLRW lapse    */
 
 /* lapse gauges (reference BSSNGaugeHandler lapse map,
  * components/bssn/BSSNGaugeHandler.h:95-110) */
@@ -132,9 +135,10 @@ int cg_destroy(cg_ctx *ctx);
 int cg_set_stream(cg_ctx *ctx, void *stream);
 int cg_get_stream(cg_ctx *ctx, void **stream);
 
-/* Number of evolved fields (18 vacuum, 22 dust, 23 scalar) and their names
- * (BSSN_APPLY_TO_FIELDS order, bssn_macros.h:77-95, then D,S1,S2,S3 or
- * phi,Pi,psi1,psi2,psi3). */
+/* Number of fields (18 vacuum, 22 dust, 23 scalar, 19 static) and their names
+ * (BSSN_APPLY_TO_FIELDS order, bssn_macros.h:77-95, then D,S1,S2,S3,
+ * phi,Pi,psi1,psi2,psi3, or the static density DIFFD, which no substep
+ * changes). */
 int cg_num_fields(int matter);
 const char *cg_field_name(int matter, int field);
 
@@ -240,17 +244,12 @@ int cg_ic_grf_dust(cg_ctx *ctx, int box, const double *delta, uint64_t seed, dou
  *                    accelerator (FP64 boxes with even nz, mixed boxes with nz
  *                    a multiple of 4); 0: every tile is copied by the CTA's
  *                    threads.  Results are identical.  Change it between
- *                    steps only.
- *   CG_OPT_PAIR      1 (default): the FP64 substep kernels run two threads
- *                    per grid point (256-thread CTAs, twice the warps per
- *                    SM); 0: one thread per point.  Results are identical.
- *                    Change it between steps only. */
+ *                    steps only. */
 #define CG_OPT_BATCH 1
 #define CG_OPT_GRAPH 2
 #define CG_OPT_AUTOTUNE 3
 #define CG_OPT_GROUP_GRID 4
 #define CG_OPT_TMA 5
-#define CG_OPT_PAIR 6
 int cg_set_option(cg_ctx *ctx, int option, int value);
 
 /* Launch groups of the context (formed on first use), and for group g:

@@ -39,6 +39,7 @@ REF_SOURCES = [
     "components/bssn/BSSNGaugeHandler.cc",
     "components/dust_fluid/dust.cc",
     "components/scalar/scalar.cc",
+    "components/static/static.cc",
     "components/Lambda/lambda.cc",
     "utils/ConfigParser.cc",
     "utils/Timer.cc",

@@ -32,7 +32,7 @@ void cgo_set_threads(int n) {
 }
 
 int cgo_num_fields(int matter) {
-  return matter == CGO_DUST ? 22 : matter == CGO_SCALAR ? 23 : 18;
+  return matter == CGO_DUST ? 22 : matter == CGO_SCALAR ? 23 : matter == CGO_STATIC ? 19 : 18;
 }
 
 /* field slots, cg_state.h order */
@@ -578,6 +578,25 @@ static void dust_sources(sim_t *s) {
   }
 }
 
+/* BSSN::clearSrc, Static::addBSSNSrc (components/static/static.cc:19-36),
+ * Lambda::addBSSNSource: the fixed density DIFFD (field 18) sources DIFFr
+ * with the current DIFFphi and the FRW getters of this substep */
+static void static_sources(sim_t *s) {
+  const long N = s->pts;
+  const double *a = s->reg_a;
+  double *q = s->src;
+  const double lam = s->p->lambda, phi_FRW = s->get_phi, rho_FRW = s->get_rho;
+  long idx;
+#pragma omp parallel for schedule(static)
+  for (idx = 0; idx < N; ++idx) {
+    for (int m = 0; m < Q_N; ++m) q[m * N + idx] = 0.0;
+    const double phid = a[F_PHI * N + idx];
+    q[Q_R * N + idx] += exp(-6.0 * (phid + phi_FRW)) * a[F_NBSSN * N + idx] + rho_FRW * expm1(-6.0 * phid);
+    q[Q_R * N + idx] += lam;
+    q[Q_S * N + idx] += -3.0 * lam;
+  }
+}
+
 /* ------------------------------------------------------------------ */
 /* Scalar: components/scalar/scalar.cc                                 */
 /* ------------------------------------------------------------------ */
@@ -805,7 +824,7 @@ static void normalize_a(sim_t *s) {
 static int sim_init(sim_t *s, const cgo_params *p) {
   if (!p || p->nx < 1 || p->ny < 1 || p->nz < 1) return -1;
   if (p->order != 2 && p->order != 4 && p->order != 6 && p->order != 8) return -2;
-  if (p->matter < 0 || p->matter > 2) return -3;
+  if (p->matter < 0 || p->matter > 3) return -3;
   if (p->nfluids < 0 || p->nfluids > CGO_MAX_FLUIDS) return -4;
   memset(s, 0, sizeof(*s));
   s->p = p;
@@ -859,6 +878,9 @@ static void evolve_substep(sim_t *s) {
           scalar_data(s, ii, j, k, &sd);
           scalar_rhs(s, &bd, &sd, out);
           nf = 23;
+        } else if (s->p->matter == CGO_STATIC) {
+          out[F_NBSSN] = 0.0;  /* DIFFD is not evolved: the register update keeps it */
+          nf = 19;
         }
         for (int f = 0; f < nf; ++f) s->reg_c[f * N + idx] = out[f];
       }
@@ -882,6 +904,8 @@ static void step_init(sim_t *s) {
     dust_sources(s);
   } else if (s->p->matter == CGO_SCALAR) {
     scalar_sources(s);
+  } else if (s->p->matter == CGO_STATIC) {
+    static_sources(s);
   }
 }
 
@@ -920,6 +944,8 @@ static void run_step(sim_t *s) {
         dust_sources(s);
       else if (s->p->matter == CGO_SCALAR)
         scalar_sources(s);
+      else if (s->p->matter == CGO_STATIC)
+        static_sources(s);
     }
     evolve_substep(s);
     /* BSSN::K{n}Finalize, bssn.cc:267-305: FRW stage, registers, reductions */

@@ -21,6 +21,7 @@ extern "C" {
 #define CGO_VACUUM 0
 #define CGO_DUST 1
 #define CGO_SCALAR 2
+#define CGO_STATIC 3  /* the static sims' matter: a fixed density DIFFD (components/static/static.cc) */
 
 /* lapse gauges (components/bssn/BSSNGaugeHandler.h:95-110) */
 #define CGO_LAPSE_STATIC 0
@@ -43,7 +44,7 @@ extern "C" {
 typedef struct {
   int nx, ny, nz;
   int order;            /* 2, 4, 6, 8 */
-  int matter;           /* CGO_VACUUM / CGO_DUST / CGO_SCALAR */
+  int matter;           /* CGO_VACUUM / CGO_DUST / CGO_SCALAR / CGO_STATIC */
   int lapse;            /* CGO_LAPSE_* */
   int normalize_metric; /* bssn.cc:19 default 1 */
   int potential;        /* CGO_POT_* */
@@ -62,7 +63,8 @@ typedef struct {
   double fluid_rho[CGO_MAX_FLUIDS], fluid_w[CGO_MAX_FLUIDS];
 } cgo_params;
 
-/* Number of evolved fields for a matter model: 18, 22 or 23. */
+/* Number of fields of a matter model: 18, 22, 23, or 19 (static: the 18
+ * BSSN fields and the fixed density DIFFD, which no substep changes). */
 int cgo_num_fields(int matter);
 
 /* Advance `steps` RK4 steps.  `fields` holds the "_p" register of every

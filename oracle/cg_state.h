@@ -9,7 +9,8 @@
  * the reference's field-list order: BSSN_APPLY_TO_FIELDS
  * (components/bssn/bssn_macros.h:77-95), then the dust registers D,S1,S2,S3
  * (components/dust_fluid/dust.h:32-35) or the scalar registers
- * phi,Pi,psi1,psi2,psi3 (components/scalar/scalar.h:35-39).
+ * phi,Pi,psi1,psi2,psi3 (components/scalar/scalar.h:35-39), or the static
+ * sims' fixed density DIFFD (components/static/static.h:17).
  *
  * The header also carries dx, dt and the reference FRW background state
  * (utils/FRW.h:14-20) so that a CPU run and a GPU run start from identical
@@ -23,12 +24,12 @@
 #define CG_STATE_MAGIC "CGSTATE1"
 #define CG_STATE_MAX_FLUIDS 4
 
-enum cg_state_matter { CG_STATE_VACUUM = 0, CG_STATE_DUST = 1, CG_STATE_SCALAR = 2 };
+enum cg_state_matter { CG_STATE_VACUUM = 0, CG_STATE_DUST = 1, CG_STATE_SCALAR = 2, CG_STATE_STATIC = 3 };
 
 typedef struct {
   char magic[8];          /* "CGSTATE1" */
   int32_t nx, ny, nz;     /* grid points per axis */
-  int32_t nfields;        /* 18 (vacuum), 22 (dust) or 23 (scalar) */
+  int32_t nfields;        /* 18 (vacuum), 22 (dust), 23 (scalar) or 19 (static) */
   int32_t matter;         /* enum cg_state_matter */
   int32_t step;           /* RK4 steps completed */
   int32_t nfluids;        /* FRW fluids in use (0..CG_STATE_MAX_FLUIDS) */

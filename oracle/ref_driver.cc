@@ -11,6 +11,9 @@
  *   dust   : DustSim::initDustStep + runDustStep   (sims/dust.cc:53-63, 114-161)
  *   scalar : ScalarSim::initScalarStep + runScalarStep (sims/scalar.cc:75-82, 97-151)
  *   vacuum : VacuumSim::initVacuumStep + runVacuumStep (sims/vacuum.cc:73-97)
+ *   static : StaticSim::initStaticStep + runStaticStep (sims/static.cc:71-167),
+ *            the fixed density DIFFD (Static, components/static/static.cc)
+ *            read from and written back as field 18
  * minus output, NaN checks and ray sheets, which never touch the fields.
  *
  * Usage: cg_ref_<...> <mode> <config.txt> <state_in> <out> [steps]
@@ -33,6 +36,7 @@
 #include "components/bssn/bssn.h"
 #include "components/dust_fluid/dust.h"
 #include "components/scalar/scalar.h"
+#include "components/static/static.h"
 #include "components/Lambda/lambda.h"
 #include "utils/math.h"
 #include "cg_state.h"
@@ -65,6 +69,7 @@ struct Sim {
   BSSN *bssn = nullptr;
   Dust *dust = nullptr;
   Scalar *scalar = nullptr;
+  Static *stat = nullptr;
   Lambda *lambda = nullptr;
   int matter = CG_STATE_VACUUM;
 
@@ -92,6 +97,8 @@ struct Sim {
       out.push_back(pick(scalar->psi1));
       out.push_back(pick(scalar->psi2));
       out.push_back(pick(scalar->psi3));
+    } else if (matter == CG_STATE_STATIC) {
+      out.push_back(stat->fields["DIFFD_a"]);  // not a register: the same array for every role
     }
     return out;
   }
@@ -108,6 +115,10 @@ struct Sim {
       scalar->stepInit();
       bssn->clearSrc();
       scalar->addBSSNSource(bssn);
+    } else if (matter == CG_STATE_STATIC) {
+      bssn->clearSrc();
+      stat->addBSSNSrc(bssn->fields, bssn->frw);
+      lambda->addBSSNSource(bssn);
     }
   }
 
@@ -135,6 +146,10 @@ struct Sim {
     } else if (matter == CG_STATE_SCALAR) {
       bssn->clearSrc();
       scalar->addBSSNSource(bssn);
+    } else if (matter == CG_STATE_STATIC) {
+      bssn->clearSrc();
+      stat->addBSSNSrc(bssn->fields, bssn->frw);
+      lambda->addBSSNSource(bssn);
     }
   }
 
@@ -202,6 +217,11 @@ int main(int argc, char **argv) {
     sim.lambda->setLambda(h.lambda);
   } else if (h.matter == CG_STATE_SCALAR) {
     sim.scalar = new Scalar();
+  } else if (h.matter == CG_STATE_STATIC) {
+    sim.stat = new Static();
+    sim.stat->init();
+    sim.lambda = new Lambda();
+    sim.lambda->setLambda(h.lambda);
   }
   std::vector<arr_t *> P = sim.reg('p');
   if ((int)P.size() != h.nfields) die("field count differs from the matter model");

@@ -38,6 +38,8 @@ CASES = [
     ("scalar_o6_constraints", S.SCALAR, (8, 8, 10), 6, 13, 2e-2, "constraints", 0, {"lapse": "Harmonic"}),
     ("sinusoid_o4", S.DUST, (16, 4, 4), 4, 0, 0.0, "evolve", 20, {"lapse": "Harmonic"}),
     ("grf_dust_o4", S.DUST, (8, 8, 8), 4, 9, 0.0, "evolve", 5, {"lapse": "Harmonic"}),
+    ("static_o4", S.STATIC, (10, 8, 12), 4, 15, 2e-2, "evolve", 4, {"lapse": "Static"}),
+    ("static_o8", S.STATIC, (12, 10, 9), 8, 16, 2e-2, "evolve", 3, {"lapse": "ConformalFLRW"}),
 ]
 
 

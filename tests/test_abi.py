@@ -43,7 +43,8 @@ def test_library_exports_every_declared_symbol(L):
 
 def test_host_only_entry_points(L):
     assert L.cg_version() == 1
-    assert [L.cg_num_fields(m) for m in (0, 1, 2)] == [18, 22, 23]
+    assert [L.cg_num_fields(m) for m in (0, 1, 2, 3)] == [18, 22, 23, 19]
+    assert L.cg_field_name(3, 18) == b"DIFFD"
     assert L.cg_field_name(1, 0) == b"DIFFgamma11"
     assert L.cg_field_name(1, 21) == b"S3"
     assert L.cg_field_name(2, 22) == b"psi3"
@@ -61,6 +62,8 @@ def test_host_only_entry_points(L):
     ("lapse", 42, "lapse"),
     ("nx", 5, None),         # with ko_coeff: order 8 dissipation needs 6 points per axis
     ("nfluids", 7, "fluids"),
+    ("matter", 3, "constant lapse"),  # static matter with the default (Harmonic) lapse
+    ("matter", 4, "matter"),
 ])
 def test_create_rejects_bad_descriptors(L, field, value, msg):
     d = _lib.BoxDesc()

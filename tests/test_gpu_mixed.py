@@ -1,8 +1,23 @@
 """The FP32-mixed substep kernel against the FP64 GPU path.
 
-Accuracy is stated relative to the perturbation: for each field,
-max|mixed - fp64| / max|fp64 - mean(fp64)| (the spread of the field about its
-mean).  Fields whose perturbation vanishes identically are skipped.
+Two measures of accuracy:
+
+* against the run's perturbation amplitude (the bound the design targets,
+  1e-6): the amplitude is the rms of the perturbation the initial data are
+  built from -- the density contrast delta of the dust runs (rms 1e-4), the
+  scalar-field fluctuation delta phi of the scalar runs (rms 1e-5).  The
+  mixed run's error in that quantity (max over the box of
+  |D_mixed - D_fp64| / mean(D), or |phi_mixed - phi_fp64|) must stay below
+  1e-6 of it, and its Hamiltonian and momentum constraint norms within 2x
+  of the FP64 run's;
+* per field, against the field's own spread about its mean,
+  max|mixed - fp64| / max|fp64 - mean(fp64)| (fields whose perturbation
+  vanishes identically are skipped).  This is the stricter measure for the
+  metric components, whose spread is small: their FP32 right-hand sides
+  carry a rounding error of a few 2^-24 per substep, which accumulates as a
+  random walk (about 2^-24 sqrt(substeps) relative); the bounds below are
+  that estimate with a margin (measured: 2.8e-7 after 13 steps at 256^3,
+  1.4e-6 after 100 and 1.6e-5 after 500 steps at 128^3).
 """
 import numpy as np
 import pytest
@@ -42,8 +57,11 @@ def test_grf_dust_against_fp64(order, steps):
     b = evolve(st, steps, BoxConfig(order=order, precision="fp64"))
     errs = perturbation_errors(a.fields, b.fields, st.names)
     worst = max(errs, key=errs.get)
-    print("mixed vs fp64, worst field", worst, errs[worst])
-    assert errs[worst] < 1e-4, errs
+    D = b.field("D")
+    delta_err = float(np.abs(a.field("D") - D).max() / D.mean())
+    print("mixed vs fp64, worst field", worst, errs[worst], "density-contrast error / amplitude", delta_err / 1e-4)
+    assert delta_err <= 1e-6 * 1e-4  # 1e-6 of the density-contrast amplitude
+    assert errs[worst] < 1e-5, errs
 
 
 def test_hamiltonian_constraint_no_worse_than_twice_fp64():
@@ -63,7 +81,8 @@ def test_vacuum_mixed_runs_and_rejects_unsupported():
     a = evolve(st, 5, BoxConfig(order=4, precision="mixed"))
     b = evolve(st, 5, BoxConfig(order=4, precision="fp64"))
     errs = perturbation_errors(a.fields, b.fields, st.names)
-    assert max(errs.values()) < 1e-4
+    print("vacuum mixed vs fp64, worst", max(errs.values()))
+    assert max(errs.values()) < 1e-5
     with pytest.raises(RuntimeError, match="mixed"):
         evolve(ics.perturbed((16, 16, 16), S.DUST), 1, BoxConfig(order=4, precision="mixed", lapse="OnePlusLog"))
 
@@ -81,10 +100,13 @@ def test_grf_scalar_against_fp64(order, potential):
             res[prec] = (ev.download(0), ev.constraints(0))
     errs = perturbation_errors(res["mixed"][0].fields, res["fp64"][0].fields, st.names)
     worst = max(errs, key=errs.get)
-    print("scalar mixed vs fp64", order, potential, worst, errs[worst],
+    f = st.names.index("phi")
+    phi_err = float(np.abs(res["mixed"][0].fields[f] - res["fp64"][0].fields[f]).max()) / 1e-5
+    print("scalar mixed vs fp64", order, potential, worst, errs[worst], "phi error / fluctuation rms", phi_err,
           "H", res["mixed"][1]["H"][7], res["fp64"][1]["H"][7])
-    assert errs[worst] < 1e-4, errs
+    assert phi_err < 1e-6  # 1e-6 of the fluctuation amplitude
     assert res["mixed"][1]["H"][7] <= 2.0 * res["fp64"][1]["H"][7]
+    assert errs[worst] < 2e-5, errs
 
 
 def test_a_register_of_a_mixed_box():
@@ -126,9 +148,9 @@ def test_grf_dust_128_order8_500_steps():
     m64, mmx = res["fp64"][1]["M"][7], res["mixed"][1]["M"][7]
     print("128^3 o8 500 steps: worst field", worst, errs[worst], "density-contrast error", delta_err,
           "H L2", hmx, h64, "M L2", mmx, m64)
-    assert errs[worst] < 1e-4
-    assert delta_err < 1e-4 * 1e-4  # below 1e-4 of the density-contrast amplitude
+    assert delta_err <= 1e-6 * 1e-4  # 1e-6 of the density-contrast amplitude
     assert hmx <= 2.0 * h64 and mmx <= 2.0 * m64
+    assert errs[worst] < 5e-5, errs  # FP32 rounding over 2000 substeps (module docstring)
 
 
 
@@ -154,6 +176,6 @@ def test_grf_scalar_256_order8_200_steps():
     h64, hmx = res["fp64"][1]["H"][7], res["mixed"][1]["H"][7]
     print("256^3 scalar o8 200 steps: worst field", worst, errs[worst], "phi error / fluctuation rms", phi_err,
           "H L2", hmx, h64)
-    assert errs[worst] < 1e-4, errs
-    assert phi_err < 1e-6
+    assert phi_err < 1e-6  # 1e-6 of the fluctuation amplitude
     assert hmx <= 2.0 * h64
+    assert errs[worst] < 5e-5, errs  # FP32 rounding over 800 substeps (module docstring)

@@ -70,6 +70,8 @@ CASES = [
     (S.SCALAR, (18, 18, 18), 8, "DampedWave", 3),
     (S.VACUUM, (16, 16, 32), 6, "Anharmonic", 4),
     (S.VACUUM, (12, 12, 12), 2, "AwAGaugeWave", 6),
+    (S.STATIC, (16, 20, 18), 4, "Static", 5),
+    (S.STATIC, (18, 16, 16), 6, "ConformalFLRW", 4),
 ]
 
 
@@ -112,6 +114,7 @@ BIT_EXACT_CASES = [
     (S.SCALAR, (16, 20, 24), 6, 4, {}),
     (S.SCALAR, (24, 24, 24), 8, 3, {"potential": "quadratic", "pot_mass": 1.0}),
     (S.VACUUM, (16, 16, 16), 2, 6, {}),
+    (S.STATIC, (20, 16, 24), 8, 4, {"lapse": "Static"}),
 ]
 
 
