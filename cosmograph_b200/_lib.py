@@ -55,7 +55,7 @@ class BoxDesc(ctypes.Structure):
         ("dw_mu_l", ctypes.c_double), ("dw_p", ctypes.c_double),
         ("pot_const", ctypes.c_double), ("pot_mass", ctypes.c_double),
         ("frw_phi", ctypes.c_double), ("frw_K", ctypes.c_double),
-        ("nfluids", ctypes.c_int), ("reserved1", ctypes.c_int),
+        ("nfluids", ctypes.c_int), ("z4c", ctypes.c_int),
         ("fluid_rho", ctypes.c_double * 4), ("fluid_w", ctypes.c_double * 4),
     ]
 

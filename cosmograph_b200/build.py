@@ -34,6 +34,9 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *ARCH, f"-I{I
 UNITS = [
     ("stage_exact.o", "cg_stage_inst.cu", ["--fmad=false", "-DCG_VARIANT_NS=exact", "-DCG_REFERENCE_ORDER=1"]),
     ("stage_fast.o", "cg_stage_inst.cu", ["--fmad=true", "-DCG_VARIANT_NS=fast"]),
+    ("stage_exact_z4c.o", "cg_stage_inst.cu",
+     ["--fmad=false", "-DCG_VARIANT_NS=exact", "-DCG_REFERENCE_ORDER=1", "-DCG_Z4C_UNIT=1"]),
+    ("stage_fast_z4c.o", "cg_stage_inst.cu", ["--fmad=true", "-DCG_VARIANT_NS=fast", "-DCG_Z4C_UNIT=1"]),
     ("abi.o", "cg_abi.cu", []),
     ("noalloc.o", "cg_noalloc.cu", []),
     ("mixed.o", "cg_mixed_inst.cu", []),

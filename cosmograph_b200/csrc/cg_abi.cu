@@ -616,7 +616,12 @@ int validate(const cg_box_desc& d, std::string& why) {
     why = "unknown precision";
     return CG_ERR_INVALID;
   }
+  if (d.z4c != 0 && d.z4c != 1) { why = "z4c must be 0 or 1"; return CG_ERR_INVALID; }
   if (d.precision == CG_PREC_MIXED) {
+    if (d.z4c) {
+      why = "Z4c damping is available in the FP64 precisions only";
+      return CG_ERR_INVALID;
+    }
     if (d.matter == CG_MATTER_STATIC) {
       why = "the FP32-mixed form evolves vacuum, dust or scalar boxes";
       return CG_ERR_INVALID;
@@ -773,7 +778,8 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
     b.dev.ny = d.ny;
     b.dev.nz = d.nz;
     b.dev.pts = d.nx * d.ny * d.nz;
-    b.dev.nfields = cg_num_fields(d.matter);
+    b.dev.nfields = cg_num_fields(d.matter) + (d.z4c ? 1 : 0);
+    b.dev.z4c = d.z4c ? 1 : 0;
     b.dev.order = d.stencil_order;
     b.dev.matter = d.matter;
     cg::Physics& ph = b.dev.ph;
@@ -1278,13 +1284,13 @@ int ensure_groups(cg_ctx* ctx) {
     g.matter = ba.desc.matter;
     g.members.push_back((int)a);
     used[a] = true;
-    // boxes with Kreiss-Oliger dissipation and x-slabs keep their own launches
-    for (size_t b = a + 1; ba.desc.ko_coeff == 0.0 && ba.desc.x_ghost == 0 && b < ctx->boxes.size() &&
+    // boxes with Kreiss-Oliger dissipation or Z4c damping and x-slabs keep their own launches
+    for (size_t b = a + 1; ba.desc.ko_coeff == 0.0 && ba.desc.z4c == 0 && ba.desc.x_ghost == 0 && b < ctx->boxes.size() &&
                            g.members.size() < (size_t)cg::kMaxGroupBoxes;
          ++b) {
       const Box& bb = ctx->boxes[b];
       if (used[b] || bb.mixed != g.mixed || bb.variant != g.variant || bb.desc.stencil_order != g.order ||
-          bb.desc.matter != g.matter || bb.desc.ko_coeff != 0.0 || bb.desc.x_ghost != 0)
+          bb.desc.matter != g.matter || bb.desc.ko_coeff != 0.0 || bb.desc.z4c != 0 || bb.desc.x_ghost != 0)
         continue;
       g.members.push_back((int)b);
       used[b] = true;

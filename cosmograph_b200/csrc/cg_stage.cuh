@@ -102,25 +102,29 @@ enum : int {
 // Phase 1 writes no slot in [S_SRC, S_MAT): that region holds the field tile
 // and its row offsets until phase 2 starts.
 constexpr int kTileSlot = S_SRC, kTileSlots = S_MAT - S_SRC;
-template <int MATTER>
+// Z4C: Z4c damping (USE_Z4c_DAMPING): the first derivatives of theta in
+// three more slots after the matter slots
+template <int MATTER, bool Z4C = false>
 struct Slots {
-  static constexpr int value = S_MAT + (MATTER == kDust ? 4 : (MATTER == kScalar ? 15 : 0));
+  static constexpr int dth = S_MAT + (MATTER == kDust ? 4 : (MATTER == kScalar ? 15 : 0));
+  static constexpr int value = dth + (Z4C ? 3 : 0);
 };
 
 // What a launch of the point kernel does with the geometry it computes.
 enum Mode : int { kEvolve = 0, kConstraints = 1 };
 // constraint mode: d_d A_q after the matter slots (18)
-template <int MATTER>
+template <int MATTER, bool Z4C = false>
 struct SlotsC {
-  static constexpr int dA = Slots<MATTER>::value;
+  static constexpr int dA = Slots<MATTER, Z4C>::value;
   static constexpr int value = dA + 18;
 };
 // A second tile buffer after the slot array lets the TMA copy of the next
 // field overlap the derivatives of the current one.  Evolve mode, dust and
-// vacuum: two CTAs per SM still fit in shared memory.
-template <int O, int MATTER, int MODE>
+// vacuum: two CTAs per SM still fit in shared memory (with Z4c's three more
+// slots they would not: one buffer).
+template <int O, int MATTER, int MODE, bool Z4C = false>
 struct TileBuffers {
-  static constexpr bool kTwo = MODE == kEvolve && MATTER != kScalar;
+  static constexpr bool kTwo = MODE == kEvolve && MATTER != kScalar && !Z4C;
   // dust also stages the x and z boxes of its flux primitives here (5 arrays
   // each, flux_from_tiles)
   static constexpr size_t kTile = TileG<O>::SIZE * sizeof(double);
@@ -132,13 +136,14 @@ struct TileBuffers {
   static constexpr size_t kBytes = (kNeed + 127) / 128 * 128;
 };
 // dynamic shared memory of a substep launch
-template <int O, int MATTER, int MODE>
+template <int O, int MATTER, int MODE, bool Z4C = false>
 constexpr size_t stage_smem() {
-  return sizeof(double) * kThreads * (MODE == kConstraints ? SlotsC<MATTER>::value : Slots<MATTER>::value) +
-         (TileBuffers<O, MATTER, MODE>::kTwo ? TileBuffers<O, MATTER, MODE>::kBytes : 0);
+  return sizeof(double) * kThreads * (MODE == kConstraints ? SlotsC<MATTER, Z4C>::value : Slots<MATTER, Z4C>::value) +
+         (TileBuffers<O, MATTER, MODE, Z4C>::kTwo ? TileBuffers<O, MATTER, MODE, Z4C>::kBytes : 0);
 }
 // two CTAs per SM (228 KB, 1 KB reserved per CTA, up to 1 KB of static shared memory)
 static_assert(2 * (stage_smem<8, kDust, kEvolve>() + 2048) <= 228 * 1024, "two dust CTAs fit on an SM");
+static_assert(2 * (stage_smem<8, kScalar, kEvolve, true>() + 2048) <= 228 * 1024, "two Z4c CTAs fit on an SM");
 // per-block partial results of the constraint pass (see constraint_reduce)
 constexpr int kCPart = 27;
 
@@ -260,12 +265,14 @@ __device__ __forceinline__ double d1p(const double* __restrict__ fa, const doubl
 // Fields copied into tiles in phase 1, in order: (constraint mode) A_q with
 // first derivatives; the metric components, phi and alpha with first and
 // second derivatives; K and Gamma^i with first derivatives; (scalar) phi, Pi,
-// psi_i with first derivatives.
-template <int MATTER, int MODE>
+// psi_i with first derivatives.  With Z4c, theta (stored after the matter
+// fields) with first derivatives after Gamma^i.
+template <int MATTER, int MODE, bool Z4C = false>
 struct Phase1 {
   static constexpr int NA = MODE == kConstraints ? 6 : 0;
+  static constexpr int NZ = Z4C ? 1 : 0;
   static constexpr int NS = MATTER == kScalar ? 5 : 0;
-  static constexpr int N = NA + 8 + 4 + NS;
+  static constexpr int N = NA + 8 + 4 + NZ + NS;
   __device__ __forceinline__ static int field(int it) {
     if (it < NA) return F_A11 + it;
     it -= NA;
@@ -273,6 +280,8 @@ struct Phase1 {
     it -= 8;
     if (it < 4) return it == 0 ? F_K : F_GAM1 + it - 1;
     it -= 4;
+    if (it < NZ) return NF<MATTER>::value;  // theta
+    it -= NZ;
     return F_SPHI + it;
   }
 };
@@ -286,21 +295,21 @@ struct Phase1 {
 // box), else by the threads' own loads with periodic wrap.  Returns false (the
 // same value in every thread) when a TMA copy did not complete within
 // kTmaWaitCycles64; the status word then carries kStatusTileTimeout64.
-template <int O, int MATTER, int MODE>
+template <int O, int MATTER, int MODE, bool Z4C>
 __device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG<O>, double>& t, const Physics& ph,
                                                   const double gi[6], double* sl);
 
 //
 // bar[0] (and bar[1] with two buffers) are the buffers' mbarriers; bit b of
 // phase is the parity bar[b] completes next.
-template <int O, int MATTER, int MODE>
+template <int O, int MATTER, int MODE, bool Z4C = false>
 __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N, const Physics& ph, const double gi[6],
                                             double* sl, double* tl, double* tl2, const int* rowoff, int tid, int x0,
                                             int y0, int z0, int nz, int cc, const CUtensorMap* tmap, uint64_t* bar,
                                             unsigned& phase, unsigned* status) {
-  using PF = Phase1<MATTER, MODE>;
+  using PF = Phase1<MATTER, MODE, Z4C>;
   using G = TileG<O>;
-  constexpr bool TWO = TileBuffers<O, MATTER, MODE>::kTwo;
+  constexpr bool TWO = TileBuffers<O, MATTER, MODE, Z4C>::kTwo;
   constexpr unsigned kBytes = (unsigned)(G::SIZE * sizeof(double));
   // TMA: field it into buffer it % 2 (one buffer: 0), field it + 1 into L2
   auto issue = [&](int it) {
@@ -357,7 +366,7 @@ __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N,
       __syncthreads();
       if (it + 1 < PF::N) ld.fetch(a + (size_t)PF::field(it + 1) * N, rowoff);
     }
-    field_derivatives<O, MATTER, MODE>(it, tile::Taps<G, double>{b ? tl2 : tl, cc}, ph, gi, sl);
+    field_derivatives<O, MATTER, MODE, Z4C>(it, tile::Taps<G, double>{b ? tl2 : tl, cc}, ph, gi, sl);
   }
   if (by_tma) {
     ok = __syncthreads_and(ok);
@@ -367,17 +376,17 @@ __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N,
 }
 
 // the derivatives of phase-1 field `it` from its tile, into the slots
-template <int O, int MATTER, int MODE>
+template <int O, int MATTER, int MODE, bool Z4C>
 __device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG<O>, double>& t, const Physics& ph,
                                                   const double gi[6], double* sl) {
-  using PF = Phase1<MATTER, MODE>;
+  using PF = Phase1<MATTER, MODE, Z4C>;
   {
     if (it < PF::NA) {
       // d_d A_q for the momentum constraint (BSSN_MI, bssn_macros.h:498-500)
       const int q = it;
-      sl[(SlotsC<MATTER>::dA + 3 * q + 0) * kThreads] = d1<O>(t, 0, ph);
-      sl[(SlotsC<MATTER>::dA + 3 * q + 1) * kThreads] = d1<O>(t, 1, ph);
-      sl[(SlotsC<MATTER>::dA + 3 * q + 2) * kThreads] = d1<O>(t, 2, ph);
+      sl[(SlotsC<MATTER, Z4C>::dA + 3 * q + 0) * kThreads] = d1<O>(t, 0, ph);
+      sl[(SlotsC<MATTER, Z4C>::dA + 3 * q + 1) * kThreads] = d1<O>(t, 1, ph);
+      sl[(SlotsC<MATTER, Z4C>::dA + 3 * q + 2) * kThreads] = d1<O>(t, 2, ph);
     } else if (it < PF::NA + 8) {
       // calculate_dgamma / calculate_ddgamma / calculate_dalpha_dphi
       // (bssn.cc:480-521).  For g_q the second derivatives are contracted at
@@ -421,9 +430,15 @@ __device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG
       sl[(b + 0) * kThreads] = d1<O>(t, 0, ph);
       sl[(b + 1) * kThreads] = d1<O>(t, 1, ph);
       sl[(b + 2) * kThreads] = d1<O>(t, 2, ph);
+    } else if (Z4C && it == PF::NA + 12) {
+      // calculate_dtheta (bssn.cc:537-544)
+      constexpr int b = Slots<MATTER, Z4C>::dth;
+      sl[(b + 0) * kThreads] = d1<O>(t, 0, ph);
+      sl[(b + 1) * kThreads] = d1<O>(t, 1, ph);
+      sl[(b + 2) * kThreads] = d1<O>(t, 2, ph);
     } else {
       // Scalar::getScalarData derivatives (scalar.cc:109-127): d_d of phi, Pi, psi1..3
-      const int m = it - PF::NA - 12;
+      const int m = it - PF::NA - 12 - PF::NZ;
       sl[(S_MAT + 3 * m + 0) * kThreads] = d1<O>(t, 0, ph);
       sl[(S_MAT + 3 * m + 1) * kThreads] = d1<O>(t, 1, ph);
       sl[(S_MAT + 3 * m + 2) * kThreads] = d1<O>(t, 2, ph);
@@ -611,14 +626,19 @@ __device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part, int cta
 // The fused substep for the brick at brick coordinates (cx, cy, cz) of one
 // box; cta numbers the CTA's partial results in constraint mode.  KO: the
 // Kreiss-Oliger terms are compiled in (a separate instantiation, so that the
-// common case carries none of their code).
-template <int O, int MATTER, int MODE, bool KO = false>
+// common case carries none of their code).  Z4C: Z4c damping (the field theta
+// after the matter fields, bssn.cc:834-848 and the theta terms of ev_*; the
+// reference's USE_Z4c_DAMPING), also a separate instantiation.
+template <int O, int MATTER, int MODE, bool KO = false, bool Z4C = false>
 __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph, StageBg bg, const StagePtrs& P,
                                            int stage, int cx, int cy, int cz, int cta, const CUtensorMap* tmap,
                                            uint64_t* bar, unsigned& phase, bool& tma_ok,
                                            const FluxMaps* fmaps = nullptr) {
-  constexpr int NFLD = NF<MATTER>::value;
-  constexpr int NSLOT = MODE == kConstraints ? SlotsC<MATTER>::value : Slots<MATTER>::value;
+  constexpr int F_THETA = NF<MATTER>::value;
+  constexpr int NFLD = NF<MATTER>::value + (Z4C ? 1 : 0);
+  constexpr int NSLOT = MODE == kConstraints ? SlotsC<MATTER, Z4C>::value : Slots<MATTER, Z4C>::value;
+  // Z4c damping amplitudes (cosmo_macros.h:94-100)
+  constexpr double k1 = Z4C ? 0.5 : 0.0, k2 = Z4C ? 0.1 : 0.0;
   static_assert(NSLOT >= S_MAT, "the tile region lies inside the slot array");
   static_assert(TileG<O>::SIZE * sizeof(double) + TileG<O>::ROWS * sizeof(int) <=
                     (size_t)kTileSlots * kThreads * sizeof(double),
@@ -675,12 +695,12 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       __syncthreads();  // every warp reads every row offset
     }
     // after a copy timed out the CTA copies by threads (the barrier's phase is unknown)
-    double* tl2 = TileBuffers<O, MATTER, MODE>::kTwo ? smem + NSLOT * kThreads : nullptr;
-    tma_ok = derivatives<O, MATTER, MODE>(a, N, ph, gi, sl, tl, tl2, rowoff, tid, x0, y0, z0, geo.nz,
+    double* tl2 = TileBuffers<O, MATTER, MODE, Z4C>::kTwo ? smem + NSLOT * kThreads : nullptr;
+    tma_ok = derivatives<O, MATTER, MODE, Z4C>(a, N, ph, gi, sl, tl, tl2, rowoff, tid, x0, y0, z0, geo.nz,
                                           tile::centre<G>(threadIdx.z, threadIdx.y, threadIdx.x),
                                           by_tma ? tmap : nullptr, bar, phase, P.status) &&
              tma_ok;
-    if constexpr (MATTER == kDust && MODE == kEvolve && TileBuffers<O, MATTER, MODE>::kTwo) {
+    if constexpr (MATTER == kDust && MODE == kEvolve && TileBuffers<O, MATTER, MODE, Z4C>::kTwo) {
       flux_tiles = fmaps && by_tma && tma_ok;
       if (flux_tiles) {
         tma_ok = flux_from_tiles<O>(fmaps, tl, tl2, tid, x0, y0, z0, ph, sl, bar, phase, threadIdx.z, threadIdx.y,
@@ -710,6 +730,14 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   const double K = Kd + bg.K_FRW;
   const double alphad = C(F_ALPHA);
   const double alpha = alphad + 1.0;
+  // Z4c's theta and its derivatives (0 without Z4c, as the reference's
+  // zero-initialised BSSNData leaves them)
+  const double theta = Z4C ? C(F_THETA) : 0.0;
+  double dth[3] = {0.0, 0.0, 0.0};
+  if constexpr (Z4C) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) dth[d] = S(Slots<MATTER, Z4C>::dth + d);
+  }
   double gm[6];
   gm[0] = g[0] + 1.0; gm[1] = g[1]; gm[2] = g[2];
   gm[3] = g[3] + 1.0; gm[4] = g[4]; gm[5] = g[5] + 1.0;
@@ -996,15 +1024,15 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   const double AijAij = Ac[0] * A[0] + Ac[3] * A[3] + Ac[5] * A[5] + 2.0 * (Ac[1] * A[1] + Ac[2] * A[2] + Ac[4] * A[4]);
   const double r = S(S_SRC + Q_R) + bg.rho_FRW;
   // Hamiltonian constraint, bssn.cc:1073-1084 (theta = 0)
-  const double H = -e5phi / 8.0 * (ricci + 2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0)) - AijAij - 16.0 * kPi * r);
+  const double H = -e5phi / 8.0 * (ricci + 2.0 / 3.0 * ((K + 2.0 * theta) * (K + 2.0 * theta)) - AijAij - 16.0 * kPi * r);
 
   if constexpr (MODE == kConstraints) {
     // BSSN::setConstraintCalcs per point (bssn.cc:983-1006)
     double v[5], sc[5];
     v[0] = H;  // hamiltonianConstraintCalc / Scale, bssn.cc:1073-1100
     sc[0] = (e5phi / 8.0) * sqrt(ricci * ricci + AijAij * AijAij +
-                                          (2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0))) *
-                                              (2.0 / 3.0 * ((K + 2.0 * 0.0) * (K + 2.0 * 0.0))) +
+                                          (2.0 / 3.0 * ((K + 2.0 * theta) * (K + 2.0 * theta))) *
+                                              (2.0 / 3.0 * ((K + 2.0 * theta) * (K + 2.0 * theta))) +
                                           (16.0 * kPi * r) * (16.0 * kPi * r));
     {  // momentum, BSSN_MI / BSSN_MI_SCALE (bssn_macros.h:487-527)
       const double e6 = e6phi;
@@ -1024,7 +1052,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
         for (int X = 0; X < 3; ++X)
 #pragma unroll
           for (int d = 0; d < 3; ++d) {
-            const double u = gi[sym(X, d)] * S(SlotsC<MATTER>::dA + 3 * sym(X, I) + d);
+            const double u = gi[sym(X, d)] * S(SlotsC<MATTER, Z4C>::dA + 3 * sym(X, I) + d);
             tD = (X == 0 && d == 0) ? u : tD + u;
           }
         tD = tD - Gd[0] * A[sym(0, I)] - Gd[1] * A[sym(1, I)] - Gd[2] * A[sym(2, I)];
@@ -1033,8 +1061,8 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
 #pragma unroll
           for (int Y = 0; Y < 3; ++Y) tD = tD - GL(Y, sym(X, I)) * Ac[sym(Y, X)];
         const double sI = S(S_SRC + Q_S1 + I);
-        mv[I] = e6 * (-2.0 / 3.0 * S(S_DK + I) - 8 * kPi * (sI) - 2.0 / 3.0 * 2.0 * 0.0 + 6.0 * (t6) + (tD));
-        ms[I] = e6 * (fabs(2.0 / 3.0 * S(S_DK + I)) + fabs(8 * kPi * (sI)) + fabs(2.0 / 3.0 * 2.0 * 0.0) +
+        mv[I] = e6 * (-2.0 / 3.0 * S(S_DK + I) - 8 * kPi * (sI) - 2.0 / 3.0 * 2.0 * dth[I] + 6.0 * (t6) + (tD));
+        ms[I] = e6 * (fabs(2.0 / 3.0 * S(S_DK + I)) + fabs(8 * kPi * (sI)) + fabs(2.0 / 3.0 * 2.0 * dth[I]) +
                       6.0 * fabs(t6) + fabs(tD));
       }
       v[1] = sqrt(mv[0] * mv[0] + mv[1] * mv[1] + mv[2] * mv[2]);
@@ -1154,7 +1182,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
         }
       const double RTF = Ric(qq) - (1.0 / 3.0) * e4phi * gm[qq] * ricci;
       const double dtA = (em4phi * (alpha * (RTF - 8.0 * kPi * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
-                          alpha * (((K + 2.0 * 0.0) * A[qq]) - 2.0 * (aa)));
+                          alpha * (((K + 2.0 * theta) * A[qq]) - 2.0 * (aa)));
       finalize(F_A11 + qq, dtA - 1.0 * ph.a_adj_amp * dt * A[qq] * H - ko(F_A11 + qq));
     }
   // ev_GammaI (bssn.cc:762-764, BSSN_DT_GAMMAI_NOSHIFT bssn_macros.h:342-361)
@@ -1169,23 +1197,39 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
          2.0 * alpha *
              (+so -
               (1.0 / 3.0) * (2.0 * (gi[sym(I, 0)] * S(S_DK + 0) + gi[sym(I, 1)] * S(S_DK + 1) + gi[sym(I, 2)] * S(S_DK + 2)) +
-                             gi[sym(I, 0)] * 0.0 + gi[sym(I, 1)] * 0.0 + gi[sym(I, 2)] * 0.0) -
-              2.0 * alpha * 0.0 * (C(F_GAM1 + I) - Gd[I]) -
+                             gi[sym(I, 0)] * dth[0] + gi[sym(I, 1)] * dth[1] + gi[sym(I, 2)] * dth[2]) -
+              2.0 * alpha * k1 * (C(F_GAM1 + I) - Gd[I]) -
               8.0 * kPi * (gi[sym(I, 0)] * sq[0] + gi[sym(I, 1)] * sq[1] + gi[sym(I, 2)] * sq[2])));
     finalize(F_GAM1 + I, ns + 0.0 - ko(F_GAM1 + I));
   }
   // ev_DIFFK (bssn.cc:766-795)
   {
-    double v = (-DDaTR + alpha * (1.0 / 3.0 * (Kd + 2.0 * 0.0) * (Kd + 2.0 * 0.0 + 2.0 * bg.K_FRW) + AijAij) +
+    double v = (-DDaTR + alpha * (1.0 / 3.0 * (Kd + 2.0 * theta) * (Kd + 2.0 * theta + 2.0 * bg.K_FRW) + AijAij) +
                 4.0 * kPi * alpha * (S(S_SRC + Q_R) + S(S_SRC + Q_S)) + 4.0 * kPi * alphad * (bg.rho_FRW + bg.S_FRW));
     if (ph.k_damping_amp != 0.0) v = v - 1.0 * ph.k_damping_amp * H * em5phi;
+    if constexpr (Z4C) v = v + k1 * (1.0 - k2) * theta;
     finalize(F_K, v - ko(F_K));
   }
   // ev_DIFFphi (bssn.cc:797-820)
-  finalize(F_PHI, (0.1 * ph.a_adj_amp * dt * H - 1.0 / 6.0 * (alpha * (Kd + 2.0 * 0.0) + alphad * bg.K_FRW - (0.0 + 0.0 + 0.0))) -
+  finalize(F_PHI, (0.1 * ph.a_adj_amp * dt * H - 1.0 / 6.0 * (alpha * (Kd + 2.0 * theta) + alphad * bg.K_FRW - (0.0 + 0.0 + 0.0))) -
                       ko(F_PHI));
   // ev_DIFFalpha (bssn.cc:822-831)
   finalize(F_ALPHA, ev_lapse(ph, bg, alpha, K, Kd, phi) - ko(F_ALPHA));
+  if constexpr (Z4C) {
+    // ev_theta (bssn.cc:834-848)
+    double kth = 0.0;
+    if constexpr (KO) {
+      if (ko_on) {
+        const bool inside = x0 >= RKO && x0 + kBX + RKO <= geo.nx && y0 >= RKO && y0 + kBY + RKO <= geo.ny &&
+                            z0 >= RKO && z0 + kBZ + RKO <= geo.nz;
+        kth = ko_dissipation<O>(a + (size_t)F_THETA * N, i, j, k, geo.nx, geo.ny, geo.nz, inside, ph.ko_coeff, ph.dx);
+      }
+    }
+    finalize(F_THETA, (0.5 * alpha * (ricci + 2.0 / 3.0 * ((K + 2.0 * theta) * (K + 2.0 * theta)) - AijAij -
+                                      16.0 * kPi * (r)) -
+                       alpha * k1 * (2.0 + k2) * theta) -
+                          kth);
+  }
   if (MATTER == kDust) {
 #pragma unroll
     for (int m = 0; m < 4; ++m) finalize(F_D + m, rhs_m[m]);
@@ -1261,7 +1305,7 @@ __device__ __forceinline__ void init_tile_barriers(uint64_t* bar, bool use) {
 
 // One box: one CTA per brick.  tmap: the TMA map of this substep's input
 // (use_tma = 0: every tile is copied by the threads).
-template <int O, int MATTER, int MODE, bool KO = false>
+template <int O, int MATTER, int MODE, bool KO = false, bool Z4C = false>
 __global__ void __launch_bounds__(kThreads, 2)
 stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage, const __grid_constant__ CUtensorMap tmap,
              int use_tma, const __grid_constant__ FluxMaps fmaps, int use_fmaps) {
@@ -1269,7 +1313,7 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage, const 
   init_tile_barriers(bar, use_tma != 0);
   unsigned phase = 0;
   bool tma_ok = true;
-  stage_body<O, MATTER, MODE, KO>(geo, ph, bg, P, stage, blockIdx.z + geo.bx0, blockIdx.y, blockIdx.x,
+  stage_body<O, MATTER, MODE, KO, Z4C>(geo, ph, bg, P, stage, blockIdx.z + geo.bx0, blockIdx.y, blockIdx.x,
                                   blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
                                   use_tma ? &tmap : nullptr, bar, phase, tma_ok,
                                   use_tma && use_fmaps ? &fmaps : nullptr);

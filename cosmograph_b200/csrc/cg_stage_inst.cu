@@ -10,9 +10,19 @@
 #error "CG_VARIANT_NS must be defined (exact or fast)"
 #endif
 
+// Built a second time with -DCG_Z4C_UNIT=1: the Z4c-damping instantiations of
+// the substep and constraint kernels (launch_stage_z4c, launch_constraints_z4c)
+// in a translation unit of their own, so that the two compile in parallel.
+#ifndef CG_Z4C_UNIT
+#define CG_Z4C_UNIT 0
+#endif
+
 namespace cg {
 namespace CG_VARIANT_NS {
 
+constexpr bool kZ4cUnit = CG_Z4C_UNIT != 0;
+
+#if !CG_Z4C_UNIT
 // BSSN::stepInit (bssn.cc:219-226) on the device: the first substep's input
 // is the normalised copy of _p (RK4Register::stepInit + set_DIFFgamma_Aij_norm);
 // for dust also the flux primitives of that input (Dust::stepInit ->
@@ -62,6 +72,8 @@ __global__ void __launch_bounds__(128) init_kernel(BoxGeom geo, Physics ph, Stag
   }
 }
 
+#endif  // !CG_Z4C_UNIT
+
 namespace {
 dim3 block_dims() { return dim3(32, 4, 1); }
 dim3 grid_dims(const BoxDev& b) {
@@ -91,29 +103,31 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
   FluxMaps fm;
   const CUtensorMap* fsrc = (stage == 1 || stage == 3) ? b.fmap0 : b.fmap1;
   for (int a = 0; a < 3; ++a) fm.m[a] = fsrc[a];
-  constexpr size_t smem = stage_smem<O, M, kEvolve>();
+  constexpr bool Z = kZ4cUnit;
+  constexpr size_t smem = stage_smem<O, M, kEvolve, Z>();
   if constexpr (O == 2 || O == 8) {
     if (b.ph.ko_coeff != 0.0) {  // Kreiss-Oliger dissipation: its own instantiation
       static bool configured_ko = false;
       if (!configured_ko) {
-        cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M, kEvolve, true>,
+        cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M, kEvolve, true, Z>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         configured_ko = true;
       }
-      stage_kernel<O, M, kEvolve, true><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage, map,
-                                                                                    b.tma, fm, b.fmaps);
+      stage_kernel<O, M, kEvolve, true, Z><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage, map,
+                                                                                       b.tma, fm, b.fmaps);
       return cudaGetLastError();
     }
   }
   static bool configured = false;  // per instantiation
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M, kEvolve>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(stage_kernel<O, M, kEvolve, false, Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  stage_kernel<O, M, kEvolve><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage, map, b.tma,
-                                                                            fm, b.fmaps);
+  stage_kernel<O, M, kEvolve, false, Z><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, stage, map,
+                                                                                    b.tma, fm, b.fmaps);
   return cudaGetLastError();
 }
 
@@ -128,17 +142,18 @@ cudaError_t go_constraints(const BoxDev& b, const StageBg& bg, double* cvals, do
   P.cvals = cvals;
   P.cpart = cpart;
   BoxGeom geo{b.nx, b.ny, b.nz, b.pts, b.xg / kBX};
-  constexpr size_t smem = stage_smem<O, M, kConstraints>();
+  constexpr bool Z = kZ4cUnit;
+  constexpr size_t smem = stage_smem<O, M, kConstraints, Z>();
   static bool configured = false;
   if (!configured) {
-    cudaError_t e =
-        cudaFuncSetAttribute(stage_kernel<O, M, kConstraints>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M, kConstraints, false, Z>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
   FluxMaps fm{};
-  stage_kernel<O, M, kConstraints><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, 1, b.mapX, b.tma,
-                                                                                fm, 0);
+  stage_kernel<O, M, kConstraints, false, Z><<<stage_grid(b), stage_block(), smem, st>>>(geo, b.ph, bg, P, 1, b.mapX,
+                                                                                         b.tma, fm, 0);
   return cudaGetLastError();
 }
 
@@ -152,6 +167,7 @@ cudaError_t go_constraints_m(const BoxDev& b, const StageBg& bg, double* cvals, 
   }
 }
 
+#if !CG_Z4C_UNIT
 template <int O, int M>
 cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, cudaStream_t st) {
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
@@ -197,6 +213,8 @@ int ctas_m(int matter) {
   }
 }
 
+#endif  // !CG_Z4C_UNIT
+
 template <int O>
 cudaError_t go_stage_m(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
   switch (b.matter) {
@@ -206,6 +224,7 @@ cudaError_t go_stage_m(const BoxDev& b, const StageBg& bg, int stage, cudaStream
     default: return go_stage<O, kVacuum>(b, bg, stage, st);
   }
 }
+#if !CG_Z4C_UNIT
 template <int O>
 bool encode_maps(BoxDev& b) {
   using G = TileG<O>;
@@ -227,8 +246,10 @@ bool encode_maps(BoxDev& b) {
   }
   return true;
 }
+#endif  // !CG_Z4C_UNIT
 }  // namespace
 
+#if !CG_Z4C_UNIT
 void make_tile_maps(BoxDev& b) {
   bool ok = false;
   switch (b.order) {
@@ -241,7 +262,14 @@ void make_tile_maps(BoxDev& b) {
   b.maps = b.tma = ok ? 1 : 0;
 }
 
+#endif  // !CG_Z4C_UNIT
+
+#if CG_Z4C_UNIT
+cudaError_t launch_stage_z4c(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
+#else
 cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
+  if (b.z4c) return launch_stage_z4c(b, bg, stage, st);
+#endif
   switch (b.order) {
     case 2: return go_stage_m<2>(b, bg, stage, st);
     case 4: return go_stage_m<4>(b, bg, stage, st);
@@ -251,7 +279,12 @@ cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStre
   }
 }
 
+#if CG_Z4C_UNIT
+cudaError_t launch_constraints_z4c(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st) {
+#else
 cudaError_t launch_constraints(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st) {
+  if (b.z4c) return launch_constraints_z4c(b, bg, cvals, cpart, st);
+#endif
   switch (b.order) {
     case 2: return go_constraints_m<2>(b, bg, cvals, cpart, st);
     case 4: return go_constraints_m<4>(b, bg, cvals, cpart, st);
@@ -261,6 +294,7 @@ cudaError_t launch_constraints(const BoxDev& b, const StageBg& bg, double* cvals
   }
 }
 
+#if !CG_Z4C_UNIT
 cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
                          cudaStream_t st) {
   switch (order) {
@@ -294,8 +328,16 @@ cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st) {
     case kStaticMatter: init_kernel<kStaticMatter><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
     default: init_kernel<kVacuum><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
   }
+  if (b.z4c) {  // theta: not normalised, copied as it is
+    const size_t pts = (size_t)b.pts;
+    cudaError_t e = cudaMemcpyAsync(b.X + (size_t)(b.nfields - 1) * pts, b.P + (size_t)(b.nfields - 1) * pts,
+                                    pts * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
   return cudaGetLastError();
 }
+
+#endif  // !CG_Z4C_UNIT
 
 }  // namespace CG_VARIANT_NS
 }  // namespace cg

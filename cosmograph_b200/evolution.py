@@ -50,6 +50,7 @@ def make_desc(state: BoxState, cfg: BoxConfig) -> _lib.BoxDesc:
     d.gd_c, d.dw_mu_l, d.dw_p = cfg.gd_c, cfg.dw_mu_l, cfg.dw_p
     d.pot_const, d.pot_mass = cfg.pot_const, cfg.pot_mass
     d.x_ghost = cfg.x_ghost
+    d.z4c = 1 if state.z4c else 0
     d.frw_phi, d.frw_K = state.frw_phi, state.frw_K
     d.nfluids = len(state.fluids)
     for n, (rho, w) in enumerate(state.fluids):

@@ -208,6 +208,8 @@ BSSN::BSSN(ConfigParser* config) {
   d.lapse = lapse_code(c("lapse", "Static"));
   if (c("shift", "Static") != "Static") raise(-1, "non-zero shift is not on this path");
   d.normalize_metric = std::stoi(c("normalize_metric", "1"));
+  // the reference's compile-time USE_Z4c_DAMPING (cosmo_macros.h:91-100) as a config key
+  d.z4c = std::stoi(c("Z4c_damping", "0")) != 0 ? 1 : 0;
   d.ko_coeff = std::stod(c("KO_damping_coefficient", "0.0"));
   d.a_adj_amp = std::stod(c("a_adj_amp", "0.0"));
   d.k_damping_amp = std::stod(c("k_damping_amp", "0.0"));
@@ -236,9 +238,9 @@ BSSN::~BSSN() {
 void BSSN::ensure_fields() {
   regs.clear();
   fields.clear();
-  const int nf = cg_num_fields(d.matter);
+  const int nf = cg_num_fields(d.matter) + d.z4c;
   for (int f = 0; f < nf; ++f) {
-    const std::string nm = cg_field_name(d.matter, f);
+    const std::string nm = f < cg_num_fields(d.matter) ? cg_field_name(d.matter, f) : "theta";
     regs.push_back(std::make_unique<RK4Register>(this, f, nm));
     RK4Register* r = regs.back().get();
     fields[nm + "_p"] = &r->_array_p;
@@ -256,6 +258,7 @@ RK4Register* BSSN::reg(const std::string& name) {
 int BSSN::field_index(const std::string& name) const {
   for (int f = 0; f < cg_num_fields(d.matter); ++f)
     if (name == cg_field_name(d.matter, f)) return f;
+  if (d.z4c && name == "theta") return cg_num_fields(d.matter);
   raise(-1, "no field `" + name + "` in this box");
 }
 
@@ -348,7 +351,10 @@ void BSSN::loadState(const std::string& path) {
   if (h.matter != d.matter)
     raise(-1, path + " holds matter model " + std::to_string(h.matter) + ", the simulation_type needs " +
                   std::to_string(d.matter));
-  if (h.nfields != cg_num_fields(h.matter) || h.nfluids < 0 || h.nfluids > 4 || h.nx <= 0 || h.ny <= 0 || h.nz <= 0)
+  const int z4c = (h.reserved & 1) ? 1 : 0;  // the header's flags: theta after the matter fields
+  if (z4c != d.z4c) raise(-1, path + (z4c ? " carries theta; set Z4c_damping = 1" : " carries no theta (Z4c_damping = 1)"));
+  if (h.nfields != cg_num_fields(h.matter) + z4c || h.nfluids < 0 || h.nfluids > 4 || h.nx <= 0 || h.ny <= 0 ||
+      h.nz <= 0)
     raise(-1, path + ": inconsistent header");
   if (c) raise(-1, "initial data must be loaded before the box is on the GPU");
   d.nx = h.nx;
@@ -379,6 +385,7 @@ void BSSN::saveState(const std::string& path, int step) {
   h.nz = d.nz;
   h.nfields = num_fields();
   h.matter = d.matter;
+  h.reserved = d.z4c ? 1 : 0;  // flags: theta after the matter fields
   h.step = step;
   h.dx = d.dx;
   h.dt = d.dt;

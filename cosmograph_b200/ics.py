@@ -125,9 +125,9 @@ def gaussian_random_field(shape, seed: int, spectrum, rms: float) -> np.ndarray:
     return field * (rms / s) if s > 0 else field
 
 
-def _empty(shape, matter, dx, dt, **kw) -> BoxState:
-    return BoxState(fields=np.zeros((len(field_names(matter)),) + tuple(shape)), matter=matter,
-                    dx=dx, dt=dt, **kw)
+def _empty(shape, matter, dx, dt, z4c: bool = False, **kw) -> BoxState:
+    return BoxState(fields=np.zeros((len(field_names(matter, z4c)),) + tuple(shape)), matter=matter,
+                    dx=dx, dt=dt, z4c=z4c, **kw)
 
 
 # ---------------------------------------------------------------------------
@@ -255,15 +255,15 @@ def grf_scalar(n, seed: int = 9, phi0: float = 1.0e-2, rms: float = 1.0e-5, mass
 
 
 def perturbed(shape, matter: int, seed: int = 1, amp: float = 1.0e-2, modes: int = 3,
-              box_len: float = 1.0, dt_frac: float = 0.1) -> BoxState:
+              box_len: float = 1.0, dt_frac: float = 0.1, z4c: bool = False) -> BoxState:
     """Every field = background + amp * (a few random smooth periodic modes,
     each a product of one sine per axis).  Backgrounds: DIFFK = -3,
     D = 3/(8 pi), alpha = 1 (DIFFalpha = 0), scalar phi = 0.1; everything
-    else 0.  Not a solution of the constraints: it exercises every term of the
-    right-hand side."""
+    else 0 (with z4c, theta too).  Not a solution of the constraints: it
+    exercises every term of the right-hand side."""
     shape = tuple(shape)
     dx = box_len / shape[0]
-    st = _empty(shape, matter, dx, default_dt(dx, dt_frac))
+    st = _empty(shape, matter, dx, default_dt(dx, dt_frac), z4c=z4c)
     rng = np.random.Generator(np.random.MT19937(seed))
     x = [np.arange(m, dtype=np.float64) / m for m in shape]
     for f, name in enumerate(st.names):

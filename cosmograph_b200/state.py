@@ -36,24 +36,29 @@ BSSN_FIELDS = (
 DUST_FIELDS = ("D", "S1", "S2", "S3")
 SCALAR_FIELDS = ("phi", "Pi", "psi1", "psi2", "psi3")
 STATIC_FIELDS = ("DIFFD",)  # the static sims' fixed density (components/static/static.h:17), not evolved
+# Z4c damping (USE_Z4c_DAMPING, cosmo_macros.h:91-100): the constraint field
+# theta (Z4c_APPLY_TO_FIELDS, bssn_macros.h:8-13), stored after the matter fields
+Z4C_FIELDS = ("theta",)
+FLAG_Z4C = 1  # header flags bit: the box carries theta
 
 # header layout (168 bytes); mirrors oracle/cg_state.h
 _HDR = struct.Struct("<8s8i4d4d4dd3d")
 assert _HDR.size == 168
 
 
-def field_names(matter: int) -> tuple[str, ...]:
+def field_names(matter: int, z4c: bool = False) -> tuple[str, ...]:
+    extra = Z4C_FIELDS if z4c else ()
     if matter == DUST:
-        return BSSN_FIELDS + DUST_FIELDS
+        return BSSN_FIELDS + DUST_FIELDS + extra
     if matter == SCALAR:
-        return BSSN_FIELDS + SCALAR_FIELDS
+        return BSSN_FIELDS + SCALAR_FIELDS + extra
     if matter == STATIC:
-        return BSSN_FIELDS + STATIC_FIELDS
-    return BSSN_FIELDS
+        return BSSN_FIELDS + STATIC_FIELDS + extra
+    return BSSN_FIELDS + extra
 
 
-def num_fields(matter: int) -> int:
-    return len(field_names(matter))
+def num_fields(matter: int, z4c: bool = False) -> int:
+    return len(field_names(matter, z4c))
 
 
 @dataclasses.dataclass
@@ -69,6 +74,7 @@ class BoxState:
     frw_K: float = 0.0
     fluids: tuple[tuple[float, float], ...] = ()   # (rho, w) pairs
     lam: float = 0.0                   # rho_Lambda (Lambda::setLambda)
+    z4c: bool = False                  # Z4c damping: theta is the last field
 
     @property
     def shape(self) -> tuple[int, int, int]:
@@ -76,7 +82,7 @@ class BoxState:
 
     @property
     def names(self) -> tuple[str, ...]:
-        return field_names(self.matter)
+        return field_names(self.matter, self.z4c)
 
     def field(self, name: str) -> np.ndarray:
         return self.fields[self.names.index(name)]
@@ -91,12 +97,12 @@ class BoxState:
         rho = [f[0] for f in self.fluids] + [0.0] * (MAX_FLUIDS - len(self.fluids))
         w = [f[1] for f in self.fluids] + [0.0] * (MAX_FLUIDS - len(self.fluids))
         return _HDR.pack(MAGIC, nx, ny, nz, self.fields.shape[0], self.matter,
-                         self.step, len(self.fluids), 0, self.dx, self.dt,
+                         self.step, len(self.fluids), FLAG_Z4C if self.z4c else 0, self.dx, self.dt,
                          self.frw_phi, self.frw_K, *rho, *w, self.lam, 0.0, 0.0, 0.0)
 
     def save(self, path: str | Path) -> None:
         f = np.ascontiguousarray(self.fields, dtype="<f8")
-        if f.shape[0] != num_fields(self.matter):
+        if f.shape[0] != num_fields(self.matter, self.z4c):
             raise ValueError("field count does not match the matter model")
         with open(path, "wb") as fh:
             fh.write(self.header_bytes())
@@ -110,10 +116,11 @@ def load(path: str | Path) -> BoxState:
     h = _HDR.unpack_from(raw, 0)
     if h[0] != MAGIC:
         raise ValueError(f"{path}: not a state file")
-    nx, ny, nz, nf, matter, step, nfl = h[1:8]
+    nx, ny, nz, nf, matter, step, nfl, flags = h[1:9]
+    z4c = bool(flags & FLAG_Z4C)
     dx, dt, phi, K = h[9:13]
     rho, w, lam = h[13:17], h[17:21], h[21]
-    if nf != num_fields(matter) or not 0 <= nfl <= MAX_FLUIDS:
+    if nf != num_fields(matter, z4c) or not 0 <= nfl <= MAX_FLUIDS:
         raise ValueError(f"{path}: inconsistent header")
     n = nf * nx * ny * nz
     if len(raw) != _HDR.size + 8 * n:
@@ -121,4 +128,4 @@ def load(path: str | Path) -> BoxState:
     fields = np.frombuffer(raw, dtype="<f8", count=n, offset=_HDR.size)
     return BoxState(fields=fields.reshape(nf, nx, ny, nz).astype(np.float64),
                     matter=matter, dx=dx, dt=dt, step=step, frw_phi=phi, frw_K=K,
-                    fluids=tuple((rho[i], w[i]) for i in range(nfl)), lam=lam)
+                    fluids=tuple((rho[i], w[i]) for i in range(nfl)), lam=lam, z4c=z4c)

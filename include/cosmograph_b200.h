@@ -115,7 +115,11 @@ typedef struct {
   double pot_mass;         /* m for CG_POT_QUADRATIC                              */
   double frw_phi, frw_K;   /* FRW reference background (utils/FRW.h:15-16)         */
   int nfluids;             /* FRW fluids (FRW::addFluid, utils/FRW.h:60-76), <= 4  */
-  int reserved1;
+  int z4c;                 /* 1: Z4c damping (the reference's USE_Z4c_DAMPING,
+                              cosmo_macros.h:91-100, damping amplitudes 0.5 and
+                              0.1): the constraint field theta is evolved and
+                              stored after the matter fields (cg_num_fields + 1
+                              fields); FP64 precisions only                    */
   double fluid_rho[4], fluid_w[4];
 } cg_box_desc;
 

@@ -48,6 +48,7 @@ class CgoParams(ctypes.Structure):
         ("frw_phi", ctypes.c_double), ("frw_K", ctypes.c_double),
         ("nfluids", ctypes.c_int),
         ("fluid_rho", ctypes.c_double * 4), ("fluid_w", ctypes.c_double * 4),
+        ("z4c", ctypes.c_int),
     ]
 
 
@@ -111,6 +112,7 @@ def make_params(state, order: int, lapse: str = "Harmonic", normalize_metric: in
     p.nfluids = len(state.fluids)
     for i, (rho, w) in enumerate(state.fluids):
         p.fluid_rho[i], p.fluid_w[i] = rho, w
+    p.z4c = 1 if getattr(state, "z4c", False) else 0
     return p
 
 

@@ -13,6 +13,8 @@ Flavours:
                                             no reassociation)
   strict_cr : strict, with the C library's exp, expm1 and log1p replaced by
            correctly rounded ones (cr_libm.c) at link time
+  strict_z4c, strict_cr_z4c : the same with Z4c damping compiled in
+           (-DUSE_Z4c_DAMPING=1, cosmo_macros.h:91-100)
   fast   : -O3 -ffast-math -march=x86-64-v3 (the reference's own optimisation
            flags, cmake/optimization.cmake:18, with a portable -march so the
            binary also runs on the GPU machine's host CPU; CPU-baseline timing)
@@ -48,6 +50,8 @@ REF_SOURCES = [
 FLAVOURS = {
     "strict": ["-O2", "-ffp-contract=off"],
     "strict_cr": ["-O2", "-ffp-contract=off"],
+    "strict_z4c": ["-O2", "-ffp-contract=off", "-DUSE_Z4c_DAMPING=1"],
+    "strict_cr_z4c": ["-O2", "-ffp-contract=off", "-DUSE_Z4c_DAMPING=1"],
     "fast": ["-O3", "-ffast-math", "-march=x86-64-v3"],
 }
 # strict_cr: the strict build linked with correctly rounded exp, expm1 and
@@ -98,7 +102,7 @@ def build(nx: int, ny: int, nz: int, order: int, flavour: str = "strict",
         with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
             list(ex.map(cc, zip(srcs, objs)))
         libs = ["-lz"]
-        if flavour == "strict_cr":
+        if flavour.startswith("strict_cr"):
             crobj = Path(tmp) / "cr_libm.o"
             subprocess.run(["gcc", "-std=gnu11", "-O2", "-ffp-contract=off", f"-I{HERE}", "-c",
                             str(HERE / "cr_libm.c"), "-o", str(crobj)], check=True)

@@ -31,6 +31,7 @@ void cgo_set_threads(int n) {
 #endif
 }
 
+/* with Z4c damping, theta follows these (its index is cgo_num_fields) */
 int cgo_num_fields(int matter) {
   return matter == CGO_DUST ? 22 : matter == CGO_SCALAR ? 23 : matter == CGO_STATIC ? 19 : 18;
 }
@@ -211,6 +212,7 @@ typedef struct {
   double DDphi[6], DDaTF[6], DDaTR;
   double Uricci[6], ricci_t[6], ricci, ricciTF[6];
   double H;
+  double theta, dtheta[3]; /* Z4c: theta and its first derivatives (0 without Z4c) */
 } bd_t;
 
 /* BSSN::set_bd_values, bssn.cc:361-421, on the "_a" register and sources */
@@ -225,6 +227,10 @@ static void set_bd(const sim_t *s, long i, long j, long k, bd_t *bd) {
   for (int q = 0; q < 3; ++q) bd->Gam[q] = a[(F_GAM1 + q) * N + idx];
   bd->alphad = a[F_ALPHA * N + idx];
   for (int q = 0; q < Q_N; ++q) bd->src[q] = s->src[q * N + idx];
+  /* Z4c: set_local_vals and calculate_dtheta (bssn.cc:430-435, 537-544) */
+  const long fth = cgo_num_fields(s->p->matter);
+  bd->theta = s->p->z4c ? a[fth * N + idx] : 0.0;
+  for (int q = 0; q < 3; ++q) bd->dtheta[q] = s->p->z4c ? deriv(s, i, j, k, q + 1, a + fth * N) : 0.0;
 
   /* set_gammai_values, bssn.cc:447-455 */
   const double *g = bd->g;
@@ -383,8 +389,8 @@ static void set_bd(const sim_t *s, long i, long j, long k, bd_t *bd) {
   for (int q = 0; q < 6; ++q)
     bd->ricciTF[q] = R[q] - (1.0 / 3.0) * exp(4.0 * bd->phi) * bd->gamma[q] * bd->ricci;
 
-  /* hamiltonianConstraintCalc, bssn.cc:1073-1084 (theta = 0) */
-  const double theta = 0.0;
+  /* hamiltonianConstraintCalc, bssn.cc:1073-1084 */
+  const double theta = bd->theta;
   bd->H = -exp(5.0 * bd->phi) / 8.0 *
           (bd->ricci + 2.0 / 3.0 * PW2(bd->K + 2.0 * theta) - bd->AijAij - 16.0 * CG_PI * bd->r);
 }
@@ -409,13 +415,18 @@ static double ev_lapse(const sim_t *s, const bd_t *bd) {
   }
 }
 
-/* The BSSN_RK_EVOLVE_PT evolution functions, bssn.cc:748-831 and
- * bssn_macros.h:292-385 (no shift, no Z4c). */
+/* Z4c damping amplitudes (cosmo_macros.h:94-100): 0.5 and 0.1 with Z4c, else 0 */
+static double z4c_k1(const sim_t *s) { return s->p->z4c ? 0.5 : 0.0; }
+static double z4c_k2(const sim_t *s) { return s->p->z4c ? 0.1 : 0.0; }
+
+/* The BSSN_RK_EVOLVE_PT evolution functions, bssn.cc:748-848 and
+ * bssn_macros.h:292-385 (no shift); with Z4c also ev_theta (bssn.cc:834-848),
+ * written to out[cgo_num_fields(matter)]. */
 static void bssn_rhs(const sim_t *s, long i, long j, long k, const bd_t *bd, double *out) {
   const cgo_params *p = s->p;
   const long N = s->pts;
   const double *a = s->reg_a;
-  const double dt = p->dt, theta = 0.0;
+  const double dt = p->dt, theta = bd->theta, k1 = z4c_k1(s), k2 = z4c_k2(s);
   const double *gi = bd->gi, *A = bd->A;
   /* ev_DIFFgammaIJ, bssn.cc:748-753 */
   for (int q = 0; q < 6; ++q)
@@ -447,8 +458,9 @@ static void bssn_rhs(const sim_t *s, long i, long j, long k, const bd_t *bd, dou
          2.0 * bd->alpha *
              (+so -
               (1.0 / 3.0) * (2.0 * (gi[SYM[I][0]] * bd->dK[0] + gi[SYM[I][1]] * bd->dK[1] + gi[SYM[I][2]] * bd->dK[2]) +
-                             gi[SYM[I][0]] * 0.0 + gi[SYM[I][1]] * 0.0 + gi[SYM[I][2]] * 0.0) -
-              2.0 * bd->alpha * 0.0 * (bd->Gam[I] - bd->Gammad[I]) -
+                             gi[SYM[I][0]] * bd->dtheta[0] + gi[SYM[I][1]] * bd->dtheta[1] +
+                             gi[SYM[I][2]] * bd->dtheta[2]) -
+              2.0 * bd->alpha * k1 * (bd->Gam[I] - bd->Gammad[I]) -
               8.0 * CG_PI *
                   (gi[SYM[I][0]] * bd->src[Q_S1] + gi[SYM[I][1]] * bd->src[Q_S2] + gi[SYM[I][2]] * bd->src[Q_S3])));
     out[F_GAM1 + I] = (ns + 0.0) - ko_diss(s, i, j, k, a + (F_GAM1 + I) * N);
@@ -458,7 +470,7 @@ static void bssn_rhs(const sim_t *s, long i, long j, long k, const bd_t *bd, dou
               bd->alpha * (1.0 / 3.0 * (bd->Kd + 2.0 * theta) * (bd->Kd + 2.0 * theta + 2.0 * s->get_K) + bd->AijAij) +
               4.0 * CG_PI * bd->alpha * (bd->src[Q_R] + bd->src[Q_S]) +
               4.0 * CG_PI * bd->alphad * (s->get_rho + s->get_S) -
-              1.0 * p->k_damping_amp * bd->H * exp(-5.0 * bd->phi) + 0.0 * (1.0 - 0.0) * theta -
+              1.0 * p->k_damping_amp * bd->H * exp(-5.0 * bd->phi) + k1 * (1.0 - k2) * theta -
               ko_diss(s, i, j, k, a + F_K * N));
   /* ev_DIFFphi, bssn.cc:797-820 */
   out[F_PHI] = (0.1 * p->a_adj_amp * dt * bd->H -
@@ -466,6 +478,13 @@ static void bssn_rhs(const sim_t *s, long i, long j, long k, const bd_t *bd, dou
                 ko_diss(s, i, j, k, a + F_PHI * N));
   /* ev_DIFFalpha, bssn.cc:822-831 */
   out[F_ALPHA] = ev_lapse(s, bd) - ko_diss(s, i, j, k, a + F_ALPHA * N);
+  if (p->z4c) {
+    /* ev_theta, bssn.cc:834-848 */
+    const long fth = cgo_num_fields(p->matter);
+    out[fth] = (0.5 * bd->alpha * (bd->ricci + 2.0 / 3.0 * PW2(bd->K + 2.0 * bd->theta) - bd->AijAij - 16.0 * CG_PI * (bd->r)) -
+                bd->alpha * k1 * (2.0 + k2) * bd->theta) -
+               ko_diss(s, i, j, k, a + fth * N);
+  }
 }
 
 /* ------------------------------------------------------------------ */
@@ -832,7 +851,7 @@ static int sim_init(sim_t *s, const cgo_params *p) {
   s->ny = p->ny;
   s->nz = p->nz;
   s->pts = s->nx * s->ny * s->nz;
-  s->nf = cgo_num_fields(p->matter);
+  s->nf = cgo_num_fields(p->matter) + (p->z4c ? 1 : 0);
   const size_t n = (size_t)s->nf * s->pts;
   s->reg_p = (double *)calloc(n, sizeof(double));
   s->reg_a = (double *)calloc(n, sizeof(double));
@@ -867,7 +886,7 @@ static void evolve_substep(sim_t *s) {
   for (ii = 0; ii < s->nx; ++ii) {
     bd_t bd;
     sd_t sd;
-    double out[23];
+    double out[24];
     for (long j = 0; j < s->ny; ++j)
       for (long k = 0; k < s->nz; ++k) {
         const long idx = IDX(s, ii, j, k);
@@ -883,6 +902,7 @@ static void evolve_substep(sim_t *s) {
           nf = 19;
         }
         for (int f = 0; f < nf; ++f) s->reg_c[f * N + idx] = out[f];
+        if (s->p->z4c) s->reg_c[(long)(s->nf - 1) * N + idx] = out[s->nf - 1];
       }
   }
   if (s->p->matter == CGO_DUST) dust_rkevolve(s);
@@ -1015,7 +1035,7 @@ static void momentum(const sim_t *s, long i, long j, long k, const bd_t *bd, int
   tD = tD - bd->Gammad[0] * A[SYM[0][I]] - bd->Gammad[1] * A[SYM[1][I]] - bd->Gammad[2] * A[SYM[2][I]];
   for (int X = 0; X < 3; ++X)
     for (int Y = 0; Y < 3; ++Y) tD = tD - bd->GL[Y][SYM[X][I]] * bd->Acont[SYM[Y][X]];
-  const double theta_d = 0.0;
+  const double theta_d = bd->dtheta[I];
   *val = e6 * (-2.0 / 3.0 * bd->dK[I] - 8 * CG_PI * (bd->src[Q_S1 + I]) - 2.0 / 3.0 * 2.0 * theta_d + 6.0 * (t6) + (tD));
   *scale = e6 * (fabs(2.0 / 3.0 * bd->dK[I]) + fabs(8 * CG_PI * (bd->src[Q_S1 + I])) +
                  fabs(2.0 / 3.0 * 2.0 * theta_d) + 6.0 * fabs(t6) + fabs(tD));

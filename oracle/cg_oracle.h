@@ -61,6 +61,8 @@ typedef struct {
   double frw_phi, frw_K;
   int nfluids;
   double fluid_rho[CGO_MAX_FLUIDS], fluid_w[CGO_MAX_FLUIDS];
+  int z4c;              /* USE_Z4c_DAMPING (cosmo_macros.h:91-100): the field theta
+                           after the matter fields, damping amplitudes 0.5, 0.1 */
 } cgo_params;
 
 /* Number of fields of a matter model: 18, 22, 23, or 19 (static: the 18

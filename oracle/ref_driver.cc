@@ -15,6 +15,8 @@
  *            the fixed density DIFFD (Static, components/static/static.cc)
  *            read from and written back as field 18
  * minus output, NaN checks and ray sheets, which never touch the fields.
+ * Built with -DUSE_Z4c_DAMPING=1 (build_ref.py flavours *_z4c) the driver
+ * reads and writes theta as the last field.
  *
  * Usage: cg_ref_<...> <mode> <config.txt> <state_in> <out> [steps]
  *   mode = evolve      : run <steps> RK4 steps, write the "_p" registers to <out>
@@ -100,6 +102,9 @@ struct Sim {
     } else if (matter == CG_STATE_STATIC) {
       out.push_back(stat->fields["DIFFD_a"]);  // not a register: the same array for every role
     }
+#if USE_Z4c_DAMPING
+    out.push_back(bssn->fields[std::string("theta_") + r]);  // stored after the matter fields
+#endif
     return out;
   }
 
@@ -197,6 +202,8 @@ int main(int argc, char **argv) {
   if (fread(&h, sizeof(h), 1, fin) != 1) die("short header");
   if (memcmp(h.magic, CG_STATE_MAGIC, 8) != 0) die("bad magic");
   if (h.nx != NX || h.ny != NY || h.nz != NZ) die("grid size differs from the compiled N");
+  if (((h.flags & CG_STATE_Z4C) != 0) != (USE_Z4c_DAMPING != 0))
+    die("the state's Z4c flag differs from the build's USE_Z4c_DAMPING");
   const long pts = (long)NX * NY * NZ;
   std::vector<double> buf((size_t)h.nfields * pts);
   if (fread(buf.data(), sizeof(double), buf.size(), fin) != buf.size()) die("short data");

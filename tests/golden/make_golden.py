@@ -40,6 +40,11 @@ CASES = [
     ("grf_dust_o4", S.DUST, (8, 8, 8), 4, 9, 0.0, "evolve", 5, {"lapse": "Harmonic"}),
     ("static_o4", S.STATIC, (10, 8, 12), 4, 15, 2e-2, "evolve", 4, {"lapse": "Static"}),
     ("static_o8", S.STATIC, (12, 10, 9), 8, 16, 2e-2, "evolve", 3, {"lapse": "ConformalFLRW"}),
+    # Z4c damping: the reference built with USE_Z4c_DAMPING (flavour strict_z4c)
+    ("dust_z4c_o4", S.DUST, (10, 8, 12), 4, 17, 2e-2, "evolve", 4, {"lapse": "Harmonic"}),
+    ("scalar_z4c_o8", S.SCALAR, (9, 10, 8), 8, 18, 2e-2, "evolve", 3, {"lapse": "Harmonic"}),
+    ("vacuum_z4c_o2", S.VACUUM, (8, 8, 10), 2, 19, 3e-2, "evolve", 4,
+     {"lapse": "OnePlusLog", "ko_coeff": 0.2}),
 ]
 
 
@@ -50,7 +55,7 @@ def make_input(name, matter, shape, order, seed, amp):
         return S.BoxState(fields=f, matter=st.matter, dx=st.dx, dt=st.dt, lam=st.lam)
     if name.startswith("grf"):
         return ics.grf_dust(shape, seed=seed, rms_delta=1e-3, order=order)
-    return ics.perturbed(shape, matter, seed=seed, amp=amp)
+    return ics.perturbed(shape, matter, seed=seed, amp=amp, z4c="_z4c" in name)
 
 
 def main() -> int:
@@ -64,7 +69,8 @@ def main() -> int:
         if only and name not in only:
             continue
         st = make_input(name, matter, shape, order, seed, amp)
-        binp = build_ref.build(*shape, order, "strict")
+        flavour = "strict_z4c" if st.z4c else "strict"
+        binp = build_ref.build(*shape, order, flavour)
         res, info = oracle.run_reference(binp, mode, st, steps=steps, threads=1, **cfg)
         arrays = {"input": st.fields, "input_header": np.frombuffer(st.header_bytes(), dtype=np.uint8)}
         if mode == "constraints":
@@ -75,7 +81,7 @@ def main() -> int:
             arrays["output_header"] = np.frombuffer(res.header_bytes(), dtype=np.uint8)
         np.savez_compressed(OUT / f"{name}.npz", **arrays)
         index[name] = {"matter": matter, "shape": list(shape), "order": order, "mode": mode,
-                       "steps": steps, "config": cfg, "generator": "reference sources, strict build",
+                       "steps": steps, "config": cfg, "generator": f"reference sources, {flavour} build",
                        "binary": binp.name}
         print(name, mode, info)
     index_path.write_text(json.dumps(index, indent=1, sort_keys=True) + "\n")

@@ -132,6 +132,29 @@ def test_parity_build_is_bit_exact(matter, shape, order, steps, kw):
     assert diff == 0, worst(field_errors(got.fields, ref.fields, st.names, floor=1e-18))
 
 
+@pytest.mark.parametrize("matter,shape,order,ko", [(S.DUST, (20, 18, 40), 8, 0.0), (S.SCALAR, (16, 20, 24), 4, 0.0),
+                                                    (S.STATIC, (16, 16, 18), 6, 0.0), (S.VACUUM, (16, 16, 16), 2, 0.3),
+                                                    (S.DUST, (24, 20, 18), 8, 0.2)])
+def test_z4c_damping_bit_exact(matter, shape, order, ko):
+    """Z4c damping (the reference's USE_Z4c_DAMPING: theta evolved, its terms
+    in the K, phi, A_ij and Gamma^i equations and in H, amplitudes 0.5, 0.1)
+    against the correctly rounded restatement, bit for bit, with and without
+    Kreiss-Oliger dissipation; and theta must matter: the same data without
+    Z4c end elsewhere."""
+    st = ics.perturbed(shape, matter, seed=23 + order, amp=2e-2, z4c=True)
+    kw = {"lapse": "Static" if matter == S.STATIC else "Harmonic", "ko_coeff": ko}
+    ref = oracle.evolve(st, 3, order, cr=True, **kw)
+    got = evolve(st, 3, BoxConfig(order=order, **kw))
+    diff = int((got.fields != ref.fields).sum())
+    print("z4c bit-exact", matter, shape, order, ko, "differing values:", diff)
+    assert diff == 0, worst(field_errors(got.fields, ref.fields, st.names, floor=1e-18))
+    plain = st.copy()
+    plain.z4c = False
+    plain.fields = st.fields[:-1].copy()
+    other = evolve(plain, 3, BoxConfig(order=order, **kw))
+    assert not np.array_equal(other.fields, got.fields[:-1])
+
+
 @pytest.mark.parametrize("matter,shape,order", [(S.DUST, (20, 18, 22), 8), (S.VACUUM, (12, 14, 16), 2),
                                                  (S.SCALAR, (16, 16, 16), 8), (S.DUST, (16, 16, 16), 4)])
 def test_kreiss_oliger_against_restatement(matter, shape, order):
