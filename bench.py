@@ -154,6 +154,25 @@ def profiled_traffic(n: int, order: int, precision: str):
         return None
 
 
+def profiled_flops(precision: str):
+    """FP64 flops per grid-point RK4 update of the substep kernel (four
+    launches), counted by ncu (dadd + dmul + 2 dfma, thread level) and
+    committed in profiles/stage_kernel_traffic.json; None if absent."""
+    prof = ROOT / "profiles" / "stage_kernel_traffic.json"
+    try:
+        return json.loads(prof.read_text()).get("fp64_flops_per_update", {}).get(precision)
+    except Exception:
+        return None
+
+
+def fp64_peak(L) -> float | None:
+    """This GPU's FP64 flop/s, measured by the library (cg_fp64_peak)."""
+    import ctypes
+
+    v = ctypes.c_double()
+    return v.value if L.cg_fp64_peak(ctypes.byref(v)) == 0 else None
+
+
 def make_state(n: int, seed: int, order: int, gpu: bool = True):
     """GRF dust initial data: the random field drawn on the host, the
     construction on the GPU (the host construction when gpu=False); both give
@@ -721,6 +740,15 @@ def main():
     launch_ms = ms_per_step / launches_per_step
     achieved = algo / (launch_ms / 1e3) / 1e9
     traffic = profiled_traffic(n, a.order, a.precision)
+    # the compute roofline beside the HBM one: counted FP64 flops per update
+    # against the measured FP64 peak of this GPU
+    compute = None
+    flops_upd, fpk = profiled_flops(a.precision), fp64_peak(L)
+    if flops_upd and fpk:
+        ach_f = flops_upd * pts / (ms_per_step / 1e3)
+        compute = {"bound": "fp64", "achieved": ach_f / 1e12, "peak": fpk / 1e12, "unit": "TFLOP/s",
+                   "frac": ach_f / fpk, "flops_per_update": flops_upd,
+                   "peak_kind": "measured (cg_fp64_peak: FMA chains, CUDA events)"}
 
     cpu = None
     if rank == 0 and a.cpu_baseline:
@@ -746,7 +774,7 @@ def main():
             "config": box_config(n, a.order, a.precision, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": algo},
+                         "algorithmic_bytes_per_launch": algo, "compute": compute},
             "e2e": {"value": e2e_value, "unit": "grid-pt RK4 updates/s",
                     "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
                     "steps": a.e2e_steps, "wall_s": e2e_wall},

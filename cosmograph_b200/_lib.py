@@ -37,7 +37,7 @@ EXPORTS = (
     "cg_kavg_sums", "cg_set_kavg", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
     "cg_status", "cg_frw_state", "cg_step_count", "cg_last_error", "cg_version",
     "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints", "cg_field_statistics",
-    "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust",
+    "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust", "cg_fp64_peak",
 )
 OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID, OPT_TMA = 1, 2, 3, 4, 5
 
@@ -112,6 +112,7 @@ def load() -> ctypes.CDLL:
         "cg_num_groups": (i, [vp, ctypes.POINTER(i)]),
         "cg_group_info": (i, [vp, i, ctypes.POINTER(i), i]),
         "cg_version": (i, []),
+        "cg_fp64_peak": (i, [dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -39,6 +39,7 @@ UNITS = [
     ("stage_fast_z4c.o", "cg_stage_inst.cu", ["--fmad=true", "-DCG_VARIANT_NS=fast", "-DCG_Z4C_UNIT=1"]),
     ("abi.o", "cg_abi.cu", []),
     ("noalloc.o", "cg_noalloc.cu", []),
+    ("peak.o", "cg_peak.cu", []),
     ("mixed.o", "cg_mixed_inst.cu", []),
     ("ics.o", "cg_ics.cu", []),
     ("tma_host.o", "cg_tma_host.cu", []),

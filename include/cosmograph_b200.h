@@ -364,6 +364,13 @@ int cg_conformal_average(cg_ctx *ctx, const double *d_field, const double *d_phi
 int cg_conformal_average_noalloc(const double *d_field, const double *d_phi, size_t n, double phi_frw,
                                  double *d_out, void *stream);
 
+/* The current GPU's FP64 arithmetic throughput in flop/s (an FMA counted as
+ * two), measured with eight independent FMA chains per thread over a grid
+ * of eight CTAs per SM, timed with CUDA events.  No counterpart in the
+ * reference: the denominator of the substep kernels' compute roofline.
+ * Synchronous; allocates 512 KiB for the duration of the call. */
+int cg_fp64_peak(double *flops_per_s);
+
 /* Message of the last failure on this context (or of cg_create, when ctx is NULL). */
 const char *cg_last_error(cg_ctx *ctx);
 
