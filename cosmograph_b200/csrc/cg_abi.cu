@@ -412,6 +412,20 @@ int launch_kavg(cg_ctx* ctx, Box& b, const double* in) {
   return CG_OK;
 }
 
+// dalpha/dt of the uniform background: the lapse gauges of
+// BSSNGaugeHandler.cc:16-275 with K_avg = K (a uniform state) and K_FRW = 0
+// (trivial FRW reference).
+double mixed_bg_lapse(const cg_box_desc& d, double al, double Kd, double phi) {
+  switch (d.lapse) {
+    case CG_LAPSE_HARMONIC: return -1.0 * al * Kd;
+    case CG_LAPSE_CONFORMAL_FLRW: return -1.0 / 3.0 * al * Kd;
+    case CG_LAPSE_AWA_GAUGE_WAVE: return -1.0 * (al * al) * Kd;
+    case CG_LAPSE_AWA_SHIFTED_WAVE: return -1.0 * Kd;
+    case CG_LAPSE_DAMPED_WAVE: return (al * al) * (d.dw_mu_l * (12.0 * phi * d.dw_p - std::log(al)) - Kd);
+    default: return 0.0;  // Static, ConformalSync (K_FRW = 0), Anharmonic and 1+log (K - K_avg = 0)
+  }
+}
+
 // Right-hand side of the uniform background (the reference's equations for a
 // spatially constant state, trivial FRW): dK/dt, dphi/dt, dalpha/dt and, for
 // a scalar field, dphi_s/dt = -alpha Pi, dPi/dt = alpha (K Pi + V'(phi_s))
@@ -434,7 +448,7 @@ void mixed_bg_rhs(const Box& b, const double* a, double phi_lag, double* rhs) {
   }
   rhs[cg::F_K] = al * (1.0 / 3.0 * Kd * Kd) + 4.0 * cg::kPi * al * rS;
   rhs[cg::F_PHI] = -1.0 / 6.0 * (al * Kd);
-  rhs[cg::F_ALPHA] = b.desc.lapse == CG_LAPSE_HARMONIC ? -1.0 * al * Kd : 0.0;
+  rhs[cg::F_ALPHA] = mixed_bg_lapse(b.desc, al, Kd, a[cg::F_PHI]);
 }
 
 void pack_bg(const double* full, double* compact) {
@@ -503,10 +517,50 @@ int mixed_init(cg_ctx* ctx, Box& b) {
   return CG_OK;
 }
 
+// K_avg - Kbar of an FP32-mixed substep input: the conformal average of the
+// perturbation, sum exp(6 dphi) dK / sum exp(6 dphi) (the factor exp(6 phibar)
+// of the reference's weights cancels), per-block partials in a fixed order
+// combined by kavg_final_kernel.
+__global__ void mixed_kavg_partial_kernel(const float* __restrict__ dK, const float* __restrict__ dphi, int pts,
+                                          double* partial) {
+  __shared__ double sK[256], sV[256];
+  double aK = 0.0, aV = 0.0;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < pts; q += (long long)gridDim.x * blockDim.x) {
+    const double e = exp(6.0 * (double)dphi[q]);
+    aK += e * (double)dK[q];
+    aV += e;
+  }
+  sK[threadIdx.x] = aK;
+  sV[threadIdx.x] = aV;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sK[threadIdx.x] += sK[threadIdx.x + o];
+      sV[threadIdx.x] += sV[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = sK[0];
+    partial[2 * blockIdx.x + 1] = sV[0];
+  }
+}
+
 // Background of substep n of a mixed box: RK4 stage of the uniform state on
-// the host (FP64), then the bookkeeping of K{n}Finalize.
-cg::mixed::Bg mixed_prepare(Box& b, int n) {
-  cg::mixed::Bg bg{};
+// the host (FP64), then the bookkeeping of K{n}Finalize.  The K_avg
+// reduction the lapse may need is queued on the context's stream.
+int mixed_prepare(cg_ctx* ctx, Box& b, int n, cg::mixed::Bg* out) {
+  if (b.needs_kavg) {
+    const float* in = (n == 1 || n == 3) ? b.mdev.X : b.mdev.Y;  // the substep's input
+    const size_t N = (size_t)b.dev.pts;
+    mixed_kavg_partial_kernel<<<b.kavg_blocks, 256, 0, ctx->stream>>>(in + (size_t)cg::F_K * N,
+                                                                     in + (size_t)cg::F_PHI * N, b.dev.pts,
+                                                                     b.kavg_partial);
+    kavg_final_kernel<<<1, 256, 0, ctx->stream>>>(b.kavg_partial, b.kavg_blocks, b.dev.pts, b.kavg);
+    CG_CUDA(ctx, cudaGetLastError());
+  }
+  cg::mixed::Bg& bg = *out;
+  bg = cg::mixed::Bg{};
   const double phi_lag = n == 1 ? b.ba[cg::F_PHI] : b.bprev[cg::F_PHI];
   double rhs[23];
   mixed_bg_rhs(b, b.ba, phi_lag, rhs);
@@ -536,6 +590,15 @@ cg::mixed::Bg mixed_prepare(Box& b, int n) {
   bg.potential = b.desc.potential;
   bg.pot_const = b.desc.pot_const;
   bg.pot_mass = b.desc.pot_mass;
+  bg.gd_c = b.desc.gd_c;
+  bg.dw_mu_l = b.desc.dw_mu_l;
+  bg.dw_p = b.desc.dw_p;
+  {
+    const double al = 1.0 + b.ba[cg::F_ALPHA];
+    bg.dw_u = b.desc.dw_mu_l * (12.0 * b.ba[cg::F_PHI] * b.desc.dw_p - std::log(al)) - b.ba[cg::F_K];
+  }
+  bg.ko_scale = b.desc.stencil_order == 2 ? b.desc.ko_coeff / (64.0 * b.desc.dx)
+                                          : -b.desc.ko_coeff / (1024.0 * b.desc.dx);
   for (int f = 0; f < 23; ++f) {
     b.bprev[f] = b.ba[f];
     b.ba[f] = o[f];
@@ -543,11 +606,13 @@ cg::mixed::Bg mixed_prepare(Box& b, int n) {
   }
   b.stage_next = n == 4 ? 1 : n + 1;
   if (n == 4) ++b.steps;
-  return bg;
+  return CG_OK;
 }
 
 int mixed_stage(cg_ctx* ctx, Box& b, int n) {
-  const cg::mixed::Bg bg = mixed_prepare(b, n);
+  cg::mixed::Bg bg;
+  int rc = mixed_prepare(ctx, b, n, &bg);
+  if (rc) return rc;
   CG_CUDA(ctx, cg::mixed::launch_stage(b.mdev, bg, n, ctx->stream));
   return CG_OK;
 }
@@ -626,10 +691,6 @@ int validate(const cg_box_desc& d, std::string& why) {
       why = "the FP32-mixed form evolves vacuum, dust or scalar boxes";
       return CG_ERR_INVALID;
     }
-    if (d.lapse != CG_LAPSE_HARMONIC && d.lapse != CG_LAPSE_STATIC) {
-      why = "the FP32-mixed form supports the Harmonic and Static lapses";
-      return CG_ERR_INVALID;
-    }
     if (d.frw_phi != 0.0 || d.frw_K != 0.0 || d.nfluids != 0) {
       why = "the FP32-mixed form evolves about its own uniform background (trivial FRW reference)";
       return CG_ERR_INVALID;
@@ -640,10 +701,6 @@ int validate(const cg_box_desc& d, std::string& why) {
     }
   }
   if (d.ko_coeff != 0.0) {
-    if (d.precision == CG_PREC_MIXED) {
-      why = "Kreiss-Oliger dissipation is not available in the FP32-mixed form";
-      return CG_ERR_INVALID;
-    }
     const int rko = d.stencil_order == 8 ? 5 : 2;  // orders 4 and 6: no dissipation (utils/math.h:36-72)
     if ((d.stencil_order == 2 || d.stencil_order == 8) && (d.nx < rko + 1 || d.ny < rko + 1 || d.nz < rko + 1)) {
       why = "Kreiss-Oliger dissipation needs stencil_order/2 + 2 points per axis (order 2) or 6 (order 8)";
@@ -667,7 +724,7 @@ int validate(const cg_box_desc& d, std::string& why) {
       return CG_ERR_INVALID;
     }
     if (lapse_needs_kavg(d.lapse) && d.precision == CG_PREC_MIXED) {
-      why = "the FP32-mixed form supports the Harmonic and Static lapses";
+      why = "an x-slab in the FP32-mixed form needs a lapse without K_avg";
       return CG_ERR_INVALID;
     }
   }
@@ -833,6 +890,8 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
       m.order = d.stencil_order; m.matter = d.matter; m.lapse = d.lapse; m.normalize = d.normalize_metric;
       m.xg = d.x_ghost;
       m.dx = d.dx; m.dt = d.dt;
+      m.ko = d.ko_coeff;
+      m.kavg = nullptr;  // set below when the lapse uses K_avg
       m.P = b.dev.P;
       m.F = b.dev.F;
       m.status = ctx->status;
@@ -859,6 +918,7 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
       b.kavg = b.kavg_partial + 2 * b.kavg_blocks;
       b.kavg_sums = b.kavg + 1;
       b.dev.kavg = b.kavg;
+      if (b.mixed) b.mdev.kavg = b.kavg;
     }
   }
   if (e != cudaSuccess) {
@@ -1215,6 +1275,7 @@ int write_table(cg_ctx* ctx, Group& g) {
       e.dt = b.mdev.dt;
       e.P = b.mdev.P; e.F = b.mdev.F; e.X = b.mdev.X; e.Y = b.mdev.Y; e.FP0 = b.mdev.FP0; e.FP1 = b.mdev.FP1;
       e.status = b.mdev.status;
+      e.kavg = b.mdev.kavg;
       e.mapX = b.mdev.mapX;
       e.mapY = b.mdev.mapY;
       e.tma = b.mdev.tma;
@@ -1332,7 +1393,10 @@ int group_launch(cg_ctx* ctx, Group& g, std::vector<Box>& boxes, int n) {
     cg::mixed::GroupBg gb{};
     gb.nboxes = (int)g.members.size();
     gb.total = g.total;
-    for (size_t q = 0; q < g.members.size(); ++q) gb.bg[q] = mixed_prepare(boxes[g.members[q]], n);
+    for (size_t q = 0; q < g.members.size(); ++q) {
+      int rc = mixed_prepare(ctx, boxes[g.members[q]], n, &gb.bg[q]);
+      if (rc) return rc;
+    }
     CG_CUDA(ctx, cg::mixed::launch_group(static_cast<const cg::mixed::GroupBox*>(g.table), gb, g.order, g.matter, n,
                                          g.grid, ctx->stream));
   } else {

@@ -44,6 +44,8 @@ struct MixedBox {
   int nx, ny, nz, pts, nfields, order, matter, lapse, normalize;
   int xg;  // ghost planes on each x face (0: periodic box)
   double dx, dt;
+  double ko;     // Kreiss-Oliger coefficient (0: none)
+  double* kavg;  // device K_avg - Kbar of the substep input (lapses with K_avg), else null
   double* P;
   double* F;
   float* X;

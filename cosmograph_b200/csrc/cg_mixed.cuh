@@ -17,8 +17,10 @@
 //   * the RK registers _p and _f and the register update stay FP64.
 // The equations are the reference's (components/bssn/bssn.cc:361-831,
 // bssn_macros.h:221-385, components/dust_fluid/dust.cc:109-264) with a
-// trivial FRW reference (the dust driver's FRW(0,0), bssn.cc:25), harmonic or
-// static lapse, a_adj_amp = k_damping_amp = 0.
+// trivial FRW reference (the dust driver's FRW(0,0), bssn.cc:25), every
+// lapse gauge of BSSNGaugeHandler (the K_avg of the ConformalFLRW, Anharmonic
+// and 1+log lapses enters as its perturbation, reduced from the FP32 inputs),
+// Kreiss-Oliger dissipation (orders 2 and 8), a_adj_amp = k_damping_amp = 0.
 #pragma once
 
 #include "cg_group.h"
@@ -50,6 +52,7 @@ struct Ptrs {
   const float* fp_in;  // dust flux primitives of a^n (FP32)
   float* fp_out;       // flux primitives of the output state
   unsigned* status;
+  const double* kavg;  // K_avg - Kbar of the substep input (lapses with K_avg), else null
 };
 
 // Uniform background of one substep (FP64).  A uniform state keeps every
@@ -66,6 +69,9 @@ struct Bg {
   double lambda;      // rho_Lambda
   double pot_const, pot_mass;  // scalar potential V = pot_const or m^2 phi^2 / 2
   int potential;
+  double gd_c;                 // 1+log lapse coefficient
+  double dw_mu_l, dw_p, dw_u;  // damped-wave lapse: mu_L, p and mu_L (12 p phibar - ln abar) - Kbar
+  double ko_scale;             // Kreiss-Oliger: c / (64 dx) (order 2) or -c / (1024 dx) (order 8)
 };
 __host__ __device__ constexpr int bgi(int f) {
   return f == F_K ? 0 : (f == F_PHI ? 1 : (f == F_ALPHA ? 2 : (f == 18 ? 3 : (f == 19 ? 4 : -1))));
@@ -82,6 +88,7 @@ struct GroupBox {
   double *P, *F;
   float *X, *Y, *FP0, *FP1;
   unsigned* status;
+  const double* kavg;
   int nbx, nby, nbz;
   int first;
   int tma;
@@ -308,8 +315,48 @@ __device__ __forceinline__ void flux_divergences(const T& t, const float* __rest
   }
 }
 
+// dalpha/dt(abar + delta) - dalpha/dt(abar) for the lapse gauges of
+// BSSNGaugeHandler.cc:16-275 with a trivial FRW reference (K_FRW = 0, so the
+// conformal-synchronous lapse is static); dKa = K_avg - Kbar.  The host adds
+// dalpha/dt(abar), in which K_avg = Kbar.
+__device__ __forceinline__ float lapse_drhs(int lapse, const Bg& bg, float alb, float dal, float alpha, float Kb,
+                                            float dK, float dphi, float dKa) {
+  switch (lapse) {
+    case kHarmonic: return -(alb * dK + dal * (Kb + dK));
+    case kConformalFLRW: return -(1.0f / 3.0f) * (alb * dKa + dal * (Kb + dKa));
+    case kAnharmonic: return alpha * alpha * (dK - dKa);
+    case kOnePlusLog: return -2.0f * (float)bg.gd_c * alpha * (dK - dKa);
+    case kAwAGaugeWave: return -(alpha * alpha * dK + (2.0f * alb + dal) * dal * Kb);
+    case kAwAShiftedWave: return -dK;
+    case kDampedWave: {
+      const float du = (float)bg.dw_mu_l * (12.0f * (float)bg.dw_p * dphi - log1pf(dal / alb)) - dK;
+      return alpha * alpha * du + (2.0f * alb + dal) * dal * (float)bg.dw_u;
+    }
+    default: return 0.0f;
+  }
+}
+
+// Kreiss-Oliger dissipation of one FP32 perturbation (the stencil of a
+// constant is zero, so it is the dissipation of the full field): the sixth
+// (order 2: fourth) undivided difference along each axis from global taps,
+// times bg.ko_scale (utils/math.h:36-72, as the FP64 kernel's ko_dissipation).
+template <int O>
+__device__ __forceinline__ float ko_f(const float* __restrict__ f, const Taps<true>& t, float scale) {
+  float s = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    auto V = [&](int n) { return __ldg(f + t.ax(a, n)); };
+    if (O == 2) s += (V(-2) + V(2)) - 4.0f * (V(-1) + V(1)) + 6.0f * V(0);
+    else
+      s += (V(-5) + V(5)) - 10.0f * (V(-4) + V(4)) + 45.0f * (V(-3) + V(3)) - 120.0f * (V(-2) + V(2)) +
+           210.0f * (V(-1) + V(1)) - 252.0f * V(0);
+  }
+  return scale * s;
+}
+
 // The FP32-mixed substep for the brick at brick coordinates (cx, cy, cz).
-template <int O, int MATTER>
+// KO: Kreiss-Oliger dissipation compiled in (orders 2 and 8 only).
+template <int O, int MATTER, bool KO = false>
 __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt,
                                            const Bg& bg, const Ptrs& P, int stage, int cx, int cy, int cz,
                                            const CUtensorMap* tmap, uint64_t* bar, unsigned& phase,
@@ -632,7 +679,11 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
 
   // ---- perturbation right-hand sides + FP64 register update ----------------------
   double outv[NFLD];
+  const Taps<true> tko{i, j, k, nx, ny, nz, ny * nz, nz, c};
   auto finalize = [&](int fld, float drhs) {
+    if constexpr (KO) {
+      if (fld < F_D) drhs -= ko_f<O>(a + (size_t)fld * N, tko, (float)bg.ko_scale);
+    }
     const double cv = bgv(bg.rhs, fld) + (double)drhs;
     const double pv = __ldcs(&P.p[(size_t)fld * N + c]);
     double o;
@@ -684,7 +735,7 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
                     4.0f * kPif * (alb * (dr + Sdust) + dal * rS_full);
   finalize(F_K, dRK);
   finalize(F_PHI, -(1.0f / 6.0f) * (alb * dK + dal * K));
-  finalize(F_ALPHA, lapse == kHarmonic ? -(alb * dK + dal * K) : 0.0f);
+  finalize(F_ALPHA, lapse_drhs(lapse, bg, alb, dal, alpha, Kb, dK, dphi0, P.kavg ? (float)__ldg(P.kavg) : 0.0f));
   if (MATTER == kDust) {
 #pragma unroll
     for (int m = 0; m < 4; ++m) finalize(F_D + m, rhs_m[m]);
@@ -765,7 +816,7 @@ __device__ __forceinline__ void init_tile_barrier(uint64_t* bar, bool use) {
 
 // One box: one CTA per updated brick.  tmap: the TMA map of this substep's
 // input (use_tma = 0: every tile is copied by the threads).
-template <int O, int MATTER>
+template <int O, int MATTER, bool KO>
 __global__ void __launch_bounds__(kThreads, 4)
 mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double dt, Bg bg, Ptrs P, int stage,
              const __grid_constant__ CUtensorMap tmap, int use_tma, int bx0) {
@@ -774,7 +825,7 @@ mixed_kernel(int nx, int ny, int nz, int lapse, int normalize, float idx, double
   unsigned phase = 0;
   bool tma_ok = true;
   // bx0: first x brick (x-slab boxes skip their ghost planes)
-  mixed_body<O, MATTER>(nx, ny, nz, lapse, normalize, idx, dt, bg, P, stage, blockIdx.z + bx0, blockIdx.y, blockIdx.x,
+  mixed_body<O, MATTER, KO>(nx, ny, nz, lapse, normalize, idx, dt, bg, P, stage, blockIdx.z + bx0, blockIdx.y, blockIdx.x,
                         use_tma ? &tmap : nullptr, &bar, phase, tma_ok);
 }
 
@@ -785,6 +836,7 @@ __device__ __forceinline__ Ptrs group_ptrs(const GroupBox& b, int stage) {
   p.f = b.F;
   p.newp = b.P;
   p.status = b.status;
+  p.kavg = b.kavg;
   switch (stage) {
     case 1: p.in = b.X; p.prev = nullptr; p.out = b.Y; p.fp_in = b.FP0; p.fp_out = b.FP1; break;
     case 2: p.in = b.Y; p.prev = b.X; p.out = b.X; p.fp_in = b.FP1; p.fp_out = b.FP0; break;

@@ -25,13 +25,14 @@ cudaError_t allow_smem(K kernel, size_t smem, bool& done) {
   return e;
 }
 
-template <int O, int M>
+template <int O, int M, bool KO>
 cudaError_t go(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
   Ptrs P{};
   P.p = b.P;
   P.f = b.F;
   P.newp = b.P;
   P.status = b.status;
+  P.kavg = b.kavg;
   switch (stage) {
     case 1: P.in = b.X; P.prev = nullptr; P.out = b.Y; P.fp_in = b.FP0; P.fp_out = b.FP1; break;
     case 2: P.in = b.Y; P.prev = b.X; P.out = b.X; P.fp_in = b.FP1; P.fp_out = b.FP0; break;
@@ -40,20 +41,28 @@ cudaError_t go(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
   }
   constexpr size_t smem = smem_bytes<M>();
   static bool done = false;
-  cudaError_t e = allow_smem(mixed_kernel<O, M>, smem, done);
+  cudaError_t e = allow_smem(mixed_kernel<O, M, KO>, smem, done);
   if (e != cudaSuccess) return e;
   const CUtensorMap& map = (stage == 1 || stage == 3) ? b.mapX : b.mapY;  // the substep's input
-  mixed_kernel<O, M><<<grid3(b.nx - 2 * b.xg, b.ny, b.nz), dim3(kBZ, kBY, kBX), smem, st>>>(
+  mixed_kernel<O, M, KO><<<grid3(b.nx - 2 * b.xg, b.ny, b.nz), dim3(kBZ, kBY, kBX), smem, st>>>(
       b.nx, b.ny, b.nz, b.lapse, b.normalize, (float)(1.0 / b.dx), b.dt, bg, P, stage, map, b.tma, b.xg / kBX);
   return cudaGetLastError();
 }
+template <int O, bool KO>
+cudaError_t go_mk(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
+  switch (b.matter) {
+    case kDust: return go<O, kDust, KO>(b, bg, stage, st);
+    case kScalar: return go<O, kScalar, KO>(b, bg, stage, st);
+    default: return go<O, kVacuum, KO>(b, bg, stage, st);
+  }
+}
+// Kreiss-Oliger dissipation exists for stencil orders 2 and 8 (utils/math.h:36-72)
 template <int O>
 cudaError_t go_m(const MixedBox& b, const Bg& bg, int stage, cudaStream_t st) {
-  switch (b.matter) {
-    case kDust: return go<O, kDust>(b, bg, stage, st);
-    case kScalar: return go<O, kScalar>(b, bg, stage, st);
-    default: return go<O, kVacuum>(b, bg, stage, st);
+  if constexpr (O == 2 || O == 8) {
+    if (b.ko != 0.0) return go_mk<O, true>(b, bg, stage, st);
   }
+  return go_mk<O, false>(b, bg, stage, st);
 }
 
 template <int O, int M>

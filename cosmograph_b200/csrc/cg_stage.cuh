@@ -558,7 +558,7 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
   return __syncthreads_and(ok);
 }
 
-// Kreiss-Oliger dissipation of one field at (i, j, k)// Kreiss-Oliger dissipation of one field at (i, j, k) (utils/math.h:36-72;
+// Kreiss-Oliger dissipation of one field at (i, j, k) (utils/math.h:36-72;
 // the reference defines it for stencil orders 2 and 8 only): the sixth
 // (order 2: fourth) undivided difference along each axis, taps from global
 // memory, plain offsets when the taps stay inside the box.

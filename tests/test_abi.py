@@ -58,7 +58,7 @@ def test_host_only_entry_points(L):
 @pytest.mark.parametrize("field,value,msg", [
     ("stencil_order", 5, "stencil_order"),
     ("nx", 2, "at least"),
-    ("precision", 2, None),  # with ko_coeff below: the mixed form has no dissipation
+    ("z4c", 2, "z4c"),
     ("lapse", 42, "lapse"),
     ("nx", 5, None),         # with ko_coeff: order 8 dissipation needs 6 points per axis
     ("nfluids", 7, "fluids"),
