@@ -24,6 +24,7 @@ LAPSE = {
     "OnePlusLog": 5, "AwAGaugeWave": 6, "AwAShiftedWave": 7, "DampedWave": 8,
 }
 PRECISION = {"fp64": 0, "fp64_fma": 1, "mixed": 2}
+SHIFT = {"Static": 1, "GammaDriver": 2, "DampedWave": 3, "AwAShiftedWave": 4, "AijDriverShift": 5}
 POTENTIAL = {"const": 0, "quadratic": 1}
 STATUS_NAN, STATUS_NONFINITE, STATUS_TILE_TIMEOUT = 1, 2, 4
 
@@ -57,6 +58,8 @@ class BoxDesc(ctypes.Structure):
         ("frw_phi", ctypes.c_double), ("frw_K", ctypes.c_double),
         ("nfluids", ctypes.c_int), ("z4c", ctypes.c_int),
         ("fluid_rho", ctypes.c_double * 4), ("fluid_w", ctypes.c_double * 4),
+        ("shift", ctypes.c_int), ("gauge_wave_dir", ctypes.c_int), ("gd_eta", ctypes.c_double),
+        ("dw_mu_s", ctypes.c_double), ("k_driver_coeff", ctypes.c_double),
     ]
 
 

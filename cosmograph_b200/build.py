@@ -37,6 +37,8 @@ UNITS = [
     ("stage_exact_z4c.o", "cg_stage_inst.cu",
      ["--fmad=false", "-DCG_VARIANT_NS=exact", "-DCG_REFERENCE_ORDER=1", "-DCG_Z4C_UNIT=1"]),
     ("stage_fast_z4c.o", "cg_stage_inst.cu", ["--fmad=true", "-DCG_VARIANT_NS=fast", "-DCG_Z4C_UNIT=1"]),
+    ("stage_exact_shift.o", "cg_stage_inst.cu",
+     ["--fmad=false", "-DCG_VARIANT_NS=exact", "-DCG_REFERENCE_ORDER=1", "-DCG_SHIFT_UNIT=1"]),
     ("abi.o", "cg_abi.cu", []),
     ("noalloc.o", "cg_noalloc.cu", []),
     ("peak.o", "cg_peak.cu", []),

@@ -682,6 +682,19 @@ int validate(const cg_box_desc& d, std::string& why) {
     return CG_ERR_INVALID;
   }
   if (d.z4c != 0 && d.z4c != 1) { why = "z4c must be 0 or 1"; return CG_ERR_INVALID; }
+  if (d.shift < CG_SHIFT_NONE || d.shift > CG_SHIFT_AIJ_DRIVER) { why = "unknown shift gauge"; return CG_ERR_INVALID; }
+  if (d.shift != CG_SHIFT_NONE) {
+    // the reference's shift (USE_BSSN_SHIFT with USE_GAMMA_DRIVER) in the parity build
+    if (d.precision != CG_PREC_FP64) { why = "the shift is available with CG_PREC_FP64 only"; return CG_ERR_INVALID; }
+    if (d.matter == CG_MATTER_STATIC) { why = "static matter has no shift"; return CG_ERR_INVALID; }
+    if (d.z4c) { why = "the shift and Z4c damping do not combine here"; return CG_ERR_INVALID; }
+    if (d.x_ghost != 0) { why = "an x-slab has no shift"; return CG_ERR_INVALID; }
+    if (d.nx < 4 || d.ny < 4 || d.nz < 4) {
+      why = "the shift's upwinded stencils need at least 4 points per axis";
+      return CG_ERR_INVALID;
+    }
+    if (d.gauge_wave_dir < 1 || d.gauge_wave_dir > 3) { why = "gauge_wave_dir must be 1, 2 or 3"; return CG_ERR_INVALID; }
+  }
   if (d.precision == CG_PREC_MIXED) {
     if (d.z4c) {
       why = "Z4c damping is available in the FP64 precisions only";
@@ -803,6 +816,9 @@ void cg_box_desc_default(cg_box_desc* d, int n) {
   d->gd_c = 1.0;
   d->pot_const = 3.0e-4;
   d->pot_mass = 1.0;
+  d->shift = CG_SHIFT_NONE;
+  d->gauge_wave_dir = 1;      // BSSNGaugeHandler.h:139-147 defaults
+  d->k_driver_coeff = 0.04;
 }
 
 int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
@@ -835,8 +851,9 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
     b.dev.ny = d.ny;
     b.dev.nz = d.nz;
     b.dev.pts = d.nx * d.ny * d.nz;
-    b.dev.nfields = cg_num_fields(d.matter) + (d.z4c ? 1 : 0);
+    b.dev.nfields = cg_num_fields(d.matter) + (d.z4c ? 1 : 0) + (d.shift != CG_SHIFT_NONE ? 7 : 0);
     b.dev.z4c = d.z4c ? 1 : 0;
+    b.dev.shift = d.shift != CG_SHIFT_NONE ? 1 : 0;
     b.dev.order = d.stencil_order;
     b.dev.matter = d.matter;
     cg::Physics& ph = b.dev.ph;
@@ -857,6 +874,11 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
     ph.dw_p = d.dw_p;
     ph.pot_const = d.pot_const;
     ph.pot_mass = d.pot_mass;
+    ph.shift = d.shift;
+    ph.gauge_wave_dir = d.gauge_wave_dir;
+    ph.gd_eta = d.gd_eta;
+    ph.dw_mu_s = d.dw_mu_s;
+    ph.k_driver_coeff = d.k_driver_coeff;
     b.frw.phi = d.frw_phi;
     b.frw.K = d.frw_K;
     b.frw.n = d.nfluids;
@@ -1345,13 +1367,15 @@ int ensure_groups(cg_ctx* ctx) {
     g.matter = ba.desc.matter;
     g.members.push_back((int)a);
     used[a] = true;
-    // boxes with Kreiss-Oliger dissipation or Z4c damping and x-slabs keep their own launches
-    for (size_t b = a + 1; ba.desc.ko_coeff == 0.0 && ba.desc.z4c == 0 && ba.desc.x_ghost == 0 && b < ctx->boxes.size() &&
+    // boxes with Kreiss-Oliger dissipation, Z4c damping or a shift and x-slabs keep their own launches
+    for (size_t b = a + 1; ba.desc.ko_coeff == 0.0 && ba.desc.z4c == 0 && ba.desc.shift == CG_SHIFT_NONE &&
+                           ba.desc.x_ghost == 0 && b < ctx->boxes.size() &&
                            g.members.size() < (size_t)cg::kMaxGroupBoxes;
          ++b) {
       const Box& bb = ctx->boxes[b];
       if (used[b] || bb.mixed != g.mixed || bb.variant != g.variant || bb.desc.stencil_order != g.order ||
-          bb.desc.matter != g.matter || bb.desc.ko_coeff != 0.0 || bb.desc.z4c != 0 || bb.desc.x_ghost != 0)
+          bb.desc.matter != g.matter || bb.desc.ko_coeff != 0.0 || bb.desc.z4c != 0 ||
+          bb.desc.shift != CG_SHIFT_NONE || bb.desc.x_ghost != 0)
         continue;
       g.members.push_back((int)b);
       used[b] = true;

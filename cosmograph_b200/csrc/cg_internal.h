@@ -22,6 +22,7 @@ struct BoxDev {
   int nx, ny, nz, pts, nfields, order, matter;
   int xg;  // ghost planes on each x face (0: periodic box)
   int z4c;  // Z4c damping: theta is field nfields - 1 (stage_kernel<..., Z4C = true>)
+  int shift;  // the shift: beta1..3, auxB1..3, expN are the last 7 fields (stage_kernel<..., SHIFT = true>)
   CUtensorMap fmap0[3], fmap1[3];  // TMA maps of the flux primitives FP0 / FP1 (x, y, z boxes)
   int fmaps;                       // those maps are encoded
   Physics ph;
@@ -91,6 +92,9 @@ int constraint_blocks(const BoxDev& b);
 // the Z4c instantiations (cg_stage_inst.cu built with -DCG_Z4C_UNIT=1)
 cudaError_t launch_stage_z4c(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
 cudaError_t launch_constraints_z4c(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st);
+// the shift instantiations (cg_stage_inst.cu built with -DCG_SHIFT_UNIT=1; the
+// parity build only)
+cudaError_t launch_stage_shift(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
 }  // namespace exact
 namespace fast {
 void make_tile_maps(BoxDev& b);
@@ -98,6 +102,7 @@ cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStre
 cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st);
 cudaError_t launch_stage_z4c(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
 cudaError_t launch_constraints_z4c(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st);
+cudaError_t launch_stage_shift(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st);
 }  // namespace fast
 
 // One launch for substep `stage` of every box of an FP64 group (table: device

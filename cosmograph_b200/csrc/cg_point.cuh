@@ -250,6 +250,19 @@ __device__ __forceinline__ double ev_lapse(const Physics& ph, const StageBg& bg,
   }
 }
 
+// with the shift, the 1+log and damped-wave lapses add beta^i d_i alpha, term
+// by term (BSSNGaugeHandler.cc:66-67, 152-153)
+__device__ __forceinline__ double ev_lapse_shift(const Physics& ph, const StageBg& bg, double alpha, double K,
+                                                 double Kd, double phi, const double beta[3], const double da[3]) {
+  double v = ev_lapse(ph, bg, alpha, K, Kd, phi);
+  if (ph.lapse == kOnePlusLog || ph.lapse == kDampedWave) {
+    v = v + beta[0] * da[0];
+    v = v + beta[1] * da[1];
+    v = v + beta[2] * da[2];
+  }
+  return v;
+}
+
 __device__ __forceinline__ double pot_V(const Physics& ph, double phi) {
   return ph.potential == kPotQuadratic ? 0.5 * (ph.pot_mass * ph.pot_mass) * (phi * phi) : ph.pot_const;
 }

@@ -238,6 +238,43 @@ __device__ __forceinline__ double dm(const T& t, int a, int b, const Physics& ph
   return divdx(divdx(s, ph), ph);
 }
 
+// taps of one stored field read from global memory through the index taps T
+// (the shift's derivatives and upwinded advection)
+template <class T>
+struct GlobalTaps {
+  const double* f;
+  T t;
+  __device__ __forceinline__ double ax(int a, int n) const { return __ldg(f + t.ax(a, n)); }
+  __device__ __forceinline__ double pl(int a, int n, int b, int m) const { return __ldg(f + t.pl(a, n, b, m)); }
+};
+
+// upwind_derivative (utils/math.h:1247-1252): c times the lopsided derivative
+// on the side c points to, lop_{forward,backward}_derivative plus the
+// matching dissipation stencil (math.h:166-230, 265-339, 888-956, 1087-1131,
+// 1220-1230).  The reference defines both as zero at orders 6 and 8.
+template <int O, class T>
+__device__ __forceinline__ double upwind(const T& t, int a, double c, const Physics& ph) {
+  auto V = [&](int n) { return t.ax(a, n); };
+  if constexpr (O == 2) {
+    if (c > 0) {
+      const double lop = divdx((-1.0 / 2.0 * V(2) + 2.0 * V(1) - 3.0 / 2.0 * V(0)), ph);
+      const double dd = divdx(divdx((2.0 * V(0) - 5.0 * V(1) + 4.0 * V(2) - 1.0 * V(3)), ph), ph);
+      return c * (lop + -1.0 / 2.0 * ph.dx * dd);
+    }
+    const double lop = divdx((+1.0 / 2.0 * V(-2) - 2.0 * V(-1) + 3.0 / 2.0 * V(0)), ph);
+    const double dd = divdx(divdx((2.0 * V(0) - 5.0 * V(-1) + 4.0 * V(-2) - 1.0 * V(-3)), ph), ph);
+    return c * (lop + +1.0 / 2.0 * ph.dx * dd);
+  } else if constexpr (O == 4) {
+    if (c > 0)
+      return c * (divdx((+1.0 / 12.0 * V(3) - 1.0 / 2.0 * V(2) + 3.0 / 2.0 * V(1) - 5.0 / 6.0 * V(0) -
+                         1.0 / 4.0 * V(-1)), ph) + 0.0);
+    return c * (divdx((-1.0 / 12.0 * V(-3) + 1.0 / 2.0 * V(-2) - 3.0 / 2.0 * V(-1) + 5.0 / 6.0 * V(0) +
+                       1.0 / 4.0 * V(1)), ph) + 0.0);
+  } else {
+    return c * (0.0 + 0.0);
+  }
+}
+
 // derivative of the product of two stored arrays (dust fluxes (alpha*D)*v^i,
 // dust.cc:121-133, and their divergence :203-224)
 template <int O, class T>
@@ -629,13 +666,16 @@ __device__ __forceinline__ void cta_reduce(double (&q)[Q], double* part, int cta
 // common case carries none of their code).  Z4C: Z4c damping (the field theta
 // after the matter fields, bssn.cc:834-848 and the theta terms of ev_*; the
 // reference's USE_Z4c_DAMPING), also a separate instantiation.
-template <int O, int MATTER, int MODE, bool KO = false, bool Z4C = false>
+template <int O, int MATTER, int MODE, bool KO = false, bool Z4C = false, bool SHIFT = false>
 __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph, StageBg bg, const StagePtrs& P,
                                            int stage, int cx, int cy, int cz, int cta, const CUtensorMap* tmap,
                                            uint64_t* bar, unsigned& phase, bool& tma_ok,
                                            const FluxMaps* fmaps = nullptr) {
   constexpr int F_THETA = NF<MATTER>::value;
-  constexpr int NFLD = NF<MATTER>::value + (Z4C ? 1 : 0);
+  // the shift fields beta1..3, auxB1..3, expN follow the matter fields (and theta)
+  constexpr int F_BETA = NF<MATTER>::value + (Z4C ? 1 : 0), F_AUXB = F_BETA + 3, F_EXPN = F_BETA + 6;
+  constexpr int NFLD = NF<MATTER>::value + (Z4C ? 1 : 0) + (SHIFT ? 7 : 0);
+  static_assert(!SHIFT || MODE == kEvolve, "constraint statistics do not read the shift");
   constexpr int NSLOT = MODE == kConstraints ? SlotsC<MATTER, Z4C>::value : Slots<MATTER, Z4C>::value;
   // Z4c damping amplitudes (cosmo_macros.h:94-100)
   constexpr double k1 = Z4C ? 0.5 : 0.0, k2 = Z4C ? 0.1 : 0.0;
@@ -741,6 +781,28 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   double gm[6];
   gm[0] = g[0] + 1.0; gm[1] = g[1]; gm[2] = g[2];
   gm[3] = g[3] + 1.0; gm[4] = g[4]; gm[5] = g[5] + 1.0;
+  // the shift (set_local_vals and calculate_dbeta, bssn.cc:430-435, 548-559):
+  // beta^i and db[j][i] = d_j beta^i, centred stencils on global taps (0
+  // without the shift, as the reference's zero-initialised BSSNData leaves
+  // them); up(f, j) = upwind_derivative of field f along axis j with beta^j
+  double beta[3] = {0.0, 0.0, 0.0};
+  double db[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  const Taps<true> tg{i, j, k, geo.nx, geo.ny, geo.nz, geo.ny * geo.nz, geo.nz, c};
+  auto gtap = [&](int fld) { return GlobalTaps<Taps<true>>{a + (size_t)fld * N, tg}; };
+  auto up = [&](int fld, int d) { return upwind<O>(gtap(fld), d, beta[d], ph); };
+  // second derivative d_x d_y of field fld (double_derivative, utils/math.h:1319-1336)
+  auto ddf = [&](int x, int y, int fld) {
+    return x == y ? d2<O>(gtap(fld), x, ph) : dm<O>(gtap(fld), x < y ? x : y, x < y ? y : x, ph);
+  };
+  if constexpr (SHIFT) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      beta[q] = C(F_BETA + q);
+#pragma unroll
+      for (int d = 0; d < 3; ++d) db[d][q] = d1<O>(gtap(F_BETA + q), d, ph);
+    }
+  }
+  const double divb = (db[0][0] + db[1][1]) + db[2][2];
   // every e^x this point's substep takes, in one batch: of phi and, for dust
   // after the first substep, of the previous substep's phi (the lagged
   // sources); static matter takes e^{-6 phi} in the sixth place
@@ -810,7 +872,18 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     const double sphi = C(F_SPHI), sPi = C(F_SPI);
     const double psi[3] = {C(F_SPSI1), C(F_SPSI1 + 1), C(F_SPSI1 + 2)};
     auto SD = [&](int m, int d) { return S(S_MAT + 3 * m + d); };  // d_d of scalar field m
-    const double nmu = ((-alpha * sPi)) / alpha;
+    // with the shift, dt_phi = beta^i d_i phi - alpha Pi and n^mu d_mu phi =
+    // (dt_phi - beta^i d_i phi) / alpha, term by term (scalar.cc:132-140, 224-229)
+    double dtphi = (-alpha * sPi), nmu_num = dtphi;
+    if constexpr (SHIFT) {
+      double u = beta[0] * SD(0, 0) + beta[1] * SD(0, 1);
+      u = u + beta[2] * SD(0, 2);
+      dtphi = u - alpha * sPi;
+      nmu_num = dtphi - beta[0] * SD(0, 0);
+      nmu_num = nmu_num - beta[1] * SD(0, 1);
+      nmu_num = nmu_num - beta[2] * SD(0, 2);
+    }
+    const double nmu = (nmu_num) / alpha;
     const double dd = (gi[0] * SD(0, 0) * SD(0, 0) + gi[3] * SD(0, 1) * SD(0, 1) + gi[5] * SD(0, 2) * SD(0, 2) +
                        2.0 * (gi[1] * SD(0, 0) * SD(0, 1) + gi[2] * SD(0, 0) * SD(0, 2) + gi[4] * SD(0, 1) * SD(0, 2)));
     const double V = pot_V(ph, sphi);
@@ -835,12 +908,28 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     for (int I = 0; I < 3; ++I)
       gt[I] = (C(F_GAM1 + I) - 2.0 * (gi[sym(I, 0)] * S(S_DPHI + 0) + gi[sym(I, 1)] * S(S_DPHI + 1) +
                                       gi[sym(I, 2)] * S(S_DPHI + 2)));
-    rhs_m[0] = (-alpha * sPi);
-    rhs_m[1] = (-em4phi * (inner) +
-                alpha * ((gt[0]) * psi[0] * em4phi + (gt[1]) * psi[1] * em4phi + (gt[2]) * psi[2] * em4phi + K * sPi +
-                         pot_dV(ph, sphi)));
+    rhs_m[0] = dtphi;
+    const double piv = alpha * ((gt[0]) * psi[0] * em4phi + (gt[1]) * psi[1] * em4phi + (gt[2]) * psi[2] * em4phi +
+                                K * sPi + pot_dV(ph, sphi));
+    if constexpr (SHIFT) {
+      double u = beta[0] * SD(1, 0) + beta[1] * SD(1, 1);
+      u = u + beta[2] * SD(1, 2);
+      rhs_m[1] = (u - em4phi * (inner)) + piv;
 #pragma unroll
-    for (int m = 0; m < 3; ++m) rhs_m[2 + m] = (-alpha * SD(1, m) - sPi * S(S_DA + m));
+      for (int m = 0; m < 3; ++m) {
+        double w = beta[0] * SD(2 + m, 0) + beta[1] * SD(2 + m, 1);
+        w = w + beta[2] * SD(2 + m, 2);
+        w = w + psi[0] * db[m][0];
+        w = w + psi[1] * db[m][1];
+        w = w + psi[2] * db[m][2];
+        w = w - alpha * SD(1, m);
+        rhs_m[2 + m] = w - sPi * S(S_DA + m);
+      }
+    } else {
+      rhs_m[1] = (-em4phi * (inner) + piv);
+#pragma unroll
+      for (int m = 0; m < 3; ++m) rhs_m[2 + m] = (-alpha * SD(1, m) - sPi * S(S_DA + m));
+    }
   } else if (MATTER == kStaticMatter) {
     // BSSN::clearSrc, Static::addBSSNSrc (components/static/static.cc:19-36)
     // and Lambda::addBSSNSource: the fixed density sources DIFFr only
@@ -1162,11 +1251,29 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     if (stage == 4 && !(renorm && fld < F_K && fld != F_PHI)) __stcs(&P.norm[(size_t)fld * N + c], o);
   };
 
-  // ev_DIFFgammaIJ (bssn.cc:748-753)
+  // ev_DIFFgammaIJ (bssn.cc:748-753, BSSN_DT_DIFFGAMMAIJ bssn_macros.h:292-307)
 #pragma unroll
-  for (int m = 0; m < 6; ++m)
-    finalize(F_G11 + m, (-2.0 * alpha * A[m]) + 0.5 * ph.a_adj_amp * dt * H * g[m] - ko(F_G11 + m));
-  // ev_AIJ (bssn.cc:755-760, BSSN_DT_AIJ bssn_macros.h:334-337)
+  for (int I = 0; I < 3; ++I)
+#pragma unroll
+    for (int J = I; J < 3; ++J) {
+      const int m = sym(I, J);
+      double v = (-2.0 * alpha * A[m]);
+      if constexpr (SHIFT) {
+        // advection and the Lie-derivative terms of the shift, term by term
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v = v + up(F_G11 + m, d);
+#pragma unroll
+        for (int X = 0; X < 3; ++X) v = v + gm[sym(I, X)] * db[J][X];
+#pragma unroll
+        for (int X = 0; X < 3; ++X) v = v + gm[sym(J, X)] * db[I][X];
+        v = v - (2.0 / 3.0) * gm[m] * (divb);
+      }
+      finalize(F_G11 + m, v + 0.5 * ph.a_adj_amp * dt * H * g[m] - ko(F_G11 + m));
+    }
+  // ev_AIJ (bssn.cc:755-760, BSSN_DT_AIJ bssn_macros.h:334-337); with the
+  // shift the A_ij and Gamma^i right-hand sides are kept for the
+  // AijDriverShift and Gamma-driver gauges
+  double rhsA[6], rhsG[3];
 #pragma unroll
   for (int I = 0; I < 3; ++I)
 #pragma unroll
@@ -1181,9 +1288,20 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
           aa = (X == 0 && Y == 0) ? u : aa + u;
         }
       const double RTF = Ric(qq) - (1.0 / 3.0) * e4phi * gm[qq] * ricci;
-      const double dtA = (em4phi * (alpha * (RTF - 8.0 * kPi * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
-                          alpha * (((K + 2.0 * theta) * A[qq]) - 2.0 * (aa)));
-      finalize(F_A11 + qq, dtA - 1.0 * ph.a_adj_amp * dt * A[qq] * H - ko(F_A11 + qq));
+      double dtA = (em4phi * (alpha * (RTF - 8.0 * kPi * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
+                    alpha * (((K + 2.0 * theta) * A[qq]) - 2.0 * (aa)));
+      if constexpr (SHIFT) {  // BSSN_DT_AIJ with the shift (bssn_macros.h:319-332)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) dtA = dtA + up(F_A11 + qq, d);
+#pragma unroll
+        for (int X = 0; X < 3; ++X) dtA = dtA + A[sym(I, X)] * db[J][X];
+#pragma unroll
+        for (int X = 0; X < 3; ++X) dtA = dtA + A[sym(J, X)] * db[I][X];
+        dtA = dtA - (2.0 / 3.0) * A[qq] * (divb);
+      }
+      const double evA = dtA - 1.0 * ph.a_adj_amp * dt * A[qq] * H - ko(F_A11 + qq);
+      if constexpr (SHIFT) rhsA[qq] = evA;
+      finalize(F_A11 + qq, evA);
     }
   // ev_GammaI (bssn.cc:762-764, BSSN_DT_GAMMAI_NOSHIFT bssn_macros.h:342-361)
   const double sq[3] = {S(S_SRC + Q_S1), S(S_SRC + Q_S2), S(S_SRC + Q_S3)};
@@ -1200,21 +1318,64 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
                              gi[sym(I, 0)] * dth[0] + gi[sym(I, 1)] * dth[1] + gi[sym(I, 2)] * dth[2]) -
               2.0 * alpha * k1 * (C(F_GAM1 + I) - Gd[I]) -
               8.0 * kPi * (gi[sym(I, 0)] * sq[0] + gi[sym(I, 1)] * sq[1] + gi[sym(I, 2)] * sq[2])));
-    finalize(F_GAM1 + I, ns + 0.0 - ko(F_GAM1 + I));
+    if constexpr (SHIFT) {
+      // BSSN_DT_GAMMAI_SHIFT (bssn_macros.h:363-382), term by term
+      double sh = up(F_GAM1 + I, 0);
+      sh = sh + up(F_GAM1 + I, 1);
+      sh = sh + up(F_GAM1 + I, 2);
+      sh = sh - Gd[0] * db[0][I];
+      sh = sh - Gd[1] * db[1][I];
+      sh = sh - Gd[2] * db[2][I];
+      sh = sh + (2.0 / 3.0) * Gd[I] * (divb);
+      double t = 0.0;  // gamma^{IJ} d_K d_J beta^K, J slow, K fast
+#pragma unroll
+      for (int Jx = 0; Jx < 3; ++Jx)
+#pragma unroll
+        for (int Kx = 0; Kx < 3; ++Kx) {
+          const double u = gi[sym(I, Jx)] * ddf(Kx, Jx, F_BETA + Kx);
+          t = (Jx == 0 && Kx == 0) ? u : t + u;
+        }
+      sh = sh + (1.0 / 3.0) * (t);
+      const double w = (gi[0] * ddf(0, 0, F_BETA + I) + gi[3] * ddf(1, 1, F_BETA + I) + gi[5] * ddf(2, 2, F_BETA + I) +
+                        2.0 * (gi[1] * ddf(0, 1, F_BETA + I) + gi[2] * ddf(0, 2, F_BETA + I) +
+                               gi[4] * ddf(1, 2, F_BETA + I)));
+      sh = sh + (w);
+      rhsG[I] = (ns + sh) - ko(F_GAM1 + I);
+      finalize(F_GAM1 + I, rhsG[I]);
+    } else {
+      finalize(F_GAM1 + I, ns + 0.0 - ko(F_GAM1 + I));
+    }
   }
   // ev_DIFFK (bssn.cc:766-795)
   {
     double v = (-DDaTR + alpha * (1.0 / 3.0 * (Kd + 2.0 * theta) * (Kd + 2.0 * theta + 2.0 * bg.K_FRW) + AijAij) +
                 4.0 * kPi * alpha * (S(S_SRC + Q_R) + S(S_SRC + Q_S)) + 4.0 * kPi * alphad * (bg.rho_FRW + bg.S_FRW));
+    if constexpr (SHIFT) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) v = v + up(F_K, d);
+    }
     if (ph.k_damping_amp != 0.0) v = v - 1.0 * ph.k_damping_amp * H * em5phi;
     if constexpr (Z4C) v = v + k1 * (1.0 - k2) * theta;
     finalize(F_K, v - ko(F_K));
   }
   // ev_DIFFphi (bssn.cc:797-820)
-  finalize(F_PHI, (0.1 * ph.a_adj_amp * dt * H - 1.0 / 6.0 * (alpha * (Kd + 2.0 * theta) + alphad * bg.K_FRW - (0.0 + 0.0 + 0.0))) -
-                      ko(F_PHI));
+  {
+    double v = (0.1 * ph.a_adj_amp * dt * H - 1.0 / 6.0 * (alpha * (Kd + 2.0 * theta) + alphad * bg.K_FRW - (divb)));
+    if constexpr (SHIFT) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) v = v + up(F_PHI, d);
+    }
+    finalize(F_PHI, v - ko(F_PHI));
+  }
   // ev_DIFFalpha (bssn.cc:822-831)
-  finalize(F_ALPHA, ev_lapse(ph, bg, alpha, K, Kd, phi) - ko(F_ALPHA));
+  if constexpr (SHIFT) {
+    double v = ev_lapse_shift(ph, bg, alpha, K, Kd, phi, beta, da);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v = v + up(F_ALPHA, d);
+    finalize(F_ALPHA, v - ko(F_ALPHA));
+  } else {
+    finalize(F_ALPHA, ev_lapse(ph, bg, alpha, K, Kd, phi) - ko(F_ALPHA));
+  }
   if constexpr (Z4C) {
     // ev_theta (bssn.cc:834-848)
     double kth = 0.0;
@@ -1229,6 +1390,53 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
                                       16.0 * kPi * (r)) -
                        alpha * k1 * (2.0 + k2) * theta) -
                           kth);
+  }
+  if constexpr (SHIFT) {
+    // ev_beta^i: the shift gauge minus the dissipation (bssn.cc:853-869,
+    // BSSNGaugeHandler.cc:113-146, 156-211, 226-273)
+#pragma unroll
+    for (int I = 0; I < 3; ++I) {
+      double v = 0.0;
+      switch (ph.shift) {
+        case kShiftGammaDriver: v = C(F_AUXB + I); break;
+        case kShiftDampedWave: {
+          // the reference's y and z shifts both read Gamma3
+          const double GamI = C(F_GAM1 + (I == 0 ? 0 : 2));
+          v = beta[0] * db[0][I] + beta[1] * db[1][I];
+          v = v + beta[2] * db[2][I];
+          v = v - ph.dw_mu_s * alpha * beta[I];
+          double X = -gi[sym(I, 0)] * da[0];
+          X = X - gi[sym(I, 1)] * da[1];
+          X = X - gi[sym(I, 2)] * da[2];
+          X = X + alpha * (GamI - 2.0 * (gi[sym(I, 0)] * dphi[0] + gi[sym(I, 1)] * dphi[1] + gi[sym(I, 2)] * dphi[2]));
+          v = v + alpha * (-ph.dw_mu_l * (12.0 * phi * ph.dw_p - log(alpha)) * beta[I] + em4phi * (X));
+          break;
+        }
+        case kShiftAwA: v = ph.gauge_wave_dir == I + 1 ? -2.0 * K * alpha : 0.0; break;
+        case kShiftAijDriver:
+          v = -ph.k_driver_coeff * (fabs(rhsA[sym(I, 0)] + A[sym(I, 0)]) + fabs(rhsA[sym(I, 1)] + A[sym(I, 1)]) +
+                                    fabs(rhsA[sym(I, 2)] + A[sym(I, 2)]));
+          break;
+        default: break;
+      }
+      double kb = 0.0;
+      if (ko_on) {
+        const bool inside = x0 >= RKO && x0 + kBX + RKO <= geo.nx && y0 >= RKO && y0 + kBY + RKO <= geo.ny &&
+                            z0 >= RKO && z0 + kBZ + RKO <= geo.nz;
+        kb = ko_dissipation<O>(a + (size_t)(F_BETA + I) * N, i, j, k, geo.nx, geo.ny, geo.nz, inside, ph.ko_coeff,
+                               ph.dx);
+      }
+      finalize(F_BETA + I, v - kb);
+    }
+    // ev_auxB^i (bssn.cc:879-892)
+#pragma unroll
+    for (int I = 0; I < 3; ++I) finalize(F_AUXB + I, 0.75 * rhsG[I] - ph.gd_eta * C(F_AUXB + I));
+    // ev_expN (bssn.cc:871-875)
+    {
+      double v = beta[0] * d1<O>(gtap(F_EXPN), 0, ph) + beta[1] * d1<O>(gtap(F_EXPN), 1, ph);
+      v = v + beta[2] * d1<O>(gtap(F_EXPN), 2, ph);
+      finalize(F_EXPN, v - alpha * K / 3.0);
+    }
   }
   if (MATTER == kDust) {
 #pragma unroll
@@ -1305,7 +1513,7 @@ __device__ __forceinline__ void init_tile_barriers(uint64_t* bar, bool use) {
 
 // One box: one CTA per brick.  tmap: the TMA map of this substep's input
 // (use_tma = 0: every tile is copied by the threads).
-template <int O, int MATTER, int MODE, bool KO = false, bool Z4C = false>
+template <int O, int MATTER, int MODE, bool KO = false, bool Z4C = false, bool SHIFT = false>
 __global__ void __launch_bounds__(kThreads, 2)
 stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage, const __grid_constant__ CUtensorMap tmap,
              int use_tma, const __grid_constant__ FluxMaps fmaps, int use_fmaps) {
@@ -1313,7 +1521,7 @@ stage_kernel(BoxGeom geo, Physics ph, StageBg bg, StagePtrs P, int stage, const 
   init_tile_barriers(bar, use_tma != 0);
   unsigned phase = 0;
   bool tma_ok = true;
-  stage_body<O, MATTER, MODE, KO, Z4C>(geo, ph, bg, P, stage, blockIdx.z + geo.bx0, blockIdx.y, blockIdx.x,
+  stage_body<O, MATTER, MODE, KO, Z4C, SHIFT>(geo, ph, bg, P, stage, blockIdx.z + geo.bx0, blockIdx.y, blockIdx.x,
                                   blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z),
                                   use_tma ? &tmap : nullptr, bar, phase, tma_ok,
                                   use_tma && use_fmaps ? &fmaps : nullptr);

@@ -16,13 +16,20 @@
 #ifndef CG_Z4C_UNIT
 #define CG_Z4C_UNIT 0
 #endif
+// Built with -DCG_SHIFT_UNIT=1 (parity build only): the shift instantiations
+// of the substep kernel (launch_stage_shift), Kreiss-Oliger compiled in.
+#ifndef CG_SHIFT_UNIT
+#define CG_SHIFT_UNIT 0
+#endif
+#define CG_AUX_UNIT (CG_Z4C_UNIT || CG_SHIFT_UNIT)
 
 namespace cg {
 namespace CG_VARIANT_NS {
 
 constexpr bool kZ4cUnit = CG_Z4C_UNIT != 0;
+constexpr bool kShiftUnit = CG_SHIFT_UNIT != 0;
 
-#if !CG_Z4C_UNIT
+#if !CG_AUX_UNIT
 // BSSN::stepInit (bssn.cc:219-226) on the device: the first substep's input
 // is the normalised copy of _p (RK4Register::stepInit + set_DIFFgamma_Aij_norm);
 // for dust also the flux primitives of that input (Dust::stepInit ->
@@ -72,7 +79,7 @@ __global__ void __launch_bounds__(128) init_kernel(BoxGeom geo, Physics ph, Stag
   }
 }
 
-#endif  // !CG_Z4C_UNIT
+#endif  // !CG_AUX_UNIT
 
 namespace {
 dim3 block_dims() { return dim3(32, 4, 1); }
@@ -105,6 +112,19 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
   for (int a = 0; a < 3; ++a) fm.m[a] = fsrc[a];
   constexpr bool Z = kZ4cUnit;
   constexpr size_t smem = stage_smem<O, M, kEvolve, Z>();
+  if constexpr (kShiftUnit) {
+    // one instantiation per order and matter; the dissipation is switched at run time
+    static bool configured_shift = false;
+    if (!configured_shift) {
+      cudaError_t e = cudaFuncSetAttribute(stage_kernel<O, M, kEvolve, true, false, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      configured_shift = true;
+    }
+    stage_kernel<O, M, kEvolve, true, false, true><<<stage_grid(b), stage_block(), smem, st>>>(
+        geo, b.ph, bg, P, stage, map, b.tma, fm, b.fmaps);
+    return cudaGetLastError();
+  }
   if constexpr (O == 2 || O == 8) {
     if (b.ph.ko_coeff != 0.0) {  // Kreiss-Oliger dissipation: its own instantiation
       static bool configured_ko = false;
@@ -131,6 +151,7 @@ cudaError_t go_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t
   return cudaGetLastError();
 }
 
+#if !CG_SHIFT_UNIT
 template <int O, int M>
 cudaError_t go_constraints(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st) {
   StagePtrs P{};
@@ -166,8 +187,9 @@ cudaError_t go_constraints_m(const BoxDev& b, const StageBg& bg, double* cvals, 
     default: return go_constraints<O, kVacuum>(b, bg, cvals, cpart, st);
   }
 }
+#endif  // !CG_SHIFT_UNIT
 
-#if !CG_Z4C_UNIT
+#if !CG_AUX_UNIT
 template <int O, int M>
 cudaError_t go_group(const GroupBox* table, const GroupBg& gb, int stage, int grid, cudaStream_t st) {
   constexpr size_t smem = stage_smem<O, M, kEvolve>();
@@ -213,18 +235,20 @@ int ctas_m(int matter) {
   }
 }
 
-#endif  // !CG_Z4C_UNIT
+#endif  // !CG_AUX_UNIT
 
 template <int O>
 cudaError_t go_stage_m(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
   switch (b.matter) {
     case kDust: return go_stage<O, kDust>(b, bg, stage, st);
     case kScalar: return go_stage<O, kScalar>(b, bg, stage, st);
+#if !CG_SHIFT_UNIT  // static matter has no shift (cg_create rejects it)
     case kStaticMatter: return go_stage<O, kStaticMatter>(b, bg, stage, st);
+#endif
     default: return go_stage<O, kVacuum>(b, bg, stage, st);
   }
 }
-#if !CG_Z4C_UNIT
+#if !CG_AUX_UNIT
 template <int O>
 bool encode_maps(BoxDev& b) {
   using G = TileG<O>;
@@ -246,10 +270,10 @@ bool encode_maps(BoxDev& b) {
   }
   return true;
 }
-#endif  // !CG_Z4C_UNIT
+#endif  // !CG_AUX_UNIT
 }  // namespace
 
-#if !CG_Z4C_UNIT
+#if !CG_AUX_UNIT
 void make_tile_maps(BoxDev& b) {
   bool ok = false;
   switch (b.order) {
@@ -262,13 +286,21 @@ void make_tile_maps(BoxDev& b) {
   b.maps = b.tma = ok ? 1 : 0;
 }
 
-#endif  // !CG_Z4C_UNIT
+#endif  // !CG_AUX_UNIT
+
+#if !CG_AUX_UNIT && !CG_REFERENCE_ORDER
+// the shift is built into the parity build only; cg_create accepts it with CG_PREC_FP64 alone
+cudaError_t launch_stage_shift(const BoxDev&, const StageBg&, int, cudaStream_t) { return cudaErrorNotSupported; }
+#endif
 
 #if CG_Z4C_UNIT
 cudaError_t launch_stage_z4c(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
+#elif CG_SHIFT_UNIT
+cudaError_t launch_stage_shift(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
 #else
 cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStream_t st) {
   if (b.z4c) return launch_stage_z4c(b, bg, stage, st);
+  if (b.shift) return launch_stage_shift(b, bg, stage, st);
 #endif
   switch (b.order) {
     case 2: return go_stage_m<2>(b, bg, stage, st);
@@ -279,6 +311,7 @@ cudaError_t launch_stage(const BoxDev& b, const StageBg& bg, int stage, cudaStre
   }
 }
 
+#if !CG_SHIFT_UNIT  // shift boxes take the constraint statistics of the plain kernels
 #if CG_Z4C_UNIT
 cudaError_t launch_constraints_z4c(const BoxDev& b, const StageBg& bg, double* cvals, double* cpart, cudaStream_t st) {
 #else
@@ -293,8 +326,9 @@ cudaError_t launch_constraints(const BoxDev& b, const StageBg& bg, double* cvals
     default: return cudaErrorInvalidValue;
   }
 }
+#endif  // !CG_SHIFT_UNIT
 
-#if !CG_Z4C_UNIT
+#if !CG_AUX_UNIT
 cudaError_t launch_group(const GroupBox* table, const GroupBg& gb, int order, int matter, int stage, int grid,
                          cudaStream_t st) {
   switch (order) {
@@ -328,16 +362,17 @@ cudaError_t launch_init(const BoxDev& b, const StageBg& bg, cudaStream_t st) {
     case kStaticMatter: init_kernel<kStaticMatter><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
     default: init_kernel<kVacuum><<<grid_dims(b), block_dims(), 0, st>>>(geo, b.ph, bg, b.P, b.X, b.FP0); break;
   }
-  if (b.z4c) {  // theta: not normalised, copied as it is
-    const size_t pts = (size_t)b.pts;
-    cudaError_t e = cudaMemcpyAsync(b.X + (size_t)(b.nfields - 1) * pts, b.P + (size_t)(b.nfields - 1) * pts,
-                                    pts * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  const int extra = (b.z4c ? 1 : 0) + (b.shift ? 7 : 0);
+  if (extra) {  // theta and the shift fields: not normalised, copied as they are
+    const size_t pts = (size_t)b.pts, f0 = (size_t)(b.nfields - extra);
+    cudaError_t e = cudaMemcpyAsync(b.X + f0 * pts, b.P + f0 * pts, (size_t)extra * pts * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return e;
   }
   return cudaGetLastError();
 }
 
-#endif  // !CG_Z4C_UNIT
+#endif  // !CG_AUX_UNIT
 
 }  // namespace CG_VARIANT_NS
 }  // namespace cg

@@ -32,6 +32,7 @@ enum Lapse : int {
   kAwAGaugeWave, kAwAShiftedWave, kDampedWave
 };
 enum Potential : int { kPotConst = 0, kPotQuadratic = 1 };
+enum Shift : int { kShiftNone = 0, kShiftStatic, kShiftGammaDriver, kShiftDampedWave, kShiftAwA, kShiftAijDriver };
 
 // Per-box physics parameters shared by all stage kernels.
 struct Physics {
@@ -42,6 +43,9 @@ struct Physics {
   double a_adj_amp, k_damping_amp, gd_c, dw_mu_l, dw_p;
   double pot_const, pot_mass;
   double ko_coeff;        // KO_damping_coefficient (orders 2 and 8)
+  int shift;              // Shift gauge (kShiftNone: no shift fields)
+  int gauge_wave_dir;     // AwAShiftedWave direction, 1..3
+  double gd_eta, dw_mu_s, k_driver_coeff;
 };
 
 // Background values for one substep (FRW stage values, grid averages).

@@ -33,6 +33,11 @@ class BoxConfig:
     gd_c: float = 1.0
     dw_mu_l: float = 0.0
     dw_p: float = 0.0
+    shift: str = "Static"   # the shift gauge of a box whose state carries the shift fields
+    gd_eta: float = 0.0
+    dw_mu_s: float = 0.0
+    gauge_wave_dir: int = 1
+    k_driver_coeff: float = 0.04
     x_ghost: int = 0  # > 0: the box is an x-slab with this many ghost planes per face (cosmograph_b200.slab)
 
 
@@ -51,6 +56,9 @@ def make_desc(state: BoxState, cfg: BoxConfig) -> _lib.BoxDesc:
     d.pot_const, d.pot_mass = cfg.pot_const, cfg.pot_mass
     d.x_ghost = cfg.x_ghost
     d.z4c = 1 if state.z4c else 0
+    d.shift = _lib.SHIFT[cfg.shift] if state.shift else 0
+    d.gauge_wave_dir, d.gd_eta, d.dw_mu_s = cfg.gauge_wave_dir, cfg.gd_eta, cfg.dw_mu_s
+    d.k_driver_coeff = cfg.k_driver_coeff
     d.frw_phi, d.frw_K = state.frw_phi, state.frw_K
     d.nfluids = len(state.fluids)
     for n, (rho, w) in enumerate(state.fluids):
@@ -109,7 +117,7 @@ class Evolution:
 
     def download(self, box: int = 0) -> BoxState:
         t = self.templates[box]
-        out = np.empty((num_fields(t.matter),) + t.shape, dtype=np.float64)
+        out = np.empty((num_fields(t.matter, t.z4c, t.shift),) + t.shape, dtype=np.float64)
         self._check(self.L.cg_download_state(self.ctx, box, _dptr(out), out.size))
         st = dataclasses.replace(t, fields=out)
         frw = np.zeros(2 + 4)

@@ -167,7 +167,7 @@ class BSSN {
   bool created() const { return c != nullptr; }
   int matter() const { return d.matter; }
   size_t points() const { return (size_t)d.nx * d.ny * d.nz; }
-  int num_fields() const { return cg_num_fields(d.matter) + d.z4c; }
+  int num_fields() const { return cg_num_fields(d.matter) + d.z4c + (d.shift != CG_SHIFT_NONE ? 7 : 0); }
   RK4Register* reg(const std::string& name);    // registers of one field
   int field_index(const std::string& name) const;
   void check(int rc, const char* what);

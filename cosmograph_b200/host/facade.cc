@@ -40,6 +40,19 @@ int lapse_code(const std::string& name) {
   return it->second;
 }
 
+// shift gauges (BSSNGaugeHandler.h:113-134)
+int shift_code(const std::string& name) {
+  static const std::map<std::string, int> m = {
+      {"Static", CG_SHIFT_STATIC}, {"GammaDriver", CG_SHIFT_GAMMA_DRIVER}, {"DampedWave", CG_SHIFT_DAMPED_WAVE},
+      {"AwAShiftedWave", CG_SHIFT_AWA_SHIFTED_WAVE}, {"AijDriverShift", CG_SHIFT_AIJ_DRIVER}};
+  auto it = m.find(name);
+  if (it == m.end()) raise(-1, "Shift gauge not found: `" + name + "`");
+  return it->second;
+}
+
+// names of the fields after the matter fields: theta (Z4c), then the shift's
+const char* const kShiftNames[7] = {"beta1", "beta2", "beta3", "auxB1", "auxB2", "auxB3", "expN"};
+
 int matter_code(const std::string& sim) {
   if (sim == "dust") return CG_MATTER_DUST;
   if (sim == "scalar") return CG_MATTER_SCALAR;
@@ -206,7 +219,17 @@ BSSN::BSSN(ConfigParser* config) {
   else if (prec == "mixed") d.precision = CG_PREC_MIXED;
   else raise(-1, "precision `" + prec + "` (fp64, fp64_fma or mixed)");
   d.lapse = lapse_code(c("lapse", "Static"));
-  if (c("shift", "Static") != "Static") raise(-1, "non-zero shift is not on this path");
+  // the reference's compile-time USE_BSSN_SHIFT (with USE_GAMMA_DRIVER,
+  // cosmo_macros.h:43-50) as the config key BSSN_shift; the gauge is `shift`
+  // (BSSNGaugeHandler.h:200-223)
+  const std::string shift = c("shift", "Static");
+  const bool with_shift = std::stoi(c("BSSN_shift", "0")) != 0;
+  if (!with_shift && shift != "Static") raise(-1, "a non-Static shift needs BSSN_shift = 1 (USE_BSSN_SHIFT)");
+  d.shift = with_shift ? shift_code(shift) : CG_SHIFT_NONE;
+  d.gauge_wave_dir = std::stoi(c("gauge_wave_dir", "1"));
+  d.gd_eta = std::stod(c("gd_eta", "0.0"));
+  d.dw_mu_s = std::stod(c("dw_mu_s", "0.0"));
+  d.k_driver_coeff = std::stod(c("k_driver_coeff", "0.04"));
   d.normalize_metric = std::stoi(c("normalize_metric", "1"));
   // the reference's compile-time USE_Z4c_DAMPING (cosmo_macros.h:91-100) as a config key
   d.z4c = std::stoi(c("Z4c_damping", "0")) != 0 ? 1 : 0;
@@ -238,9 +261,10 @@ BSSN::~BSSN() {
 void BSSN::ensure_fields() {
   regs.clear();
   fields.clear();
-  const int nf = cg_num_fields(d.matter) + d.z4c;
+  const int nb = cg_num_fields(d.matter), nf = num_fields();
   for (int f = 0; f < nf; ++f) {
-    const std::string nm = f < cg_num_fields(d.matter) ? cg_field_name(d.matter, f) : "theta";
+    const std::string nm = f < nb ? cg_field_name(d.matter, f)
+                                  : (d.z4c && f == nb ? "theta" : kShiftNames[f - nb - d.z4c]);
     regs.push_back(std::make_unique<RK4Register>(this, f, nm));
     RK4Register* r = regs.back().get();
     fields[nm + "_p"] = &r->_array_p;
@@ -259,6 +283,9 @@ int BSSN::field_index(const std::string& name) const {
   for (int f = 0; f < cg_num_fields(d.matter); ++f)
     if (name == cg_field_name(d.matter, f)) return f;
   if (d.z4c && name == "theta") return cg_num_fields(d.matter);
+  if (d.shift != CG_SHIFT_NONE)
+    for (int q = 0; q < 7; ++q)
+      if (name == kShiftNames[q]) return cg_num_fields(d.matter) + d.z4c + q;
   raise(-1, "no field `" + name + "` in this box");
 }
 
@@ -353,7 +380,10 @@ void BSSN::loadState(const std::string& path) {
                   std::to_string(d.matter));
   const int z4c = (h.reserved & 1) ? 1 : 0;  // the header's flags: theta after the matter fields
   if (z4c != d.z4c) raise(-1, path + (z4c ? " carries theta; set Z4c_damping = 1" : " carries no theta (Z4c_damping = 1)"));
-  if (h.nfields != cg_num_fields(h.matter) + z4c || h.nfluids < 0 || h.nfluids > 4 || h.nx <= 0 || h.ny <= 0 ||
+  const int shift = (h.reserved & 2) ? 1 : 0;  // flag bit 1: the shift fields after those
+  if (shift != (d.shift != CG_SHIFT_NONE ? 1 : 0))
+    raise(-1, path + (shift ? " carries the shift; set BSSN_shift = 1" : " carries no shift (BSSN_shift = 1)"));
+  if (h.nfields != cg_num_fields(h.matter) + z4c + 7 * shift || h.nfluids < 0 || h.nfluids > 4 || h.nx <= 0 || h.ny <= 0 ||
       h.nz <= 0)
     raise(-1, path + ": inconsistent header");
   if (c) raise(-1, "initial data must be loaded before the box is on the GPU");
@@ -385,7 +415,7 @@ void BSSN::saveState(const std::string& path, int step) {
   h.nz = d.nz;
   h.nfields = num_fields();
   h.matter = d.matter;
-  h.reserved = d.z4c ? 1 : 0;  // flags: theta after the matter fields
+  h.reserved = (d.z4c ? 1 : 0) | (d.shift != CG_SHIFT_NONE ? 2 : 0);  // flags: theta, then the shift fields
   h.step = step;
   h.dx = d.dx;
   h.dt = d.dt;

@@ -125,9 +125,9 @@ def gaussian_random_field(shape, seed: int, spectrum, rms: float) -> np.ndarray:
     return field * (rms / s) if s > 0 else field
 
 
-def _empty(shape, matter, dx, dt, z4c: bool = False, **kw) -> BoxState:
-    return BoxState(fields=np.zeros((len(field_names(matter, z4c)),) + tuple(shape)), matter=matter,
-                    dx=dx, dt=dt, z4c=z4c, **kw)
+def _empty(shape, matter, dx, dt, z4c: bool = False, shift: bool = False, **kw) -> BoxState:
+    return BoxState(fields=np.zeros((len(field_names(matter, z4c, shift)),) + tuple(shape)), matter=matter,
+                    dx=dx, dt=dt, z4c=z4c, shift=shift, **kw)
 
 
 # ---------------------------------------------------------------------------
@@ -255,15 +255,18 @@ def grf_scalar(n, seed: int = 9, phi0: float = 1.0e-2, rms: float = 1.0e-5, mass
 
 
 def perturbed(shape, matter: int, seed: int = 1, amp: float = 1.0e-2, modes: int = 3,
-              box_len: float = 1.0, dt_frac: float = 0.1, z4c: bool = False) -> BoxState:
+              box_len: float = 1.0, dt_frac: float = 0.1, z4c: bool = False,
+              shift: bool = False) -> BoxState:
     """Every field = background + amp * (a few random smooth periodic modes,
     each a product of one sine per axis).  Backgrounds: DIFFK = -3,
     D = 3/(8 pi), alpha = 1 (DIFFalpha = 0), scalar phi = 0.1; everything
-    else 0 (with z4c, theta too).  Not a solution of the constraints: it
+    else 0 (with z4c, theta too; with the shift, beta^i, auxB^i and expN,
+    beta^i at ten times the amplitude, so that the advection terms of both
+    signs matter).  Not a solution of the constraints: it
     exercises every term of the right-hand side."""
     shape = tuple(shape)
     dx = box_len / shape[0]
-    st = _empty(shape, matter, dx, default_dt(dx, dt_frac), z4c=z4c)
+    st = _empty(shape, matter, dx, default_dt(dx, dt_frac), z4c=z4c, shift=shift)
     rng = np.random.Generator(np.random.MT19937(seed))
     x = [np.arange(m, dtype=np.float64) / m for m in shape]
     for f, name in enumerate(st.names):
@@ -278,6 +281,8 @@ def perturbed(shape, matter: int, seed: int = 1, amp: float = 1.0e-2, modes: int
             v = RHO_FRW * v            # keep the density positive
         if matter == STATIC and name == "DIFFK":
             base = 0.0                 # K sits in the FRW background
+        if name.startswith("beta"):
+            v = 10.0 * v
         st.fields[f] = base + v
     if matter in (DUST, STATIC):
         st.lam = 1.0e-6 * RHO_FRW

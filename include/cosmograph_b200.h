@@ -66,8 +66,18 @@ extern "C" {
 #define CG_PREC_FP64_FMA 1  /* FP64 with FMA contraction                          */
 #define CG_PREC_MIXED 2     /* FP32 perturbations about an FP64 uniform background,
                                FP32 stencils and right-hand side, FP64 RK registers
-                               (vacuum, dust or scalar; Harmonic or Static lapse;
-                               trivial FRW reference)                               */
+                               (vacuum, dust or scalar; every lapse; Kreiss-Oliger;
+                               trivial FRW reference; no Z4c, shift or
+                               a_adj_amp / k_damping_amp)                           */
+
+/* shift gauges (BSSNGaugeHandler.h:113-134); a box with a shift carries the
+ * reference's USE_BSSN_SHIFT and USE_GAMMA_DRIVER fields */
+#define CG_SHIFT_NONE 0             /* no shift fields                           */
+#define CG_SHIFT_STATIC 1           /* "Static": beta^i fixed (advection stays)  */
+#define CG_SHIFT_GAMMA_DRIVER 2     /* "GammaDriver": d_t beta^i = B^i           */
+#define CG_SHIFT_DAMPED_WAVE 3      /* "DampedWave"                              */
+#define CG_SHIFT_AWA_SHIFTED_WAVE 4 /* "AwAShiftedWave"                          */
+#define CG_SHIFT_AIJ_DRIVER 5       /* "AijDriverShift"                          */
 
 /* scalar potentials */
 #define CG_POT_CONST 0      /* V = pot_const, dV = 0 (components/scalar/scalar.cc:262-274) */
@@ -121,6 +131,20 @@ typedef struct {
                               stored after the matter fields (cg_num_fields + 1
                               fields); FP64 precisions only                    */
   double fluid_rho[4], fluid_w[4];
+  int shift;               /* CG_SHIFT_*.  Not CG_SHIFT_NONE: the shift beta^i,
+                              the Gamma-driver's B^i and expN (the reference
+                              built with USE_BSSN_SHIFT and USE_GAMMA_DRIVER,
+                              cosmo_macros.h:43-50) are evolved and stored
+                              after the matter fields as beta1..3, auxB1..3,
+                              expN (cg_num_fields + 7 fields), every field is
+                              advected with upwinded stencils (the reference
+                              defines them for orders 2 and 4; zero at 6 and
+                              8).  CG_PREC_FP64 only; vacuum, dust or scalar;
+                              no Z4c, no x-slab; >= 4 points per axis        */
+  int gauge_wave_dir;      /* config gauge_wave_dir (AwAShiftedWave), default 1 */
+  double gd_eta;           /* config gd_eta (B^i damping), default 0            */
+  double dw_mu_s;          /* config dw_mu_s (DampedWave shift), default 0      */
+  double k_driver_coeff;   /* config k_driver_coeff (AijDriverShift), 0.04      */
 } cg_box_desc;
 
 /* Fill a descriptor with the reference's defaults (Harmonic lapse, order 8,

@@ -99,6 +99,8 @@ def make_params(state, order: int, lapse: str = "Harmonic", normalize_metric: in
                 potential: str = "const", pot_const: float = 3.0e-4, pot_mass: float = 1.0,
                 ko_coeff: float = 0.0, a_adj_amp: float = 0.0, k_damping_amp: float = 0.0,
                 gd_c: float = 1.0, dw_mu_l: float = 0.0, dw_p: float = 0.0) -> CgoParams:
+    if getattr(state, "shift", False):
+        raise ValueError("the restatement has no shift: shift runs are checked against the reference build (oracle/_ref)")
     nx, ny, nz = state.shape
     p = CgoParams()
     p.nx, p.ny, p.nz = nx, ny, nz
@@ -185,14 +187,24 @@ def frw_evolve(phi: float, K: float, fluids, h: float, steps: int):
 # the reference's own sources (oracle/_ref)
 # ---------------------------------------------------------------------------
 
+# gauge keys written only when a run sets them (BSSNGaugeHandler.h:137-147,
+# bssn.cc:18); the reference's defaults apply otherwise
+GAUGE_KEYS = ("shift", "gd_c", "gd_eta", "dw_mu_l", "dw_mu_s", "dw_p", "gauge_wave_dir", "k_driver_coeff")
+
+
 def reference_config_text(lapse: str = "Harmonic", normalize_metric: int = 1,
                           ko_coeff: float = 0.0, a_adj_amp: float = 0.0,
-                          k_damping_amp: float = 0.0, **_ignored) -> str:
+                          k_damping_amp: float = 0.0, **extra) -> str:
     """The reference's `key = value` config keys read by the BSSN constructor
     (components/bssn/bssn.cc:15-22) and the gauge handler."""
-    return (f"lapse = {lapse}\nnormalize_metric = {normalize_metric}\n"
+    text = (f"lapse = {lapse}\nnormalize_metric = {normalize_metric}\n"
             f"KO_damping_coefficient = {ko_coeff!r}\na_adj_amp = {a_adj_amp!r}\n"
             f"k_damping_amp = {k_damping_amp!r}\n")
+    for key in GAUGE_KEYS:
+        if extra.get(key) is not None:
+            v = extra[key]
+            text += f"{key} = {v if isinstance(v, (str, int)) else repr(float(v))}\n"
+    return text
 
 
 def run_reference(binary: Path, mode: str, state, steps: int = 1, threads: int = 0,

@@ -52,6 +52,9 @@ FLAVOURS = {
     "strict_cr": ["-O2", "-ffp-contract=off"],
     "strict_z4c": ["-O2", "-ffp-contract=off", "-DUSE_Z4c_DAMPING=1"],
     "strict_cr_z4c": ["-O2", "-ffp-contract=off", "-DUSE_Z4c_DAMPING=1"],
+    # the shift (beta^i, expN, upwinded advection) with the Gamma-driver's auxB^i
+    "strict_shift": ["-O2", "-ffp-contract=off", "-DUSE_BSSN_SHIFT=1", "-DUSE_GAMMA_DRIVER=1"],
+    "strict_cr_shift": ["-O2", "-ffp-contract=off", "-DUSE_BSSN_SHIFT=1", "-DUSE_GAMMA_DRIVER=1"],
     "fast": ["-O3", "-ffast-math", "-march=x86-64-v3"],
 }
 # strict_cr: the strict build linked with correctly rounded exp, expm1 and

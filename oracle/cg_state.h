@@ -24,6 +24,7 @@
 #define CG_STATE_MAGIC "CGSTATE1"
 #define CG_STATE_MAX_FLUIDS 4
 #define CG_STATE_Z4C 1
+#define CG_STATE_SHIFT 2
 
 enum cg_state_matter { CG_STATE_VACUUM = 0, CG_STATE_DUST = 1, CG_STATE_SCALAR = 2, CG_STATE_STATIC = 3 };
 
@@ -31,12 +32,14 @@ typedef struct {
   char magic[8];          /* "CGSTATE1" */
   int32_t nx, ny, nz;     /* grid points per axis */
   int32_t nfields;        /* 18 (vacuum), 22 (dust), 23 (scalar) or 19 (static),
-                             one more with Z4c */
+                             one more with Z4c, seven more with the shift */
   int32_t matter;         /* enum cg_state_matter */
   int32_t step;           /* RK4 steps completed */
   int32_t nfluids;        /* FRW fluids in use (0..CG_STATE_MAX_FLUIDS) */
   int32_t flags;          /* bit 0 (CG_STATE_Z4C): Z4c damping, the constraint
-                             field theta is stored after the matter fields */
+                             field theta is stored after the matter fields;
+                             bit 1 (CG_STATE_SHIFT): the shift, seven fields
+                             beta1..3, auxB1..3, expN stored after those */
   double dx, dt;
   double frw_phi, frw_K;  /* FRW reference background (utils/FRW.h:15-16) */
   double fluid_rho[CG_STATE_MAX_FLUIDS];

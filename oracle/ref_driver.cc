@@ -16,7 +16,9 @@
  *            read from and written back as field 18
  * minus output, NaN checks and ray sheets, which never touch the fields.
  * Built with -DUSE_Z4c_DAMPING=1 (build_ref.py flavours *_z4c) the driver
- * reads and writes theta as the last field.
+ * reads and writes theta after the matter fields; built with
+ * -DUSE_BSSN_SHIFT=1 -DUSE_GAMMA_DRIVER=1 (flavours *_shift), beta1..3,
+ * auxB1..3 and expN after those.
  *
  * Usage: cg_ref_<...> <mode> <config.txt> <state_in> <out> [steps]
  *   mode = evolve      : run <steps> RK4 steps, write the "_p" registers to <out>
@@ -104,6 +106,14 @@ struct Sim {
     }
 #if USE_Z4c_DAMPING
     out.push_back(bssn->fields[std::string("theta_") + r]);  // stored after the matter fields
+#endif
+#if USE_BSSN_SHIFT
+    // then the shift, the Gamma-driver's auxB and expN (bssn_macros.h:73-75)
+    for (const char *n : {"beta1", "beta2", "beta3"}) out.push_back(bssn->fields[std::string(n) + "_" + r]);
+#if USE_GAMMA_DRIVER
+    for (const char *n : {"auxB1", "auxB2", "auxB3"}) out.push_back(bssn->fields[std::string(n) + "_" + r]);
+#endif
+    out.push_back(bssn->fields[std::string("expN_") + r]);
 #endif
     return out;
   }
@@ -204,6 +214,8 @@ int main(int argc, char **argv) {
   if (h.nx != NX || h.ny != NY || h.nz != NZ) die("grid size differs from the compiled N");
   if (((h.flags & CG_STATE_Z4C) != 0) != (USE_Z4c_DAMPING != 0))
     die("the state's Z4c flag differs from the build's USE_Z4c_DAMPING");
+  if (((h.flags & CG_STATE_SHIFT) != 0) != (USE_BSSN_SHIFT != 0))
+    die("the state's shift flag differs from the build's USE_BSSN_SHIFT");
   const long pts = (long)NX * NY * NZ;
   std::vector<double> buf((size_t)h.nfields * pts);
   if (fread(buf.data(), sizeof(double), buf.size(), fin) != buf.size()) die("short data");

@@ -2,7 +2,9 @@
 
 Each fixture holds an input state and the reference's output on it, produced
 by the reference's BSSN / Dust / Scalar / Lambda classes compiled unmodified
-(strict FP build, oracle/build_ref.py) and driven by oracle/ref_driver.cc.
+(strict FP build, oracle/build_ref.py; with USE_Z4c_DAMPING for the *_z4c
+cases, with USE_BSSN_SHIFT and USE_GAMMA_DRIVER for the *_shift cases) and
+driven by oracle/ref_driver.cc.
 Needs the reference checkout, so it runs only where that exists; the
 resulting .npz files are committed and need nothing at test time.
 
@@ -45,6 +47,18 @@ CASES = [
     ("scalar_z4c_o8", S.SCALAR, (9, 10, 8), 8, 18, 2e-2, "evolve", 3, {"lapse": "Harmonic"}),
     ("vacuum_z4c_o2", S.VACUUM, (8, 8, 10), 2, 19, 3e-2, "evolve", 4,
      {"lapse": "OnePlusLog", "ko_coeff": 0.2}),
+    # the shift: the reference built with USE_BSSN_SHIFT and USE_GAMMA_DRIVER
+    # (flavour strict_shift); beta^i at ten times the amplitude of the rest
+    ("dust_shift_o4", S.DUST, (10, 8, 12), 4, 41, 2e-2, "evolve", 3,
+     {"lapse": "Harmonic", "shift": "GammaDriver", "gd_eta": 0.5}),
+    ("scalar_shift_o2", S.SCALAR, (8, 10, 8), 2, 42, 2e-2, "evolve", 3,
+     {"lapse": "OnePlusLog", "shift": "AijDriverShift", "ko_coeff": 0.2}),
+    ("vacuum_shift_o8", S.VACUUM, (10, 10, 9), 8, 43, 2e-2, "evolve", 2,
+     {"lapse": "DampedWave", "shift": "DampedWave", "dw_mu_l": 0.2, "dw_mu_s": 0.3, "dw_p": 0.5,
+      "ko_coeff": 0.1}),
+    ("dust_shift_awa_o4", S.DUST, (8, 12, 10), 4, 44, 2e-2, "evolve", 3,
+     {"lapse": "AwAShiftedWave", "shift": "AwAShiftedWave", "gauge_wave_dir": 2}),
+    ("scalar_shift_o6", S.SCALAR, (9, 8, 10), 6, 45, 2e-2, "evolve", 2, {"lapse": "Harmonic", "shift": "Static"}),
 ]
 
 
@@ -55,7 +69,7 @@ def make_input(name, matter, shape, order, seed, amp):
         return S.BoxState(fields=f, matter=st.matter, dx=st.dx, dt=st.dt, lam=st.lam)
     if name.startswith("grf"):
         return ics.grf_dust(shape, seed=seed, rms_delta=1e-3, order=order)
-    return ics.perturbed(shape, matter, seed=seed, amp=amp, z4c="_z4c" in name)
+    return ics.perturbed(shape, matter, seed=seed, amp=amp, z4c="_z4c" in name, shift="_shift" in name)
 
 
 def main() -> int:
@@ -69,7 +83,7 @@ def main() -> int:
         if only and name not in only:
             continue
         st = make_input(name, matter, shape, order, seed, amp)
-        flavour = "strict_z4c" if st.z4c else "strict"
+        flavour = "strict_z4c" if st.z4c else ("strict_shift" if st.shift else "strict")
         binp = build_ref.build(*shape, order, flavour)
         res, info = oracle.run_reference(binp, mode, st, steps=steps, threads=1, **cfg)
         arrays = {"input": st.fields, "input_header": np.frombuffer(st.header_bytes(), dtype=np.uint8)}

@@ -20,7 +20,7 @@ def _state_from(arr: np.ndarray, header: np.ndarray) -> S.BoxState:
     st = S.BoxState(fields=np.array(arr, dtype=np.float64), matter=hdr[5], dx=hdr[9], dt=hdr[10],
                     step=hdr[6], frw_phi=hdr[11], frw_K=hdr[12],
                     fluids=tuple((hdr[13 + i], hdr[17 + i]) for i in range(hdr[7])), lam=hdr[21],
-                    z4c=bool(hdr[8] & S.FLAG_Z4C))
+                    z4c=bool(hdr[8] & S.FLAG_Z4C), shift=bool(hdr[8] & S.FLAG_SHIFT))
     return st
 
 

@@ -77,6 +77,27 @@ def test_create_rejects_bad_descriptors(L, field, value, msg):
     assert msg in L.cg_last_error(None).decode()
 
 
+@pytest.mark.parametrize("changes,msg", [
+    ({"shift": 6}, "unknown shift gauge"),
+    ({"shift": 2, "precision": 1}, "CG_PREC_FP64 only"),
+    ({"shift": 2, "precision": 2}, "CG_PREC_FP64 only"),
+    ({"shift": 1, "matter": 3, "lapse": 0}, "static matter has no shift"),
+    ({"shift": 1, "z4c": 1}, "do not combine"),
+    ({"shift": 1, "nx": 3, "stencil_order": 2}, "4 points per axis"),
+    ({"shift": 4, "gauge_wave_dir": 4}, "gauge_wave_dir"),
+])
+def test_create_rejects_bad_shift_descriptors(L, changes, msg):
+    d = _lib.BoxDesc()
+    L.cg_box_desc_default(ctypes.byref(d), 16)
+    assert (d.shift, d.gauge_wave_dir, d.k_driver_coeff) == (0, 1, 0.04)
+    for k, v in changes.items():
+        setattr(d, k, v)
+    h = ctypes.c_void_p()
+    rc = L.cg_create(ctypes.byref(d), 1, ctypes.byref(h))
+    assert rc == -1 and not h.value
+    assert msg in L.cg_last_error(None).decode()
+
+
 @pytest.mark.parametrize("n", [0, (1 << 30) + 1, 1 << 31, (1 << 32) + 5])
 def test_noalloc_average_rejects_sizes_before_touching_cuda(L, n):
     """The allocation-free average checks n against its fixed scratch (at most

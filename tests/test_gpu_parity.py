@@ -41,6 +41,8 @@ def floor_for(name: str) -> float:
 @pytest.mark.parametrize("name", GOLDEN_EVOLVE)
 def test_golden_evolve(name, precision):
     inp, out, _, meta = load_golden(name)
+    if inp.shift and precision != "fp64":
+        pytest.skip("the shift is built into the parity build (CG_PREC_FP64) only")
     got = evolve(inp, meta["steps"], cfg_from(meta, precision))
     errs = field_errors(got.fields, out.fields, inp.names, floor=floor_for(name))
     print("golden", name, precision, "worst", worst(errs))

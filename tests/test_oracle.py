@@ -12,7 +12,9 @@ import pytest
 import oracle
 from helpers import field_errors, golden_index, load_golden, worst
 
-EVOLVE_CASES = [k for k, v in golden_index().items() if v["mode"] == "evolve"]
+# the shift fixtures pin the CUDA path on the reference build directly (the
+# restatement has no shift)
+EVOLVE_CASES = [k for k, v in golden_index().items() if v["mode"] == "evolve" and "shift" not in v["config"]]
 
 
 @pytest.mark.parametrize("name", EVOLVE_CASES)
