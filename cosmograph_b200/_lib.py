@@ -38,9 +38,9 @@ EXPORTS = (
     "cg_kavg_sums", "cg_set_kavg", "cg_step_init", "cg_rk_stage", "cg_step", "cg_synchronize",
     "cg_status", "cg_frw_state", "cg_step_count", "cg_last_error", "cg_version",
     "cg_conformal_average", "cg_conformal_average_noalloc", "cg_constraints", "cg_field_statistics",
-    "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust", "cg_fp64_peak",
+    "cg_set_option", "cg_num_groups", "cg_group_info", "cg_ic_grf_dust", "cg_ic_grf_scalar", "cg_fp64_peak",
 )
-OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID, OPT_TMA = 1, 2, 3, 4, 5
+OPT_BATCH, OPT_GRAPH, OPT_AUTOTUNE, OPT_GROUP_GRID, OPT_TMA, OPT_TMA_WAIT = 1, 2, 3, 4, 5, 6
 
 
 class BoxDesc(ctypes.Structure):
@@ -112,6 +112,8 @@ def load() -> ctypes.CDLL:
         "cg_field_statistics": (i, [vp, i, dp, i]),
         "cg_set_option": (i, [vp, i, i]),
         "cg_ic_grf_dust": (i, [vp, i, dp, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
+        "cg_ic_grf_scalar": (i, [vp, i, dp, ctypes.c_uint64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double]),
         "cg_num_groups": (i, [vp, ctypes.POINTER(i)]),
         "cg_group_info": (i, [vp, i, ctypes.POINTER(i), i]),
         "cg_version": (i, []),

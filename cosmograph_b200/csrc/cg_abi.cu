@@ -164,6 +164,10 @@ int cuda_fail(cg_ctx* ctx, cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
   } while (0)
 
+// cycles a CTA waits for a TMA tile copy before it flags CG_STATUS_TILE_TIMEOUT
+// (about a second; CG_OPT_TMA_WAIT changes it)
+constexpr long long kTmaWaitDefault = 2000000000LL;
+
 bool lapse_needs_kavg(int lapse) {
   return lapse == CG_LAPSE_CONFORMAL_FLRW || lapse == CG_LAPSE_ANHARMONIC || lapse == CG_LAPSE_ONE_PLUS_LOG;
 }
@@ -597,6 +601,7 @@ int mixed_prepare(cg_ctx* ctx, Box& b, int n, cg::mixed::Bg* out) {
     const double al = 1.0 + b.ba[cg::F_ALPHA];
     bg.dw_u = b.desc.dw_mu_l * (12.0 * b.ba[cg::F_PHI] * b.desc.dw_p - std::log(al)) - b.ba[cg::F_K];
   }
+  bg.tma_wait = b.dev.ph.tma_wait;
   bg.ko_scale = b.desc.stencil_order == 2 ? b.desc.ko_coeff / (64.0 * b.desc.dx)
                                           : -b.desc.ko_coeff / (1024.0 * b.desc.dx);
   for (int f = 0; f < 23; ++f) {
@@ -879,6 +884,7 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
     ph.gd_eta = d.gd_eta;
     ph.dw_mu_s = d.dw_mu_s;
     ph.k_driver_coeff = d.k_driver_coeff;
+    ph.tma_wait = kTmaWaitDefault;
     b.frw.phi = d.frw_phi;
     b.frw.K = d.frw_K;
     b.frw.n = d.nfluids;
@@ -1642,6 +1648,32 @@ int cg_ic_grf_dust(cg_ctx* ctx, int box, const double* delta, uint64_t seed, dou
   return CG_OK;
 }
 
+int cg_ic_grf_scalar(cg_ctx* ctx, int box, const double* dphi, uint64_t seed, double phi0, double rms,
+                     double mass, double cutoff) {
+  int rc = check_box(ctx, box);
+  if (rc) return rc;
+  Box& b = ctx->boxes[box];
+  if (b.desc.matter != CG_MATTER_SCALAR) return fail(ctx, CG_ERR_INVALID, "GRF scalar initial data need a scalar box");
+  if (!(rms >= 0.0) || !std::isfinite(phi0) || !std::isfinite(mass))
+    return fail(ctx, CG_ERR_INVALID, "rms >= 0, finite phi0 and mass");
+  for (Box& o : ctx->boxes)
+    if (o.stage_next > 1) return fail(ctx, CG_ERR_STATE, "initial data are set between steps");
+  const cg::GridSpec gs{b.desc.nx, b.desc.ny, b.desc.nz, b.desc.stencil_order, b.desc.dx};
+  const double kc = cutoff > 0.0 ? cutoff : std::min({gs.nx, gs.ny, gs.nz}) / 4.0;
+  if (b.dev.nfields > cg_num_fields(CG_MATTER_SCALAR))  // Z4c's theta and the shift fields start at zero
+    CG_CUDA(ctx, cudaMemsetAsync(b.dev.P, 0, sizeof(double) * (size_t)b.dev.nfields * b.dev.pts, ctx->stream));
+  double* scratch = nullptr;
+  CG_CUDA(ctx, cudaMalloc(&scratch, sizeof(double) * cg::ics::grf_scratch_doubles(gs)));
+  std::string err;
+  rc = cg::ics::grf_scalar(gs, b.dev.P, scratch, dphi, seed, rms, phi0, mass, kc, ctx->stream, err);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(scratch);
+  if (rc) return fail(ctx, rc, "GRF scalar initial data: " + err);
+  b.stage_next = 0;
+  b.steps = 0;
+  return CG_OK;
+}
+
 int cg_set_option(cg_ctx* ctx, int option, int value) {
   if (!ctx) return CG_ERR_INVALID;
   switch (option) {
@@ -1652,6 +1684,13 @@ int cg_set_option(cg_ctx* ctx, int option, int value) {
         ctx->opt_batch = value != 0;
         ctx->grouped = false;
       }
+      return CG_OK;
+    case CG_OPT_TMA_WAIT:
+      for (Box& b : ctx->boxes)
+        if (b.stage_next > 1) return fail(ctx, CG_ERR_STATE, "change CG_OPT_TMA_WAIT between steps");
+      if (value < 0) return fail(ctx, CG_ERR_INVALID, "CG_OPT_TMA_WAIT takes a cycle count >= 0");
+      for (Box& b : ctx->boxes) b.dev.ph.tma_wait = value > 0 ? (long long)value : kTmaWaitDefault;
+      ctx->grouped = false;  // the group tables carry the boxes' parameters
       return CG_OK;
     case CG_OPT_TMA:
       for (Box& b : ctx->boxes)

@@ -18,6 +18,13 @@
 //   D          = e^{6 phi} (rho_ADM - rho_Lambda)                  (:135)
 // The random field of this file uses its own counter-based generator; given
 // the same delta the result matches the host construction to rounding.
+//
+// Scalar-field initial data (grf_scalar, the host version ics.grf_scalar):
+//   dphi       seeded Gaussian random field, P(k) ~ k^-3 for k <= kc, else 0,
+//              zero mean, rms normalised (or a caller-supplied field)
+//   phi        = phi0 + dphi, Pi = 0, psi_a = d_a phi (the relation of the
+//              reference's wave data, components/scalar/scalar_ic.cc:43-48)
+//   DIFFK      = -sqrt(24 pi rho), rho = m^2 phi^2 / 2 + |d phi|^2 / 2
 #include <cufft.h>
 
 #include <cmath>
@@ -44,15 +51,18 @@ __device__ inline uint64_t mix64(uint64_t z) {
 }
 __device__ inline double u01(uint64_t x) { return ((double)(x >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
 
-// complex Gaussian noise times sqrt(P(k)) on the half spectrum (nx, ny, nz/2+1)
-__global__ void noise_kernel(cufftDoubleComplex* out, int nx, int ny, int nz, uint64_t seed, double ns, double kc) {
+// complex Gaussian noise times sqrt(P(k)) on the half spectrum (nx, ny, nz/2+1);
+// P(k) = k^ns exp(-(k/kc)^2) (sharp = 0) or k^ns for k <= kc, else 0 (sharp = 1)
+__global__ void noise_kernel(cufftDoubleComplex* out, int nx, int ny, int nz, uint64_t seed, double ns, double kc,
+                             int sharp) {
   const int nzh = nz / 2 + 1;
   const long long total = (long long)nx * ny * nzh;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(q % nzh), j = (int)((q / nzh) % ny), i = (int)(q / ((long long)nzh * ny));
     const double px = freq(i, nx), py = freq(j, ny), pz = k;
     const double kk = sqrt(px * px + py * py + pz * pz);
-    const double amp = kk > 0.0 ? sqrt(pow(kk, ns) * exp(-(kk / kc) * (kk / kc))) : 0.0;
+    const double pk = sharp ? (kk <= kc ? pow(kk, ns) : 0.0) : pow(kk, ns) * exp(-(kk / kc) * (kk / kc));
+    const double amp = kk > 0.0 ? sqrt(pk) : 0.0;
     const uint64_t base = mix64(seed ^ 0x9e3779b97f4a7c15ULL);
     const double u1 = u01(mix64(base + 2 * (uint64_t)q)), u2 = u01(mix64(base + 2 * (uint64_t)q + 1));
     const double r = sqrt(-2.0 * log(u1));
@@ -259,6 +269,33 @@ __global__ void assemble_kernel(Grid g, const double* phiN, const double* lapPhi
   }
 }
 
+// phi0 + dphi
+__global__ void offset_kernel(double* out, const double* in, long long n, double phi0) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    out[q] = phi0 + in[q];
+}
+
+// scalar fields, psi_a, DIFFK; every other field zero (23 fields)
+__global__ void assemble_scalar_kernel(Grid g, const double* phi, double mass, double* P) {
+  const long long N = (long long)g.nx * g.ny * g.nz;
+  CG_IC_LOOP(g) {
+    const int k = (int)(q % g.nz), j = (int)((q / g.nz) % g.ny), i = (int)(q / ((long long)g.nz * g.ny));
+    double d[3], grad2 = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      d[a] = d1(phi, g, i, j, k, a);
+      grad2 = grad2 + d[a] * d[a];
+    }
+    const double rho = 0.5 * mass * mass * phi[q] * phi[q] + 0.5 * grad2;
+    for (int f = 0; f < 23; ++f) {
+      double v = 0.0;
+      if (f == F_K) v = -sqrt(24.0 * kPiD * rho);
+      else if (f == F_SPHI) v = phi[q];
+      else if (f >= F_SPSI1 && f < F_SPSI1 + 3) v = d[f - F_SPSI1];
+      P[(long long)f * N + q] = v;
+    }
+  }
+}
+
 int blocks_for(long long n) {
   const long long b = (n + kT - 1) / kT;
   return (int)(b < 4096 ? b : 4096);
@@ -315,7 +352,7 @@ int grf_dust(const GridSpec& s, double* P, double* scratch, const double* delta_
     if (delta_host) {
       ok = cu(cudaMemcpyAsync(delta, delta_host, sizeof(double) * N, cudaMemcpyHostToDevice, st), "upload delta");
     } else {
-      noise_kernel<<<nb, kT, 0, st>>>(spec, s.nx, s.ny, s.nz, seed, ns, kc);
+      noise_kernel<<<nb, kT, 0, st>>>(spec, s.nx, s.ny, s.nz, seed, ns, kc, 0);
       ok = cu(cudaGetLastError(), "noise_kernel") && ff(cufftExecZ2D(inv, spec, delta), "cufftExecZ2D");
       if (ok) {
         // zero mean, rms normalised (population standard deviation)
@@ -363,6 +400,57 @@ int grf_dust(const GridSpec& s, double* P, double* scratch, const double* delta_
     return CG_ERR_INVALID;
   }
   return CG_OK;
+}
+
+// Scalar-field initial data; scratch as for grf_dust.  dphi_host: optional
+// host copy of the fluctuation.
+int grf_scalar(const GridSpec& s, double* P, double* scratch, const double* dphi_host, uint64_t seed, double rms,
+               double phi0, double mass, double kc, cudaStream_t st, std::string& err) {
+  const long long N = (long long)s.nx * s.ny * s.nz;
+  double* dphi = scratch;
+  double* phi = scratch + N;
+  auto* spec = reinterpret_cast<cufftDoubleComplex*>(scratch + 9 * N);
+  double* red = scratch + 9 * N + 2 * (long long)s.nx * s.ny * (s.nz / 2 + 1);
+  const Grid g{s.nx, s.ny, s.nz, s.order, 1.0 / s.dx};
+  const int nb = blocks_for(N);
+  cufftHandle inv = 0;
+  auto cu = [&](cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+  };
+  bool ok = true;
+  if (dphi_host) {
+    ok = cu(cudaMemcpyAsync(dphi, dphi_host, sizeof(double) * N, cudaMemcpyHostToDevice, st), "upload dphi");
+  } else {
+    cufftResult r = cufftPlan3d(&inv, s.nx, s.ny, s.nz, CUFFT_Z2D);
+    if (r == CUFFT_SUCCESS) r = cufftSetStream(inv, st);
+    if (r == CUFFT_SUCCESS) {
+      noise_kernel<<<nb, kT, 0, st>>>(spec, s.nx, s.ny, s.nz, seed, -3.0, kc, 1);
+      ok = cu(cudaGetLastError(), "noise_kernel");
+      if (ok) r = cufftExecZ2D(inv, spec, dphi);
+    }
+    if (r != CUFFT_SUCCESS) {
+      err = "cuFFT error " + std::to_string((int)r);
+      ok = false;
+    }
+    if (ok) {
+      // zero mean, rms normalised (population standard deviation)
+      moment_kernel<<<nb, kT, 0, st>>>(dphi, N, nullptr, red);
+      sum_parts_kernel<<<1, kT, 0, st>>>(red, nb, N, red + 4096);
+      moment_kernel<<<nb, kT, 0, st>>>(dphi, N, red + 4096, red);
+      sum_parts_kernel<<<1, kT, 0, st>>>(red, nb, N, red + 4097);
+      normalise_kernel<<<nb, kT, 0, st>>>(dphi, N, red + 4096, red + 4097, rms);
+      ok = cu(cudaGetLastError(), "normalise");
+    }
+  }
+  if (ok) {
+    offset_kernel<<<nb, kT, 0, st>>>(phi, dphi, N, phi0);
+    assemble_scalar_kernel<<<nb, kT, 0, st>>>(g, phi, mass, P);
+    ok = cu(cudaGetLastError(), "assemble_scalar_kernel") && cu(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+  }
+  if (inv) cufftDestroy(inv);
+  return ok ? CG_OK : CG_ERR_CUDA;
 }
 
 }  // namespace ics

@@ -142,6 +142,8 @@ namespace ics {
 size_t grf_scratch_doubles(const GridSpec& s);
 int grf_dust(const GridSpec& s, double* P, double* scratch, const double* delta_host, uint64_t seed, double rms,
              double ns, double kc, double rho_L, cudaStream_t st, std::string& err);
+int grf_scalar(const GridSpec& s, double* P, double* scratch, const double* dphi_host, uint64_t seed, double rms,
+               double phi0, double mass, double kc, cudaStream_t st, std::string& err);
 }  // namespace ics
 
 // Message returned by cg_last_error(NULL) on this host thread.

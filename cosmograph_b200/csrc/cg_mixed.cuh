@@ -39,8 +39,7 @@ constexpr int kBX = Brick::BX, kBY = Brick::BY, kBZ = Brick::BZ, kThreads = Bric
 // for every stencil order
 template <int O>
 using TileG = tile::Geom<O, Brick, 24, 4>;
-constexpr unsigned kStatusTileTimeout = CG_STATUS_TILE_TIMEOUT;  // a TMA tile copy did not complete
-constexpr long long kTmaWaitCycles = 2000000000;  // about a second
+constexpr unsigned kStatusTileTimeout = CG_STATUS_TILE_TIMEOUT;  // a TMA tile copy was late or lost
 
 struct Ptrs {
   const float* in;     // delta of a^n
@@ -72,6 +71,7 @@ struct Bg {
   double gd_c;                 // 1+log lapse coefficient
   double dw_mu_l, dw_p, dw_u;  // damped-wave lapse: mu_L, p and mu_L (12 p phibar - ln abar) - Kbar
   double ko_scale;             // Kreiss-Oliger: c / (64 dx) (order 2) or -c / (1024 dx) (order 8)
+  long long tma_wait;          // cycles a CTA waits for a TMA tile copy before it flags a timeout
 };
 __host__ __device__ constexpr int bgi(int f) {
   return f == F_K ? 0 : (f == F_PHI ? 1 : (f == F_ALPHA ? 2 : (f == 18 ? 3 : (f == 19 ? 4 : -1))));
@@ -256,17 +256,20 @@ __device__ __forceinline__ void field_derivatives(int it, const T& t, float idx,
 // The tile copies: by TMA (tmap != null, a brick whose halo lies inside the
 // box) or by the threads' own loads with periodic wrap.  Returns false (the
 // same value in every thread) when a TMA copy did not complete within
-// kTmaWaitCycles; the status word then carries kStatusTileTimeout.
+// tma_wait cycles; the status word then carries kStatusTileTimeout.  A late
+// copy is still waited for (tma::wait_drain), so that none is in flight when
+// the tile is reused or the CTA leaves; after a copy that never lands the CTA
+// issues no more.
 template <int O, int MATTER>
 __device__ __forceinline__ bool derivatives(const float* __restrict__ a, int N, float idx, float idx2,
                                             const float gi[6], float* sl, float* tl, const int* rowoff, int tid,
                                             int x0, int y0, int z0, int nz, int cc, const CUtensorMap* tmap,
-                                            uint64_t* bar, unsigned& phase, unsigned* status) {
+                                            uint64_t* bar, unsigned& phase, unsigned* status, long long tma_wait) {
   using G = TileG<O>;
   const tile::Taps<G, float> t{tl, cc};
   constexpr int NIT = 8;  // fields with second derivatives; first-derivative-only fields use global taps
   const bool by_tma = tmap != nullptr;
-  bool ok = true;
+  bool ok = true, lost = false;
   tile::Loader<G, Brick, float> ld;
   if (!by_tma) {
     ld.init(tid, z0, nz);
@@ -276,16 +279,20 @@ __device__ __forceinline__ bool derivatives(const float* __restrict__ a, int N, 
 #pragma unroll 1
   for (int it = 0; it < NIT; ++it) {
     if (by_tma) {
-      tma::fence_proxy_async();  // this thread's shared-memory accesses come before the copy's writes
-      __syncthreads();           // the previous tile has been read
-      if (tid == 0) {
-        tma::arrive_expect_tx(bar, (unsigned)(G::SIZE * sizeof(float)));
-        tma::load_4d(tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, phase1_field(it), bar);
-        // the next field's tile into L2 while this one is used
-        if (it + 1 < NIT) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, phase1_field(it + 1));
+      tma::fence_proxy_async();        // this thread's shared-memory accesses come before the copy's writes
+      lost = __syncthreads_or(lost);   // the previous tile has been read
+      if (!lost) {
+        if (tid == 0) {
+          tma::arrive_expect_tx(bar, (unsigned)(G::SIZE * sizeof(float)));
+          tma::load_4d(tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, phase1_field(it), bar);
+          // the next field's tile into L2 while this one is used
+          if (it + 1 < NIT) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, phase1_field(it + 1));
+        }
+        const int w = tma::wait_drain(bar, phase, tma_wait);
+        ok = ok && w == 0;
+        if (w == 2) lost = true;
+        else phase ^= 1u;
       }
-      if (ok && !tma::wait(bar, phase, kTmaWaitCycles)) ok = false;
-      phase ^= 1u;
     } else {
       __syncthreads();
       ld.store(tl);
@@ -295,7 +302,7 @@ __device__ __forceinline__ bool derivatives(const float* __restrict__ a, int N, 
     field_derivatives<O>(it, t, idx, idx2, gi, sl);
   }
   if (by_tma) {
-    ok = __syncthreads_and(ok);
+    ok = __syncthreads_and(ok && !lost);
     if (!ok && tid == 0) atomicOr(status, kStatusTileTimeout);
   }
   return ok;
@@ -411,7 +418,7 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
     // after a copy timed out the CTA copies by threads (the barrier's phase is unknown)
     tma_ok = derivatives<O, MATTER>(a, N, idx, idx2, gi, sl, tl, rowoff, tid, x0, y0, z0, nz,
                                     tile::centre<G>(threadIdx.z, threadIdx.y, threadIdx.x), by_tma ? tmap : nullptr,
-                                    bar, phase, P.status) && tma_ok;
+                                    bar, phase, P.status, bg.tma_wait) && tma_ok;
     __syncthreads();
   }
   if (!live) return;

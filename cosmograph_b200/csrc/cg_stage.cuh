@@ -65,8 +65,7 @@ struct BoxGeom {
 
 constexpr unsigned kStatusNaN = 1u;
 constexpr unsigned kStatusNonFinite = 2u;
-constexpr unsigned kStatusTileTimeout64 = CG_STATUS_TILE_TIMEOUT;  // a TMA tile copy did not complete
-constexpr long long kTmaWaitCycles64 = 2000000000LL;               // about a second
+constexpr unsigned kStatusTileTimeout64 = CG_STATUS_TILE_TIMEOUT;  // a TMA tile copy was late or lost
 
 template <int MATTER>
 struct NF {
@@ -331,7 +330,10 @@ struct Phase1 {
 // The copies: by TMA when tmap is set (a brick whose halo lies inside the
 // box), else by the threads' own loads with periodic wrap.  Returns false (the
 // same value in every thread) when a TMA copy did not complete within
-// kTmaWaitCycles64; the status word then carries kStatusTileTimeout64.
+// ph.tma_wait cycles; the status word then carries kStatusTileTimeout64.  A
+// late copy is still waited for (tma::wait_drain), so that no copy is in
+// flight when a buffer is reused or the CTA leaves; after a copy that never
+// lands the CTA issues no more.
 template <int O, int MATTER, int MODE, bool Z4C>
 __device__ __forceinline__ void field_derivatives(int it, const tile::Taps<TileG<O>, double>& t, const Physics& ph,
                                                   const double gi[6], double* sl);
@@ -348,22 +350,38 @@ __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N,
   using G = TileG<O>;
   constexpr bool TWO = TileBuffers<O, MATTER, MODE, Z4C>::kTwo;
   constexpr unsigned kBytes = (unsigned)(G::SIZE * sizeof(double));
-  // TMA: field it into buffer it % 2 (one buffer: 0), field it + 1 into L2
+  // TMA: field it into buffer it % 2 (one buffer: 0), field it + 1 into L2;
+  // thread 0 copies, every thread notes the buffer's copy as pending
+  unsigned pending = 0;
   auto issue = [&](int it) {
     const int b = TWO ? (it & 1) : 0;
-    tma::arrive_expect_tx(bar + b, kBytes);
-    tma::load_4d(b ? tl2 : tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it), bar + b);
-    if (it + 1 < PF::N) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it + 1));
+    if (tid == 0) {
+      tma::arrive_expect_tx(bar + b, kBytes);
+      tma::load_4d(b ? tl2 : tl, tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it), bar + b);
+      if (it + 1 < PF::N) tma::prefetch_4d(tmap, z0 - G::ZO, y0 - G::R, x0 - G::R, PF::field(it + 1));
+    }
+    pending |= 1u << b;
+  };
+  // ok: every copy landed within ph.tma_wait cycles; lost: one never landed
+  // (the CTA then issues no more copies, waits for the ones in flight and
+  // returns with the status flagged)
+  bool ok = true, lost = false;
+  auto wait = [&](int b) {
+    if (!(pending & (1u << b))) return;
+    const int w = tma::wait_drain(bar + b, (phase >> b) & 1u, ph.tma_wait);
+    ok = ok && w == 0;
+    pending &= ~(1u << b);
+    if (w == 2) lost = true;
+    else phase ^= 1u << b;
   };
   const bool by_tma = tmap != nullptr;
-  bool ok = true;
   tile::Loader<G, Brick, double> ld;
   tile::AsyncLoader<G, Brick> ald;
   if (by_tma) {
     if (TWO) {
       tma::fence_proxy_async();  // this thread's shared-memory accesses come before the copy's writes
       __syncthreads();
-      if (tid == 0) issue(0);
+      issue(0);
     }
   } else if (TWO) {
     // two buffers: cp.async copies of field it + 1 run while field it is differentiated
@@ -379,14 +397,13 @@ __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N,
     int b = 0;
     if (by_tma) {
       tma::fence_proxy_async();
-      __syncthreads();  // the buffer the next copy writes has been read
-      if (tid == 0) {
+      lost = __syncthreads_or(lost);  // the buffer the next copy writes has been read
+      if (!lost) {
         if (!TWO) issue(it);
         else if (it + 1 < PF::N) issue(it + 1);
       }
       b = TWO ? (it & 1) : 0;
-      if (ok && !tma::wait(bar + b, (phase >> b) & 1u, kTmaWaitCycles64)) ok = false;
-      phase ^= 1u << b;
+      wait(b);
     } else if (TWO) {
       __syncthreads();  // the buffer the next copies write has been read
       if (it + 1 < PF::N) {
@@ -406,7 +423,9 @@ __device__ __forceinline__ bool derivatives(const double* __restrict__ a, int N,
     field_derivatives<O, MATTER, MODE, Z4C>(it, tile::Taps<G, double>{b ? tl2 : tl, cc}, ph, gi, sl);
   }
   if (by_tma) {
-    ok = __syncthreads_and(ok);
+    wait(0);  // after a lost copy: the other buffer's copy in flight
+    wait(1);
+    ok = __syncthreads_and(ok && !lost);
     if (!ok && tid == 0) atomicOr(status, kStatusTileTimeout64);
   }
   return ok;
@@ -548,10 +567,17 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
   static_assert(5 * FB::XB * sizeof(double) <= TileBuffers<O, kDust, kEvolve>::kBytes, "x boxes fit");
   static_assert(5 * FB::ZB * sizeof(double) <= TileBuffers<O, kDust, kEvolve>::kBytes, "z boxes fit");
   static_assert(5 * FB::YB * sizeof(double) <= (size_t)kTileSlots * kThreads * sizeof(double), "y boxes fit");
-  bool ok = true;
+  // as in derivatives: bounded waits that let late copies land; after a lost
+  // copy no more copies, the ones in flight waited for
+  bool ok = true, lost = false;
+  unsigned pending = 0;
   auto wait = [&](int b) {
-    if (ok && !tma::wait(bar + b, (phase >> b) & 1u, kTmaWaitCycles64)) ok = false;
-    phase ^= 1u << b;
+    if (!(pending & (1u << b))) return;
+    const int w = tma::wait_drain(bar + b, (phase >> b) & 1u, ph.tma_wait);
+    ok = ok && w == 0;
+    pending &= ~(1u << b);
+    if (w == 2) lost = true;
+    else phase ^= 1u << b;
   };
   auto load5 = [&](int a, double* dst, uint64_t* b, int len) {
     tma::arrive_expect_tx(b, (unsigned)(5 * len * sizeof(double)));
@@ -566,6 +592,7 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
     load5(0, tl2, bar + 1, FB::XB);
     load5(1, tl, bar, FB::YB);
   }
+  pending = 3u;
   wait(1);
   {
     const int c = ((tx + R) * kBY + ty) * kBZ + tz;
@@ -574,8 +601,11 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
       sl[(S_MAT + m) * kThreads] = d1p_tile<O>(tl2 + (size_t)m * FB::XB, tl2 + (size_t)4 * FB::XB, c, kBY * kBZ, ph);
   }
   tma::fence_proxy_async();
-  __syncthreads();  // the x boxes have been read
-  if (tid == 0) load5(2, tl2, bar + 1, FB::ZB);
+  lost = __syncthreads_or(lost);  // the x boxes have been read
+  if (!lost) {
+    if (tid == 0) load5(2, tl2, bar + 1, FB::ZB);
+    pending |= 2u;
+  }
   wait(0);
   {
     const int c = (tx * (kBY + 2 * R) + ty + R) * kBZ + tz;
@@ -592,7 +622,7 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
       sl[(S_MAT + m) * kThreads] =
           sl[(S_MAT + m) * kThreads] + d1p_tile<O>(tl2 + (size_t)m * FB::ZB, tl2 + (size_t)4 * FB::ZB, c, 1, ph);
   }
-  return __syncthreads_and(ok);
+  return __syncthreads_and(ok && !lost);
 }
 
 // Kreiss-Oliger dissipation of one field at (i, j, k) (utils/math.h:36-72;

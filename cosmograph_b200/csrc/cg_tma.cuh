@@ -75,5 +75,15 @@ __device__ __forceinline__ bool wait(uint64_t* bar, unsigned phase, long long li
   }
 }
 
+// A bounded wait that lets a late copy land: after the first `limit` cycles
+// the wait goes on for up to kDrainCycles more, so that a copy that is only
+// slow completes before its buffer is reused or the CTA exits.  Returns 0
+// (in time), 1 (late: landed during the drain) or 2 (lost: never landed).
+constexpr long long kDrainCycles = 2000000000LL;  // about a second
+__device__ __forceinline__ int wait_drain(uint64_t* bar, unsigned phase, long long limit) {
+  if (wait(bar, phase, limit)) return 0;
+  return wait(bar, phase, kDrainCycles) ? 1 : 2;
+}
+
 }  // namespace tma
 }  // namespace cg

@@ -46,6 +46,7 @@ struct Physics {
   int shift;              // Shift gauge (kShiftNone: no shift fields)
   int gauge_wave_dir;     // AwAShiftedWave direction, 1..3
   double gd_eta, dw_mu_s, k_driver_coeff;
+  long long tma_wait;     // cycles a CTA waits for a TMA tile copy before it flags a timeout
 };
 
 // Background values for one substep (FRW stage values, grid averages).

@@ -183,10 +183,23 @@ class Evolution:
             dptr = _dptr(delta)
         self._check(self.L.cg_ic_grf_dust(self.ctx, box, dptr, ctypes.c_uint64(seed), rms_delta, ns, cutoff))
 
+    def ic_grf_scalar(self, box: int, seed: int = 9, phi0: float = 1.0e-2, rms: float = 1.0e-5, mass: float = 1.0,
+                      cutoff: float = 0.0, dphi: np.ndarray | None = None) -> None:
+        """GRF scalar initial data built on the GPU (cg_ic_grf_scalar); `dphi`
+        (host fluctuation) replaces the GPU's own random field."""
+        dptr = None
+        if dphi is not None:
+            dphi = np.ascontiguousarray(dphi, dtype=np.float64)
+            if dphi.shape != self.templates[box].shape:
+                raise ValueError("dphi must have the box's shape")
+            dptr = _dptr(dphi)
+        self._check(self.L.cg_ic_grf_scalar(self.ctx, box, dptr, ctypes.c_uint64(seed), phi0, rms, mass, cutoff))
+
     def set_option(self, option: str, value: int) -> None:
-        """Launch options: "batch", "graph", "autotune", "group_grid", "tma" (cg_set_option)."""
+        """Launch options: "batch", "graph", "autotune", "group_grid", "tma",
+        "tma_wait" (cg_set_option)."""
         code = {"batch": _lib.OPT_BATCH, "graph": _lib.OPT_GRAPH, "autotune": _lib.OPT_AUTOTUNE,
-                "group_grid": _lib.OPT_GROUP_GRID, "tma": _lib.OPT_TMA}[option]
+                "group_grid": _lib.OPT_GROUP_GRID, "tma": _lib.OPT_TMA, "tma_wait": _lib.OPT_TMA_WAIT}[option]
         self._check(self.L.cg_set_option(self.ctx, code, int(value)))
 
     def groups(self) -> list[dict]:

@@ -254,6 +254,28 @@ def grf_scalar(n, seed: int = 9, phi0: float = 1.0e-2, rms: float = 1.0e-5, mass
     return st
 
 
+def grf_scalar_gpu(n, seed: int = 9, phi0: float = 1.0e-2, rms: float = 1.0e-5, mass: float = 1.0,
+                   order: int = 8, box_len: float = 1.0, dt_frac: float = 0.1, dphi=None,
+                   host_field: bool = False) -> BoxState:
+    """grf_scalar built on the GPU (cg_ic_grf_scalar).  The fluctuation comes
+    from the GPU's own generator unless `dphi` is given; host_field=True draws
+    it on the host exactly as grf_scalar does, so the result equals
+    grf_scalar's to rounding."""
+    from .evolution import BoxConfig, Evolution
+
+    shape = (n, n, n) if np.isscalar(n) else tuple(n)
+    kc = min(shape) / 4.0
+    if host_field and dphi is None:
+        dphi = gaussian_random_field(shape, seed, lambda k: np.where(k <= kc, k ** -3.0, 0.0), rms)
+    dx = box_len / shape[0]
+    st = _empty(shape, SCALAR, dx, default_dt(dx, dt_frac))
+    with Evolution(st, BoxConfig(order=order)) as ev:
+        ev.ic_grf_scalar(0, seed=seed, phi0=phi0, rms=rms, mass=mass, cutoff=kc, dphi=dphi)
+        out = ev.download(0)
+    out.step = 0
+    return out
+
+
 def perturbed(shape, matter: int, seed: int = 1, amp: float = 1.0e-2, modes: int = 3,
               box_len: float = 1.0, dt_frac: float = 0.1, z4c: bool = False,
               shift: bool = False) -> BoxState:
@@ -294,6 +316,6 @@ def perturbed(shape, matter: int, seed: int = 1, amp: float = 1.0e-2, modes: int
     return st
 
 
-__all__ = ["sinusoid_dust", "grf_dust", "grf_scalar", "perturbed", "derivative",
+__all__ = ["sinusoid_dust", "grf_dust", "grf_scalar", "grf_scalar_gpu", "perturbed", "derivative",
            "double_derivative", "laplacian", "inverse_laplacian", "default_dt",
            "gaussian_random_field", "BSSN_FIELDS", "VACUUM", "DUST", "SCALAR", "STATIC"]

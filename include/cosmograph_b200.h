@@ -250,6 +250,20 @@ int cg_step(cg_ctx *ctx, int nsteps);
 int cg_ic_grf_dust(cg_ctx *ctx, int box, const double *delta, uint64_t seed, double rms_delta, double ns,
                    double cutoff);
 
+/* Initial data on the GPU for a scalar box (the GRF scalar configuration;
+ * the host version is cosmograph_b200.ics.grf_scalar): phi = phi0 + a
+ * Gaussian random fluctuation with P(k) ~ k^-3 for k <= cutoff (units of the
+ * fundamental mode; cutoff <= 0: min(nx,ny,nz)/4), else 0, zero mean and rms
+ * `rms`, drawn from the counter-based generator seeded with `seed`, or taken
+ * from `dphi` (host, nx*ny*nz doubles) when it is not NULL; Pi = 0, psi_i =
+ * d_i phi with the box's stencils (the relation of the reference's wave data,
+ * components/scalar/scalar_ic.cc:43-48), DIFFK = -sqrt(24 pi rho) with
+ * rho = mass^2 phi^2 / 2 + |d phi|^2 / 2, every other field zero.  Writes the
+ * _p register and resets the box like cg_upload_state.  Synchronous;
+ * allocates its scratch for the duration of the call. */
+int cg_ic_grf_scalar(cg_ctx *ctx, int box, const double *dphi, uint64_t seed, double phi0, double rms, double mass,
+                     double cutoff);
+
 /* Launch options (cg_set_option).  No reference counterpart: the reference
  * evolves one box per process.
  *   CG_OPT_BATCH     1 (default): boxes of a context with the same precision,
@@ -272,12 +286,19 @@ int cg_ic_grf_dust(cg_ctx *ctx, int box, const double *delta, uint64_t seed, dou
  *                    accelerator (FP64 boxes with even nz, mixed boxes with nz
  *                    a multiple of 4); 0: every tile is copied by the CTA's
  *                    threads.  Results are identical.  Change it between
- *                    steps only. */
+ *                    steps only.
+ *   CG_OPT_TMA_WAIT  clock cycles a CTA waits for one TMA tile copy before it
+ *                    raises CG_STATUS_TILE_TIMEOUT (0, the default: 2e9, about
+ *                    a second).  A late copy is still waited for, up to 2e9
+ *                    cycles more, before its buffer is reused or the CTA
+ *                    leaves, so a small value tests the reporting path without
+ *                    leaving copies in flight.  Change it between steps only. */
 #define CG_OPT_BATCH 1
 #define CG_OPT_GRAPH 2
 #define CG_OPT_AUTOTUNE 3
 #define CG_OPT_GROUP_GRID 4
 #define CG_OPT_TMA 5
+#define CG_OPT_TMA_WAIT 6
 int cg_set_option(cg_ctx *ctx, int option, int value);
 
 /* Launch groups of the context (formed on first use), and for group g:

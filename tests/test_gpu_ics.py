@@ -62,3 +62,37 @@ def test_gpu_ics_reject_non_dust_and_negative_density():
             ev.ic_grf_dust(0)
     with pytest.raises(RuntimeError, match="negative density"):
         ics.grf_dust_gpu(16, seed=3, rms_delta=3.0, order=4)
+
+
+@pytest.mark.parametrize("shape,order", [((32, 32, 32), 8), ((24, 20, 16), 4)])
+def test_gpu_scalar_construction_matches_host_given_the_fluctuation(shape, order):
+    """cg_ic_grf_scalar with the host's fluctuation against ics.grf_scalar:
+    phi, psi_i and DIFFK to rounding, every other field zero."""
+    ref = ics.grf_scalar(shape, seed=6, phi0=1e-2, rms=1e-5, mass=1.0, order=order)
+    got = ics.grf_scalar_gpu(shape, seed=6, phi0=1e-2, rms=1e-5, mass=1.0, order=order, host_field=True)
+    assert got.dx == ref.dx and got.dt == ref.dt
+    for f, name in enumerate(ref.names):
+        r, g = ref.fields[f], got.fields[f]
+        scale = np.abs(r).max()
+        if scale == 0.0:
+            assert np.abs(g).max() == 0.0, name
+        else:
+            assert np.abs(g - r).max() <= 1e-12 * scale, (name, np.abs(g - r).max() / scale)
+
+
+def test_gpu_scalar_random_field():
+    a = ics.grf_scalar_gpu(32, seed=7, phi0=1e-2, rms=1e-5, order=8)
+    b = ics.grf_scalar_gpu(32, seed=7, phi0=1e-2, rms=1e-5, order=8)
+    c = ics.grf_scalar_gpu(32, seed=8, phi0=1e-2, rms=1e-5, order=8)
+    assert np.array_equal(a.fields, b.fields)
+    assert not np.array_equal(a.fields, c.fields)
+    phi = a.field("phi")
+    assert abs(phi.mean() - 1e-2) < 1e-14 and abs(phi.std() - 1e-5) < 1e-12
+    # a k^-3 spectrum cut at N/4: no power above the cutoff
+    spec = np.abs(np.fft.rfftn(phi - phi.mean())) ** 2
+    px, py, pz = np.meshgrid(np.fft.fftfreq(32) * 32, np.fft.fftfreq(32) * 32, np.arange(17), indexing="ij")
+    k = np.sqrt(px ** 2 + py ** 2 + pz ** 2)
+    assert spec[k > 8.0].max() < 1e-20 * spec[k <= 8.0].max()
+    with pytest.raises(RuntimeError, match="scalar"):
+        with Evolution(ics.perturbed((16, 16, 16), S.DUST, amp=0.0), BoxConfig(order=4)) as ev:
+            ev.ic_grf_scalar(0)
