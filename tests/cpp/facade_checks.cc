@@ -92,6 +92,32 @@ int main(int argc, char** argv) {
   cosmo::ConfigParser cfg3(dir + "/cfg3.txt");
   EXPECT(thrown([&] { cosmo::BSSN b3(&cfg3); }) == 2);
 
+  // the shift: the compile-time switch as the key BSSN_shift, the gauge as `shift`
+  {
+    std::ofstream o(dir + "/cfg4.txt");
+    o << "simulation_type = scalar\nN = 8\nstencil_order = 4\nBSSN_shift = 1\nshift = GammaDriver\n"
+         "gd_eta = 0.5\nZ4c_damping = 0\n";
+  }
+  cosmo::ConfigParser cfg4(dir + "/cfg4.txt");
+  cosmo::BSSN b4(&cfg4);
+  EXPECT(b4.desc().shift == CG_SHIFT_GAMMA_DRIVER && b4.desc().gd_eta == 0.5);
+  EXPECT(b4.desc().gauge_wave_dir == 1 && b4.desc().k_driver_coeff == 0.04);
+  EXPECT(b4.num_fields() == 23 + 7);
+  EXPECT(b4.field_index("beta1") == 23 && b4.field_index("auxB3") == 28 && b4.field_index("expN") == 29);
+  EXPECT(b4.fields.count("expN_p") == 1 && b4.fields.size() == 3 * 30);
+  {
+    std::ofstream o(dir + "/cfg5.txt");
+    o << "simulation_type = dust\nN = 8\nshift = GammaDriver\n";
+  }
+  cosmo::ConfigParser cfg5(dir + "/cfg5.txt");
+  EXPECT(thrown([&] { cosmo::BSSN b5(&cfg5); }) == -1);  // a shift gauge without the shift fields
+  {
+    std::ofstream o(dir + "/cfg6.txt");
+    o << "simulation_type = dust\nN = 8\nBSSN_shift = 1\nshift = NoSuchShift\n";
+  }
+  cosmo::ConfigParser cfg6(dir + "/cfg6.txt");
+  EXPECT(thrown([&] { cosmo::BSSN b6(&cfg6); }) == -1);
+
   std::printf(failures ? "facade checks: %d failures\n" : "facade checks: ok\n", failures);
   return failures ? 1 : 0;
 }
