@@ -838,11 +838,23 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   // sources); static matter takes e^{-6 phi} in the sixth place
   double phip = phi;
   if (MATTER == kDust && stage > 1) phip = __ldcs(&P.prev[(size_t)F_PHI * N + c]) + bg.phi_FRW_prev;
+  // (without dust the previous substep's phi is not needed: five values, six
+  // with static matter)
   double ex[8];
-  {
-    const double xa[8] = {-4.0 * phi, 4.0 * phi, 6.0 * phi, 5.0 * phi, -5.0 * phi,
-                          MATTER == kStaticMatter ? -6.0 * phi : -4.0 * phip, 4.0 * phip, 6.0 * phip};
+  if constexpr (MATTER == kDust) {
+    const double xa[8] = {-4.0 * phi, 4.0 * phi, 6.0 * phi, 5.0 * phi, -5.0 * phi, -4.0 * phip, 4.0 * phip, 6.0 * phip};
     xexp_n<8>(xa, ex);
+  } else {
+    constexpr int NX = MATTER == kStaticMatter ? 6 : 5;
+    double xa[NX], ey[NX];
+#pragma unroll
+    for (int q = 0; q < NX; ++q) xa[q] = (q == 0 ? -4.0 : q == 1 ? 4.0 : q == 2 ? 6.0 : q == 3 ? 5.0 : q == 4 ? -5.0 : -6.0) * phi;
+    xexp_n<NX>(xa, ey);
+#pragma unroll
+    for (int q = 0; q < NX; ++q) ex[q] = ey[q];
+    if constexpr (NX == 5) ex[5] = ey[0];
+    ex[6] = ey[1];
+    ex[7] = ey[2];
   }
   const double em4phi = ex[0], e4phi = ex[1], e6phi = ex[2], e5phi = ex[3], em5phi = ex[4];
   const double em4phip = ex[5], e4phip = ex[6], e6phip = ex[7];
