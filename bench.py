@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--ncu", action="store_true", help="short run for profiler capture (no JSON extras)")
     ap.add_argument("--variants", default="fp64_fma,mixed", help="comma list of extra precisions timed alongside")
     ap.add_argument("--ensemble", type=int, default=1, help="also time the 48-box ensemble (variants.ensemble)")
+    ap.add_argument("--scalar", type=int, default=1, help="also time the GRF scalar configuration (variants.scalar)")
     ap.add_argument("--workload", choices=["box", "ensemble", "slab"], default="box",
                     help="box: one 256^3 box per GPU; ensemble: 48 boxes of 32^3/64^3/96^3 split over the GPUs; "
                          "slab: one (256 N) x 256 x 256 box cut into N x-slabs with a ghost exchange per substep")
@@ -325,6 +326,55 @@ def ensemble_variant(a, world, rank, stream):
                 "max_field_err_rel_perturbation": max(v["field_err_rel_perturbation"] for v in acc_all.values()),
                 "max_H_ratio": max(v["H_ratio"] for v in acc_all.values()),
                 "min_H_ratio": min(v["H_ratio"] for v in acc_all.values()), "boxes": len(acc_all)}}
+
+
+def scalar_variant(a, world, rank, stream):
+    """The GRF scalar configuration timed beside the default box: BSSN + a
+    minimally coupled scalar field with V = m^2 phi^2 / 2 (m = 1), phi0 = 1e-2
+    plus a k^-3 fluctuation of rms 1e-5 cut off at N/4 (initial data built on
+    the GPU, cg_ic_grf_scalar), the box's N and order, harmonic lapse; FP64
+    and FP32-mixed updates/s over all ranks, and the mixed run against the
+    FP64 run of the same steps (scalar-field error over the fluctuation rms,
+    worst field error against its spread, Hamiltonian L2 ratio)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from cosmograph_b200 import ics
+    from cosmograph_b200.evolution import BoxConfig, Evolution
+
+    st = ics.grf_scalar_gpu(a.n, seed=21 + rank, phi0=1e-2, rms=1e-5, mass=1.0, order=a.order)
+    out, final = {}, {}
+    for prec in ("fp64", "mixed"):
+        cfg = BoxConfig(order=a.order, lapse="Harmonic", precision=prec, potential="quadratic", pot_mass=1.0)
+        with Evolution(st, cfg) as ev:
+            ev.set_stream(stream.cuda_stream)
+            ev.step(max(a.warmup, 0))
+            ev.synchronize()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ev.step(a.steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ev.synchronize()
+            ms = e0.elapsed_time(e1)
+            if world > 1:
+                t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ms = float(t.item())
+            out[prec] = {"value": world * a.n ** 3 * a.steps / (ms / 1e3), "ms_per_step": ms / a.steps}
+            final[prec] = (ev.download(0), ev.constraints(0))
+    acc = accuracy(final["fp64"][0], final["mixed"][0], final["fp64"][1], final["mixed"][1])
+    f = st.names.index("phi")
+    acc["phi_err_rel_fluctuation"] = float(np.abs(final["mixed"][0].fields[f] - final["fp64"][0].fields[f]).max()) / 1e-5
+    out["mixed"]["speedup_vs_fp64"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["mixed"]["accuracy_vs_fp64"] = acc
+    out["workload"] = (f"BSSN + scalar field, {a.n}^3, order {a.order}, V = m^2 phi^2/2 (m = 1), phi0 = 1e-2, "
+                       f"k^-3 fluctuation rms 1e-5, {world} box(es)")
+    return out
 
 
 def run_ensemble(a, world, rank, local):
@@ -698,6 +748,8 @@ def main():
     del ref_state
     if a.ensemble:
         variants["ensemble"] = ensemble_variant(a, world, rank, stream)
+    if a.scalar:
+        variants["scalar"] = scalar_variant(a, world, rank, stream)
 
     # end to end through the C ABI: pinned host state in, one RK4 step, state out
     state_bytes = st.fields.nbytes
