@@ -430,6 +430,22 @@ double mixed_bg_lapse(const cg_box_desc& d, double al, double Kd, double phi) {
   }
 }
 
+// Hamiltonian constraint of the uniform background, bssn.cc:1073-1084 with
+// every gradient, A_ij and theta zero: Hc = 2/3 K^2 - 16 pi rho, H = -e^{5 phi}/8 Hc
+void mixed_bg_hamiltonian(const Box& b, const double* a, double phi_lag, double* Hc, double* H) {
+  const double Kd = a[cg::F_K];
+  double rho = 0.0;
+  if (b.desc.matter == CG_MATTER_DUST) {
+    rho = a[cg::F_D] * std::exp(-6.0 * phi_lag) + b.desc.lambda;  // W = 1
+  } else if (b.desc.matter == CG_MATTER_SCALAR) {
+    const double sphi = a[cg::F_SPHI], Pi = a[cg::F_SPI];
+    const double m2 = b.desc.pot_mass * b.desc.pot_mass;
+    rho = 0.5 * Pi * Pi + (b.desc.potential == CG_POT_QUADRATIC ? 0.5 * m2 * sphi * sphi : b.desc.pot_const);
+  }
+  *Hc = 2.0 / 3.0 * Kd * Kd - 16.0 * cg::kPi * rho;
+  *H = -std::exp(5.0 * a[cg::F_PHI]) / 8.0 * *Hc;
+}
+
 // Right-hand side of the uniform background (the reference's equations for a
 // spatially constant state, trivial FRW): dK/dt, dphi/dt, dalpha/dt and, for
 // a scalar field, dphi_s/dt = -alpha Pi, dPi/dt = alpha (K Pi + V'(phi_s))
@@ -453,6 +469,14 @@ void mixed_bg_rhs(const Box& b, const double* a, double phi_lag, double* rhs) {
   rhs[cg::F_K] = al * (1.0 / 3.0 * Kd * Kd) + 4.0 * cg::kPi * al * rS;
   rhs[cg::F_PHI] = -1.0 / 6.0 * (al * Kd);
   rhs[cg::F_ALPHA] = mixed_bg_lapse(b.desc, al, Kd, a[cg::F_PHI]);
+  if (b.desc.a_adj_amp != 0.0 || b.desc.k_damping_amp != 0.0) {
+    // constraint damping of phi and K (bssn.cc:766-820): 0.1 a_adj_amp dt H,
+    // -k_damping_amp H e^{-5 phi}
+    double Hc, H;
+    mixed_bg_hamiltonian(b, a, phi_lag, &Hc, &H);
+    rhs[cg::F_PHI] += 0.1 * b.desc.a_adj_amp * b.desc.dt * H;
+    rhs[cg::F_K] += -1.0 * b.desc.k_damping_amp * H * std::exp(-5.0 * a[cg::F_PHI]);
+  }
 }
 
 void pack_bg(const double* full, double* compact) {
@@ -602,6 +626,13 @@ int mixed_prepare(cg_ctx* ctx, Box& b, int n, cg::mixed::Bg* out) {
     bg.dw_u = b.desc.dw_mu_l * (12.0 * b.ba[cg::F_PHI] * b.desc.dw_p - std::log(al)) - b.ba[cg::F_K];
   }
   bg.tma_wait = b.dev.ph.tma_wait;
+  bg.damping = b.desc.a_adj_amp != 0.0 || b.desc.k_damping_amp != 0.0;
+  if (bg.damping) {
+    mixed_bg_hamiltonian(b, b.ba, phi_lag, &bg.Hcbar, &bg.Hbar);
+    bg.e5phib = std::exp(5.0 * b.ba[cg::F_PHI]);
+    bg.a_adj_dt = b.desc.a_adj_amp * b.desc.dt;
+    bg.k_damp8 = b.desc.k_damping_amp / 8.0;
+  }
   bg.ko_scale = b.desc.stencil_order == 2 ? b.desc.ko_coeff / (64.0 * b.desc.dx)
                                           : -b.desc.ko_coeff / (1024.0 * b.desc.dx);
   for (int f = 0; f < 23; ++f) {
@@ -711,10 +742,6 @@ int validate(const cg_box_desc& d, std::string& why) {
     }
     if (d.frw_phi != 0.0 || d.frw_K != 0.0 || d.nfluids != 0) {
       why = "the FP32-mixed form evolves about its own uniform background (trivial FRW reference)";
-      return CG_ERR_INVALID;
-    }
-    if (d.a_adj_amp != 0.0 || d.k_damping_amp != 0.0) {
-      why = "the FP32-mixed form needs a_adj_amp = k_damping_amp = 0";
       return CG_ERR_INVALID;
     }
   }

@@ -72,6 +72,11 @@ struct Bg {
   double dw_mu_l, dw_p, dw_u;  // damped-wave lapse: mu_L, p and mu_L (12 p phibar - ln abar) - Kbar
   double ko_scale;             // Kreiss-Oliger: c / (64 dx) (order 2) or -c / (1024 dx) (order 8)
   long long tma_wait;          // cycles a CTA waits for a TMA tile copy before it flags a timeout
+  // constraint damping (a_adj_amp, k_damping_amp): the background's
+  // Hamiltonian constraint Hbar = -e^{5 phibar} / 8 * Hcbar, Hcbar =
+  // 2/3 Kbar^2 - 16 pi rhobar, and a_adj_amp dt, k_damping_amp / 8
+  double Hbar, Hcbar, e5phib, a_adj_dt, k_damp8;
+  int damping;                 // either amplitude is nonzero
 };
 __host__ __device__ constexpr int bgi(int f) {
   return f == F_K ? 0 : (f == F_PHI ? 1 : (f == F_ALPHA ? 2 : (f == 18 ? 3 : (f == 19 ? 4 : -1))));
@@ -712,8 +717,22 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
     }
     outv[fld] = o;
   };
+  // constraint damping (bssn.cc:748-820): H in perturbation form,
+  // H - Hbar = -(e^{5 phibar}/8) (expm1(5 dphi) Hcbar + e^{5 dphi} dHc) with
+  // dHc = ricci + 2/3 (2 Kbar + dK) dK - A_ij A^ij - 16 pi drho
+  float Hd = 0.f, dH = 0.f, dHc = 0.f;
+  if (bg.damping) {
+    dHc = ricci + (2.0f / 3.0f) * (2.0f * Kb + dK) * dK - AijAij - 16.0f * kPif * S(S_SRC + Q_R);
+    dH = -(float)(bg.e5phib * (1.0 / 8.0)) * (expm1f(5.0f * dphi0) * (float)bg.Hcbar + __expf(5.0f * dphi0) * dHc);
+    Hd = (float)bg.Hbar + dH;
+  }
+  const float adt = (float)bg.a_adj_dt;
 #pragma unroll
-  for (int m = 0; m < 6; ++m) finalize(F_G11 + m, -2.0f * alpha * A[m]);
+  for (int m = 0; m < 6; ++m) {
+    float v = -2.0f * alpha * A[m];
+    if (bg.damping) v += 0.5f * adt * Hd * g[m];
+    finalize(F_G11 + m, v);
+  }
 #pragma unroll
   for (int I = 0; I < 3; ++I)
 #pragma unroll
@@ -725,8 +744,10 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
 #pragma unroll
         for (int Y = 0; Y < 3; ++Y) aa += gi[sym(X, Y)] * A[sym(X, I)] * A[sym(Y, J)];
       const float RTF = Ric(qq) - (1.0f / 3.0f) * e4phi * gm[qq] * ricci;
-      finalize(F_A11 + qq, em4phi * (alpha * (RTF - 8.0f * kPif * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
-                               alpha * (K * A[qq] - 2.0f * aa));
+      float v = em4phi * (alpha * (RTF - 8.0f * kPif * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
+                alpha * (K * A[qq] - 2.0f * aa);
+      if (bg.damping) v -= adt * A[qq] * Hd;
+      finalize(F_A11 + qq, v);
     }
 #pragma unroll
   for (int I = 0; I < 3; ++I) {
@@ -740,8 +761,9 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
   // zeroth-order equations in explicit perturbation form
   const float dRK = -DDaTR + (alb * (2.0f * Kb + dK) * dK + dal * K * K) * (1.0f / 3.0f) + alpha * AijAij +
                     4.0f * kPif * (alb * (dr + Sdust) + dal * rS_full);
-  finalize(F_K, dRK);
-  finalize(F_PHI, -(1.0f / 6.0f) * (alb * dK + dal * K));
+  finalize(F_K, bg.damping ? dRK + (float)bg.k_damp8 * dHc : dRK);
+  finalize(F_PHI, bg.damping ? -(1.0f / 6.0f) * (alb * dK + dal * K) + 0.1f * adt * dH
+                             : -(1.0f / 6.0f) * (alb * dK + dal * K));
   finalize(F_ALPHA, lapse_drhs(lapse, bg, alb, dal, alpha, Kb, dK, dphi0, P.kavg ? (float)__ldg(P.kavg) : 0.0f));
   if (MATTER == kDust) {
 #pragma unroll

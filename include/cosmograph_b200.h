@@ -67,8 +67,8 @@ extern "C" {
 #define CG_PREC_MIXED 2     /* FP32 perturbations about an FP64 uniform background,
                                FP32 stencils and right-hand side, FP64 RK registers
                                (vacuum, dust or scalar; every lapse; Kreiss-Oliger;
-                               trivial FRW reference; no Z4c, shift or
-                               a_adj_amp / k_damping_amp)                           */
+                               a_adj_amp / k_damping_amp; trivial FRW reference;
+                               no Z4c or shift)                                     */
 
 /* shift gauges (BSSNGaugeHandler.h:113-134); a box with a shift carries the
  * reference's USE_BSSN_SHIFT and USE_GAMMA_DRIVER fields */
