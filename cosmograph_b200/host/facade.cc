@@ -814,7 +814,22 @@ void ScalarSim::init() {
 
 void ScalarSim::setICs() {
   iodata->log("Setting initial conditions (ICs).");
-  loadICs();
+  if (cfg->has("ic_file")) {
+    loadICs();
+  } else {
+    // the GRF scalar configuration built on the GPU: phi = scalar_phi0 + a
+    // k^-3 Gaussian random fluctuation of rms scalar_rms cut off at
+    // ic_spec_cut modes (default N/4), Pi = 0, psi_i = d_i phi, K from the
+    // local energy density with the run's scalar_mass
+    const uint64_t seed = std::stoull((*cfg)("seed", "9"));
+    const double phi0 = std::stod((*cfg)("scalar_phi0", "1.0e-2"));
+    const double rms = std::stod((*cfg)("scalar_rms", "1.0e-5"));
+    const double cut = std::stod((*cfg)("ic_spec_cut", "0"));
+    const double mass = bssnSim->desc().pot_mass;
+    iodata->log("Setting GRF scalar ICs (GPU): seed " + std::to_string(seed) + ", phi0 " + fmt15(phi0) + ", rms " +
+                fmt15(rms));
+    bssnSim->check(cg_ic_grf_scalar(bssnSim->ctx(), 0, nullptr, seed, phi0, rms, mass, cut), "GRF scalar initial data");
+  }
   iodata->log("Finished setting ICs.");
 }
 

@@ -122,6 +122,22 @@ def test_dust_run_with_gpu_initial_data(tmp_path):
     assert len(h) == 5 and all(np.isfinite(r).all() for r in h)
 
 
+def test_scalar_run_with_gpu_initial_data(tmp_path):
+    """Without ic_file the scalar driver builds the GRF scalar data on the GPU
+    (cg_ic_grf_scalar) and evolves them: the same as the Python front end's
+    run of the same GPU initial data, bit for bit."""
+    run_driver(tmp_path, "\n".join([
+        "simulation_type = scalar", "steps = 2", "N = 24", "stencil_order = 4", "lapse = Harmonic",
+        "H_LEN_FRAC = 1", "potential = quadratic", "scalar_mass = 1.0", "seed = 12", "scalar_phi0 = 0.01",
+        "scalar_rms = 1e-5", "output_file = final.bin", "output_dir = out", ""]))
+    got = S.load(tmp_path / "final.bin")
+    ic = ics.grf_scalar_gpu(24, seed=12, phi0=0.01, rms=1e-5, mass=1.0, order=4)
+    ic.dx, ic.dt = got.dx, got.dt
+    ref = evolve(ic, 3, BoxConfig(order=4, lapse="Harmonic", potential="quadratic", pot_mass=1.0))
+    assert got.step == 3
+    assert np.array_equal(got.fields, ref.fields)
+
+
 def test_field_snapshots(tmp_path):
     """IO_3D / IO_2D / IO_1D keys (the reference's io_bssn_fields_snapshot) for
     the _a register after stepInit at the output steps."""
