@@ -309,6 +309,27 @@ def ensemble_variant(a, world, rank, stream):
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
+    # the same boxes looped with one launch per box and substep (no batching)
+    single = Evolution(states, [cfg] * len(states))
+    single.set_option("batch", 0)
+    single.set_stream(stream.cuda_stream)
+    single.step(max(a.warmup, 0))
+    single.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    single.step(a.steps)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    single.synchronize()
+    ms_single = s0.elapsed_time(s1)
+    if world > 1:
+        t = torch.tensor([ms_single], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_single = float(t.item())
+    single.close()
     fp64 = Evolution(states, [BoxConfig(order=4, lapse="Harmonic")] * len(states))
     fp64.set_stream(stream.cuda_stream)
     fp64.step(max(a.warmup, 0) + a.steps)
@@ -322,6 +343,8 @@ def ensemble_variant(a, world, rank, stream):
     acc_all = ensemble.gather(acc, world)
     return {"workload": ensemble_config(specs, world)["workload"], "value": all_pts * a.steps / (ms / 1e3),
             "ms_per_step": ms / a.steps, "groups": groups,
+            "single_launches": {"value": all_pts * a.steps / (ms_single / 1e3), "ms_per_step": ms_single / a.steps},
+            "speedup_vs_single_launches": ms_single / ms,
             "accuracy_vs_fp64": {
                 "max_field_err_rel_perturbation": max(v["field_err_rel_perturbation"] for v in acc_all.values()),
                 "max_H_ratio": max(v["H_ratio"] for v in acc_all.values()),
