@@ -28,6 +28,24 @@ def test_restatement_matches_reference_evolve(name):
     assert worst(errs)[1] <= tol, worst(errs)
 
 
+SHIFT_CASES = [k for k, v in golden_index().items() if v["mode"] == "evolve" and "shift" in v["config"]]
+
+
+@pytest.mark.parametrize("name", SHIFT_CASES)
+def test_shift_fixtures_reproduce_on_the_reference_build(name):
+    """The shift fixtures (the CUDA path's parity cases for USE_BSSN_SHIFT with
+    USE_GAMMA_DRIVER) come back bit for bit from a fresh run of the
+    reference's own shift build; runs only where the reference checkout is."""
+    from oracle import build_ref
+
+    if not build_ref.reference_available():
+        pytest.skip("reference checkout not present")
+    inp, out, _, meta = load_golden(name)
+    binp = build_ref.build(*meta["shape"], meta["order"], "strict_shift")
+    got, _ = oracle.run_reference(binp, "evolve", inp, steps=meta["steps"], threads=1, **meta["config"])
+    assert got.shift and np.array_equal(got.fields, out.fields)
+
+
 def test_restatement_matches_reference_rhs():
     inp, out, _, meta = load_golden("dust_o4_rhs")
     got = oracle.rhs(inp, meta["order"], **meta["config"])
