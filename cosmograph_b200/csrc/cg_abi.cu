@@ -900,6 +900,8 @@ int cg_create(const cg_box_desc* boxes, int nboxes, cg_ctx** out) {
     ph.lambda = d.lambda;
     ph.a_adj_amp = d.a_adj_amp;
     ph.ko_coeff = d.ko_coeff;
+    ph.ko_pden = std::pow(d.dx, d.stencil_order == 8 ? 10.0 : 4.0);
+    ph.ko_pnum = std::pow(d.dx, d.stencil_order == 8 ? 9.0 : 3.0);
     ph.k_damping_amp = d.k_damping_amp;
     ph.gd_c = d.gd_c;
     ph.dw_mu_l = d.dw_mu_l;

@@ -631,7 +631,8 @@ __device__ __forceinline__ bool flux_from_tiles(const FluxMaps* fm, double* tl, 
 // memory, plain offsets when the taps stay inside the box.
 template <int O>
 __device__ __forceinline__ double ko_dissipation(const double* __restrict__ f, int i, int j, int k, int nx, int ny, int nz,
-                                              bool inside, double c, double dx) {
+                                              bool inside, const Physics& ph) {
+  const double c = ph.ko_coeff;
   auto at = [&](int a, int n) {
     int ii = i + (a == 0 ? n : 0), jj = j + (a == 1 ? n : 0), kk = k + (a == 2 ? n : 0);
     if (!inside) {
@@ -648,8 +649,8 @@ __device__ __forceinline__ double ko_dissipation(const double* __restrict__ f, i
     const double st = (1.0 * X(-2) + 1.0 * Y(-2) + 1.0 * Z(-2) - 4.0 * X(-1) - 4.0 * Y(-1) - 4.0 * Z(-1) +
                        6.0 * X(0) + 6.0 * Y(0) + 6.0 * Z(0) - 4.0 * X(1) - 4.0 * Y(1) - 4.0 * Z(1) + 1.0 * X(2) +
                        1.0 * Y(2) + 1.0 * Z(2)) /
-                      pow(dx, 4.0);
-    return c * pow(dx, 3.0) / 64.0 * st;
+                      ph.ko_pden;
+    return c * ph.ko_pnum / 64.0 * st;
   }
   const double st = (1.0 * X(-5) + 1.0 * Y(-5) + 1.0 * Z(-5) - 10.0 * X(-4) - 10.0 * Y(-4) - 10.0 * Z(-4) +
                      45.0 * X(-3) + 45.0 * Y(-3) + 45.0 * Z(-3) - 120.0 * X(-2) - 120.0 * Y(-2) - 120.0 * Z(-2) +
@@ -657,8 +658,8 @@ __device__ __forceinline__ double ko_dissipation(const double* __restrict__ f, i
                      210.0 * X(1) + 210.0 * Y(1) + 210.0 * Z(1) - 120.0 * X(2) - 120.0 * Y(2) - 120.0 * Z(2) +
                      45.0 * X(3) + 45.0 * Y(3) + 45.0 * Z(3) - 10.0 * X(4) - 10.0 * Y(4) - 10.0 * Z(4) +
                      1.0 * X(5) + 1.0 * Y(5) + 1.0 * Z(5)) /
-                    pow(dx, 10.0);
-  return -c * pow(dx, 9.0) / 1024.0 * st;
+                    ph.ko_pden;
+  return -c * ph.ko_pnum / 1024.0 * st;
 }
 
 // Deterministic CTA reduction of Q values per thread: the first NSUM are
@@ -1077,8 +1078,11 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     // the parity build: the reference's 27 terms per component, summed over
     // (K, L, M) with M fastest, each term formed as the macro forms it; the
     // six components advance together, so the symbols of one K are loaded
-    // once for all of them
-#pragma unroll
+    // once for all of them.  K is a rolled loop: its body (54 terms) stays
+    // in the instruction cache for the second and third pass, where the
+    // unrolled 162 terms did not (the slot addresses take K at run time; the
+    // sum starts from +0, which changes no value)
+#pragma unroll 1
     for (int Kx = 0; Kx < 3; ++Kx)
 #pragma unroll
       for (int L = 0; L < 3; ++L)
@@ -1091,7 +1095,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
               const double u =
                   gi[sym(L, M)] * (G(Kx, sym(L, I)) * GL(J, sym(Kx, M)) + G(Kx, sym(L, J)) * GL(I, sym(Kx, M)) +
                                    0.5 * (G(Kx, sym(I, M)) * GL(Kx, sym(L, J)) + G(Kx, sym(J, M)) * GL(Kx, sym(L, I))));
-              t4[sym(I, J)] = (Kx == 0 && L == 0 && M == 0) ? u : t4[sym(I, J)] + u;
+              t4[sym(I, J)] = t4[sym(I, J)] + u;
             }
   } else {
 #pragma unroll
@@ -1264,7 +1268,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
                           z0 >= RKO && z0 + kBZ + RKO <= geo.nz;
 #pragma unroll 1
       for (int f = 0; f < F_NBSSN; ++f)
-        S(S_DG + f) = ko_dissipation<O>(a + (size_t)f * N, i, j, k, geo.nx, geo.ny, geo.nz, inside, ph.ko_coeff, ph.dx);
+        S(S_DG + f) = ko_dissipation<O>(a + (size_t)f * N, i, j, k, geo.nx, geo.ny, geo.nz, inside, ph);
     }
   }
   auto ko = [&](int fld) -> double { return ko_on ? S(S_DG + fld) : 0.0; };
@@ -1425,7 +1429,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       if (ko_on) {
         const bool inside = x0 >= RKO && x0 + kBX + RKO <= geo.nx && y0 >= RKO && y0 + kBY + RKO <= geo.ny &&
                             z0 >= RKO && z0 + kBZ + RKO <= geo.nz;
-        kth = ko_dissipation<O>(a + (size_t)F_THETA * N, i, j, k, geo.nx, geo.ny, geo.nz, inside, ph.ko_coeff, ph.dx);
+        kth = ko_dissipation<O>(a + (size_t)F_THETA * N, i, j, k, geo.nx, geo.ny, geo.nz, inside, ph);
       }
     }
     finalize(F_THETA, (0.5 * alpha * (ricci + 2.0 / 3.0 * ((K + 2.0 * theta) * (K + 2.0 * theta)) - AijAij -
@@ -1465,8 +1469,7 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       if (ko_on) {
         const bool inside = x0 >= RKO && x0 + kBX + RKO <= geo.nx && y0 >= RKO && y0 + kBY + RKO <= geo.ny &&
                             z0 >= RKO && z0 + kBZ + RKO <= geo.nz;
-        kb = ko_dissipation<O>(a + (size_t)(F_BETA + I) * N, i, j, k, geo.nx, geo.ny, geo.nz, inside, ph.ko_coeff,
-                               ph.dx);
+        kb = ko_dissipation<O>(a + (size_t)(F_BETA + I) * N, i, j, k, geo.nx, geo.ny, geo.nz, inside, ph);
       }
       finalize(F_BETA + I, v - kb);
     }

@@ -60,18 +60,26 @@ __device__ __forceinline__ void prefetch_4d(const CUtensorMap* map, int c0, int 
 }
 
 // Wait until the barrier completes the phase with parity `phase`; gives up
-// after `limit` clock cycles and returns false.
+// after `limit` clock cycles and returns false.  Each round tests the phase
+// without blocking, then checks the limit, then waits with try_wait (which
+// may suspend the thread for a while), so that a small limit is honoured.
 __device__ __forceinline__ bool wait(uint64_t* bar, unsigned phase, long long limit) {
   const long long t0 = clock64();
   while (true) {
     unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > limit) return false;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
         : "=r"(done)
         : "r"(smem_addr(bar)), "r"(phase)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > limit) return false;
   }
 }
 

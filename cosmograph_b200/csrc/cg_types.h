@@ -43,6 +43,9 @@ struct Physics {
   double a_adj_amp, k_damping_amp, gd_c, dw_mu_l, dw_p;
   double pot_const, pot_mass;
   double ko_coeff;        // KO_damping_coefficient (orders 2 and 8)
+  // pow(dx, 4) and pow(dx, 3) (order 2) or pow(dx, 10) and pow(dx, 9) (order
+  // 8), from the host's pow as the reference's KO_dissipation_Q takes them
+  double ko_pden, ko_pnum;
   int shift;              // Shift gauge (kShiftNone: no shift fields)
   int gauge_wave_dir;     // AwAShiftedWave direction, 1..3
   double gd_eta, dw_mu_s, k_driver_coeff;

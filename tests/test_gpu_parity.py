@@ -167,6 +167,12 @@ def test_kreiss_oliger_against_restatement(matter, shape, order):
     got = evolve(st, 4, BoxConfig(order=order, ko_coeff=0.3))
     errs = field_errors(got.fields, ref.fields, st.names, floor=1e-18)
     assert worst(errs)[1] <= TOL["fp64"], worst(errs)
+    # bit for bit against the correctly rounded restatement (the powers of dx
+    # come from the host's pow, as in the reference)
+    ref_cr = oracle.evolve(st, 4, order, cr=True, ko_coeff=0.3)
+    diff = int((got.fields != ref_cr.fields).sum())
+    print("KO", matter, shape, order, "differing values against the correctly rounded restatement:", diff)
+    assert diff == 0, worst(field_errors(got.fields, ref_cr.fields, st.names, floor=1e-18))
     plain = evolve(st, 4, BoxConfig(order=order))
     if order in (2, 8):
         assert not np.array_equal(plain.fields, got.fields)
