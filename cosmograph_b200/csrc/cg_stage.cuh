@@ -841,21 +841,49 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   if (MATTER == kDust && stage > 1) phip = __ldcs(&P.prev[(size_t)F_PHI * N + c]) + bg.phi_FRW_prev;
   // (without dust the previous substep's phi is not needed: five values, six
   // with static matter)
+  // The parity build evaluates the batch through this thread's slots of the
+  // Christoffel symbols (free until they are formed): arguments in S_G,
+  // results in S_G + NX, the fast evaluation in a rolled loop (one copy of its
+  // code, which stays in the instruction cache), the accurate phase for the
+  // undecided ones after it; the same correctly rounded values as xexp_n.
+  constexpr int NX = MATTER == kDust ? 8 : (MATTER == kStaticMatter ? 6 : 5);
+  static_assert(2 * NX <= 18, "the batch fits the Christoffel slots");
   double ex[8];
-  if constexpr (MATTER == kDust) {
-    const double xa[8] = {-4.0 * phi, 4.0 * phi, 6.0 * phi, 5.0 * phi, -5.0 * phi, -4.0 * phip, 4.0 * phip, 6.0 * phip};
-    xexp_n<8>(xa, ex);
-  } else {
-    constexpr int NX = MATTER == kStaticMatter ? 6 : 5;
-    double xa[NX], ey[NX];
+  {
+    double xa[NX];
 #pragma unroll
-    for (int q = 0; q < NX; ++q) xa[q] = (q == 0 ? -4.0 : q == 1 ? 4.0 : q == 2 ? 6.0 : q == 3 ? 5.0 : q == 4 ? -5.0 : -6.0) * phi;
-    xexp_n<NX>(xa, ey);
+    for (int q = 0; q < NX; ++q)
+      xa[q] = q < 5 ? (q == 0 ? -4.0 : q == 1 ? 4.0 : q == 2 ? 6.0 : q == 3 ? 5.0 : -5.0) * phi
+                    : (MATTER == kStaticMatter ? -6.0 * phi : (q == 5 ? -4.0 : q == 6 ? 4.0 : 6.0) * phip);
+    if constexpr (kReferenceOrder) {
 #pragma unroll
-    for (int q = 0; q < NX; ++q) ex[q] = ey[q];
-    if constexpr (NX == 5) ex[5] = ey[0];
-    ex[6] = ey[1];
-    ex[7] = ey[2];
+      for (int q = 0; q < NX; ++q) S(S_G + q) = xa[q];
+      unsigned bad = 0;
+#pragma unroll 1
+      for (int q = 0; q < NX; ++q) {
+        double y;
+        if (!crm::exp_fast(S(S_G + q), y)) bad |= 1u << q;
+        S(S_G + NX + q) = y;
+      }
+#pragma unroll 1
+      while (bad) {
+        const int q = __ffs(bad) - 1;
+        bad &= bad - 1;
+        S(S_G + NX + q) = crm::exp_full(S(S_G + q));
+      }
+#pragma unroll
+      for (int q = 0; q < NX; ++q) ex[q] = S(S_G + NX + q);
+    } else {
+      double ey[NX];
+      xexp_n<NX>(xa, ey);
+#pragma unroll
+      for (int q = 0; q < NX; ++q) ex[q] = ey[q];
+    }
+  }
+  if constexpr (NX < 8) {  // without dust the previous substep's phi is this one's
+    if constexpr (NX == 5) ex[5] = ex[0];
+    ex[6] = ex[1];
+    ex[7] = ex[2];
   }
   const double em4phi = ex[0], e4phi = ex[1], e6phi = ex[2], e5phi = ex[3], em5phi = ex[4];
   const double em4phip = ex[5], e4phip = ex[6], e6phip = ex[7];
