@@ -1300,23 +1300,23 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     }
   }
   auto ko = [&](int fld) -> double { return ko_on ? S(S_DG + fld) : 0.0; };
+  // RK4Register::K{n}Finalize (RK4Register.h:180-230) with the substep's
+  // divisors chosen once: f = f + dt cv / 6 (substep 1, from f = 0), / 3
+  // (2, 3); a = p + dt cv / 2 (1, 2), / 1 (3); p = f + (dt cv / 6 + p) (4).
+  // IEEE division rounds the same for a divisor held in a register, and
+  // 0 + x = x, so the values are those of the four separate forms with one
+  // copy of the code per field.
+  const double fdiv = stage == 1 ? 6.0 : 3.0, odiv = stage == 3 ? 1.0 : 2.0;
   auto finalize = [&](int fld, double cv) {
     const double pv = __ldcs(&P.p[(size_t)fld * N + c]);
+    const double fv = stage == 1 ? 0.0 : __ldcs(&P.f[(size_t)fld * N + c]);
+    const double t = dt * cv;
     double o;
-    if (stage == 1) {
-      __stcs(&P.f[(size_t)fld * N + c], dt * cv / 6.0);
-      o = pv + dt * cv / 2.0;
-    } else if (stage == 2) {
-      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
-      __stcs(&P.f[(size_t)fld * N + c], fv + dt * cv / 3.0);
-      o = pv + dt * cv / 2.0;
-    } else if (stage == 3) {
-      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
-      __stcs(&P.f[(size_t)fld * N + c], fv + dt * cv / 3.0);
-      o = pv + dt * cv;
+    if (stage == 4) {
+      o = fv + (t / 6.0 + pv);
     } else {
-      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
-      o = fv + (dt * cv / 6.0 + pv);
+      __stcs(&P.f[(size_t)fld * N + c], fv + t / fdiv);
+      o = pv + t / odiv;
     }
     __stcs(&P.out[(size_t)fld * N + c], o);
     outv[fld] = o;
