@@ -1020,18 +1020,23 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   // -- Christoffels (bssn.cc:577-590, bssn_macros.h:221-229) --
   // Gamma^I_q go to their own slots; the lowered Gamma_{I q} then replace
   // d_I g_q, which nothing reads afterwards.
+  // the pair (J, K) in a rolled loop (slot addresses at run time, one copy of
+  // the code), the three brackets shared by the three I
+#pragma unroll 1
+  for (int q = 0; q < 6; ++q) {
+    const int J = q < 3 ? 0 : (q < 5 ? 1 : 2), Kx = q < 3 ? q : (q < 5 ? q - 2 : 2);  // sym(J, Kx) = q
+    auto dg = [&](int d, int qq) { return S(S_DG + 6 * d + qq); };
+    const double b0 = dg(J, sym(Kx, 0)) + dg(Kx, sym(J, 0)) - dg(0, q);
+    const double b1 = dg(J, sym(Kx, 1)) + dg(Kx, sym(J, 1)) - dg(1, q);
+    const double b2 = dg(J, sym(Kx, 2)) + dg(Kx, sym(J, 2)) - dg(2, q);
 #pragma unroll
-  for (int I = 0; I < 3; ++I)
-#pragma unroll
-    for (int J = 0; J < 3; ++J)
-#pragma unroll
-      for (int Kx = J; Kx < 3; ++Kx) {
-        auto dg = [&](int d, int qq) { return S(S_DG + 6 * d + qq); };
-        double u = gi[sym(I, 0)] * (dg(J, sym(Kx, 0)) + dg(Kx, sym(J, 0)) - dg(0, sym(J, Kx)));
-        u = u + gi[sym(I, 1)] * (dg(J, sym(Kx, 1)) + dg(Kx, sym(J, 1)) - dg(1, sym(J, Kx)));
-        u = u + gi[sym(I, 2)] * (dg(J, sym(Kx, 2)) + dg(Kx, sym(J, 2)) - dg(2, sym(J, Kx)));
-        S(S_G + 6 * I + sym(J, Kx)) = 0.5 * (u);
-      }
+    for (int I = 0; I < 3; ++I) {
+      double u = gi[sym(I, 0)] * (b0);
+      u = u + gi[sym(I, 1)] * (b1);
+      u = u + gi[sym(I, 2)] * (b2);
+      S(S_G + 6 * I + q) = 0.5 * (u);
+    }
+  }
   {
     double GLv[3][6];
 #pragma unroll
@@ -1300,30 +1305,13 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     }
   }
   auto ko = [&](int fld) -> double { return ko_on ? S(S_DG + fld) : 0.0; };
-  // RK4Register::K{n}Finalize (RK4Register.h:180-230) with the substep's
-  // divisors chosen once: f = f + dt cv / 6 (substep 1, from f = 0), / 3
-  // (2, 3); a = p + dt cv / 2 (1, 2), / 1 (3); p = f + (dt cv / 6 + p) (4).
-  // IEEE division rounds the same for a divisor held in a register, and
-  // 0 + x = x, so the values are those of the four separate forms with one
-  // copy of the code per field.
-  const double fdiv = stage == 1 ? 6.0 : 3.0, odiv = stage == 3 ? 1.0 : 2.0;
-  auto finalize = [&](int fld, double cv) {
-    const double pv = __ldcs(&P.p[(size_t)fld * N + c]);
-    const double fv = stage == 1 ? 0.0 : __ldcs(&P.f[(size_t)fld * N + c]);
-    const double t = dt * cv;
-    double o;
-    if (stage == 4) {
-      o = fv + (t / 6.0 + pv);
-    } else {
-      __stcs(&P.f[(size_t)fld * N + c], fv + t / fdiv);
-      o = pv + t / odiv;
-    }
-    __stcs(&P.out[(size_t)fld * N + c], o);
-    outv[fld] = o;
-    // at the last substep the new state is also the next step's first input,
-    // except gamma and A, which are renormalised below
-    if (stage == 4 && !(renorm && fld < F_K && fld != F_PHI)) __stcs(&P.norm[(size_t)fld * N + c], o);
-  };
+  // Each right-hand side is parked in a slot free in the epilogue (the
+  // lowered Christoffels for the 18 BSSN fields, after the field's
+  // dissipation value there has been read; d_J Gamma^K and D_i D_j phi for the
+  // rest), and one rolled loop below updates the registers of every field.
+  static_assert(NFLD <= F_NBSSN + 9 + 6, "every right-hand side has a slot");
+  auto cvslot = [](int fld) { return fld < F_NBSSN ? S_DG + fld : (fld < F_NBSSN + 9 ? S_DGAM + fld - F_NBSSN : S_DDPHI + fld - F_NBSSN - 9); };
+  auto finalize = [&](int fld, double cv) { S(cvslot(fld)) = cv; };
 
   // ev_DIFFgammaIJ (bssn.cc:748-753, BSSN_DT_DIFFGAMMAIJ bssn_macros.h:292-307)
 #pragma unroll
@@ -1522,8 +1510,47 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
     const double pv = __ldcs(&P.p[(size_t)F_DIFFD * N + c]);
     __stcs(&P.out[(size_t)F_DIFFD * N + c], pv);
     if (stage == 4) __stcs(&P.norm[(size_t)F_DIFFD * N + c], pv);
-    outv[F_DIFFD] = pv;
+    S(cvslot(F_DIFFD)) = pv;
   }
+
+  // RK4Register::K{n}Finalize (RK4Register.h:180-230) of every field, one
+  // rolled loop (one copy of the code) with the next field's registers
+  // loaded while this one is updated; the substep's divisors chosen once:
+  // f = f + dt cv / 6 (substep 1, from f = 0), / 3 (2, 3); a = p + dt cv / 2
+  // (1, 2), / 1 (3); p = f + (dt cv / 6 + p) (4).  IEEE division rounds the
+  // same for a divisor held in a register, and 0 + x = x, so the values are
+  // those of the four separate forms.  The new values replace the
+  // right-hand sides in the slots.
+  {
+    const double fdiv = stage == 1 ? 6.0 : 3.0, odiv = stage == 3 ? 1.0 : 2.0;
+    auto skip = [](int fld) { return MATTER == kStaticMatter && fld == F_DIFFD; };
+    double pv = __ldcs(&P.p[c]);
+    double fv = stage == 1 ? 0.0 : __ldcs(&P.f[c]);
+#pragma unroll 1
+    for (int fld = 0; fld < NFLD; ++fld) {
+      const double pcur = pv, fcur = fv;
+      if (fld + 1 < NFLD) {
+        pv = __ldcs(&P.p[(size_t)(fld + 1) * N + c]);
+        fv = stage == 1 ? 0.0 : __ldcs(&P.f[(size_t)(fld + 1) * N + c]);
+      }
+      if (skip(fld)) continue;
+      const double t = dt * S(cvslot(fld));
+      double o;
+      if (stage == 4) {
+        o = fcur + (t / 6.0 + pcur);
+      } else {
+        __stcs(&P.f[(size_t)fld * N + c], fcur + t / fdiv);
+        o = pcur + t / odiv;
+      }
+      __stcs(&P.out[(size_t)fld * N + c], o);
+      // at the last substep the new state is also the next step's first
+      // input, except gamma and A, which are renormalised below
+      if (stage == 4 && !(renorm && fld < F_K && fld != F_PHI)) __stcs(&P.norm[(size_t)fld * N + c], o);
+      S(cvslot(fld)) = o;
+    }
+  }
+#pragma unroll
+  for (int f = 0; f < NFLD; ++f) outv[f] = S(cvslot(f));
 
   // ---- the next substep's inputs -----------------------------------------------
   if (stage == 4) {
