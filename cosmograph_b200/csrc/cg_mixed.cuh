@@ -692,28 +692,24 @@ __device__ __forceinline__ void mixed_body(int nx, int ny, int nz, int lapse, in
   // ---- perturbation right-hand sides + FP64 register update ----------------------
   double outv[NFLD];
   const Taps<true> tko{i, j, k, nx, ny, nz, ny * nz, nz, c};
+  // the RK4 register update (RK4Register.h:180-230) with the substep's
+  // divisors chosen once, one code path per field (as the FP64 kernel's)
+  const double fdiv = stage == 1 ? 6.0 : 3.0, odiv = stage == 3 ? 1.0 : 2.0;
   auto finalize = [&](int fld, float drhs) {
     if constexpr (KO) {
       if (fld < F_D) drhs -= ko_f<O>(a + (size_t)fld * N, tko, (float)bg.ko_scale);
     }
     const double cv = bgv(bg.rhs, fld) + (double)drhs;
     const double pv = __ldcs(&P.p[(size_t)fld * N + c]);
+    const double fv = stage == 1 ? 0.0 : __ldcs(&P.f[(size_t)fld * N + c]);
+    const double t = dt * cv;
     double o;
-    if (stage == 1) {
-      __stcs(&P.f[(size_t)fld * N + c], dt * cv / 6.0);
-      o = pv + dt * cv / 2.0;
-    } else if (stage == 2) {
-      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
-      __stcs(&P.f[(size_t)fld * N + c], fv + dt * cv / 3.0);
-      o = pv + dt * cv / 2.0;
-    } else if (stage == 3) {
-      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
-      __stcs(&P.f[(size_t)fld * N + c], fv + dt * cv / 3.0);
-      o = pv + dt * cv;
-    } else {
-      const double fv = __ldcs(&P.f[(size_t)fld * N + c]);
-      o = fv + (dt * cv / 6.0 + pv);
+    if (stage == 4) {
+      o = fv + (t / 6.0 + pv);
       __stcs(&P.newp[(size_t)fld * N + c], o);
+    } else {
+      __stcs(&P.f[(size_t)fld * N + c], fv + t / fdiv);
+      o = pv + t / odiv;
     }
     outv[fld] = o;
   };
