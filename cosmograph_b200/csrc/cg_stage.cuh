@@ -1174,33 +1174,21 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
   double A[6], Ac[6];
 #pragma unroll
   for (int q = 0; q < 6; ++q) A[q] = C(F_A11 + q);
-  // copies of g^ij and A_ij in slots free from here on (D_i D_j phi, d_i phi,
-  // d_i alpha), so that the loops over the pairs (I, J) below can be rolled
-  // (one copy of their code) with the components addressed at run time
-  auto GIs = [&](int q) -> double& { return S(S_DDPHI + q); };
-  auto As = [&](int q) -> double& { return q < 3 ? S(S_DPHI + q) : S(S_DA + q - 3); };
 #pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    GIs(q) = gi[q];
-    As(q) = A[q];
-  }
-  // A^IJ of the pair q = sym(I, J), through the slots of d_J Gamma^K
-#pragma unroll 1
-  for (int q = 0; q < 6; ++q) {
-    const int I = q < 3 ? 0 : (q < 5 ? 1 : 2), J = q < 3 ? q : (q < 5 ? q - 2 : 2);
-    double t = GIs(sym(I, 0)) * GIs(sym(J, 0)) * As(sym(0, 0));
-    t = t + GIs(sym(I, 1)) * GIs(sym(J, 0)) * As(sym(1, 0));
-    t = t + GIs(sym(I, 2)) * GIs(sym(J, 0)) * As(sym(2, 0));
-    t = t + GIs(sym(I, 0)) * GIs(sym(J, 1)) * As(sym(0, 1));
-    t = t + GIs(sym(I, 1)) * GIs(sym(J, 1)) * As(sym(1, 1));
-    t = t + GIs(sym(I, 2)) * GIs(sym(J, 1)) * As(sym(2, 1));
-    t = t + GIs(sym(I, 0)) * GIs(sym(J, 2)) * As(sym(0, 2));
-    t = t + GIs(sym(I, 1)) * GIs(sym(J, 2)) * As(sym(1, 2));
-    t = t + GIs(sym(I, 2)) * GIs(sym(J, 2)) * As(sym(2, 2));
-    S(S_DGAM + q) = t;
-  }
+  for (int I = 0; I < 3; ++I)
 #pragma unroll
-  for (int q = 0; q < 6; ++q) Ac[q] = S(S_DGAM + q);
+    for (int J = I; J < 3; ++J) {
+      double t = gi[sym(I, 0)] * gi[sym(J, 0)] * A[sym(0, 0)];
+      t = t + gi[sym(I, 1)] * gi[sym(J, 0)] * A[sym(1, 0)];
+      t = t + gi[sym(I, 2)] * gi[sym(J, 0)] * A[sym(2, 0)];
+      t = t + gi[sym(I, 0)] * gi[sym(J, 1)] * A[sym(0, 1)];
+      t = t + gi[sym(I, 1)] * gi[sym(J, 1)] * A[sym(1, 1)];
+      t = t + gi[sym(I, 2)] * gi[sym(J, 1)] * A[sym(2, 1)];
+      t = t + gi[sym(I, 0)] * gi[sym(J, 2)] * A[sym(0, 2)];
+      t = t + gi[sym(I, 1)] * gi[sym(J, 2)] * A[sym(1, 2)];
+      t = t + gi[sym(I, 2)] * gi[sym(J, 2)] * A[sym(2, 2)];
+      Ac[sym(I, J)] = t;
+    }
   const double AijAij = Ac[0] * A[0] + Ac[3] * A[3] + Ac[5] * A[5] + 2.0 * (Ac[1] * A[1] + Ac[2] * A[2] + Ac[4] * A[4]);
   const double r = S(S_SRC + Q_R) + bg.rho_FRW;
   // Hamiltonian constraint, bssn.cc:1073-1084 (theta = 0)
@@ -1344,39 +1332,39 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
       }
       finalize(F_G11 + m, v + 0.5 * ph.a_adj_amp * dt * H * g[m] - ko(F_G11 + m));
     }
-  // ev_AIJ (bssn.cc:755-760, BSSN_DT_AIJ bssn_macros.h:334-337), the pairs
-  // (I, J) in a rolled loop over the slot copies of g^ij and A_ij; the
-  // trace-free Ricci tensor first replaces the Ricci tensor in its slots.
-  // With the shift the Gamma^i right-hand sides are kept for the Gamma-driver
-  // (the A_ij ones stay in their slots for AijDriverShift).
-  double rhsG[3];
+  // ev_AIJ (bssn.cc:755-760, BSSN_DT_AIJ bssn_macros.h:334-337); with the
+  // shift the A_ij and Gamma^i right-hand sides are kept for the
+  // AijDriverShift and Gamma-driver gauges
+  double rhsA[6], rhsG[3];
 #pragma unroll
-  for (int qq = 0; qq < 6; ++qq) S(S_T1 + qq) = Ric(qq) - (1.0 / 3.0) * e4phi * gm[qq] * ricci;
-#pragma unroll 1
-  for (int qq = 0; qq < 6; ++qq) {
-    const int I = qq < 3 ? 0 : (qq < 5 ? 1 : 2), J = qq < 3 ? qq : (qq < 5 ? qq - 2 : 2);
-    double aa = 0.0;
+  for (int I = 0; I < 3; ++I)
 #pragma unroll
-    for (int X = 0; X < 3; ++X)
+    for (int J = I; J < 3; ++J) {
+      const int qq = sym(I, J);
+      double aa = 0.0;
 #pragma unroll
-      for (int Y = 0; Y < 3; ++Y) {
-        const double u = GIs(sym(X, Y)) * As(sym(X, I)) * As(sym(Y, J));
-        aa = (X == 0 && Y == 0) ? u : aa + u;
+      for (int X = 0; X < 3; ++X)
+#pragma unroll
+        for (int Y = 0; Y < 3; ++Y) {
+          const double u = gi[sym(X, Y)] * A[sym(X, I)] * A[sym(Y, J)];
+          aa = (X == 0 && Y == 0) ? u : aa + u;
+        }
+      const double RTF = Ric(qq) - (1.0 / 3.0) * e4phi * gm[qq] * ricci;
+      double dtA = (em4phi * (alpha * (RTF - 8.0 * kPi * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
+                    alpha * (((K + 2.0 * theta) * A[qq]) - 2.0 * (aa)));
+      if constexpr (SHIFT) {  // BSSN_DT_AIJ with the shift (bssn_macros.h:319-332)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) dtA = dtA + up(F_A11 + qq, d);
+#pragma unroll
+        for (int X = 0; X < 3; ++X) dtA = dtA + A[sym(I, X)] * db[J][X];
+#pragma unroll
+        for (int X = 0; X < 3; ++X) dtA = dtA + A[sym(J, X)] * db[I][X];
+        dtA = dtA - (2.0 / 3.0) * A[qq] * (divb);
       }
-    const double RTF = S(S_T1 + qq);
-    double dtA = (em4phi * (alpha * (RTF - 8.0 * kPi * S(S_SRC + Q_STF11 + qq)) - S(S_DDA + qq)) +
-                  alpha * (((K + 2.0 * theta) * As(qq)) - 2.0 * (aa)));
-    if constexpr (SHIFT) {  // BSSN_DT_AIJ with the shift (bssn_macros.h:319-332)
-#pragma unroll
-      for (int d = 0; d < 3; ++d) dtA = dtA + up(F_A11 + qq, d);
-#pragma unroll
-      for (int X = 0; X < 3; ++X) dtA = dtA + As(sym(I, X)) * db[J][X];
-#pragma unroll
-      for (int X = 0; X < 3; ++X) dtA = dtA + As(sym(J, X)) * db[I][X];
-      dtA = dtA - (2.0 / 3.0) * As(qq) * (divb);
+      const double evA = dtA - 1.0 * ph.a_adj_amp * dt * A[qq] * H - ko(F_A11 + qq);
+      if constexpr (SHIFT) rhsA[qq] = evA;
+      finalize(F_A11 + qq, evA);
     }
-    finalize(F_A11 + qq, dtA - 1.0 * ph.a_adj_amp * dt * As(qq) * H - ko(F_A11 + qq));
-  }
   // ev_GammaI (bssn.cc:762-764, BSSN_DT_GAMMAI_NOSHIFT bssn_macros.h:342-361)
   const double sq[3] = {S(S_SRC + Q_S1), S(S_SRC + Q_S2), S(S_SRC + Q_S3)};
 #pragma unroll
@@ -1488,9 +1476,8 @@ __device__ __forceinline__ void stage_body(const BoxGeom& geo, const Physics& ph
         }
         case kShiftAwA: v = ph.gauge_wave_dir == I + 1 ? -2.0 * K * alpha : 0.0; break;
         case kShiftAijDriver:
-          v = -ph.k_driver_coeff * (fabs(S(cvslot(F_A11 + sym(I, 0))) + A[sym(I, 0)]) +
-                                    fabs(S(cvslot(F_A11 + sym(I, 1))) + A[sym(I, 1)]) +
-                                    fabs(S(cvslot(F_A11 + sym(I, 2))) + A[sym(I, 2)]));
+          v = -ph.k_driver_coeff * (fabs(rhsA[sym(I, 0)] + A[sym(I, 0)]) + fabs(rhsA[sym(I, 1)] + A[sym(I, 1)]) +
+                                    fabs(rhsA[sym(I, 2)] + A[sym(I, 2)]));
           break;
         default: break;
       }
