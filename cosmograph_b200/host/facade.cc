@@ -572,8 +572,18 @@ void CosmoSim::outputSnapshots() {
         iodata->log("Error opening file: " + fn);
         return;
       }
-      gzwrite(f, v.data(), (unsigned)(count * sizeof(double)));
-      gzclose(f);
+      // gzwrite takes an unsigned byte count: write in pieces of at most
+      // 1 GiB so that boxes above 4 GiB per field are written whole
+      const char* p = reinterpret_cast<const char*>(v.data());
+      size_t left = count * sizeof(double);
+      bool ok = true;
+      while (left > 0 && ok) {
+        const unsigned piece = (unsigned)std::min<size_t>(left, (size_t)1 << 30);
+        ok = gzwrite(f, p, piece) == (int)piece;
+        p += piece;
+        left -= piece;
+      }
+      if (gzclose(f) != Z_OK || !ok) iodata->log("Error writing file: " + fn);
     };
     if (w3) dump_raw(iodata->dir() + "3D_" + name + step_str + ".3d_grid.f64.gz", v.size());
     if (w2) dump_raw(iodata->dir() + "2D_" + name + step_str + ".2d_grid.f64.gz", (size_t)d.ny * d.nz);

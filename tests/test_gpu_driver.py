@@ -12,7 +12,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from cosmograph_b200 import build, ics, state as S
+from cosmograph_b200 import build, ics, snapshots, state as S
 from cosmograph_b200.evolution import BoxConfig, Evolution, evolve
 
 pytestmark = pytest.mark.gpu
@@ -153,6 +153,8 @@ def test_field_snapshots(tmp_path):
     assert np.array_equal(phi0, st.field("DIFFphi"))
     D0 = np.frombuffer(gzip.open(out / "2D_D_a0.2d_grid.f64.gz").read(), dtype="<f8").reshape(16, 16)
     assert np.array_equal(D0, st.field("D")[0])
+    with np.load(snapshots.convert(out / "3D_DIFFphi_a0.3d_grid.f64.gz", 16, 16, 16)) as z:
+        assert np.array_equal(z["DS1"], phi0)
     assert (out / "3D_DIFFphi_a2.3d_grid.f64.gz").exists() and not (out / "3D_DIFFphi_a1.3d_grid.f64.gz").exists()
     strip = rows(out / "1D_DIFFK_a.strip.dat.gz")
     assert len(strip) == 3 and len(strip[0]) == 16
